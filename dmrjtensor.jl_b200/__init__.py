@@ -1,0 +1,19 @@
+"""dmrjtensor_b200 -- a B200-native two-site DMRG engine, drop-in for DMRJtensor.jl's
+``dmrg(psi, mpo; m, sweeps, cutoff)`` path and its ``makeEnv``/``Lupdate``/``Rupdate`` API.
+
+The compute runs in ``libdmrgb200.so`` (hand-written sm_100a kernels behind a C ABI,
+``include/dmrg_b200.h``); this package is the host-side mirror of the reference interface.
+Import it with :func:`load` from the repository root when the directory name is not importable.
+"""
+from ._lib import DmrgError, PREC, lib
+from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heisenbergCylinderMPO,
+                     heisenbergMPO, hubbardMPO, makeMPO, spinOps, tfiMPO)
+from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
+                    default_context, dmrg, make_params, makeEnv, neelMPS, product_MPS, randMPS)
+
+__all__ = [
+    "DmrgError", "PREC", "lib", "HUBBARD_QN", "SPIN_QN", "XXZ", "cylinder_bonds", "fermionOps",
+    "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
+    "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",
+    "default_context", "dmrg", "make_params", "makeEnv", "neelMPS", "product_MPS", "randMPS",
+]

@@ -1,0 +1,109 @@
+"""ctypes binding of libdmrgb200.so (the C ABI declared in include/dmrg_b200.h).
+
+The library is required: importing this module without the built ``libdmrgb200.so`` raises,
+and every call that needs a GPU raises when the library reports no CUDA device. There is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libdmrgb200.so"
+
+OK, ERR_ARG, ERR_SHAPE, ERR_QN, ERR_OOM, ERR_BUDGET, ERR_TIMEOUT, ERR_CUDA, ERR_STATE, ERR_NOCUDA = range(10)
+PREC = {"fp64": 0, "3xtf32": 1, "bf16x9": 2}
+
+ERRNAMES = {1: "ERR_ARG", 2: "ERR_SHAPE", 3: "ERR_QN", 4: "ERR_OOM", 5: "ERR_BUDGET",
+            6: "ERR_TIMEOUT", 7: "ERR_CUDA", 8: "ERR_STATE", 9: "ERR_NOCUDA"}
+
+
+class Params(C.Structure):
+    _fields_ = [("maxm", C.c_int), ("minm", C.c_int), ("cutoff", C.c_double),
+                ("krylov", C.c_int), ("precision", C.c_int), ("svnbond", C.c_int),
+                ("degen_rtol", C.c_double), ("betatest", C.c_double), ("fp64_final", C.c_int),
+                ("reserved", C.c_int * 7)]
+
+
+class SweepStats(C.Structure):
+    _fields_ = [("energy", C.c_double), ("max_truncerr", C.c_double), ("biggest_m", C.c_int),
+                ("n_matvec", C.c_int), ("entropy", C.c_double), ("seconds", C.c_double),
+                ("heff_flops", C.c_double), ("heff_seconds", C.c_double),
+                ("env_flops", C.c_double), ("env_seconds", C.c_double),
+                ("eig_seconds", C.c_double), ("vec_seconds", C.c_double),
+                ("d_top", C.c_double * 8)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "d_top"}
+        d["d_top"] = list(self.d_top)
+        return d
+
+
+class DmrgError(RuntimeError):
+    """Raised for every non-zero status returned by the library."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+_IP = C.POINTER(C.c_int)
+_DP = C.POINTER(C.c_double)
+_DPP = C.POINTER(_DP)
+_IPP = C.POINTER(_IP)
+
+SIGNATURES = {
+    "dmrg_abi_version": (C.c_int, []),
+    "dmrg_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(_P)]),
+    "dmrg_ctx_destroy": (C.c_int, [_P]),
+    "dmrg_last_error": (C.c_char_p, [_P]),
+    "dmrg_ctx_memory": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "dmrg_mpo_upload": (C.c_int, [_P, C.c_int, C.c_int, _IP, _IP, _IP, _DPP, _IPP, _IPP,
+                                  C.POINTER(_P)]),
+    "dmrg_mpo_destroy": (C.c_int, [_P]),
+    "dmrg_mps_upload": (C.c_int, [_P, _P, _IP, _IP, _DPP, _IPP, C.c_int, C.POINTER(_P)]),
+    "dmrg_mps_upload_blocks": (C.c_int, [_P, _P, _IP, _IPP, _IPP, _DPP, C.c_int, C.POINTER(_P)]),
+    "dmrg_state_destroy": (C.c_int, [_P]),
+    "dmrg_state_oc": (C.c_int, [_P, _IP]),
+    "dmrg_bond_info": (C.c_int, [_P, C.c_int, _IP, _IP, _IP]),
+    "dmrg_site_size": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int64)]),
+    "dmrg_mps_download_blocks": (C.c_int, [_P, C.c_int, _DP]),
+    "dmrg_mps_download": (C.c_int, [_P, C.c_int, _DP, _IP, _IP]),
+    "dmrg_env_build": (C.c_int, [_P, _P]),
+    "dmrg_lupdate": (C.c_int, [_P, _P, C.c_int]),
+    "dmrg_rupdate": (C.c_int, [_P, _P, C.c_int]),
+    "dmrg_env_get": (C.c_int, [_P, C.c_int, C.c_int, _DP, _IP]),
+    "dmrg_heff_apply": (C.c_int, [_P, _P, C.c_int, _DP, _DP, C.c_int]),
+    "dmrg_twosite_dims": (C.c_int, [_P, _P, C.c_int, _IP]),
+    "dmrg_sweep": (C.c_int, [_P, _P, C.POINTER(Params), C.POINTER(SweepStats)]),
+    "dmrg_params_default": (None, [C.POINTER(Params)]),
+    "dmrg_test_gemm": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int,
+                                 _DP, C.c_int, _DP, C.c_int]),
+    "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library (loaded on first use; raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with dmrjtensor.jl_b200/build.py "
+                              "(there is no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code, ctx=None):
+    if code != OK:
+        msg = lib().dmrg_last_error(ctx)
+        raise DmrgError(code, msg.decode() if msg else "")

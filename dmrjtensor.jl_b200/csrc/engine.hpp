@@ -1,0 +1,251 @@
+// engine.hpp -- host-side structures of the device DMRG engine.
+//
+// Data layout in HBM (all FP64, column-major blocks, one contiguous buffer per tensor):
+//  * bond b: sectors (charge q, dim) sorted by q; a dense bond is one sector of charge 0.
+//  * MPS site A[a,s,b]: block (ka, s) -> kb = sector(q(ka)+p(s)) is a [dim ka x dim kb] matrix;
+//    blocks are stored ka-major then s, so the blocks of one left sector form one matrix
+//    [dim ka x sum_s dim kb(s)] ("left group") -- the B operand of every L*A product.
+//  * two-site psi[a,s1,s2,d]: block (ka,s1,s2) -> kd, same ka-major grouping.
+//  * left env L[a(bra), w, b(ket)]: one matrix per ket sector kb with rows (a in ka(w), w)
+//    stacked over the MPO states w (ka = sector(q(kb) - r(w))), columns b. This is the
+//    reference's L[bra,w,ket] viewed as a (bra*w) x ket matrix, restricted to one ket sector.
+//  * right env R[b(ket), w, a(bra)]: one matrix per bra sector ka, rows (b in kb(w), w),
+//    kb = sector(q(ka) + r(w)), columns a.
+//  MPO bond labels follow r(w') = r(w) + p(ket) - p(bra) (lib/MPO/makeqMPO.jl:23-84), so an
+//  environment block links ket = bra + r(w).
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/dmrg_b200.h"
+#include "kernels.cuh"
+
+namespace dmrg {
+
+struct QN {
+  int v[2] = {0, 0};
+  QN() = default;
+  QN(int a, int b) { v[0] = a; v[1] = b; }
+};
+inline bool operator<(const QN& a, const QN& b) {
+  return a.v[0] < b.v[0] || (a.v[0] == b.v[0] && a.v[1] < b.v[1]);
+}
+inline bool operator==(const QN& a, const QN& b) { return a.v[0] == b.v[0] && a.v[1] == b.v[1]; }
+inline bool operator!=(const QN& a, const QN& b) { return !(a == b); }
+inline QN operator+(const QN& a, const QN& b) { return QN(a.v[0] + b.v[0], a.v[1] + b.v[1]); }
+inline QN operator-(const QN& a, const QN& b) { return QN(a.v[0] - b.v[0], a.v[1] - b.v[1]); }
+
+struct Bond {
+  std::vector<QN> q;
+  std::vector<int> dim;
+  int nsec() const { return int(q.size()); }
+  int find(const QN& x) const;
+  int64_t total() const;
+  std::vector<int64_t> offsets() const;  // dense-equivalent position of each sector
+};
+
+struct MPOSite {
+  int wl = 0, d = 0, wr = 0;
+  std::vector<QN> rl, rr, p;   // left/right bond labels, physical labels
+  struct El { int w, s, t, w2; double v; };
+  std::vector<El> nz;          // non-zeros of W[w,s,t,w2]
+  std::vector<double> dense;   // [wl,d,d,wr] column-major
+};
+
+// W_L x W_R contracted over the shared bond, grouped by output (t1,t2,w'').
+struct TwoSiteOp {
+  struct Term { int w, s1, s2; double c; };
+  int d1 = 0, d2 = 0, wl = 0, wr = 0;
+  std::vector<std::vector<Term>> out;   // index ((t1*d2)+t2)*wr + w''
+};
+
+struct SiteLayout {      // A[a,s,b]
+  int nl = 0, d = 0;
+  std::vector<int> kb;         // [ka*d+s] right sector or -1
+  std::vector<int64_t> off;    // [ka*d+s] block offset
+  std::vector<int64_t> goff;   // [ka] group offset
+  std::vector<int> gcols;      // [ka] group columns
+  int64_t size = 0;
+};
+
+struct TwoLayout {       // psi[a,s1,s2,d]
+  int nl = 0, d1 = 0, d2 = 0;
+  std::vector<int> kd;         // [(ka*d1+s1)*d2+s2]
+  std::vector<int64_t> off;
+  std::vector<int64_t> goff;
+  std::vector<int> gcols;
+  int64_t size = 0;
+  int idx(int ka, int s1, int s2) const { return (ka * d1 + s1) * d2 + s2; }
+};
+
+struct EnvLayout {       // L: groups by ket sector; R: groups by bra sector
+  int nsec = 0, w = 0;
+  std::vector<int> other;      // [k*w+wi] bra sector (L) / ket sector (R), or -1
+  std::vector<int> rowoff;     // [k*w+wi]
+  std::vector<int> rows;       // [k]
+  std::vector<int64_t> goff;   // [k]
+  int64_t size = 0;
+};
+
+struct DBuf {
+  double* p = nullptr;
+  int64_t n = 0;   // capacity in doubles
+};
+
+// Pinned host staging + device copy for one family of task descriptors.
+struct DescSlot {
+  char* h = nullptr;
+  char* d = nullptr;
+  size_t cap = 0;
+  cudaEvent_t ev = nullptr;
+};
+
+struct GemmList {
+  bool tA = false, tB = false;
+  std::vector<GemmTask> tasks;
+  std::vector<GemmSeg> segs;
+  int tiles = 0;
+  double flops = 0;
+  size_t t_off = 0, s_off = 0;  // byte offsets inside the uploaded slot
+  void clear() { tasks.clear(); segs.clear(); tiles = 0; flops = 0; }
+  void add(int64_t c_off, int ldc, int M, int N, double alpha, double beta);
+  void seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K);
+};
+
+struct MixList {
+  std::vector<MixTask> tasks;
+  std::vector<MixTerm> terms;
+  int tiles = 0;
+  double flops = 0;
+  size_t t_off = 0, m_off = 0;
+  void clear() { tasks.clear(); terms.clear(); tiles = 0; flops = 0; }
+  void add(int64_t out_off, int ld, int rows, int cols);
+  void term(int64_t in_off, int ld, double c);
+};
+
+struct CopyList {
+  std::vector<CopyTask> tasks;
+  int tiles = 0;
+  size_t t_off = 0;
+  void clear() { tasks.clear(); tiles = 0; }
+  void add(int64_t src_off, int lds, int64_t dst_off, int ldd, int rows, int cols, int trans,
+           double scale);
+};
+
+}  // namespace dmrg
+
+struct dmrg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0, in_use = 0, peak = 0;
+  std::string err;
+  int nsm = 148;
+  dmrg::DescSlot slot[4];
+  double* d_scal = nullptr;      // small scalar workspace (256 doubles)
+  double* d_partial = nullptr;   // reduction partials (16 * 296 doubles)
+  int* d_status = nullptr;
+  double* h_scal = nullptr;      // pinned mirror of d_scal
+  cudaEvent_t ev[8] = {};
+  // growable scratch buffers
+  dmrg::DBuf X, Y, K, H, M, R, W, T1, T2;
+  std::map<void*, size_t> sizes;
+};
+
+struct dmrg_mpo {
+  dmrg_ctx* ctx = nullptr;
+  int L = 0, nsym = 0;
+  std::vector<dmrg::MPOSite> site;
+  std::vector<dmrg::TwoSiteOp> two;   // per bond (iL, iL+1)
+};
+
+struct dmrg_state {
+  dmrg_ctx* ctx = nullptr;
+  const dmrg_mpo* mpo = nullptr;
+  int L = 0, nsym = 0, oc = 0, dir = 1;
+  std::vector<dmrg::Bond> bond;                 // L+1
+  std::vector<dmrg::SiteLayout> lay;            // L
+  std::vector<dmrg::DBuf> A;                    // L
+  std::vector<dmrg::EnvLayout> Llay, Rlay;      // L
+  std::vector<dmrg::DBuf> Lenv, Renv;           // L
+  std::vector<char> Lvalid, Rvalid;
+  bool env_built = false;
+};
+
+namespace dmrg {
+
+// ---- errors: thrown inside the library, converted to status codes at the ABI
+struct Error {
+  int code;
+  std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+
+// ---- memory
+void dalloc(dmrg_ctx* c, DBuf& b, int64_t n);      // (re)allocate to exactly n doubles
+void dfree(dmrg_ctx* c, DBuf& b);
+void ensure(dmrg_ctx* c, DBuf& b, int64_t n);      // grow-only scratch
+
+// ---- layouts (engine_layout.cpp)
+SiteLayout make_site_layout(const Bond& Bl, const std::vector<QN>& p, const Bond& Br);
+TwoLayout make_two_layout(const Bond& Bl, const std::vector<QN>& p1, const std::vector<QN>& p2,
+                          const Bond& Br);
+EnvLayout make_left_env_layout(const Bond& B, const std::vector<QN>& r);
+EnvLayout make_right_env_layout(const Bond& B, const std::vector<QN>& r);
+TwoSiteOp make_two_site_op(const MPOSite& a, const MPOSite& b);
+
+// ---- descriptor upload
+struct Upload {
+  std::vector<char> bytes;
+  template <class T>
+  size_t put(const std::vector<T>& v) {
+    size_t off = (bytes.size() + 15) / 16 * 16;
+    bytes.resize(off + v.size() * sizeof(T));
+    if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+  }
+  void put(GemmList& g) { g.t_off = put(g.tasks); g.s_off = put(g.segs); }
+  void put(MixList& m) { m.t_off = put(m.tasks); m.m_off = put(m.terms); }
+  void put(CopyList& c) { c.t_off = put(c.tasks); }
+  char* send(dmrg_ctx* c, int slot);   // returns the device base of the copied bytes
+};
+
+// Launch wrappers. Every launch first checks on the host that each task's extent lies inside
+// the sizes (in doubles) of the buffers it addresses; a violation is a DMRG_ERR_ARG, never a
+// device fault.
+void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
+              const double* B, int64_t nB, double* C, int64_t nC);
+void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,
+             double* out, int64_t nout);
+void run_copy(dmrg_ctx* c, const CopyList& l, char* dbase, const double* src, int64_t nsrc,
+              double* dst, int64_t ndst);
+void check_eig(const std::vector<EigTask>& t, int64_t nbase);
+
+// ---- contractions (engine_contract.cpp)
+struct HeffPlan {
+  TwoLayout tl;
+  GemmList g1, g3;
+  MixList mix;
+  int64_t x_size = 0, y_size = 0;
+  double flops = 0;
+  char* dbase = nullptr;
+};
+void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp);
+void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot);
+// y = Heff x for vectors in the tl layout (device pointers).
+void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
+                int precision);
+
+void env_boundaries(dmrg_state* st);
+void lupdate(dmrg_state* st, int i, double* flops);
+void rupdate(dmrg_state* st, int i, double* flops);
+
+// ---- sweep (engine_sweep.cpp)
+void do_sweep(dmrg_state* st, const dmrg_params& p, dmrg_sweep_stats& out);
+
+}  // namespace dmrg

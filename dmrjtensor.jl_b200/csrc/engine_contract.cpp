@@ -1,0 +1,322 @@
+// engine_contract.cpp -- the effective Hamiltonian and the environment updates as block plans.
+//
+// Heff psi (make2site / inline form, algs/DMRG.jl:48-54,69-73) in three launches:
+//   1. X_kb = L_kb * psi_kb          one GEMM per ket sector kb (rows (a,w), cols (s1,s2,d))
+//   2. Y = ops . X                   sparse two-site MPO ops[w,s1,t1,s2,t2,w''] mixing of blocks
+//   3. psi'_(ka,t1,t2) = Y * R_ka'   one GEMM per output block, K = the stacked (d, w'') rows
+// Lupdate / Rupdate (lib/MPO_MPS/Lupdate.jl:17-26, Rupdate.jl:17-26) in the same three shapes.
+#include <algorithm>
+#include <map>
+
+#include "engine.hpp"
+
+namespace dmrg {
+
+void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp) {
+  const int iR = iL + 1;
+  const Bond& Bl = st->bond[iL];
+  const Bond& Br = st->bond[iL + 2];
+  const MPOSite& ml = st->mpo->site[iL];
+  const MPOSite& mr = st->mpo->site[iR];
+  const TwoSiteOp& op = st->mpo->two[iL];
+  const EnvLayout& LL = st->Llay[iL];
+  const EnvLayout& RL = st->Rlay[iR];
+  hp.tl = make_two_layout(Bl, ml.p, mr.p, Br);
+  const TwoLayout& tl = hp.tl;
+  const int d1 = tl.d1, d2 = tl.d2, wl = ml.wl, wr = mr.wr;
+
+  hp.g1.clear();
+  hp.g3.clear();
+  hp.mix.clear();
+  hp.g1.tA = hp.g1.tB = false;
+  hp.g3.tA = hp.g3.tB = false;
+
+  std::vector<int64_t> xoff(Bl.nsec(), 0);
+  int64_t x = 0;
+  for (int kb = 0; kb < Bl.nsec(); ++kb) {
+    xoff[kb] = x;
+    x += int64_t(LL.rows[kb]) * tl.gcols[kb];
+  }
+  hp.x_size = x;
+  for (int kb = 0; kb < Bl.nsec(); ++kb) {
+    if (LL.rows[kb] == 0 || tl.gcols[kb] == 0) continue;
+    hp.g1.add(xoff[kb], LL.rows[kb], LL.rows[kb], tl.gcols[kb], 1.0, 0.0);
+    hp.g1.seg(LL.goff[kb], LL.rows[kb], tl.goff[kb], Bl.dim[kb], Bl.dim[kb]);
+  }
+
+  std::vector<int64_t> yoff(tl.kd.size(), -1);
+  int64_t y = 0;
+  for (int ka = 0; ka < tl.nl; ++ka)
+    for (int t1 = 0; t1 < d1; ++t1)
+      for (int t2 = 0; t2 < d2; ++t2) {
+        const int id = tl.idx(ka, t1, t2);
+        const int kap = tl.kd[id];
+        if (kap < 0) continue;
+        yoff[id] = y;
+        y += int64_t(Bl.dim[ka]) * RL.rows[kap];
+      }
+  hp.y_size = y;
+
+  for (int ka = 0; ka < tl.nl; ++ka) {
+    const int dka = Bl.dim[ka];
+    for (int t1 = 0; t1 < d1; ++t1)
+      for (int t2 = 0; t2 < d2; ++t2) {
+        const int id = tl.idx(ka, t1, t2);
+        const int kap = tl.kd[id];
+        if (kap < 0) continue;
+        for (int w2 = 0; w2 < wr; ++w2) {
+          const int kd = RL.other[kap * wr + w2];
+          if (kd < 0) continue;
+          hp.mix.add(yoff[id] + int64_t(RL.rowoff[kap * wr + w2]) * dka, dka, dka, Br.dim[kd]);
+          for (const auto& tm : op.out[(size_t(t1) * d2 + t2) * wr + w2]) {
+            const int kb = Bl.find(Bl.q[ka] + ml.rl[tm.w]);
+            if (kb < 0 || LL.other[kb * wl + tm.w] != ka) continue;
+            const int id2 = tl.idx(kb, tm.s1, tm.s2);
+            if (tl.kd[id2] != kd) continue;
+            const int64_t colX = (tl.off[id2] - tl.goff[kb]) / Bl.dim[kb];
+            hp.mix.term(xoff[kb] + LL.rowoff[kb * wl + tm.w] + colX * LL.rows[kb], LL.rows[kb],
+                        tm.c);
+          }
+        }
+      }
+  }
+
+  for (int ka = 0; ka < tl.nl; ++ka)
+    for (int t1 = 0; t1 < d1; ++t1)
+      for (int t2 = 0; t2 < d2; ++t2) {
+        const int id = tl.idx(ka, t1, t2);
+        const int kap = tl.kd[id];
+        if (kap < 0) continue;
+        hp.g3.add(tl.off[id], Bl.dim[ka], Bl.dim[ka], Br.dim[kap], 1.0, 0.0);
+        if (RL.rows[kap] > 0)
+          hp.g3.seg(yoff[id], Bl.dim[ka], RL.goff[kap], RL.rows[kap], RL.rows[kap]);
+      }
+  hp.flops = hp.g1.flops + hp.g3.flops + hp.mix.flops;
+}
+
+void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot) {
+  Upload u;
+  u.put(hp.g1);
+  u.put(hp.mix);
+  u.put(hp.g3);
+  hp.dbase = u.send(c, slot);
+}
+
+void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
+                int precision) {
+  (void)precision;
+  dmrg_ctx* c = st->ctx;
+  ensure(c, c->X, std::max<int64_t>(hp.x_size, 1));
+  ensure(c, c->Y, std::max<int64_t>(hp.y_size, 1));
+  const int64_t n = hp.tl.size;
+  run_gemm(c, hp.g1, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
+  run_mix(c, hp.mix, hp.dbase, c->X.p, c->X.n, c->Y.p, c->Y.n);
+  run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n, y, n);
+}
+
+// ------------------------------------------------------------------ environments
+
+void env_boundaries(dmrg_state* st) {
+  dmrg_ctx* c = st->ctx;
+  const int L = st->L;
+  const Bond& b0 = st->bond[0];
+  const Bond& bL = st->bond[L];
+  const MPOSite& s0 = st->mpo->site[0];
+  const MPOSite& sL = st->mpo->site[L - 1];
+  if (b0.nsec() != 1 || b0.dim[0] != 1 || bL.nsec() != 1 || bL.dim[0] != 1)
+    fail(DMRG_ERR_SHAPE, "edge bonds of the MPS must be one-dimensional");
+  if (s0.wl != 1 || sL.wr != 1)
+    fail(DMRG_ERR_SHAPE, "edge bonds of the MPO must be one-dimensional");
+  st->Llay[0] = make_left_env_layout(b0, s0.rl);
+  st->Rlay[L - 1] = make_right_env_layout(bL, sL.rr);
+  if (st->Llay[0].other[0] != 0 || st->Rlay[L - 1].other[0] != 0)
+    fail(DMRG_ERR_QN, "MPO edge labels do not connect the MPS edge sectors");
+  const double one = 1.0;
+  dalloc(c, st->Lenv[0], 1);
+  dalloc(c, st->Renv[L - 1], 1);
+  cuda_check(cudaMemcpyAsync(st->Lenv[0].p, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream),
+             "boundary");
+  cuda_check(cudaMemcpyAsync(st->Renv[L - 1].p, &one, sizeof(double), cudaMemcpyHostToDevice,
+                             c->stream), "boundary");
+  cuda_check(cudaStreamSynchronize(c->stream), "boundary sync");
+  st->Lvalid.assign(L, 0);
+  st->Rvalid.assign(L, 0);
+  st->Lvalid[0] = 1;
+  st->Rvalid[L - 1] = 1;
+}
+
+void lupdate(dmrg_state* st, int i, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  if (i < 0 || i + 1 >= st->L) fail(DMRG_ERR_ARG, "lupdate: site out of range");
+  if (!st->Lvalid[i]) fail(DMRG_ERR_STATE, "lupdate: Lenv[site] has not been built");
+  const Bond& Bl = st->bond[i];
+  const Bond& Br = st->bond[i + 1];
+  const MPOSite& ms = st->mpo->site[i];
+  const SiteLayout& lay = st->lay[i];
+  const EnvLayout& LL = st->Llay[i];
+  EnvLayout LN = make_left_env_layout(Br, ms.rr);
+  const int d = ms.d, wl = ms.wl, wr = ms.wr;
+
+  GemmList g1, g3;
+  MixList mx;
+  g3.tA = true;
+  std::vector<int64_t> t1off(Bl.nsec(), 0);
+  int64_t t1 = 0;
+  for (int kb = 0; kb < Bl.nsec(); ++kb) {
+    t1off[kb] = t1;
+    t1 += int64_t(LL.rows[kb]) * lay.gcols[kb];
+  }
+  for (int kb = 0; kb < Bl.nsec(); ++kb) {
+    if (LL.rows[kb] == 0 || lay.gcols[kb] == 0) continue;
+    g1.add(t1off[kb], LL.rows[kb], LL.rows[kb], lay.gcols[kb], 1.0, 0.0);
+    g1.seg(LL.goff[kb], LL.rows[kb], lay.goff[kb], Bl.dim[kb], Bl.dim[kb]);
+  }
+  // non-zeros grouped by (t, w')
+  std::vector<std::vector<const MPOSite::El*>> byTW(size_t(d) * wr);
+  for (const auto& e : ms.nz) byTW[size_t(e.t) * wr + e.w2].push_back(&e);
+
+  struct Out { int kbp, w2, rows; int64_t off; std::vector<int> ka, roff; };
+  std::vector<Out> outs;
+  int64_t t2 = 0;
+  for (int kbp = 0; kbp < Br.nsec(); ++kbp)
+    for (int w2 = 0; w2 < wr; ++w2) {
+      const int kap = LN.other[kbp * wr + w2];
+      if (kap < 0) continue;
+      Out o{kbp, w2, 0, t2, std::vector<int>(d, -1), std::vector<int>(d, 0)};
+      for (int t = 0; t < d; ++t) {
+        const int ka = Bl.find(Br.q[kap] - ms.p[t]);
+        if (ka < 0 || lay.kb[ka * d + t] != kap) continue;
+        o.ka[t] = ka;
+        o.roff[t] = o.rows;
+        o.rows += Bl.dim[ka];
+      }
+      t2 += int64_t(o.rows) * Br.dim[kbp];
+      outs.push_back(std::move(o));
+    }
+  for (const Out& o : outs) {
+    for (int t = 0; t < d; ++t) {
+      const int ka = o.ka[t];
+      if (ka < 0) continue;
+      mx.add(o.off + o.roff[t], o.rows, Bl.dim[ka], Br.dim[o.kbp]);
+      for (const MPOSite::El* e : byTW[size_t(t) * wr + o.w2]) {
+        const int kb = Bl.find(Bl.q[ka] + ms.rl[e->w]);
+        if (kb < 0 || LL.other[kb * wl + e->w] != ka) continue;
+        if (lay.kb[kb * d + e->s] != o.kbp) continue;
+        const int64_t colA = (lay.off[kb * d + e->s] - lay.goff[kb]) / Bl.dim[kb];
+        mx.term(t1off[kb] + LL.rowoff[kb * wl + e->w] + colA * LL.rows[kb], LL.rows[kb], e->v);
+      }
+    }
+  }
+  for (const Out& o : outs) {
+    const int kap = LN.other[o.kbp * wr + o.w2];
+    g3.add(LN.goff[o.kbp] + LN.rowoff[o.kbp * wr + o.w2], LN.rows[o.kbp], Br.dim[kap],
+           Br.dim[o.kbp], 1.0, 0.0);
+    for (int t = 0; t < d; ++t) {
+      const int ka = o.ka[t];
+      if (ka < 0) continue;
+      g3.seg(lay.off[ka * d + t], Bl.dim[ka], o.off + o.roff[t], o.rows, Bl.dim[ka]);
+    }
+  }
+  Upload u;
+  u.put(g1);
+  u.put(mx);
+  u.put(g3);
+  char* db = u.send(c, 2);
+  ensure(c, c->T1, std::max<int64_t>(t1, 1));
+  ensure(c, c->T2, std::max<int64_t>(t2, 1));
+  st->Llay[i + 1] = LN;
+  dalloc(c, st->Lenv[i + 1], std::max<int64_t>(LN.size, 1));
+  run_gemm(c, g1, db, st->Lenv[i].p, st->Lenv[i].n, st->A[i].p, st->A[i].n, c->T1.p, c->T1.n);
+  run_mix(c, mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
+  run_gemm(c, g3, db, st->A[i].p, st->A[i].n, c->T2.p, c->T2.n, st->Lenv[i + 1].p,
+           st->Lenv[i + 1].n);
+  st->Lvalid[i + 1] = 1;
+  if (flops) *flops += g1.flops + g3.flops + mx.flops;
+}
+
+void rupdate(dmrg_state* st, int i, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  if (i <= 0 || i >= st->L) fail(DMRG_ERR_ARG, "rupdate: site out of range");
+  if (!st->Rvalid[i]) fail(DMRG_ERR_STATE, "rupdate: Renv[site] has not been built");
+  const Bond& Bl = st->bond[i];
+  const Bond& Br = st->bond[i + 1];
+  const MPOSite& ms = st->mpo->site[i];
+  const SiteLayout& lay = st->lay[i];
+  const EnvLayout& RL = st->Rlay[i];
+  EnvLayout RN = make_right_env_layout(Bl, ms.rl);
+  const int d = ms.d, wl = ms.wl, wr = ms.wr;
+
+  GemmList g1, g3;
+  MixList mx;
+  g1.tB = true;
+  std::vector<int64_t> t1off(size_t(Bl.nsec()) * d, -1);
+  int64_t t1 = 0;
+  for (int ka = 0; ka < Bl.nsec(); ++ka)
+    for (int t = 0; t < d; ++t) {
+      const int kap = lay.kb[ka * d + t];
+      if (kap < 0) continue;
+      t1off[ka * d + t] = t1;
+      t1 += int64_t(RL.rows[kap]) * Bl.dim[ka];
+    }
+  for (int ka = 0; ka < Bl.nsec(); ++ka)
+    for (int t = 0; t < d; ++t) {
+      const int kap = lay.kb[ka * d + t];
+      if (kap < 0 || RL.rows[kap] == 0) continue;
+      g1.add(t1off[ka * d + t], RL.rows[kap], RL.rows[kap], Bl.dim[ka], 1.0, 0.0);
+      g1.seg(RL.goff[kap], RL.rows[kap], lay.off[ka * d + t], Bl.dim[ka], Br.dim[kap]);
+    }
+  std::vector<std::vector<const MPOSite::El*>> byWS(size_t(wl) * d);
+  for (const auto& e : ms.nz) byWS[size_t(e.w) * d + e.s].push_back(&e);
+
+  std::vector<int64_t> t2off(size_t(Bl.nsec()) * wl, -1);
+  int64_t t2 = 0;
+  for (int ka = 0; ka < Bl.nsec(); ++ka)
+    for (int w = 0; w < wl; ++w) {
+      const int kb = RN.other[ka * wl + w];
+      if (kb < 0) continue;
+      t2off[ka * wl + w] = t2;
+      t2 += int64_t(lay.gcols[kb]) * Bl.dim[ka];
+    }
+  for (int ka = 0; ka < Bl.nsec(); ++ka)
+    for (int w = 0; w < wl; ++w) {
+      const int kb = RN.other[ka * wl + w];
+      if (kb < 0) continue;
+      for (int s = 0; s < d; ++s) {
+        const int kbp = lay.kb[kb * d + s];
+        if (kbp < 0) continue;
+        const int64_t colA = (lay.off[kb * d + s] - lay.goff[kb]) / Bl.dim[kb];
+        mx.add(t2off[ka * wl + w] + colA, lay.gcols[kb], Br.dim[kbp], Bl.dim[ka]);
+        for (const MPOSite::El* e : byWS[size_t(w) * d + s]) {
+          const int kap = lay.kb[ka * d + e->t];
+          if (kap < 0 || RL.rows[kap] == 0) continue;
+          if (RL.other[kap * wr + e->w2] != kbp) continue;
+          mx.term(t1off[ka * d + e->t] + RL.rowoff[kap * wr + e->w2], RL.rows[kap], e->v);
+        }
+      }
+    }
+  for (int ka = 0; ka < Bl.nsec(); ++ka)
+    for (int w = 0; w < wl; ++w) {
+      const int kb = RN.other[ka * wl + w];
+      if (kb < 0) continue;
+      g3.add(RN.goff[ka] + RN.rowoff[ka * wl + w], RN.rows[ka], Bl.dim[kb], Bl.dim[ka], 1.0, 0.0);
+      if (lay.gcols[kb] > 0)
+        g3.seg(lay.goff[kb], Bl.dim[kb], t2off[ka * wl + w], lay.gcols[kb], lay.gcols[kb]);
+    }
+  Upload u;
+  u.put(g1);
+  u.put(mx);
+  u.put(g3);
+  char* db = u.send(c, 2);
+  ensure(c, c->T1, std::max<int64_t>(t1, 1));
+  ensure(c, c->T2, std::max<int64_t>(t2, 1));
+  st->Rlay[i - 1] = RN;
+  dalloc(c, st->Renv[i - 1], std::max<int64_t>(RN.size, 1));
+  run_gemm(c, g1, db, st->Renv[i].p, st->Renv[i].n, st->A[i].p, st->A[i].n, c->T1.p, c->T1.n);
+  run_mix(c, mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
+  run_gemm(c, g3, db, st->A[i].p, st->A[i].n, c->T2.p, c->T2.n, st->Renv[i - 1].p,
+           st->Renv[i - 1].n);
+  st->Rvalid[i - 1] = 1;
+  if (flops) *flops += g1.flops + g3.flops + mx.flops;
+}
+
+}  // namespace dmrg

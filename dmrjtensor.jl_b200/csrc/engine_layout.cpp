@@ -1,0 +1,372 @@
+// engine_layout.cpp -- block layouts, device memory, descriptor upload, launch wrappers.
+#include <algorithm>
+#include <map>
+
+#include "engine.hpp"
+
+namespace dmrg {
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    int code = (e == cudaErrorMemoryAllocation) ? DMRG_ERR_OOM : DMRG_ERR_CUDA;
+    fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+int Bond::find(const QN& x) const {
+  auto it = std::lower_bound(q.begin(), q.end(), x);
+  if (it == q.end() || !(*it == x)) return -1;
+  return int(it - q.begin());
+}
+
+int64_t Bond::total() const {
+  int64_t t = 0;
+  for (int d : dim) t += d;
+  return t;
+}
+
+std::vector<int64_t> Bond::offsets() const {
+  std::vector<int64_t> o(dim.size());
+  int64_t t = 0;
+  for (size_t i = 0; i < dim.size(); ++i) { o[i] = t; t += dim[i]; }
+  return o;
+}
+
+// ------------------------------------------------------------------ memory
+
+void dalloc(dmrg_ctx* c, DBuf& b, int64_t n) {
+  dfree(c, b);
+  if (n <= 0) return;
+  size_t bytes = size_t(n) * sizeof(double);
+  if (c->budget && c->in_use + bytes > c->budget)
+    fail(DMRG_ERR_BUDGET, "device allocation of " + std::to_string(bytes) +
+                              " bytes exceeds the context's HBM budget");
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, c->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(DMRG_ERR_OOM, "cudaMallocAsync(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+  }
+  b.p = static_cast<double*>(p);
+  b.n = n;
+  c->in_use += bytes;
+  c->peak = std::max(c->peak, c->in_use);
+  c->sizes[p] = bytes;
+}
+
+void dfree(dmrg_ctx* c, DBuf& b) {
+  if (!b.p) return;
+  auto it = c->sizes.find(b.p);
+  if (it != c->sizes.end()) {
+    c->in_use -= it->second;
+    c->sizes.erase(it);
+  }
+  cudaFreeAsync(b.p, c->stream);
+  b.p = nullptr;
+  b.n = 0;
+}
+
+void ensure(dmrg_ctx* c, DBuf& b, int64_t n) {
+  if (n <= b.n) return;
+  int64_t want = std::max<int64_t>(n, b.n + b.n / 4);
+  dalloc(c, b, want);
+}
+
+// ------------------------------------------------------------------ layouts
+
+SiteLayout make_site_layout(const Bond& Bl, const std::vector<QN>& p, const Bond& Br) {
+  SiteLayout L;
+  L.nl = Bl.nsec();
+  L.d = int(p.size());
+  L.kb.assign(size_t(L.nl) * L.d, -1);
+  L.off.assign(size_t(L.nl) * L.d, 0);
+  L.goff.assign(L.nl, 0);
+  L.gcols.assign(L.nl, 0);
+  int64_t off = 0;
+  for (int ka = 0; ka < L.nl; ++ka) {
+    L.goff[ka] = off;
+    for (int s = 0; s < L.d; ++s) {
+      int kb = Br.find(Bl.q[ka] + p[s]);
+      L.kb[ka * L.d + s] = kb;
+      if (kb < 0) continue;
+      L.off[ka * L.d + s] = off;
+      off += int64_t(Bl.dim[ka]) * Br.dim[kb];
+      L.gcols[ka] += Br.dim[kb];
+    }
+  }
+  L.size = off;
+  return L;
+}
+
+TwoLayout make_two_layout(const Bond& Bl, const std::vector<QN>& p1, const std::vector<QN>& p2,
+                          const Bond& Br) {
+  TwoLayout T;
+  T.nl = Bl.nsec();
+  T.d1 = int(p1.size());
+  T.d2 = int(p2.size());
+  const size_t nb = size_t(T.nl) * T.d1 * T.d2;
+  T.kd.assign(nb, -1);
+  T.off.assign(nb, 0);
+  T.goff.assign(T.nl, 0);
+  T.gcols.assign(T.nl, 0);
+  int64_t off = 0;
+  for (int ka = 0; ka < T.nl; ++ka) {
+    T.goff[ka] = off;
+    for (int s1 = 0; s1 < T.d1; ++s1)
+      for (int s2 = 0; s2 < T.d2; ++s2) {
+        int kd = Br.find(Bl.q[ka] + p1[s1] + p2[s2]);
+        int id = T.idx(ka, s1, s2);
+        T.kd[id] = kd;
+        if (kd < 0) continue;
+        T.off[id] = off;
+        off += int64_t(Bl.dim[ka]) * Br.dim[kd];
+        T.gcols[ka] += Br.dim[kd];
+      }
+  }
+  T.size = off;
+  return T;
+}
+
+// Left env on bond B with MPO labels r: ket sector kb, MPO state w -> bra sector q(kb) - r(w).
+EnvLayout make_left_env_layout(const Bond& B, const std::vector<QN>& r) {
+  EnvLayout E;
+  E.nsec = B.nsec();
+  E.w = int(r.size());
+  E.other.assign(size_t(E.nsec) * E.w, -1);
+  E.rowoff.assign(size_t(E.nsec) * E.w, 0);
+  E.rows.assign(E.nsec, 0);
+  E.goff.assign(E.nsec, 0);
+  int64_t off = 0;
+  for (int kb = 0; kb < E.nsec; ++kb) {
+    int rows = 0;
+    for (int w = 0; w < E.w; ++w) {
+      int ka = B.find(B.q[kb] - r[w]);
+      E.other[kb * E.w + w] = ka;
+      E.rowoff[kb * E.w + w] = rows;
+      if (ka >= 0) rows += B.dim[ka];
+    }
+    E.rows[kb] = rows;
+    E.goff[kb] = off;
+    off += int64_t(rows) * B.dim[kb];
+  }
+  E.size = off;
+  return E;
+}
+
+// Right env on bond B with MPO labels r: bra sector ka, MPO state w -> ket sector q(ka) + r(w).
+EnvLayout make_right_env_layout(const Bond& B, const std::vector<QN>& r) {
+  EnvLayout E;
+  E.nsec = B.nsec();
+  E.w = int(r.size());
+  E.other.assign(size_t(E.nsec) * E.w, -1);
+  E.rowoff.assign(size_t(E.nsec) * E.w, 0);
+  E.rows.assign(E.nsec, 0);
+  E.goff.assign(E.nsec, 0);
+  int64_t off = 0;
+  for (int ka = 0; ka < E.nsec; ++ka) {
+    int rows = 0;
+    for (int w = 0; w < E.w; ++w) {
+      int kb = B.find(B.q[ka] + r[w]);
+      E.other[ka * E.w + w] = kb;
+      E.rowoff[ka * E.w + w] = rows;
+      if (kb >= 0) rows += B.dim[kb];
+    }
+    E.rows[ka] = rows;
+    E.goff[ka] = off;
+    off += int64_t(rows) * B.dim[ka];
+  }
+  E.size = off;
+  return E;
+}
+
+// ops[w,s1,t1,s2,t2,w''] = sum_w' WL[w,s1,t1,w'] WR[w',s2,t2,w''] (contract(mpoL,4,mpoR,1),
+// algs/DMRG.jl:70), kept sparse and grouped by the output channel (t1,t2,w'').
+TwoSiteOp make_two_site_op(const MPOSite& a, const MPOSite& b) {
+  TwoSiteOp op;
+  op.d1 = a.d;
+  op.d2 = b.d;
+  op.wl = a.wl;
+  op.wr = b.wr;
+  op.out.assign(size_t(a.d) * b.d * b.wr, {});
+  std::vector<std::vector<const MPOSite::El*>> byw(b.wl);
+  for (const auto& e : b.nz) byw[e.w].push_back(&e);
+  std::map<std::tuple<int, int, int, int, int, int>, double> acc;
+  for (const auto& ea : a.nz)
+    for (const MPOSite::El* eb : byw[ea.w2])
+      acc[{ea.t, eb->t, eb->w2, ea.w, ea.s, eb->s}] += ea.v * eb->v;
+  for (const auto& kv : acc) {
+    if (kv.second == 0.0) continue;
+    auto [t1, t2, w2, w, s1, s2] = kv.first;
+    op.out[(size_t(t1) * b.d + t2) * b.wr + w2].push_back({w, s1, s2, kv.second});
+  }
+  return op;
+}
+
+// ------------------------------------------------------------------ task lists
+
+void GemmList::add(int64_t c_off, int ldc, int M, int N, double alpha, double beta) {
+  GemmTask t{};
+  t.c_off = c_off;
+  t.ldc = ldc;
+  t.M = M;
+  t.N = N;
+  t.seg0 = int(segs.size());
+  t.nseg = 0;
+  t.tiles_m = (M + GEMM_BM - 1) / GEMM_BM;
+  t.tile0 = tiles;
+  t.alpha = alpha;
+  t.beta = beta;
+  if (M <= 0 || N <= 0) { t.tiles_m = 0; }
+  tiles += t.tiles_m * ((N + GEMM_BN - 1) / GEMM_BN);
+  tasks.push_back(t);
+}
+
+void GemmList::seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K) {
+  if (K <= 0) return;
+  GemmSeg s{};
+  s.a_off = a_off;
+  s.b_off = b_off;
+  s.lda = lda;
+  s.ldb = ldb;
+  s.K = K;
+  segs.push_back(s);
+  GemmTask& t = tasks.back();
+  t.nseg += 1;
+  flops += 2.0 * t.M * double(t.N) * K;
+}
+
+void MixList::add(int64_t out_off, int ld, int rows, int cols) {
+  MixTask t{};
+  t.out_off = out_off;
+  t.ld = ld;
+  t.rows = rows;
+  t.cols = cols;
+  t.term0 = int(terms.size());
+  t.nterm = 0;
+  t.tile0 = tiles;
+  t.ntiles = (rows > 0 && cols > 0) ? (cols + 31) / 32 : 0;
+  tiles += t.ntiles;
+  tasks.push_back(t);
+}
+
+void MixList::term(int64_t in_off, int ld, double c) {
+  MixTerm m{};
+  m.in_off = in_off;
+  m.ld = ld;
+  m.coef = c;
+  terms.push_back(m);
+  MixTask& t = tasks.back();
+  t.nterm += 1;
+  flops += 2.0 * t.rows * double(t.cols);
+}
+
+void CopyList::add(int64_t src_off, int lds, int64_t dst_off, int ldd, int rows, int cols,
+                   int trans, double scale) {
+  if (rows <= 0 || cols <= 0) return;
+  CopyTask t{};
+  t.src_off = src_off;
+  t.dst_off = dst_off;
+  t.lds = lds;
+  t.ldd = ldd;
+  t.rows = rows;
+  t.cols = cols;
+  t.trans = trans;
+  t.tile0 = tiles;
+  t.ntiles = (cols + 31) / 32;
+  t.scale = scale;
+  tiles += t.ntiles;
+  tasks.push_back(t);
+}
+
+char* Upload::send(dmrg_ctx* c, int slot) {
+  DescSlot& s = c->slot[slot];
+  if (s.ev) cuda_check(cudaEventSynchronize(s.ev), "descriptor slot wait");
+  size_t need = bytes.size() < 16 ? 16 : bytes.size();
+  if (need > s.cap) {
+    size_t cap = std::max(need, s.cap * 2);
+    if (s.h) cudaFreeHost(s.h);
+    if (s.d) cudaFreeAsync(s.d, c->stream);
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&s.h), cap), "cudaMallocHost(desc)");
+    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&s.d), cap, c->stream), "cudaMalloc(desc)");
+    s.cap = cap;
+  }
+  if (!bytes.empty()) {
+    std::memcpy(s.h, bytes.data(), bytes.size());
+    cuda_check(cudaMemcpyAsync(s.d, s.h, bytes.size(), cudaMemcpyHostToDevice, c->stream),
+               "descriptor upload");
+  }
+  if (!s.ev) cuda_check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
+  cuda_check(cudaEventRecord(s.ev, c->stream), "event record");
+  return s.d;
+}
+
+namespace {
+inline bool in_range(int64_t off, int64_t last, int64_t n) { return off >= 0 && off + last < n; }
+[[noreturn]] void bad_plan(const char* what) {
+  fail(DMRG_ERR_ARG, std::string("internal plan check failed: ") + what + " out of bounds");
+}
+}  // namespace
+
+void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
+              const double* B, int64_t nB, double* C, int64_t nC) {
+  if (g.tiles == 0) return;
+  for (const GemmTask& t : g.tasks) {
+    if (t.M <= 0 || t.N <= 0) continue;
+    if (t.ldc < t.M || !in_range(t.c_off, (t.M - 1) + int64_t(t.N - 1) * t.ldc, nC)) bad_plan("gemm C");
+    for (int q = 0; q < t.nseg; ++q) {
+      const GemmSeg& s = g.segs[t.seg0 + q];
+      const int64_t ea = g.tA ? (s.K - 1) + int64_t(t.M - 1) * s.lda : (t.M - 1) + int64_t(s.K - 1) * s.lda;
+      const int64_t eb = g.tB ? (t.N - 1) + int64_t(s.K - 1) * s.ldb : (s.K - 1) + int64_t(t.N - 1) * s.ldb;
+      if (s.lda < (g.tA ? s.K : t.M) || !in_range(s.a_off, ea, nA)) bad_plan("gemm A");
+      if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
+    }
+  }
+  launch_gemm_f64(c->stream, g.tA, g.tB, A, B, C,
+                  reinterpret_cast<const GemmTask*>(dbase + g.t_off), int(g.tasks.size()),
+                  reinterpret_cast<const GemmSeg*>(dbase + g.s_off), g.tiles, c->nsm * 4);
+}
+
+void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,
+             double* out, int64_t nout) {
+  if (m.tiles == 0) return;
+  for (const MixTask& t : m.tasks) {
+    if (t.rows <= 0 || t.cols <= 0) continue;
+    const int64_t ext = (t.rows - 1) + int64_t(t.cols - 1) * t.ld;
+    if (t.ld < t.rows || !in_range(t.out_off, ext, nout)) bad_plan("mix out");
+    for (int q = 0; q < t.nterm; ++q) {
+      const MixTerm& tm = m.terms[t.term0 + q];
+      if (tm.ld < t.rows || !in_range(tm.in_off, (t.rows - 1) + int64_t(t.cols - 1) * tm.ld, nin))
+        bad_plan("mix in");
+    }
+  }
+  launch_mix(c->stream, in, out, reinterpret_cast<const MixTask*>(dbase + m.t_off),
+             int(m.tasks.size()), reinterpret_cast<const MixTerm*>(dbase + m.m_off), m.tiles);
+}
+
+void run_copy(dmrg_ctx* c, const CopyList& l, char* dbase, const double* src, int64_t nsrc,
+              double* dst, int64_t ndst) {
+  if (l.tiles == 0) return;
+  for (const CopyTask& t : l.tasks) {
+    const int64_t es = t.trans ? (t.cols - 1) + int64_t(t.rows - 1) * t.lds
+                               : (t.rows - 1) + int64_t(t.cols - 1) * t.lds;
+    if (!in_range(t.src_off, es, nsrc)) bad_plan("copy src");
+    if (t.ldd < t.rows || !in_range(t.dst_off, (t.rows - 1) + int64_t(t.cols - 1) * t.ldd, ndst))
+      bad_plan("copy dst");
+  }
+  launch_copy(c->stream, src, dst, reinterpret_cast<const CopyTask*>(dbase + l.t_off),
+              int(l.tasks.size()), l.tiles);
+}
+
+void check_eig(const std::vector<EigTask>& ts, int64_t nbase) {
+  for (const EigTask& t : ts) {
+    const int64_t nn = int64_t(t.n) * t.n;
+    if (t.n <= 0 || !in_range(t.a_off, nn - 1, nbase) || !in_range(t.v_off, nn - 1, nbase) ||
+        !in_range(t.w_off, t.n - 1, nbase))
+      bad_plan("eigensolver task");
+    if (t.n > 4096) fail(DMRG_ERR_SHAPE, "density-matrix block larger than 4096");
+  }
+}
+
+}  // namespace dmrg

@@ -1,0 +1,533 @@
+// engine_sweep.cpp -- twostep (algs/DMRG.jl:362-405) and the optmps sweep
+// (algs/optimizeMPS.jl:790-835) on the device.
+//
+// Per bond: normalise the centre tensor, AA = psi_L psi_R (one grouped GEMM), Krylov solve
+// (reference 2-vector step or Lanczos-k with full re-orthogonalisation), reduced density matrix
+// per centre-charge group (gather + one grouped GEMM), batched Jacobi eigensolve, global
+// truncation on the host from the downloaded eigenvalues, split back into the two site tensors
+// (copies + one grouped GEMM), then the environment update of the site left behind.
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+#include "engine.hpp"
+
+namespace dmrg {
+namespace {
+
+// Small dense symmetric eigenproblem on the host (Krylov tridiagonal, k <= 16): cyclic Jacobi,
+// eigenvalues ascending, eigenvectors in the columns of V (column-major n x n).
+void host_syev(int n, std::vector<double> A, std::vector<double>& w, std::vector<double>& V) {
+  V.assign(size_t(n) * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + i * n] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) off += A[p + q * n] * A[p + q * n];
+    if (off < 1e-300) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = A[p + q * n];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double theta = (A[q + q * n] - A[p + p * n]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {  // rows
+          const double ap = A[p + k * n], aq = A[q + k * n];
+          A[p + k * n] = c * ap - s * aq;
+          A[q + k * n] = s * ap + c * aq;
+        }
+        for (int k = 0; k < n; ++k) {  // columns
+          const double ap = A[k + p * n], aq = A[k + q * n];
+          A[k + p * n] = c * ap - s * aq;
+          A[k + q * n] = s * ap + c * aq;
+          const double vp = V[k + p * n], vq = V[k + q * n];
+          V[k + p * n] = c * vp - s * vq;
+          V[k + q * n] = s * vp + c * vq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(),
+                   [&](int a, int b) { return A[a + a * n] < A[b + b * n]; });
+  w.resize(n);
+  std::vector<double> Vs(size_t(n) * n);
+  for (int k = 0; k < n; ++k) {
+    w[k] = A[ord[k] + ord[k] * n];
+    for (int i = 0; i < n; ++i) Vs[i + k * n] = V[i + ord[k] * n];
+  }
+  V.swap(Vs);
+}
+
+// Device scalars: value written by a reduction at d_scal[slot], read back synchronously.
+double read_scalar(dmrg_ctx* c, int slot) {
+  cuda_check(cudaMemcpyAsync(c->h_scal + slot, c->d_scal + slot, sizeof(double),
+                             cudaMemcpyDeviceToHost, c->stream), "scalar D2H");
+  cuda_check(cudaStreamSynchronize(c->stream), "scalar sync");
+  return c->h_scal[slot];
+}
+
+double dot_dev(dmrg_ctx* c, const double* x, const double* y, int64_t n, int slot = 0) {
+  launch_mdot(c->stream, x, 0, 1, y, n, c->d_partial, c->d_scal + slot);
+  return read_scalar(c, slot);
+}
+
+// Same rule as oracle/qtensor.py select_kept (global over all groups).
+struct Sel {
+  std::vector<int> keep;
+  double truncerr = 0.0;
+};
+Sel select_kept(const std::vector<std::vector<double>>& vals, int maxm, int minm, double cutoff,
+                double mag, double degen_rtol) {
+  struct E { double v; int g, i; };
+  std::vector<E> flat;
+  for (int g = 0; g < int(vals.size()); ++g)
+    for (int i = 0; i < int(vals[g].size()); ++i) flat.push_back({vals[g][i], g, i});
+  std::stable_sort(flat.begin(), flat.end(), [](const E& a, const E& b) {
+    if (a.v != b.v) return a.v > b.v;
+    if (a.g != b.g) return a.g < b.g;
+    return a.i < b.i;
+  });
+  Sel s;
+  s.keep.assign(vals.size(), 0);
+  const int N = int(flat.size());
+  if (N == 0) return s;
+  double tot = 0.0;
+  if (mag == 0.0) for (const E& e : flat) tot += e.v; else tot = mag;
+  std::vector<double> tail(N + 1, 0.0);
+  for (int k = N - 1; k >= 0; --k) tail[k] = tail[k + 1] + flat[k].v;
+  int kc = N;
+  for (int k = 1; k <= N; ++k)
+    if (tail[k] <= cutoff * tot) { kc = k; break; }
+  int k = std::max(minm, kc);
+  if (maxm > 0) k = std::min(k, maxm);
+  k = std::max(1, std::min(k, N));
+  if (degen_rtol > 0 && k < N) {
+    const double thr = degen_rtol * std::fabs(flat[k - 1].v);
+    if (flat[k - 1].v - flat[k].v <= thr) {
+      int jj = k - 1;
+      while (jj >= 1 && flat[jj - 1].v - flat[jj].v <= thr) --jj;
+      if (jj >= std::max(minm, 1)) k = jj;
+    }
+  }
+  for (int n = 0; n < k; ++n) s.keep[flat[n].g] += 1;
+  s.truncerr = tail[k];
+  return s;
+}
+
+struct EvPool {
+  std::vector<cudaEvent_t> ev;
+  std::vector<std::pair<int, int>> pairs;   // (start idx, category)
+  int used = 0;
+  cudaEvent_t next() {
+    if (used == int(ev.size())) {
+      cudaEvent_t e;
+      cuda_check(cudaEventCreate(&e), "event create");
+      ev.push_back(e);
+    }
+    return ev[used++];
+  }
+  ~EvPool() { for (auto e : ev) cudaEventDestroy(e); }
+};
+
+struct Timing {
+  EvPool pool;
+  struct Span { cudaEvent_t a, b; int cat; };
+  std::vector<Span> spans;
+  double acc[4] = {0, 0, 0, 0};   // heff, env, eig, vec
+  cudaEvent_t begin(dmrg_ctx* c) {
+    cudaEvent_t e = pool.next();
+    cudaEventRecord(e, c->stream);
+    return e;
+  }
+  void end(dmrg_ctx* c, cudaEvent_t a, int cat) {
+    cudaEvent_t e = pool.next();
+    cudaEventRecord(e, c->stream);
+    spans.push_back({a, e, cat});
+  }
+  void flush() {   // call after a stream sync
+    for (const Span& s : spans) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, s.a, s.b);
+      acc[s.cat] += ms * 1e-3;
+    }
+    spans.clear();
+    pool.used = 0;
+  }
+};
+
+}  // namespace
+
+namespace {
+
+struct StepOut {
+  double energy = 0, truncerr = 0;
+  int m = 0, nmv = 0;
+  std::vector<double> D;       // kept singular values, descending
+  double heff_flops = 0;
+};
+
+struct Piece { int sec, s, off; };
+struct Group {
+  QN q;
+  int n = 0, np = 0, keep = 0, kc = -1;
+  std::vector<Piece> rows, cols;
+  int64_t moff = 0, roff = 0, woff = 0;
+};
+
+void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing& tm,
+             StepOut& so) {
+  dmrg_ctx* c = st->ctx;
+  cudaStream_t s = c->stream;
+  const MPOSite& ml = st->mpo->site[iL];
+  const MPOSite& mr = st->mpo->site[iR];
+  const Bond Bl = st->bond[iL];
+  const Bond Bc = st->bond[iL + 1];
+  const Bond Br = st->bond[iL + 2];
+  const int d1 = ml.d, d2 = mr.d;
+  if (!st->Lvalid[iL] || !st->Rvalid[iR]) fail(DMRG_ERR_STATE, "environments are not built");
+
+  // psi[iL] (j>0) or psi[iR] (j<0) /= norm  (algs/DMRG.jl:365-369)
+  cudaEvent_t tv = tm.begin(c);
+  const int ic = j > 0 ? iL : iR;
+  const double nr = std::sqrt(dot_dev(c, st->A[ic].p, st->A[ic].p, st->lay[ic].size));
+  if (nr > 0) launch_scale(s, st->A[ic].p, st->lay[ic].size, 1.0 / nr);
+
+  HeffPlan hp;
+  plan_heff(st, iL, hp);
+  const TwoLayout& tl = hp.tl;
+  const SiteLayout& la = st->lay[iL];
+  const SiteLayout& lb = st->lay[iR];
+  GemmList gaa;   // AA = contract(psiL, 3, psiR, 1)
+  for (int ka = 0; ka < tl.nl; ++ka)
+    for (int s1 = 0; s1 < d1; ++s1)
+      for (int s2 = 0; s2 < d2; ++s2) {
+        const int id = tl.idx(ka, s1, s2);
+        const int kd = tl.kd[id];
+        if (kd < 0) continue;
+        gaa.add(tl.off[id], Bl.dim[ka], Bl.dim[ka], Br.dim[kd], 1.0, 0.0);
+        const int kc = la.kb[ka * d1 + s1];
+        if (kc >= 0 && lb.kb[kc * d2 + s2] == kd)
+          gaa.seg(la.off[ka * d1 + s1], Bl.dim[ka], lb.off[kc * d2 + s2], Bc.dim[kc], Bc.dim[kc]);
+      }
+  Upload u;
+  u.put(hp.g1);
+  u.put(hp.mix);
+  u.put(hp.g3);
+  u.put(gaa);
+  hp.dbase = u.send(c, 0);
+  const int64_t n = tl.size;
+  const int kdim = std::max(2, std::min(P.krylov, 16));
+  ensure(c, c->K, std::max<int64_t>(int64_t(kdim) * n, 1));
+  ensure(c, c->H, std::max<int64_t>(n, 1));
+  double* K = c->K.p;
+  double* H = c->H.p;
+  run_gemm(c, gaa, hp.dbase, st->A[iL].p, st->A[iL].n, st->A[iR].p, st->A[iR].n, K, n);
+  tm.end(c, tv, 3);
+
+  auto heff = [&](const double* x, double* y) {
+    cudaEvent_t th = tm.begin(c);
+    apply_heff(st, iL, hp, x, y, P.precision);
+    tm.end(c, th, 0);
+    so.nmv += 1;
+    so.heff_flops += hp.flops;
+  };
+
+  double E = 0.0;
+  const double* psi = K;
+  if (P.krylov <= 2) {
+    // simplelanczos (algs/DMRG.jl:57-90): H is applied to AA before its normalisation
+    heff(K, H);
+    tv = tm.begin(c);
+    const double nAA = std::sqrt(dot_dev(c, K, K, n));
+    launch_scale(s, K, n, 1.0 / nAA);
+    const double a1 = dot_dev(c, K, H, n);
+    launch_axpby(s, n, -a1, nullptr, 0, K, 1.0, nullptr, 0, H, 0);
+    const double b1 = std::sqrt(dot_dev(c, H, H, n));
+    tm.end(c, tv, 3);
+    if (b1 > P.betatest) {
+      double* K1 = K + n;
+      launch_axpby(s, n, 1.0 / b1, nullptr, 0, H, 0.0, nullptr, 0, K1, 0);
+      heff(K1, H);
+      const double a2 = dot_dev(c, K1, H, n);
+      std::vector<double> w, V;
+      host_syev(2, {a1, b1, b1, a2}, w, V);
+      E = w[0];
+      launch_axpby(s, n, V[0], nullptr, 0, K, 0.0, nullptr, 0, H, 0);
+      launch_axpby(s, n, V[1], nullptr, 0, K1, 1.0, nullptr, 0, H, 0);
+      psi = H;
+    } else {
+      E = a1;
+      psi = K;
+    }
+  } else {
+    tv = tm.begin(c);
+    const double nAA = std::sqrt(dot_dev(c, K, K, n));
+    launch_scale(s, K, n, 1.0 / nAA);
+    tm.end(c, tv, 3);
+    std::vector<double> al, be;
+    for (int jj = 0; jj < kdim; ++jj) {
+      double* Kj = K + int64_t(jj) * n;
+      heff(Kj, H);
+      tv = tm.begin(c);
+      const double a = dot_dev(c, Kj, H, n);
+      al.push_back(a);
+      if (jj == kdim - 1) { tm.end(c, tv, 3); break; }
+      launch_axpby(s, n, -a, nullptr, 0, Kj, 1.0, nullptr, 0, H, 0);
+      if (jj > 0) launch_axpby(s, n, -be[jj - 1], nullptr, 0, Kj - n, 1.0, nullptr, 0, H, 0);
+      for (int pass = 0; pass < 2; ++pass) {   // full re-orthogonalisation (CGS2)
+        launch_mdot(s, K, n, jj + 1, H, n, c->d_partial, c->d_scal);
+        launch_msub(s, K, n, jj + 1, c->d_scal, H, n);
+      }
+      const double b = std::sqrt(dot_dev(c, H, H, n));
+      tm.end(c, tv, 3);
+      if (b <= P.betatest) break;
+      be.push_back(b);
+      launch_axpby(s, n, 1.0 / b, nullptr, 0, H, 0.0, nullptr, 0, K + int64_t(jj + 1) * n, 0);
+    }
+    const int m = int(al.size());
+    std::vector<double> T(size_t(m) * m, 0.0), w, V;
+    for (int a = 0; a < m; ++a) {
+      T[a + a * m] = al[a];
+      if (a + 1 < m) T[a + (a + 1) * m] = T[a + 1 + a * m] = be[a];
+    }
+    host_syev(m, T, w, V);
+    E = w[0];
+    for (int a = 0; a < m; ++a) c->h_scal[32 + a] = -V[a];
+    cuda_check(cudaMemcpyAsync(c->d_scal + 32, c->h_scal + 32, sizeof(double) * m,
+                               cudaMemcpyHostToDevice, s), "ritz coefficients");
+    launch_zero(s, H, n);
+    launch_msub(s, K, n, m, c->d_scal + 32, H, n);
+    psi = H;
+  }
+  so.energy = E;
+
+  // ---------------- reduced density matrix per centre-charge group (algs/DMRG.jl:425-429)
+  cudaEvent_t te = tm.begin(c);
+  std::map<QN, Group> gm;
+  for (int ka = 0; ka < Bl.nsec(); ++ka)
+    for (int s1 = 0; s1 < d1; ++s1) {
+      Group& g = gm[Bl.q[ka] + ml.p[s1]];
+      g.q = Bl.q[ka] + ml.p[s1];
+      g.rows.push_back({ka, s1, g.n});
+      g.n += Bl.dim[ka];
+    }
+  for (int kd = 0; kd < Br.nsec(); ++kd)
+    for (int s2 = 0; s2 < d2; ++s2) {
+      auto it = gm.find(Br.q[kd] - mr.p[s2]);
+      if (it == gm.end()) continue;
+      it->second.cols.push_back({kd, s2, it->second.np});
+      it->second.np += Br.dim[kd];
+    }
+  std::vector<Group> G;
+  for (auto& kv : gm) G.push_back(kv.second);
+  std::vector<int> gofrow(size_t(Bl.nsec()) * d1, -1), rowoff(size_t(Bl.nsec()) * d1, 0);
+  std::vector<int> coloff(size_t(Br.nsec()) * d2, -1);
+  for (int g = 0; g < int(G.size()); ++g) {
+    for (const Piece& p : G[g].rows) { gofrow[p.sec * d1 + p.s] = g; rowoff[p.sec * d1 + p.s] = p.off; }
+    for (const Piece& p : G[g].cols) coloff[p.sec * d2 + p.s] = p.off;
+  }
+  int64_t mtot = 0, rtot = 0, wtot = 0;
+  for (Group& g : G) {
+    const int side = j > 0 ? g.n : g.np;
+    g.moff = mtot; mtot += int64_t(g.n) * g.np;
+    g.roff = rtot; rtot += int64_t(side) * side;
+    g.woff = wtot; wtot += side;
+  }
+  ensure(c, c->M, std::max<int64_t>(mtot, 1));
+  ensure(c, c->R, std::max<int64_t>(2 * rtot + wtot, 1));
+  CopyList gather;
+  for (int ka = 0; ka < tl.nl; ++ka)
+    for (int s1 = 0; s1 < d1; ++s1)
+      for (int s2 = 0; s2 < d2; ++s2) {
+        const int id = tl.idx(ka, s1, s2);
+        const int kd = tl.kd[id];
+        if (kd < 0) continue;
+        const Group& g = G[gofrow[ka * d1 + s1]];
+        const int co = coloff[kd * d2 + s2];
+        gather.add(tl.off[id], Bl.dim[ka], g.moff + rowoff[ka * d1 + s1] + int64_t(co) * g.n, g.n,
+                   Bl.dim[ka], Br.dim[kd], 0, 1.0);
+      }
+  GemmList grho;
+  grho.tA = j < 0;
+  grho.tB = j > 0;
+  std::vector<EigTask> esmall, elarge;
+  int nsmall = 0, nlarge = 0;
+  for (const Group& g : G) {
+    const int side = j > 0 ? g.n : g.np;
+    if (side == 0) continue;
+    grho.add(g.roff, side, side, side, 1.0, 0.0);
+    const int K2 = j > 0 ? g.np : g.n;
+    if (K2 > 0) grho.seg(g.moff, g.n, g.moff, g.n, K2);
+    EigTask et{};
+    et.a_off = g.roff;
+    et.v_off = rtot + g.roff;
+    et.w_off = 2 * rtot + g.woff;
+    et.n = side;
+    if (side <= 100) { esmall.push_back(et); nsmall = std::max(nsmall, side); }
+    else { elarge.push_back(et); nlarge = std::max(nlarge, side); }
+  }
+  Upload u2;
+  u2.put(gather);
+  u2.put(grho);
+  const size_t es_off = u2.put(esmall), el_off = u2.put(elarge);
+  char* db2 = u2.send(c, 1);
+  run_copy(c, gather, db2, psi, n, c->M.p, c->M.n);
+  run_gemm(c, grho, db2, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
+  check_eig(esmall, c->R.n);
+  check_eig(elarge, c->R.n);
+  cuda_check(cudaMemsetAsync(c->d_status, 0, sizeof(int), s), "status");
+  launch_jacobi(s, c->R.p, reinterpret_cast<const EigTask*>(db2 + es_off), int(esmall.size()),
+                nsmall, c->d_status);
+  launch_jacobi(s, c->R.p, reinterpret_cast<const EigTask*>(db2 + el_off), int(elarge.size()),
+                nlarge, c->d_status);
+  std::vector<double> lam(std::max<int64_t>(wtot, 1));
+  int jstat = 0;
+  cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + 2 * rtot, sizeof(double) * wtot,
+                             cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
+  cuda_check(cudaMemcpyAsync(&jstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "status");
+  cuda_check(cudaStreamSynchronize(s), "eigen sync");
+  cuda_check(cudaGetLastError(), "eigensolve");
+  if (jstat != 0) fail(DMRG_ERR_CUDA, "Jacobi eigensolver did not converge");
+
+  std::vector<std::vector<double>> vals(G.size());
+  for (int g = 0; g < int(G.size()); ++g) {
+    const int side = j > 0 ? G[g].n : G[g].np;
+    vals[g].assign(lam.begin() + G[g].woff, lam.begin() + G[g].woff + side);
+  }
+  const Sel sel = select_kept(vals, P.maxm, P.minm, P.cutoff, 1.0, P.degen_rtol);
+  Bond C;
+  std::vector<double> kept;
+  for (int g = 0; g < int(G.size()); ++g) {
+    G[g].keep = sel.keep[g];
+    if (G[g].keep == 0) continue;
+    G[g].kc = C.nsec();
+    C.q.push_back(G[g].q);
+    C.dim.push_back(G[g].keep);
+    for (int a = 0; a < G[g].keep; ++a) kept.push_back(vals[g][a]);
+  }
+  std::sort(kept.begin(), kept.end(), std::greater<double>());
+  so.D.resize(kept.size());
+  for (size_t a = 0; a < kept.size(); ++a) so.D[a] = std::sqrt(std::max(kept[a], 0.0));
+  so.truncerr = sel.truncerr;
+  so.m = int(kept.size());
+
+  // ---------------- split back into the two site tensors (algs/DMRG.jl:389-395, 483-490)
+  SiteLayout nl = make_site_layout(Bl, ml.p, C);
+  SiteLayout nrl = make_site_layout(C, mr.p, Br);
+  DBuf nA, nB;
+  dalloc(c, nA, std::max<int64_t>(nl.size, 1));
+  dalloc(c, nB, std::max<int64_t>(nrl.size, 1));
+  CopyList cp;
+  GemmList gs;
+  if (j > 0) {
+    gs.tA = true;
+    for (int ka = 0; ka < Bl.nsec(); ++ka)
+      for (int s1 = 0; s1 < d1; ++s1) {
+        const Group& g = G[gofrow[ka * d1 + s1]];
+        if (g.keep == 0) continue;
+        cp.add(g.roff + rowoff[ka * d1 + s1], g.n, nl.off[ka * d1 + s1], Bl.dim[ka], Bl.dim[ka],
+               g.keep, 0, 1.0);
+      }
+    for (const Group& g : G) {
+      if (g.keep == 0) continue;
+      for (const Piece& p : g.cols) {   // p.sec = kd, p.s = s2
+        if (nrl.kb[g.kc * d2 + p.s] != p.sec) continue;
+        gs.add(nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1.0, 0.0);
+        gs.seg(g.roff, g.n, g.moff + int64_t(p.off) * g.n, g.n, g.n);
+      }
+    }
+  } else {
+    for (const Group& g : G) {
+      if (g.keep == 0) continue;
+      for (const Piece& p : g.cols) {
+        if (nrl.kb[g.kc * d2 + p.s] != p.sec) continue;
+        cp.add(g.roff + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
+               1.0);
+      }
+      for (const Piece& p : g.rows) {   // p.sec = ka, p.s = s1
+        gs.add(nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec], g.keep, 1.0, 0.0);
+        if (g.np > 0) gs.seg(g.moff + p.off, g.n, g.roff, g.np, g.np);
+      }
+    }
+  }
+  Upload u3;
+  u3.put(cp);
+  u3.put(gs);
+  char* db3 = u3.send(c, 3);
+  if (j > 0) {
+    run_copy(c, cp, db3, c->R.p, c->R.n, nA.p, nA.n);
+    run_gemm(c, gs, db3, c->R.p, c->R.n, c->M.p, c->M.n, nB.p, nB.n);
+  } else {
+    run_copy(c, cp, db3, c->R.p, c->R.n, nB.p, nB.n);
+    run_gemm(c, gs, db3, c->M.p, c->M.n, c->R.p, c->R.n, nA.p, nA.n);
+  }
+  dfree(c, st->A[iL]);
+  dfree(c, st->A[iR]);
+  st->A[iL] = nA;
+  st->A[iR] = nB;
+  st->lay[iL] = nl;
+  st->lay[iR] = nrl;
+  st->bond[iL + 1] = C;
+  if (j > 0) st->Rvalid[iL] = 0; else st->Lvalid[iL + 1] = 0;
+  tm.end(c, te, 2);
+}
+
+}  // namespace
+
+void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
+  dmrg_ctx* c = st->ctx;
+  const int L = st->L;
+  if (L < 2) fail(DMRG_ERR_SHAPE, "a two-site sweep needs at least two sites");
+  if (!st->env_built) fail(DMRG_ERR_STATE, "call dmrg_env_build before dmrg_sweep");
+  std::memset(&out, 0, sizeof(out));
+  const int svn = P.svnbond > 0 ? P.svnbond : (L + 1) / 2;
+  const int svn_site = std::min(std::max(2, svn + 1), L) - 1;   // 0-based i of SvNcheck!
+  Timing tm;
+  cudaEvent_t t0 = tm.pool.next(), t1 = tm.pool.next();
+  cudaEventRecord(t0, c->stream);
+  int j = st->dir;
+  for (int ns = 0; ns < 2 * (L - 1); ++ns) {
+    const int i = st->oc;
+    const int iL = j > 0 ? i : i - 1, iR = j > 0 ? i + 1 : i;
+    StepOut so;
+    twostep(st, P, j, iL, iR, tm, so);
+    cudaEvent_t tenv = tm.begin(c);
+    double ef = 0.0;
+    if (j > 0) lupdate(st, i, &ef); else rupdate(st, i, &ef);
+    tm.end(c, tenv, 1);
+    out.energy = so.energy;
+    out.max_truncerr = std::max(out.max_truncerr, so.truncerr);
+    out.biggest_m = std::max(out.biggest_m, so.m);
+    out.n_matvec += so.nmv;
+    out.heff_flops += so.heff_flops;
+    out.env_flops += ef;
+    if (i == svn_site && j < 0) {
+      double S = 0.0;
+      for (double x : so.D) {
+        const double p2 = x * x;
+        if (p2 > 0) S -= p2 * std::log(p2);
+      }
+      out.entropy = S;
+      for (int a = 0; a < 8; ++a) out.d_top[a] = a < int(so.D.size()) ? so.D[a] : 0.0;
+    }
+    st->oc += j;
+    if ((st->oc == L - 1 && j > 0) || (st->oc == 0 && j < 0)) j = -j;
+    cuda_check(cudaStreamSynchronize(c->stream), "step sync");
+    tm.flush();
+    tm.pool.used = 2;
+  }
+  st->dir = j;
+  cudaEventRecord(t1, c->stream);
+  cuda_check(cudaEventSynchronize(t1), "sweep sync");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  out.seconds = ms * 1e-3;
+  out.heff_seconds = tm.acc[0];
+  out.env_seconds = tm.acc[1];
+  out.eig_seconds = tm.acc[2];
+  out.vec_seconds = tm.acc[3];
+}
+
+}  // namespace dmrg

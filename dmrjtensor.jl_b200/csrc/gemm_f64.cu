@@ -1,0 +1,201 @@
+// gemm_f64.cu -- persistent grouped FP64 GEMM on the FP64 tensor-core path (DMMA, m8n8k4).
+//
+// One launch executes every block product of one contraction step (all QN block triples), as
+// a flat list of 64x64 output tiles; each CTA walks tiles with a stride of gridDim.x. A tile
+// accumulates over the K-segments of its task (stacked MPO channels, physical states) through a
+// 3-stage cp.async pipeline. Operands may be transposed (NN, NT, TN) so that no permute copies
+// are needed anywhere in the sweep. B200 has no tcgen05 FP64 kind; mma.sync f64 is the FP64
+// tensor-core instruction on sm_100a.
+#include "kernels.cuh"
+
+namespace dmrg {
+namespace {
+
+constexpr int BM = GEMM_BM, BN = GEMM_BN, BK = GEMM_BK;
+constexpr int STAGES = 3, PAD = 4, THREADS = 128;
+constexpr int LDS_A = BM + PAD;   // 68 doubles: rows of a k-slice are 8 banks apart (no conflicts)
+constexpr int LDS_B = BN + PAD;
+constexpr size_t SMEM_BYTES = size_t(STAGES) * BK * (LDS_A + LDS_B) * sizeof(double);
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// D(8x8) += A(8x4, row) * B(4x8, col). Lane l holds A[l>>2][l&3], B[l&3][l>>2],
+// D[l>>2][2*(l&3) + {0,1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(THREADS)
+k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
+           const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
+           int total_tiles) {
+  extern __shared__ double smem[];
+  double* As = smem;
+  double* Bs = smem + STAGES * BK * LDS_A;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int g = lane >> 2, t = lane & 3;
+
+  for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (tasks[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+    }
+    const GemmTask tk = tasks[lo];
+    const int local = tile - tk.tile0;
+    const int m0 = (local % tk.tiles_m) * BM;
+    const int n0 = (local / tk.tiles_m) * BN;
+    int nsteps = 0;
+    for (int q = 0; q < tk.nseg; ++q) nsteps += (segs[tk.seg0 + q].K + BK - 1) / BK;
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    int p_seg = 0, p_k = 0;  // producer cursor
+    auto issue = [&](int stage) {
+      while (segs[tk.seg0 + p_seg].K <= p_k) { ++p_seg; p_k = 0; }
+      const GemmSeg sg = segs[tk.seg0 + p_seg];
+      const double* Ab = A + sg.a_off;
+      const double* Bb = B + sg.b_off;
+      double* as = As + stage * BK * LDS_A;
+      double* bs = Bs + stage * BK * LDS_B;
+      if (!TA) {  // A(i,k) = Ab[i + k*lda]
+        const int i = tid & 63, kq = tid >> 6;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int k = kq + 2 * r, gi = m0 + i, gk = p_k + k;
+          const bool ok = gi < tk.M && gk < sg.K;
+          cp_async8(&as[k * LDS_A + i], ok ? Ab + gi + int64_t(gk) * sg.lda : Ab, ok);
+        }
+      } else {    // A(i,k) = Ab[k + i*lda]
+        const int k = tid & 15, iq = tid >> 4;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int i = iq + 8 * r, gi = m0 + i, gk = p_k + k;
+          const bool ok = gi < tk.M && gk < sg.K;
+          cp_async8(&as[k * LDS_A + i], ok ? Ab + gk + int64_t(gi) * sg.lda : Ab, ok);
+        }
+      }
+      if (!TB) {  // B(k,j) = Bb[k + j*ldb]
+        const int k = tid & 15, jq = tid >> 4;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int j = jq + 8 * r, gj = n0 + j, gk = p_k + k;
+          const bool ok = gj < tk.N && gk < sg.K;
+          cp_async8(&bs[k * LDS_B + j], ok ? Bb + gk + int64_t(gj) * sg.ldb : Bb, ok);
+        }
+      } else {    // B(k,j) = Bb[j + k*ldb]
+        const int j = tid & 63, kq = tid >> 6;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int k = kq + 2 * r, gj = n0 + j, gk = p_k + k;
+          const bool ok = gj < tk.N && gk < sg.K;
+          cp_async8(&bs[k * LDS_B + j], ok ? Bb + gj + int64_t(gk) * sg.ldb : Bb, ok);
+        }
+      }
+      p_k += BK;
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (s < nsteps) issue(s);
+      cp_commit();
+    }
+    for (int step = 0; step < nsteps; ++step) {
+      cp_wait<STAGES - 2>();
+      __syncthreads();
+      const int nxt = step + STAGES - 1;
+      if (nxt < nsteps) issue(nxt % STAGES);
+      cp_commit();
+      const double* as = As + (step % STAGES) * BK * LDS_A;
+      const double* bs = Bs + (step % STAGES) * BK * LDS_B;
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) a[mi] = as[(kk + t) * LDS_A + wm * 32 + mi * 8 + g];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) b[ni] = bs[(kk + t) * LDS_B + wn * 32 + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+      }
+    }
+    cp_wait<0>();
+    __syncthreads();
+
+    double* Cb = C + tk.c_off;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      const int row = m0 + wm * 32 + mi * 8 + g;
+      if (row >= tk.M) continue;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = n0 + wn * 32 + ni * 8 + 2 * t + e;
+          if (col < tk.N) {
+            const int64_t idx = row + int64_t(col) * tk.ldc;
+            double v = tk.alpha * acc[mi][ni][e];
+            if (tk.beta != 0.0) v += tk.beta * Cb[idx];
+            Cb[idx] = v;
+          }
+        }
+      }
+    }
+  }
+}
+
+template <bool TA, bool TB>
+void launch_variant(cudaStream_t s, const double* A, const double* B, double* C,
+                    const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
+                    int grid_cap) {
+  static bool configured = false;  // attribute is per device function; idempotent
+  if (!configured) {
+    cudaFuncSetAttribute(k_gemm_f64<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(SMEM_BYTES));
+    configured = true;
+  }
+  int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
+  k_gemm_f64<TA, TB><<<grid, THREADS, SMEM_BYTES, s>>>(A, B, C, tasks, ntasks, segs, total_tiles);
+}
+
+}  // namespace
+
+void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
+                     double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
+                     int total_tiles, int grid_cap) {
+  if (total_tiles <= 0 || ntasks <= 0) return;
+  if (!transA && !transB)
+    launch_variant<false, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  else if (!transA && transB)
+    launch_variant<false, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  else if (transA && !transB)
+    launch_variant<true, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  else
+    launch_variant<true, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+}
+
+int device_sm_count() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+}  // namespace dmrg

@@ -1,0 +1,93 @@
+// kernels.cuh -- device kernels of the two-site DMRG engine (sm_100a).
+//
+// Every contraction of the hot path (Heff steps, environment updates, density matrices, the
+// split back into site tensors) is a list of independent dense block products C = op(A) op(B)
+// whose operands are sub-matrices of a few device buffers. The host plans the lists; one
+// persistent grouped-GEMM launch executes a whole list. Offsets are element offsets from the
+// launch's base pointers, so one plan serves every Lanczos vector.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dmrg {
+
+// One K-segment of a block product: C += op(A_seg) op(B_seg), A_seg is M x K, B_seg is K x N.
+struct GemmSeg {
+  int64_t a_off, b_off;
+  int lda, ldb, K, pad;
+};
+
+// One output block C (M x N, column-major, leading dimension ldc) = alpha * sum_seg + beta * C.
+struct GemmTask {
+  int64_t c_off;
+  int ldc, M, N;
+  int seg0, nseg;
+  int tiles_m;      // ceil(M / BM)
+  int tile0;        // first global tile index of this task
+  int pad;
+  double alpha, beta;
+};
+
+// out block (rows x cols, ld) = sum_t coef_t * in_t (same shape, own ld); sparse MPO mixing.
+struct MixTerm {
+  int64_t in_off;
+  int ld, pad;
+  double coef;
+};
+struct MixTask {
+  int64_t out_off;
+  int ld, rows, cols;
+  int term0, nterm;
+  int tile0;        // first tile (tiles of 32 columns x all rows)
+  int ntiles;
+  int pad;
+};
+
+// dst (rows x cols, ldd) = scale * src (or src^T when trans), src leading dimension lds.
+struct CopyTask {
+  int64_t src_off, dst_off;
+  int lds, ldd, rows, cols;
+  int trans, tile0, ntiles, pad;
+  double scale;
+};
+
+// Symmetric eigenproblem of an n x n column-major matrix at a_off (leading dim n); eigenvalues
+// go to w_off (n doubles, descending) and eigenvectors (columns, same order) to v_off (n x n).
+struct EigTask {
+  int64_t a_off, v_off, w_off;
+  int n, pad;
+};
+
+constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
+
+// Persistent grouped FP64 GEMM (DMMA m8n8k4 tensor-core path).
+void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
+                     double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
+                     int total_tiles, int grid_cap);
+
+void launch_mix(cudaStream_t s, const double* in, double* out, const MixTask* tasks, int ntasks,
+                const MixTerm* terms, int total_tiles);
+
+void launch_copy(cudaStream_t s, const double* src, double* dst, const CopyTask* tasks,
+                 int ntasks, int total_tiles);
+
+// Deterministic reductions: out[j] = <x_j, y> for j < k (x_j = X + j*ldx), written to device memory.
+void launch_mdot(cudaStream_t s, const double* X, int64_t ldx, int k, const double* y, int64_t n,
+                 double* partial, double* out);
+// y = a*x + b*y with a, b either immediate (ap == nullptr) or read from device pointers.
+void launch_axpby(cudaStream_t s, int64_t n, double a, const double* ap, double asign,
+                  const double* x, double b, const double* bp, double bsign, double* y,
+                  int b_recip);
+// y -= sum_j c[j] * X_j  (c in device memory), j < k.
+void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c,
+                 double* y, int64_t n);
+void launch_scale(cudaStream_t s, double* x, int64_t n, double a);
+void launch_zero(cudaStream_t s, double* x, int64_t n);
+
+// Batched cyclic Jacobi: one CTA per task. Overwrites the matrices.
+void launch_jacobi(cudaStream_t s, double* base, const EigTask* tasks, int ntasks, int max_n,
+                   int* status);
+
+int device_sm_count();
+
+}  // namespace dmrg

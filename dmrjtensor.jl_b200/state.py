@@ -1,0 +1,466 @@
+"""MPS / MPO containers and the device-backed drop-in for the reference's two-site path.
+
+``dmrg(psi, mpo; m, minm, sweeps, cutoff)`` mirrors ``algs/DMRG.jl:549-588`` (method "twosite"):
+it returns the energy of the last bond step and updates ``psi`` in place (tensors and ``oc``).
+``makeEnv``/``Lupdate``/``Rupdate`` mirror ``lib/Env/makeEnv.jl:196-246`` and
+``lib/MPO_MPS/{L,R}update.jl`` on device-resident environments.
+
+Indices are 0-based here (site ``i`` is the reference's site ``i+1``; ``psi.oc`` is ``oc-1``).
+All arithmetic happens in libdmrgb200.so on the GPU; nothing here computes a contraction.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import Params, SweepStats, check, lib
+
+# ------------------------------------------------------------------ context
+
+
+class Context:
+    """One CUDA stream on one device, with an optional HBM budget (bytes, 0 = none)."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        h = C.c_void_p()
+        code = lib().dmrg_ctx_create(int(device), C.c_size_t(int(hbm_budget)), C.byref(h))
+        check(code, None)
+        self.h = h
+        self.device = device
+
+    def memory(self):
+        a, b = C.c_size_t(), C.c_size_t()
+        check(lib().dmrg_ctx_memory(self.h, C.byref(a), C.byref(b)), self.h)
+        return a.value, b.value
+
+    def close(self):
+        if self.h:
+            lib().dmrg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None or _default_ctx.h is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _ptr_array(arrs, ctype):
+    P = C.POINTER(ctype)
+    out = (P * len(arrs))()
+    for i, a in enumerate(arrs):
+        out[i] = a.ctypes.data_as(P) if a is not None else None
+    return out
+
+
+def _int_arr(vals):
+    return (C.c_int * len(vals))(*[int(v) for v in vals])
+
+
+# ------------------------------------------------------------------ host containers
+
+
+class MPO:
+    """``W[i]``: array [wl, d, d, wr] (ket = index 1, bra = index 2). ``qlabels``: per-site list
+    of physical charges (tuples) or None for a dense MPO (``makeqMPO`` = :meth:`with_qn`)."""
+
+    def __init__(self, tensors, qlabels=None):
+        self.W = [np.asarray(w, dtype=float) for w in tensors]
+        self.qlabels = qlabels
+        self._dev = {}
+
+    def __len__(self):
+        return len(self.W)
+
+    def __getitem__(self, i):
+        return self.W[i]
+
+    @property
+    def nsym(self):
+        return 0 if self.qlabels is None else len(self.qlabels[0][0])
+
+    def with_qn(self, Qlabels):
+        """``makeqMPO(Qlabels, mpo)``: the same operator with physical charges attached
+        (``Qlabels`` repeats over the sites, ``lib/MPO/makeqMPO.jl:23-84``)."""
+        ql = [list(map(tuple, Qlabels[i % len(Qlabels)])) if isinstance(Qlabels[0], list)
+              else list(map(tuple, Qlabels)) for i in range(len(self))]
+        return MPO(self.W, ql)
+
+    def device(self, ctx=None):
+        ctx = ctx or default_context()
+        key = id(ctx)
+        if key not in self._dev:
+            self._dev[key] = DeviceMPO(self, ctx)
+        return self._dev[key]
+
+
+class MPS:
+    """Matrix product state ``psi[i]``: [ml, d, mr]. Dense tensors, or QN block form.
+
+    ``bond_labels[b]`` (optional) gives the charge of every state of bond b. After a device run
+    with charges the state is held in block form (``sectors``, ``blocks``) like a Qtens; ``psi[i]``
+    always returns the dense-equivalent tensor."""
+
+    def __init__(self, tensors=None, oc=0, bond_labels=None):
+        self.tensors = [np.asarray(a, dtype=float) for a in tensors] if tensors is not None else None
+        self.oc = int(oc)
+        self.bond_labels = bond_labels
+        self.sectors = None     # L+1 lists of (qn tuple, dim)
+        self.blocks = None      # L flat arrays (canonical block order)
+        self.phys = None        # per-site physical labels when in block form
+        self.sweep_stats = []
+        self._dev = None
+
+    def __len__(self):
+        return len(self.tensors) if self.tensors is not None else len(self.blocks)
+
+    def __getitem__(self, i):
+        if self.tensors is None:
+            return self._dense_site(i)
+        return self.tensors[i]
+
+    def __setitem__(self, i, A):
+        self.materialize()
+        self.tensors[i] = np.asarray(A, dtype=float)
+        self._dev = None
+
+    def _dense_site(self, i):
+        Bl, Br, p = self.sectors[i], self.sectors[i + 1], self.phys[i]
+        ml, mr = sum(d for _, d in Bl), sum(d for _, d in Br)
+        out = np.zeros((ml, len(p), mr), order="F")
+        ol = np.cumsum([0] + [d for _, d in Bl])
+        orr = np.cumsum([0] + [d for _, d in Br])
+        rq = {q: k for k, (q, _) in enumerate(Br)}
+        off = 0
+        data = self.blocks[i]
+        for ka, (qa, da) in enumerate(Bl):
+            for s, ps in enumerate(p):
+                kb = rq.get(tuple(x + y for x, y in zip(qa, ps)))
+                if kb is None:
+                    continue
+                db = Br[kb][1]
+                blk = data[off:off + da * db].reshape((da, db), order="F")
+                out[ol[ka]:ol[ka] + da, s, orr[kb]:orr[kb] + db] = blk
+                off += da * db
+        return out
+
+    def materialize(self):
+        """Convert block form into dense-equivalent tensors (with their bond labels)."""
+        if self.tensors is not None:
+            return self
+        L = len(self.blocks)
+        self.tensors = [self._dense_site(i) for i in range(L)]
+        self.bond_labels = [[q for q, d in sec for _ in range(d)] for sec in self.sectors]
+        self.sectors = self.blocks = None
+        return self
+
+
+def product_MPS(states, d, oc=0):
+    """Product state with site i in basis state ``states[i]`` (``MPS(initTensor)`` pattern of
+    ``test/dmrg_test.jl:55-58``)."""
+    out = []
+    for s in states:
+        A = np.zeros((1, d, 1))
+        A[0, s, 0] = 1.0
+        out.append(A)
+    return MPS(out, oc=oc)
+
+
+def neelMPS(L):
+    """Neel product state: up on odd (1-based) sites, down on even ones."""
+    return product_MPS([0 if i % 2 == 0 else 1 for i in range(L)], 2)
+
+
+def applyOps(psi, sites, op, trail=None):
+    """``applyOps!`` (``lib/MPO_MPS/applyMPO.jl:21-34``) on a dense host MPS (initial states)."""
+    psi.materialize()
+    for p in sites:
+        psi.tensors[p] = np.einsum("st,atb->asb", op, psi.tensors[p])
+        if trail is not None:
+            for j in range(p):
+                psi.tensors[j] = np.einsum("st,atb->asb", trail, psi.tensors[j])
+    psi._dev = None
+    return psi
+
+
+def randMPS(d, L, m, seed=0, oc=0):
+    """Seeded random MPS: bond dim min(d^k, d^(L-k), m), entries standard normal, each tensor
+    normalised, then moved to a right-canonical form with centre ``oc`` (the seeded stand-in for
+    ``randMPS``, ``lib/MPS/randMPS.jl:27-56``; the gauge moves are exact QR/LQ, host-side set-up)."""
+    rng = np.random.default_rng(seed)
+    dims = [min(d ** k, d ** (L - k), m) for k in range(L + 1)]
+    T = []
+    for i in range(L):
+        A = rng.standard_normal((dims[i], d, dims[i + 1]))
+        T.append(A / np.linalg.norm(A))
+    for i in range(L - 1, oc, -1):            # LQ from the right
+        a, dd, b = T[i].shape
+        Q, R = np.linalg.qr(T[i].reshape(a, dd * b).T)
+        T[i] = Q.T.reshape(Q.shape[1], dd, b)
+        T[i - 1] = np.tensordot(T[i - 1], R.T, axes=(2, 0))
+    for i in range(0, oc):                    # QR from the left
+        a, dd, b = T[i].shape
+        Q, R = np.linalg.qr(T[i].reshape(a * dd, b))
+        T[i] = Q.reshape(a, dd, Q.shape[1])
+        T[i + 1] = np.tensordot(R, T[i + 1], axes=(1, 0))
+    T[oc] = T[oc] / np.linalg.norm(T[oc])
+    return MPS(T, oc=oc)
+
+
+# ------------------------------------------------------------------ device handles
+
+
+class DeviceMPO:
+    def __init__(self, mpo: MPO, ctx: Context):
+        self.ctx = ctx
+        self.mpo = mpo
+        L = len(mpo)
+        nsym = mpo.nsym
+        Ws = [np.asfortranarray(w) for w in mpo.W]
+        d = [w.shape[1] for w in Ws]
+        wl = [w.shape[0] for w in Ws]
+        wr = [w.shape[3] for w in Ws]
+        self._keep = [Ws]
+        if nsym:
+            phys = [np.asarray(mpo.qlabels[i], dtype=np.int32).reshape(-1) for i in range(L)]
+            self._keep.append(phys)
+            pq = _ptr_array(phys, C.c_int)
+        else:
+            pq = None
+        h = C.c_void_p()
+        check(lib().dmrg_mpo_upload(ctx.h, L, nsym, _int_arr(d), _int_arr(wl), _int_arr(wr),
+                                    _ptr_array(Ws, C.c_double), pq, None, C.byref(h)), ctx.h)
+        self.h = h
+        self.L, self.nsym, self.d = L, nsym, d
+
+    def __del__(self):
+        try:
+            if self.h and self.ctx.h:
+                lib().dmrg_mpo_destroy(self.h)
+        except Exception:
+            pass
+
+
+class DeviceState:
+    """A device-resident MPS plus its environments (``dmrg_state``)."""
+
+    def __init__(self, psi: MPS, dmpo: DeviceMPO):
+        self.ctx = dmpo.ctx
+        self.dmpo = dmpo
+        L = len(psi)
+        if len(dmpo.mpo) != L:
+            raise ValueError("MPS and MPO lengths differ")
+        h = C.c_void_p()
+        if psi.tensors is None:
+            nsym = dmpo.nsym
+            nsec = _int_arr([len(s) for s in psi.sectors])
+            qn = [np.asarray([q for q, _ in s], dtype=np.int32).reshape(-1) for s in psi.sectors]
+            dims = [np.asarray([dd for _, dd in s], dtype=np.int32) for s in psi.sectors]
+            data = [np.ascontiguousarray(b, dtype=float) for b in psi.blocks]
+            self._keep = (qn, dims, data)
+            check(lib().dmrg_mps_upload_blocks(self.ctx.h, dmpo.h, nsec,
+                                               _ptr_array(qn, C.c_int) if nsym else None,
+                                               _ptr_array(dims, C.c_int),
+                                               _ptr_array(data, C.c_double), psi.oc, C.byref(h)),
+                  self.ctx.h)
+        else:
+            As = [np.asfortranarray(a) for a in psi.tensors]
+            ml = _int_arr([a.shape[0] for a in As])
+            mr = _int_arr([a.shape[2] for a in As])
+            bq = None
+            keep = [As]
+            if psi.bond_labels is not None and dmpo.nsym:
+                lab = [np.asarray(b, dtype=np.int32).reshape(-1) for b in psi.bond_labels]
+                keep.append(lab)
+                bq = _ptr_array(lab, C.c_int)
+            self._keep = keep
+            check(lib().dmrg_mps_upload(self.ctx.h, dmpo.h, ml, mr, _ptr_array(As, C.c_double),
+                                        bq, psi.oc, C.byref(h)), self.ctx.h)
+        self.h = h
+        self.L = L
+
+    # -- queries
+    @property
+    def oc(self):
+        v = C.c_int()
+        check(lib().dmrg_state_oc(self.h, C.byref(v)), self.ctx.h)
+        return v.value
+
+    def bond(self, b):
+        n = C.c_int()
+        check(lib().dmrg_bond_info(self.h, b, C.byref(n), None, None), self.ctx.h)
+        ns = self.dmpo.nsym
+        q = (C.c_int * max(n.value * max(ns, 1), 1))()
+        dd = (C.c_int * max(n.value, 1))()
+        check(lib().dmrg_bond_info(self.h, b, C.byref(n), q, dd), self.ctx.h)
+        return [(tuple(q[k * ns:(k + 1) * ns]), dd[k]) for k in range(n.value)]
+
+    def site_blocks(self, i):
+        n = C.c_int64()
+        check(lib().dmrg_site_size(self.h, i, C.byref(n)), self.ctx.h)
+        out = np.empty(n.value)
+        check(lib().dmrg_mps_download_blocks(self.h, i, out.ctypes.data_as(C.POINTER(C.c_double))),
+              self.ctx.h)
+        return out
+
+    def site_dense(self, i):
+        ml, mr = C.c_int(), C.c_int()
+        check(lib().dmrg_mps_download(self.h, i, None, C.byref(ml), C.byref(mr)), self.ctx.h)
+        out = np.zeros((ml.value, self.dmpo.d[i], mr.value), order="F")
+        check(lib().dmrg_mps_download(self.h, i, out.ctypes.data_as(C.POINTER(C.c_double)), None,
+                                      None), self.ctx.h)
+        return out
+
+    def download_into(self, psi: MPS, blocks=None):
+        """Write the device MPS back into ``psi`` (block form when charges are present)."""
+        use_blocks = (self.dmpo.nsym > 0) if blocks is None else blocks
+        if use_blocks:
+            psi.sectors = [self.bond(b) for b in range(self.L + 1)]
+            psi.blocks = [self.site_blocks(i) for i in range(self.L)]
+            psi.phys = [list(map(tuple, self.dmpo.mpo.qlabels[i])) if self.dmpo.nsym
+                        else [()] * self.dmpo.d[i] for i in range(self.L)]
+            psi.tensors = None
+            psi.bond_labels = None
+        else:
+            psi.tensors = [self.site_dense(i) for i in range(self.L)]
+            psi.bond_labels = ([[q for q, d in self.bond(b) for _ in range(d)]
+                                for b in range(self.L + 1)] if self.dmpo.nsym else None)
+            psi.sectors = psi.blocks = None
+        psi.oc = self.oc
+        psi._dev = self
+
+    # -- environments and contractions
+    def env_build(self):
+        check(lib().dmrg_env_build(self.h, self.dmpo.h), self.ctx.h)
+
+    def lupdate(self, i):
+        check(lib().dmrg_lupdate(self.h, self.dmpo.h, i), self.ctx.h)
+
+    def rupdate(self, i):
+        check(lib().dmrg_rupdate(self.h, self.dmpo.h, i), self.ctx.h)
+
+    def env(self, i, left):
+        dims = (C.c_int * 3)()
+        check(lib().dmrg_env_get(self.h, i, 1 if left else 0, None, dims), self.ctx.h)
+        out = np.zeros(tuple(dims), order="F")
+        check(lib().dmrg_env_get(self.h, i, 1 if left else 0,
+                                 out.ctypes.data_as(C.POINTER(C.c_double)), dims), self.ctx.h)
+        return out
+
+    def heff(self, iL, psi2, precision="fp64"):
+        dims = (C.c_int * 4)()
+        check(lib().dmrg_twosite_dims(self.h, self.dmpo.h, iL, dims), self.ctx.h)
+        x = np.asfortranarray(psi2, dtype=float)
+        if x.shape != tuple(dims):
+            raise ValueError(f"two-site vector has shape {x.shape}, expected {tuple(dims)}")
+        y = np.zeros(tuple(dims), order="F")
+        check(lib().dmrg_heff_apply(self.h, self.dmpo.h, iL, x.ctypes.data_as(C.POINTER(C.c_double)),
+                                    y.ctypes.data_as(C.POINTER(C.c_double)),
+                                    _lib.PREC[precision]), self.ctx.h)
+        return y
+
+    def sweep(self, params: Params):
+        st = SweepStats()
+        check(lib().dmrg_sweep(self.h, self.dmpo.h, C.byref(params), C.byref(st)), self.ctx.h)
+        return st.as_dict()
+
+    def __del__(self):
+        try:
+            if self.h and self.ctx.h:
+                lib().dmrg_state_destroy(self.h)
+        except Exception:
+            pass
+
+
+def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
+                degen_rtol=0.0, betatest=1e-10, fp64_final=1):
+    p = Params()
+    lib().dmrg_params_default(C.byref(p))
+    p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)
+    p.krylov = int(krylov)
+    p.precision = _lib.PREC[precision] if isinstance(precision, str) else int(precision)
+    p.svnbond, p.degen_rtol, p.betatest, p.fp64_final = int(svnbond), float(degen_rtol), \
+        float(betatest), int(fp64_final)
+    return p
+
+
+# ------------------------------------------------------------------ the drop-in
+
+def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, silent=True,
+         method="twosite", krylov=2, precision="fp64", SvNbond=0, degen_rtol=0.0, ctx=None,
+         download=True):
+    """Two-site DMRG on the GPU: ``dmrg(psi, mpo; m, minm, sweeps, cutoff)`` of
+    ``algs/DMRG.jl:549-588``. ``maxm`` is accepted as an alias of ``m``; ``m`` may also be a
+    per-sweep list (a bond-dimension ramp). Returns the energy of the last bond step and updates
+    ``psi`` (tensors, ``oc``) in place; per-sweep records go to ``psi.sweep_stats``.
+    ``download=False`` leaves the result on the device (``psi`` keeps a handle to it)."""
+    if method != "twosite":
+        raise ValueError(f"DMRG method ({method}) not defined")
+    mm = m if m is not None else (maxm if maxm is not None else 0)
+    sched = list(mm) if np.ndim(mm) else [int(mm)] * int(sweeps)
+    dmpo = mpo.device(ctx)
+    dev = psi._dev if (psi._dev is not None and psi._dev.dmpo is dmpo) else DeviceState(psi, dmpo)
+    dev.env_build()
+    energy = 0.0
+    stats = []
+    for n, mcur in enumerate(sched):
+        st = dev.sweep(make_params(mcur, minm, cutoff, krylov, precision, SvNbond, degen_rtol))
+        energy = st["energy"]
+        stats.append(st)
+        if not silent:
+            print(f"Sweep {n + 1} (back and forth): {st['seconds']:.5f} sec")
+            print(f"Largest truncation = {st['max_truncerr']}, m = {st['biggest_m']}")
+            print(f"Energy at sweep {n + 1} is {energy:.12f}\n")
+    psi.sweep_stats = stats
+    if download:
+        dev.download_into(psi)
+    else:
+        psi._dev = dev
+        psi.oc = dev.oc
+    return energy
+
+
+class Env:
+    """Device-backed environment list (``environment{W}``, ``lib/types.jl:113-115``):
+    ``Lenv[i]`` downloads the dense-equivalent [m, w, m] tensor of site i."""
+
+    def __init__(self, dev: DeviceState, left: bool):
+        self.dev, self.left = dev, left
+
+    def __getitem__(self, i):
+        return self.dev.env(i, self.left)
+
+    def __len__(self):
+        return self.dev.L
+
+
+def makeEnv(psi: MPS, mpo: MPO, ctx=None):
+    """``makeEnv(psi, mpo)`` (``lib/Env/makeEnv.jl:196-221,244-246``): returns ``(Lenv, Renv)``
+    built on the device for the centre ``psi.oc``."""
+    dmpo = mpo.device(ctx)
+    dev = psi._dev if (psi._dev is not None and psi._dev.dmpo is dmpo) else DeviceState(psi, dmpo)
+    psi._dev = dev
+    dev.env_build()
+    return Env(dev, True), Env(dev, False)
+
+
+def Lupdate(i, Lenv: Env, psi: MPS = None, mpo: MPO = None):
+    """``Lupdate!(i, Lenv, psi, mpo)``: ``Lenv[i+1] = Lupdate(Lenv[i], psi[i], psi[i], mpo[i])``."""
+    Lenv.dev.lupdate(i)
+
+
+def Rupdate(i, Renv: Env, psi: MPS = None, mpo: MPO = None):
+    """``Rupdate!(i, Renv, psi, mpo)``: ``Renv[i-1] = Rupdate(Renv[i], psi[i], psi[i], mpo[i])``."""
+    Renv.dev.rupdate(i)

@@ -1,0 +1,189 @@
+/*
+ * dmrg_b200.h -- C ABI of libdmrgb200.so, a B200 (sm_100a) two-site DMRG engine.
+ *
+ * The library is the device side of a drop-in for DMRJtensor.jl's two-site path:
+ *   dmrg(psi::MPS, mpo::MPO; m, minm, sweeps, cutoff)          algs/DMRG.jl:549-588
+ *     -> dmrg_twosite -> optmps -> twostep                      algs/DMRG.jl:675-691,362-405
+ *                                                              algs/optimizeMPS.jl:759-849
+ *   makeEnv(psi, mpo) / Lupdate / Rupdate / Lupdate! / Rupdate!  lib/Env/makeEnv.jl:196-246
+ *                                                              lib/MPO_MPS/Lupdate.jl:17-37
+ *                                                              lib/MPO_MPS/Rupdate.jl:17-37
+ * A Julia host binds these with ccall; Python tests bind them with ctypes. Plain C types only.
+ *
+ * Conventions
+ *  - Host arrays are column-major with the reference's index order:
+ *      MPS site   A[ml, d, mr]            (lib/types.jl:84-101)
+ *      MPO site   W[wl, d, d, wr]         ket = index 2, bra = index 3 (lib/MPO/makeMPO.jl:76)
+ *      left env   L[m(bra), w, m(ket)]    right env R[m(ket), w, m(bra)]  (lib/Env/makeEnv.jl:17-26)
+ *  - Sites and bonds are 0-based: site i in [0, L); bond b in [0, L] is left of site b.
+ *  - Quantum numbers: nsym in {0,1,2} int32 charges per state (0 = dense, no symmetry).
+ *    A physical label array has d*nsym ints (state-major). Abelian U(1)^nsym fusion by addition.
+ *    MPS bond labels obey q(right) = q(left) + p(s); MPO bond labels obey
+ *    r(right) = r(left) + p(ket) - p(bra) (the makeqMPO rule of lib/MPO/makeqMPO.jl:23-84).
+ *    Inside the library each bond basis is grouped by charge (a permutation = a gauge change);
+ *    downloads report the grouped order and its labels.
+ *  - Every function returns 0 (DMRG_OK) or an error code; dmrg_last_error() gives the text.
+ *    No C++ exception crosses this boundary. A context is used by one host thread at a time.
+ *  - Caller-owned host buffers are read/written only during the call. Device objects belong to
+ *    their handles and are released by the matching *_destroy.
+ */
+#ifndef DMRG_B200_H
+#define DMRG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DMRG_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define DMRG_API __attribute__((visibility("default")))
+#else
+#define DMRG_API
+#endif
+
+enum dmrg_status {
+  DMRG_OK = 0,
+  DMRG_ERR_ARG = 1,      /* bad argument / null handle */
+  DMRG_ERR_SHAPE = 2,    /* inconsistent dimensions */
+  DMRG_ERR_QN = 3,       /* data in a block that the quantum numbers forbid */
+  DMRG_ERR_OOM = 4,      /* device allocation failed */
+  DMRG_ERR_BUDGET = 5,   /* request exceeds the context's HBM budget */
+  DMRG_ERR_TIMEOUT = 6,  /* a bounded device wait gave up */
+  DMRG_ERR_CUDA = 7,     /* CUDA runtime error */
+  DMRG_ERR_STATE = 8,    /* object not in a usable state (e.g. environments not built) */
+  DMRG_ERR_NOCUDA = 9    /* no CUDA device */
+};
+
+enum dmrg_precision {
+  DMRG_PREC_FP64 = 0,    /* plain form: every contraction in FP64 (DMMA) */
+  DMRG_PREC_3XTF32 = 1,  /* chosen form: Heff contractions as 3 TF32 tensor-core products */
+  DMRG_PREC_BF16X9 = 2   /* chosen form: Heff contractions as 9 BF16 tensor-core products */
+};
+
+typedef struct dmrg_ctx dmrg_ctx;
+typedef struct dmrg_mpo dmrg_mpo;
+typedef struct dmrg_state dmrg_state;
+
+/* Parameters of one sweep: the two-site subset of algvars (algs/optimizeMPS.jl:36-106,514-577). */
+typedef struct dmrg_params {
+  int maxm;          /* `m` keyword; <= 0 means unlimited                      */
+  int minm;          /* default 2                                              */
+  double cutoff;     /* discarded weight bound, mag = 1 (algs/DMRG.jl:387)      */
+  int krylov;        /* 2 = the reference's 2-vector step (algs/DMRG.jl:57-90); k>2 Lanczos with
+                        full re-orthogonalisation                               */
+  int precision;     /* enum dmrg_precision                                    */
+  int svnbond;       /* bond whose entropy is reported (1-based, cld(L,2) by default; 0 = default) */
+  double degen_rtol; /* >0: never split a cluster of equal weights at the cut  */
+  double betatest;   /* Krylov breakdown threshold, 1e-10 (algs/DMRG.jl:57)     */
+  int fp64_final;    /* chosen forms: 1 = re-evaluate the Ritz energy with one FP64 matvec */
+  int reserved[7];
+} dmrg_params;
+
+/* Per-sweep record (what dmrgcvg prints, algs/DMRG.jl:610-652, plus timings). */
+typedef struct dmrg_sweep_stats {
+  double energy;        /* energy of the last bond step of the sweep          */
+  double max_truncerr;  /* maxtrunc over the sweep                            */
+  int biggest_m;        /* largest kept bond dimension in the sweep           */
+  int n_matvec;         /* Heff applications in the sweep                     */
+  double entropy;       /* -sum D^2 log D^2 at bond svnbond, leftward step    */
+  double seconds;       /* device-timed sweep duration                        */
+  double heff_flops;    /* algorithmic FLOPs of all Heff applications         */
+  double heff_seconds;  /* device time inside Heff applications               */
+  double env_flops;     /* algorithmic FLOPs of the environment updates       */
+  double env_seconds;
+  double eig_seconds;   /* density-matrix formation + eigensolve + split      */
+  double vec_seconds;   /* Lanczos vector operations                          */
+  double d_top[8];      /* largest singular values at bond svnbond            */
+} dmrg_sweep_stats;
+
+/* ---------------------------------------------------------------- context */
+DMRG_API int dmrg_abi_version(void);
+/* Creates a context on `device` (one CUDA stream). hbm_budget_bytes = 0: no budget. */
+DMRG_API int dmrg_ctx_create(int device, size_t hbm_budget_bytes, dmrg_ctx** out);
+DMRG_API int dmrg_ctx_destroy(dmrg_ctx* ctx);
+DMRG_API const char* dmrg_last_error(const dmrg_ctx* ctx);
+/* Bytes currently allocated on the device by this context, and its peak. */
+DMRG_API int dmrg_ctx_memory(const dmrg_ctx* ctx, size_t* in_use, size_t* peak);
+
+/* ---------------------------------------------------------------- MPO (MPO(...), makeMPO, makeqMPO)
+ * W[i]: column-major [wl[i], d[i], d[i], wr[i]] doubles (lib/MPO/makeMPO.jl:59-92 layout).
+ * phys_qn[i]: d[i]*nsym ints or NULL when nsym = 0.
+ * bond_qn: NULL (labels derived with the makeqMPO largest-weight rule) or L+1 arrays of
+ *          (bond dim)*nsym ints. Replaces makeqMPO (lib/MPO/makeqMPO.jl:23-84). */
+DMRG_API int dmrg_mpo_upload(dmrg_ctx* ctx, int L, int nsym, const int* d, const int* wl, const int* wr,
+                    const double* const* W, const int* const* phys_qn, const int* const* bond_qn,
+                    dmrg_mpo** out);
+DMRG_API int dmrg_mpo_destroy(dmrg_mpo* mpo);
+
+/* ---------------------------------------------------------------- MPS
+ * Dense-equivalent upload (MPS(...) / makeqMPS, lib/MPS/MPS.jl:17-37, lib/MPS/makeqMPS.jl:26-102):
+ * A[i] column-major [ml[i], d[i], mr[i]] (mr[i] == ml[i+1]). bond_qn: NULL (labels from the
+ * largest-magnitude element, the assignflux! rule of lib/MPS/MPS.jl:206-219) or L+1 arrays.
+ * oc: 0-based orthogonality centre (psi.oc - 1). Elements in QN-forbidden positions must be 0. */
+DMRG_API int dmrg_mps_upload(dmrg_ctx* ctx, const dmrg_mpo* mpo, const int* ml, const int* mr,
+                    const double* const* A, const int* const* bond_qn, int oc, dmrg_state** out);
+/* Block-form upload: bond b has nsec[b] sectors with charges sec_qn[b] (nsec[b]*nsym ints,
+ * strictly increasing lexicographically) and sizes sec_dim[b]. data[i] holds site i's blocks in
+ * canonical order: for each left sector ka (ascending), for each physical state s, if the right
+ * sector with q = q(ka)+p(s) exists, the column-major block [dim ka, dim kb]. */
+DMRG_API int dmrg_mps_upload_blocks(dmrg_ctx* ctx, const dmrg_mpo* mpo, const int* nsec,
+                           const int* const* sec_qn, const int* const* sec_dim,
+                           const double* const* data, int oc, dmrg_state** out);
+DMRG_API int dmrg_state_destroy(dmrg_state* st);
+DMRG_API int dmrg_state_oc(const dmrg_state* st, int* oc);
+/* Sector structure of bond b: *nsec; if qn/dims are non-NULL they receive nsec*nsym / nsec ints. */
+DMRG_API int dmrg_bond_info(const dmrg_state* st, int bond, int* nsec, int* qn, int* dims);
+/* Number of doubles of site i in block form. */
+DMRG_API int dmrg_site_size(const dmrg_state* st, int site, int64_t* n_blocks_doubles);
+DMRG_API int dmrg_mps_download_blocks(dmrg_state* st, int site, double* out);
+/* Dense-equivalent download of site i: out [ml, d, mr] column-major in the grouped bond order;
+ * ml/mr receive the bond sizes (out may be NULL to query them). */
+DMRG_API int dmrg_mps_download(dmrg_state* st, int site, double* out, int* ml, int* mr);
+
+/* ---------------------------------------------------------------- environments
+ * makeEnv(psi, mpo) (lib/Env/makeEnv.jl:196-221): boundary ones(1,1,1), Lenv[0..oc], Renv[oc..L-1]. */
+DMRG_API int dmrg_env_build(dmrg_state* st, const dmrg_mpo* mpo);
+/* Lupdate!(i, Lenv, psi, mpo): Lenv[i+1] = Lupdate(Lenv[i], psi[i], psi[i], mpo[i])
+ * (lib/MPO_MPS/Lupdate.jl:17-37). Requires Lenv[i]. */
+DMRG_API int dmrg_lupdate(dmrg_state* st, const dmrg_mpo* mpo, int site);
+/* Rupdate!(i, Renv, psi, mpo): Renv[i-1] = Rupdate(Renv[i], ...) (lib/MPO_MPS/Rupdate.jl:17-37). */
+DMRG_API int dmrg_rupdate(dmrg_state* st, const dmrg_mpo* mpo, int site);
+/* Lenv[i] (left=1) or Renv[i] (left=0) as a dense-equivalent column-major [m, w, m] array
+ * (L[bra,w,ket] / R[ket,w,bra]). dims receives the 3 sizes; out may be NULL to query them. */
+DMRG_API int dmrg_env_get(dmrg_state* st, int site, int left, double* out, int* dims);
+
+/* ---------------------------------------------------------------- contractions (tests / Env API)
+ * Two-site effective Hamiltonian on sites (iL, iL+1) applied to a dense-equivalent vector
+ * psi_in [ml, d1, d2, mr] (make2site / inline Heff, algs/DMRG.jl:48-54,69-73), psi_out same shape.
+ * Uses Lenv[iL] and Renv[iL+1]. precision: enum dmrg_precision. */
+DMRG_API int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
+                    double* psi_out, int precision);
+/* Dense-equivalent dims of the two-site space at (iL, iL+1): dims[4] = {ml, d1, d2, mr}. */
+DMRG_API int dmrg_twosite_dims(const dmrg_state* st, const dmrg_mpo* mpo, int iL, int* dims);
+
+/* ---------------------------------------------------------------- the sweep
+ * One optmps sweep (algs/optimizeMPS.jl:790-835): 2(L-1) twostep calls, each followed by an
+ * environment update; the centre reverses at the edges. Requires dmrg_env_build first. */
+DMRG_API int dmrg_sweep(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_sweep_stats* out);
+/* ---------------------------------------------------------------- kernel test hooks
+ * No reference counterpart: these expose single device kernels to the parity tests.
+ * C[M,N] = op(A) op(B) with the grouped FP64 GEMM (one task, one K segment), host arrays,
+ * column-major with leading dimensions lda/ldb/ldc; op = transpose when trans* != 0. */
+DMRG_API int dmrg_test_gemm(dmrg_ctx* ctx, int transA, int transB, int M, int N, int K,
+                            const double* A, int lda, const double* B, int ldb, double* C, int ldc);
+/* Batched symmetric eigensolve (the truncation's Jacobi kernel): nmat column-major matrices of
+ * sizes n[i] packed back to back in A; eigenvalues (descending) packed into w and eigenvectors
+ * (columns) overwrite A. */
+DMRG_API int dmrg_test_eigh(dmrg_ctx* ctx, int nmat, const int* n, double* A, double* w);
+
+/* Fills *p with the reference defaults (minm 2, krylov 2, betatest 1e-10, ...). */
+DMRG_API void dmrg_params_default(dmrg_params* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DMRG_B200_H */

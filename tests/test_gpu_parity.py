@@ -1,0 +1,141 @@
+"""Device vs oracle parity for the hot-path contractions (through the C ABI).
+
+Tolerances: the plain form is FP64 end to end, so single contractions must agree to 1e-12
+relative (max-abs error / max-abs value); whole sweeps are compared on invariants (energy,
+truncation error, centre-bond entropy), never on gauge-dependent tensors.
+"""
+import numpy as np
+import pytest
+
+from oracle import dmrg as od, models as om, qtensor as oq
+
+pytestmark = pytest.mark.gpu
+
+RTOL_CONTRACT = 1e-12
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _heis(pkg, L, qn):
+    mpo = pkg.makeMPO(pkg.heisenbergMPO, 2, L)
+    ompo = om.make_mpo([om.heisenberg_bulk()] * L, 2)
+    if qn:
+        mpo = mpo.with_qn(pkg.SPIN_QN)
+    return mpo, ompo
+
+
+def _qn_random_mps(L, m, seed):
+    """A U(1) MPS (Sz=0 sector) with random blocks: built by DMRG-free QN-aware random filling."""
+    rng = np.random.default_rng(seed)
+    pq = [[(1,), (-1,)]] * L
+    # bond charges: allowed partial magnetisations, m states spread over sectors
+    bonds = [[(0,)]]
+    for k in range(1, L + 1):
+        lo, hi = max(-k, -(L - k)), min(k, L - k)
+        qs = [(q,) for q in range(lo, hi + 1) if (q - lo) % 2 == 0]
+        bonds.append(qs)
+    dims = []
+    for k, qs in enumerate(bonds):
+        if k == 0 or k == L:
+            dims.append([1] * len(qs))
+        else:
+            per = max(1, m // len(qs))
+            dims.append([per] * len(qs))
+    tens = []
+    for i in range(L):
+        ia = oq.Index(bonds[i], dims[i], +1)
+        isx = oq.Index(pq[i], [1, 1], +1)
+        ib = oq.Index(bonds[i + 1], dims[i + 1], -1)
+        T = oq.QTensor([ia, isx, ib], {}, (0,))
+        for ka in range(len(bonds[i])):
+            for s in range(2):
+                q = bonds[i][ka][0] + pq[i][s][0]
+                if (q,) in bonds[i + 1]:
+                    kb = bonds[i + 1].index((q,))
+                    T.blocks[(ka, s, kb)] = rng.standard_normal((dims[i][ka], 1, dims[i + 1][kb]))
+        tens.append(T)
+    return tens, bonds, dims
+
+
+def _labels_from(bonds, dims):
+    return [[q for q, d in zip(qs, ds) for _ in range(d)] for qs, ds in zip(bonds, dims)]
+
+
+@pytest.mark.parametrize("qn", [False, True])
+def test_env_and_heff_match_oracle(dmrgb, ctx, qn):
+    L, m = 8, 12
+    mpo, ompo = _heis(dmrgb, L, qn)
+    if qn:
+        qt, bonds, dims = _qn_random_mps(L, m, seed=7)
+        dense = [oq.to_dense(T) for T in qt]
+        psi = dmrgb.MPS(dense, oc=3, bond_labels=_labels_from(bonds, dims))
+        otens = qt
+        ompo_t = om.to_qmpo(ompo, [[(1,), (-1,)]] * L)
+    else:
+        rng = np.random.default_rng(5)
+        dimsb = [min(2 ** k, 2 ** (L - k), m) for k in range(L + 1)]
+        dense = [rng.standard_normal((dimsb[i], 2, dimsb[i + 1])) for i in range(L)]
+        psi = dmrgb.MPS(dense, oc=3)
+        otens = dense
+        ompo_t = ompo
+    Lenv, Renv = dmrgb.makeEnv(psi, mpo, ctx=ctx)
+    OL, OR = od.make_env(otens, ompo_t, 3)
+    for i in range(0, 4):
+        assert _rel(Lenv[i], oq.to_dense(OL[i])) < RTOL_CONTRACT, f"Lenv[{i}]"
+    for i in range(3, L):
+        assert _rel(Renv[i], oq.to_dense(OR[i])) < RTOL_CONTRACT, f"Renv[{i}]"
+    # Heff on a random two-site vector at (iL, iL+1) = (3, 4) needs Renv[4]: move the right env
+    dev = Lenv.dev
+    # two-site vector in the QN-allowed pattern of the oracle
+    AA = od.contract(otens[3], 2, otens[4], 0)
+    if qn:
+        rng = np.random.default_rng(11)
+        AA = oq.QTensor(AA.indices, {k: rng.standard_normal(v.shape) for k, v in AA.blocks.items()},
+                        AA.flux)
+    x = oq.to_dense(AA)
+    # Renv[4] is valid (built for oc=3); Lenv[3] valid
+    y = dev.heff(3, x)
+    yo = oq.to_dense(od.heff_twosite(OL[3], OR[4], AA, ompo_t[3], ompo_t[4]))
+    assert _rel(y, yo) < RTOL_CONTRACT
+    # make2site order gives the same vector (reference's two Heff forms agree)
+    y2 = oq.to_dense(od.make2site(OL[3], OR[4], otens[3], otens[4], ompo_t[3], ompo_t[4]))
+    if not qn:
+        assert _rel(dev.heff(3, oq.to_dense(od.contract(otens[3], 2, otens[4], 0))), y2) < RTOL_CONTRACT
+    # Lupdate! / Rupdate! through the Env API agree with the oracle's next environments
+    dmrgb.Lupdate(3, Lenv)
+    assert _rel(Lenv[4], oq.to_dense(od.Lupdate(OL[3], otens[3], otens[3], ompo_t[3]))) < RTOL_CONTRACT
+    dmrgb.Rupdate(3, Renv)
+    assert _rel(Renv[2], oq.to_dense(od.Rupdate(OR[3], otens[3], otens[3], ompo_t[3]))) < RTOL_CONTRACT
+
+
+@pytest.mark.parametrize("krylov", [2, 6])
+def test_dense_dmrg_matches_oracle(dmrgb, ctx, krylov):
+    L = 10
+    mpo, ompo = _heis(dmrgb, L, False)
+    psi = dmrgb.randMPS(2, L, 8, seed=1)
+    ref = [a.copy() for a in psi.tensors]
+    E = dmrgb.dmrg(psi, mpo, m=32, sweeps=4, cutoff=1e-12, krylov=krylov, ctx=ctx)
+    E0, info = od.dmrg(ref, ompo, m=32, sweeps=4, cutoff=1e-12, krylov=krylov, trunc="rho")
+    st = psi.sweep_stats[-1]
+    o = info["sweeps"][-1]
+    assert abs(E - E0) <= 1e-10 * abs(E0)
+    assert abs(st["max_truncerr"] - o["maxtrunc"]) <= 1e-8
+    assert abs(st["entropy"] - o["entropy"]) <= 1e-8
+    assert abs(E - (-4.258035207282883)) < 1e-8
+    assert psi.oc == 0
+
+
+def test_qn_heisenberg_dmrg_matches_oracle_and_ed(dmrgb, ctx):
+    L = 10
+    mpo, ompo = _heis(dmrgb, L, True)
+    psi = dmrgb.neelMPS(L)
+    ref = om.to_qmps(om.neel_mps(L), [[(1,), (-1,)]] * L)
+    E = dmrgb.dmrg(psi, mpo, m=45, sweeps=8, cutoff=1e-12, ctx=ctx)
+    E0, info = od.dmrg(ref, om.to_qmpo(ompo, [[(1,), (-1,)]] * L), m=45, sweeps=8, cutoff=1e-12,
+                       trunc="rho")
+    assert abs(E - E0) <= 1e-10 * abs(E0)
+    assert abs(psi.sweep_stats[-1]["entropy"] - info["sweeps"][-1]["entropy"]) <= 1e-8
+    assert abs(E - (-4.258035207282883)) < 1e-8
