@@ -1,0 +1,417 @@
+#!/usr/bin/env python3
+"""Two-site DMRG sweep benchmark on B200 (one process per GPU; N GPUs run independent replicas).
+
+Workload (the headline configuration): spin-1/2 Heisenberg chain, L = 100, J = 1, open ends,
+U(1) block-sparse (Sz_total = 0), MPO bond dimension 5, Neel product start, cutoff 1e-10,
+maxm ramped 64 -> 1024 over 12 sweeps (64, 82, 105, 135, 173, 222, 284, 364, 467, 598, 766, 1024).
+The first 11 ramp sweeps prepare the state (untimed); a "step" is one full sweep (2(L-1) two-site
+bond steps with their environment updates) at maxm = 1024. W warm-up steps, then K timed steps.
+The resident MPS + environments (several hundred MB) exceed the 126 MB L2, so no flush is needed.
+
+Reported: value = sweeps/s over all ranks (device-timed, state resident in HBM); e2e = the same
+through the public ``dmrg(psi, mpo; m, sweeps=1)`` call with the MPS in host memory (upload,
+environment build, sweep, download inside the timed region); roofline of the dominant kernel
+(the grouped FP64 GEMM) against the FP64 GEMM peak measured here with cuBLAS; and the CPU oracle
+timed on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+RAMP = [64, 82, 105, 135, 173, 222, 284, 364, 467, 598, 766, 1024]
+L_CHAIN = 100
+CUTOFF = 1e-10
+METRIC = "sweep s & Heff TFLOP/s, chosen vs plain FP64 at |dE|<=1e-8; solves/s, p99 latency"
+
+
+def load_pkg():
+    if "dmrjtensor_b200" in sys.modules:
+        return sys.modules["dmrjtensor_b200"]
+    pkg_dir = ROOT / "dmrjtensor.jl_b200"
+    spec = importlib.util.spec_from_file_location(
+        "dmrjtensor_b200", pkg_dir / "__init__.py", submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["dmrjtensor_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ------------------------------------------------------------------ clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------ workload
+
+def build_workload(pkg):
+    mpo = pkg.makeMPO(pkg.heisenbergMPO, 2, L_CHAIN).with_qn(pkg.SPIN_QN)
+    psi = pkg.neelMPS(L_CHAIN)
+    return mpo, psi
+
+
+def params(pkg, m, args, profile=0):
+    return pkg.make_params(maxm=m, minm=2, cutoff=CUTOFF, krylov=args.krylov,
+                           precision=args.precision, profile=profile)
+
+
+def fp64_gemm_peak(device):
+    """cuBLAS DGEMM 8192^3 on this GPU (best of 5): the FP64 tensor-pipe roofline denominator."""
+    import torch
+    dev = torch.device("cuda", device)
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def host_block_bytes(psi):
+    return int(sum(b.size for b in psi.blocks) * 8)
+
+
+# ------------------------------------------------------------------ CPU oracle sample
+
+def bond_profile_from_sectors(sectors):
+    """Relative per-bond cost proxy for scaling a sampled bond step to a sweep: the dense-equivalent
+    two-site contraction volume m_l * m_r * (m_l + m_r) of every bond step."""
+    tot = [sum(d for _, d in s) for s in sectors]
+    L = len(sectors) - 1
+    cost = [tot[i] * tot[i + 2] * (tot[i] + tot[i + 2]) for i in range(L - 1)]
+    return cost
+
+
+def oracle_sample(sectors, krylov, nsteps=2, seed=0):
+    """Time the oracle's twostep + environment update at the centre bond(s) of a chain with the
+    given bond sector structure (random block values: the cost does not depend on them).
+    Returns (seconds per sampled step, sweep-seconds estimate, description)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import dmrg as od, models as om, qtensor as oq
+    rng = np.random.default_rng(seed)
+    L = len(sectors) - 1
+    pq = [(1,), (-1,)]
+    mpo = om.to_qmpo(om.make_mpo([om.heisenberg_bulk()] * L, 2), [pq] * L)
+    c = L // 2 - 1
+    idx = {b: oq.Index([q for q, _ in sectors[b]], [d for _, d in sectors[b]], +1)
+           for b in range(c, c + 2 + nsteps + 1)}
+
+    def rand_site(b):
+        ia, ib = idx[b], idx[b + 1].dual()
+        T = oq.QTensor([ia, oq.Index(pq, [1, 1], +1), ib], {}, (0,))
+        for ka, qa in enumerate(ia.qns):
+            for s, ps in enumerate(pq):
+                q = (qa[0] + ps[0],)
+                if q in ib.qns:
+                    kb = ib.qns.index(q)
+                    T.blocks[(ka, s, kb)] = rng.standard_normal((ia.dims[ka], 1, ib.dims[kb]))
+        return T
+
+    def rand_env(b, site_mpo_index, left):
+        ia = idx[b]
+        iw = site_mpo_index
+        if left:
+            ind = [ia, iw.dual(), ia.dual()]
+        else:
+            ind = [ia, iw.dual(), ia.dual()]
+        T = oq.QTensor(ind, {}, (0,))
+        for k1 in range(len(ia.dims)):
+            for w in range(len(iw.dims)):
+                for k3 in range(len(ia.dims)):
+                    if T.allowed((k1, w, k3)):
+                        T.blocks[(k1, w, k3)] = rng.standard_normal((ia.dims[k1], 1, ia.dims[k3]))
+        return T
+
+    psi = {b: rand_site(b) for b in range(c, c + 1 + nsteps)}
+    Lenv = {c: rand_env(c, mpo[c].indices[0], True)}
+    P = od.Params(L, RAMP[-1], 2, CUTOFF, krylov, "svd")
+    times = []
+    for k in range(nsteps):
+        iL, iR = c + k, c + k + 1
+        # a right environment of the correct structure for site iR
+        ib = idx[iR + 1]
+        R = oq.QTensor([ib, mpo[iR].indices[3].dual(), ib.dual()], {}, (0,))
+        for k1 in range(len(ib.dims)):
+            for w in range(len(mpo[iR].indices[3].dims)):
+                for k3 in range(len(ib.dims)):
+                    if R.allowed((k1, w, k3)):
+                        R.blocks[(k1, w, k3)] = rng.standard_normal((ib.dims[k1], 1, ib.dims[k3]))
+        Renv_list = [None] * L
+        Lenv_list = [None] * L
+        Renv_list[iR] = R
+        Lenv_list[iL] = Lenv[iL]
+        plist = [None] * L
+        plist[iL], plist[iR] = psi[iL], psi[iR]
+        t0 = time.perf_counter()
+        od.twostep(1, iL, iL, iR, plist, mpo, Lenv_list, Renv_list, P)
+        Lenv[iL + 1] = od.Lupdate(Lenv[iL], plist[iL], plist[iL], mpo[iL])
+        times.append(time.perf_counter() - t0)
+        psi[iR] = plist[iR]
+        # keep the next step's left tensor on the original sector structure
+        idx[iR] = plist[iR].indices[0]
+    t_step = statistics.mean(times)
+    cost = bond_profile_from_sectors(sectors)
+    est = t_step * 2 * sum(cost) / (statistics.mean(cost[c:c + nsteps]))
+    desc = (f"oracle twostep+Lupdate at bonds {c}..{c + nsteps} of the m={RAMP[-1]} sector "
+            f"structure (random block values, krylov {krylov}); sweep = 2(L-1) steps scaled by "
+            f"the dense-equivalent m_l*m_r*(m_l+m_r) cost of every bond")
+    return t_step, est, desc
+
+
+def cpu_threads():
+    try:
+        import threadpoolctl
+        info = threadpoolctl.threadpool_info()
+        return max([i.get("num_threads", 1) for i in info] or [os.cpu_count() or 1])
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ arms
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    sectors = json.load(open(ROOT / "tests" / "golden" / "c2_sectors_m1024.json"))["sectors"]
+    sectors = [[(tuple(q), d) for q, d in b] for b in sectors]
+    steps = []
+    for _ in range(args.warmup_ref):
+        oracle_sample(sectors, args.krylov, nsteps=1)
+    for _ in range(args.steps_ref):
+        t_step, est, desc = oracle_sample(sectors, args.krylov, nsteps=2)
+        steps.append(est)
+    sweep_s = statistics.mean(steps)
+    cores = cpu_threads()
+    value = 1.0 / sweep_s
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
+           "n_gpus": args.gpus, "steps": args.steps_ref, "warmup": args.warmup_ref,
+           "ms_per_step": sweep_s * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "heisenberg L=100 U(1) Sz=0, maxm 1024 sweep (two-site)",
+                      "krylov": args.krylov, "cutoff": CUTOFF},
+           "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": cores, "kind": "port",
+                            "sample": desc},
+           "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_ours(args, world, rank, local, dist):
+    pkg = load_pkg()
+    ctx = pkg.Context(local)
+    mpo, psi0 = build_workload(pkg)
+    dmpo = mpo.device(ctx)
+    dev = pkg.DeviceState(psi0, dmpo)
+    dev.env_build()
+    t_setup = time.perf_counter()
+    for m in RAMP[:-1]:
+        dev.sweep(params(pkg, m, args))
+    t_setup = time.perf_counter() - t_setup
+    mfin = RAMP[-1]
+    for _ in range(args.warmup):
+        dev.sweep(params(pkg, mfin, args))
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    if rank == 0:
+        sampler.start()
+    n0 = pkg.kernel_launches()
+    t0 = time.perf_counter()
+    stats = [dev.sweep(params(pkg, mfin, args)) for _ in range(args.steps)]
+    wall = time.perf_counter() - t0
+    launches = pkg.kernel_launches() - n0
+    clocks = sampler.stop() if rank == 0 else None
+    dev_s = sum(s["seconds"] for s in stats)
+    tmax = dev_s
+    if dist:
+        import torch
+        t = torch.tensor([dev_s], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tmax = float(t.item())
+    value = world * args.steps / tmax
+    heff_flops = sum(s["heff_flops"] for s in stats) / args.steps
+    heff_sec = sum(s["heff_seconds"] for s in stats) / args.steps
+    sweep_s = dev_s / args.steps
+    energy = stats[-1]["energy"]
+    # one extra profiled sweep: per-launch timing of the dominant kernel
+    prof = dev.sweep(params(pkg, mfin, args, profile=1))
+    sectors = [dev.bond(b) for b in range(L_CHAIN + 1)]
+    if args.dump_sectors:
+        Path(args.dump_sectors).write_text(json.dumps(
+            {"what": "bond sectors (2Sz, dim) after the ramp of the L=100 Heisenberg U(1) workload "
+                     "at maxm 1024", "sectors": [[[list(q), d] for q, d in b] for b in sectors]}))
+    # e2e through the public API with a host MPS
+    e2e = None
+    if args.e2e_steps > 0:
+        psi_host = pkg.MPS()
+        dev.download_into(psi_host)
+        psi_host._dev = None
+        e2e_times = []
+        for _ in range(args.e2e_steps):
+            psi_host._dev = None
+            t1 = time.perf_counter()
+            pkg.dmrg(psi_host, mpo, m=mfin, sweeps=1, cutoff=CUTOFF, krylov=args.krylov,
+                     precision=args.precision, ctx=ctx)
+            e2e_times.append(time.perf_counter() - t1)
+            psi_host._dev = None
+        nbytes = host_block_bytes(psi_host)
+        e2e = {"value": 1.0 / statistics.mean(e2e_times), "unit": "sweeps/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "seconds_per_step": statistics.mean(e2e_times)}
+    if rank != 0:
+        return
+    peak = fp64_gemm_peak(local)
+    g_ach = prof["gemm_flops"] / prof["gemm_seconds"] / 1e12 if prof["gemm_seconds"] > 0 else None
+    traffic = None
+    tfile = ROOT / "profiles" / "gemm_f64_traffic.json"
+    if tfile.exists() and prof["gemm_launches"]:
+        tj = json.loads(tfile.read_text())
+        # bytes per algorithmic FLOP from the committed ncu capture, scaled to a mean launch
+        traffic = tj["dram_bytes_per_flop"] * prof["gemm_flops"] / prof["gemm_launches"]
+    cpu = None
+    if not args.no_cpu:
+        t_step, est, desc = oracle_sample(sectors, args.krylov, nsteps=2)
+        cpu = {"value": 1.0 / est, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
+               "sample": desc, "seconds_per_sampled_step": t_step}
+    out = {
+        "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sweep_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "heisenberg L=100 U(1) Sz=0, maxm 1024 sweep (two-site), after "
+                               "the 64->1024 ramp", "krylov": args.krylov, "cutoff": CUTOFF,
+                   "precision": args.precision, "l2": "state larger than L2 (no flush)",
+                   "parallelism": f"replicas x{world}"},
+        "energy": energy,
+        "sweep_seconds": sweep_s,
+        "heff_tflops": heff_flops / heff_sec / 1e12 if heff_sec > 0 else None,
+        "phase_seconds": {k: statistics.mean(s[k] for s in stats) for k in
+                          ("heff_seconds", "env_seconds", "eig_seconds", "vec_seconds")},
+        "eig_max_n": max(s["eig_max_n"] for s in stats),
+        "n_matvec_per_sweep": stats[-1]["n_matvec"],
+        "setup_seconds_ramp": t_setup,
+        "wall_seconds_timed": wall,
+        "gpu_launches": launches,
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64 (grouped FP64 DMMA GEMM)",
+                     "achieved": g_ach, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (g_ach / peak) if (g_ach and peak) else None, "traffic": traffic,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
+                                    "MEASURED_PEAKS.json)",
+                     "launches": prof["gemm_launches"],
+                     "mean_launch_us": prof["gemm_seconds"] / max(prof["gemm_launches"], 1) * 1e6},
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "3xtf32", "bf16x9"])
+    ap.add_argument("--krylov", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dump-sectors", default=None)
+    ap.add_argument("--steps-ref", type=int, default=2)
+    ap.add_argument("--warmup-ref", type=int, default=1)
+    args = ap.parse_args()
+    world, rank, local, dist = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

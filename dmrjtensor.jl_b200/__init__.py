@@ -11,7 +11,15 @@ from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heise
 from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
                     default_context, dmrg, make_params, makeEnv, neelMPS, product_MPS, randMPS)
 
+
+
+def kernel_launches():
+    """Kernel launches issued by libdmrgb200.so in this process."""
+    return int(lib().dmrg_kernel_launches())
+
+
 __all__ = [
+    "kernel_launches",
     "DmrgError", "PREC", "lib", "HUBBARD_QN", "SPIN_QN", "XXZ", "cylinder_bonds", "fermionOps",
     "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
     "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",

@@ -23,7 +23,7 @@ class Params(C.Structure):
     _fields_ = [("maxm", C.c_int), ("minm", C.c_int), ("cutoff", C.c_double),
                 ("krylov", C.c_int), ("precision", C.c_int), ("svnbond", C.c_int),
                 ("degen_rtol", C.c_double), ("betatest", C.c_double), ("fp64_final", C.c_int),
-                ("reserved", C.c_int * 7)]
+                ("profile", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class SweepStats(C.Structure):
@@ -32,7 +32,8 @@ class SweepStats(C.Structure):
                 ("heff_flops", C.c_double), ("heff_seconds", C.c_double),
                 ("env_flops", C.c_double), ("env_seconds", C.c_double),
                 ("eig_seconds", C.c_double), ("vec_seconds", C.c_double),
-                ("d_top", C.c_double * 8)]
+                ("d_top", C.c_double * 8), ("gemm_flops", C.c_double),
+                ("gemm_seconds", C.c_double), ("gemm_launches", C.c_int), ("eig_max_n", C.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "d_top"}
@@ -56,6 +57,7 @@ _IPP = C.POINTER(_IP)
 
 SIGNATURES = {
     "dmrg_abi_version": (C.c_int, []),
+    "dmrg_kernel_launches": (C.c_longlong, []),
     "dmrg_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(_P)]),
     "dmrg_ctx_destroy": (C.c_int, [_P]),
     "dmrg_last_error": (C.c_char_p, [_P]),
@@ -82,6 +84,7 @@ SIGNATURES = {
     "dmrg_test_gemm": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int,
                                  _DP, C.c_int, _DP, C.c_int]),
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),
+    "dmrg_test_svd": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP, _IP]),
 }
 
 _lib = None

@@ -99,6 +99,8 @@ extern "C" {
 
 int dmrg_abi_version(void) { return DMRG_ABI_VERSION; }
 
+long long dmrg_kernel_launches(void) { return launch_count(); }
+
 void dmrg_params_default(dmrg_params* p) {
   if (!p) return;
   std::memset(p, 0, sizeof(*p));
@@ -142,6 +144,9 @@ int dmrg_ctx_create(int device, size_t hbm_budget_bytes, dmrg_ctx** out) {
       cuda_check(cudaMalloc(&c->d_partial, 16 * 296 * sizeof(double)), "partials");
       cuda_check(cudaMalloc(&c->d_status, 16 * sizeof(int)), "status");
       cuda_check(cudaMallocHost(&c->h_scal, 256 * sizeof(double)), "pinned scalars");
+      cuda_check(cudaMalloc(&c->d_flags, c->max_groups * sizeof(int)), "flags");
+      cuda_check(cudaMallocHost(&c->h_flags, c->max_groups * sizeof(int)), "pinned flags");
+      cuda_check(cudaMalloc(&c->d_floors, c->max_groups * sizeof(double)), "floors");
     } catch (...) {
       delete c;
       throw;
@@ -165,6 +170,9 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaFree(c->d_partial);
   cudaFree(c->d_status);
   cudaFreeHost(c->h_scal);
+  cudaFree(c->d_flags);
+  cudaFreeHost(c->h_flags);
+  cudaFree(c->d_floors);
   cudaStreamDestroy(c->stream);
   delete c;
   return DMRG_OK;
@@ -610,6 +618,52 @@ int dmrg_sweep(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_s
   });
 }
 
+int dmrg_test_svd(dmrg_ctx* c, int nmat, const int* r, const int* cc, double* X, double* V,
+                  double* w, int* sweeps) {
+  if (!c) return DMRG_ERR_ARG;
+  return guarded(c, [&] {
+    if (nmat <= 0 || !r || !cc || !X || !V || !w) fail(DMRG_ERR_ARG, "bad svd arguments");
+    set_device(c);
+    int64_t tx = 0, tv = 0, tw = 0;
+    for (int i = 0; i < nmat; ++i) {
+      tx += int64_t(r[i]) * cc[i];
+      tv += int64_t(cc[i]) * cc[i];
+      tw += cc[i];
+    }
+    std::vector<SvdTask> tasks;
+    size_t smem = 0;
+    int64_t ox = 0, ov = tx, ow = tx + tv;
+    for (int i = 0; i < nmat; ++i) {
+      SvdTask t{ox, ov, ow, r[i], cc[i]};
+      tasks.push_back(t);
+      smem = std::max(smem, hestenes_smem(r[i], cc[i]));
+      ox += int64_t(r[i]) * cc[i];
+      ov += int64_t(cc[i]) * cc[i];
+      ow += cc[i];
+    }
+    if (smem > HESTENES_SMEM_MAX) fail(DMRG_ERR_SHAPE, "matrix too large for the shared-memory kernel");
+    DBuf buf;
+    dalloc(c, buf, tx + tv + tw);
+    cuda_check(cudaMemcpyAsync(buf.p, X, tx * 8, cudaMemcpyHostToDevice, c->stream), "X");
+    Upload u;
+    const size_t off = u.put(tasks);
+    char* db = u.send(c, 0);
+    cuda_check(cudaMemsetAsync(c->d_status, 0, 2 * sizeof(int), c->stream), "status");
+    launch_hestenes(c->stream, buf.p, reinterpret_cast<const SvdTask*>(db + off), nmat, smem,
+                    c->d_status);
+    int st[2] = {0, 0};
+    cuda_check(cudaMemcpyAsync(X, buf.p, tx * 8, cudaMemcpyDeviceToHost, c->stream), "X D2H");
+    cuda_check(cudaMemcpyAsync(V, buf.p + tx, tv * 8, cudaMemcpyDeviceToHost, c->stream), "V D2H");
+    cuda_check(cudaMemcpyAsync(w, buf.p + tx + tv, tw * 8, cudaMemcpyDeviceToHost, c->stream), "w");
+    cuda_check(cudaMemcpyAsync(st, c->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+               "st");
+    cuda_check(cudaStreamSynchronize(c->stream), "svd sync");
+    dfree(c, buf);
+    if (sweeps) *sweeps = st[1];
+    if (st[0]) fail(DMRG_ERR_CUDA, "one-sided Jacobi did not converge");
+  });
+}
+
 }  // extern "C"
 
 extern "C" {
@@ -653,41 +707,29 @@ int dmrg_test_eigh(dmrg_ctx* c, int nmat, const int* n, double* A, double* w) {
     if (nmat <= 0 || !n || !A || !w) fail(DMRG_ERR_ARG, "bad eigh arguments");
     set_device(c);
     int64_t tot = 0, totw = 0;
-    std::vector<EigTask> small, large;
-    int ns = 0, nl = 0;
     for (int i = 0; i < nmat; ++i) { tot += int64_t(n[i]) * n[i]; totw += n[i]; }
+    std::vector<EigTask> tasks;
     int64_t off = 0, woff = 0;
     for (int i = 0; i < nmat; ++i) {
       EigTask t{};
       t.a_off = off;
-      t.v_off = tot + off;
-      t.w_off = 2 * tot + woff;
+      t.v_off = off;
+      t.w_off = tot + woff;
       t.n = n[i];
       off += int64_t(n[i]) * n[i];
       woff += n[i];
-      if (n[i] <= 100) { small.push_back(t); ns = std::max(ns, n[i]); }
-      else { large.push_back(t); nl = std::max(nl, n[i]); }
+      tasks.push_back(t);
     }
+    const int64_t ws = eig_workspace(tasks);
     DBuf buf;
-    dalloc(c, buf, 2 * tot + totw);
-    check_eig(small, buf.n);
-    check_eig(large, buf.n);
+    dalloc(c, buf, tot + totw + ws);
     cuda_check(cudaMemcpyAsync(buf.p, A, tot * 8, cudaMemcpyHostToDevice, c->stream), "A");
-    Upload u;
-    const size_t so = u.put(small), lo = u.put(large);
-    char* db = u.send(c, 0);
-    cuda_check(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream), "status");
-    launch_jacobi(c->stream, buf.p, reinterpret_cast<const EigTask*>(db + so), int(small.size()),
-                  ns, c->d_status);
-    launch_jacobi(c->stream, buf.p, reinterpret_cast<const EigTask*>(db + lo), int(large.size()),
-                  nl, c->d_status);
-    int stat = 0;
+    int sweeps = 0;
+    run_eigs(c, buf.p, buf.n, tasks, tot + totw, &sweeps);
     cuda_check(cudaMemcpyAsync(A, buf.p, tot * 8, cudaMemcpyDeviceToHost, c->stream), "V D2H");
-    cuda_check(cudaMemcpyAsync(w, buf.p + 2 * tot, totw * 8, cudaMemcpyDeviceToHost, c->stream), "w");
-    cuda_check(cudaMemcpyAsync(&stat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "st");
+    cuda_check(cudaMemcpyAsync(w, buf.p + tot, totw * 8, cudaMemcpyDeviceToHost, c->stream), "w");
     cuda_check(cudaStreamSynchronize(c->stream), "eigh sync");
     dfree(c, buf);
-    if (stat) fail(DMRG_ERR_CUDA, "Jacobi eigensolver did not converge");
   });
 }
 

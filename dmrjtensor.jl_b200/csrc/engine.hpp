@@ -145,12 +145,16 @@ struct dmrg_ctx {
   size_t budget = 0, in_use = 0, peak = 0;
   std::string err;
   int nsm = 148;
-  dmrg::DescSlot slot[4];
+  dmrg::DescSlot slot[8];
   double* d_scal = nullptr;      // small scalar workspace (256 doubles)
   double* d_partial = nullptr;   // reduction partials (16 * 296 doubles)
   int* d_status = nullptr;
   double* h_scal = nullptr;      // pinned mirror of d_scal
   cudaEvent_t ev[8] = {};
+  int max_groups = 4096;
+  int* d_flags = nullptr;        // block-Jacobi per-group flags
+  int* h_flags = nullptr;        // pinned
+  double* d_floors = nullptr;    // block-Jacobi per-group thresholds
   // growable scratch buffers
   dmrg::DBuf X, Y, K, H, M, R, W, T1, T2;
   std::map<void*, size_t> sizes;
@@ -226,6 +230,19 @@ void run_copy(dmrg_ctx* c, const CopyList& l, char* dbase, const double* src, in
               double* dst, int64_t ndst);
 void check_eig(const std::vector<EigTask>& t, int64_t nbase);
 
+// Optional per-launch timing of GEMM launches (CUDA events on the context stream).
+struct GemmProfile {
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, double>> pending;   // (event index of the start, flops)
+  int used = 0;
+  double flops = 0, seconds = 0;
+  int launches = 0;
+  void begin(cudaStream_t s, double fl);
+  void end(cudaStream_t s);
+  void flush();
+  ~GemmProfile();
+};
+
 // ---- contractions (engine_contract.cpp)
 struct HeffPlan {
   TwoLayout tl;
@@ -239,11 +256,16 @@ void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp);
 void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot);
 // y = Heff x for vectors in the tl layout (device pointers).
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
-                int precision);
+                int precision, GemmProfile* prof = nullptr);
 
 void env_boundaries(dmrg_state* st);
 void lupdate(dmrg_state* st, int i, double* flops);
 void rupdate(dmrg_state* st, int i, double* flops);
+
+// ---- eigensolves (engine_eig.cpp)
+int64_t eig_workspace(const std::vector<EigTask>& tasks);
+void run_eigs(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<EigTask>& tasks,
+              int64_t ws_off, int* sweeps);
 
 // ---- sweep (engine_sweep.cpp)
 void do_sweep(dmrg_state* st, const dmrg_params& p, dmrg_sweep_stats& out);

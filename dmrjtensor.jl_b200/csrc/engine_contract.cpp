@@ -102,16 +102,46 @@ void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot) {
   hp.dbase = u.send(c, slot);
 }
 
+void GemmProfile::begin(cudaStream_t s, double fl) {
+  if (used == int(pool.size())) {
+    cudaEvent_t a, b;
+    cuda_check(cudaEventCreate(&a), "event");
+    cuda_check(cudaEventCreate(&b), "event");
+    pool.push_back(a);
+    pool.push_back(b);
+  }
+  cudaEventRecord(pool[used], s);
+  pending.push_back({used, fl});
+  used += 2;
+}
+void GemmProfile::end(cudaStream_t s) { cudaEventRecord(pool[pending.back().first + 1], s); }
+void GemmProfile::flush() {
+  for (auto& pr : pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, pool[pr.first], pool[pr.first + 1]);
+    seconds += ms * 1e-3;
+    flops += pr.second;
+    launches += 1;
+  }
+  pending.clear();
+  used = 0;
+}
+GemmProfile::~GemmProfile() { for (auto e : pool) cudaEventDestroy(e); }
+
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
-                int precision) {
+                int precision, GemmProfile* prof) {
   (void)precision;
   dmrg_ctx* c = st->ctx;
   ensure(c, c->X, std::max<int64_t>(hp.x_size, 1));
   ensure(c, c->Y, std::max<int64_t>(hp.y_size, 1));
   const int64_t n = hp.tl.size;
+  if (prof) prof->begin(c->stream, hp.g1.flops);
   run_gemm(c, hp.g1, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
+  if (prof) prof->end(c->stream);
   run_mix(c, hp.mix, hp.dbase, c->X.p, c->X.n, c->Y.p, c->Y.n);
+  if (prof) prof->begin(c->stream, hp.g3.flops);
   run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n, y, n);
+  if (prof) prof->end(c->stream);
 }
 
 // ------------------------------------------------------------------ environments

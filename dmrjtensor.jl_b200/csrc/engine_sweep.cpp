@@ -136,6 +136,7 @@ struct Timing {
   struct Span { cudaEvent_t a, b; int cat; };
   std::vector<Span> spans;
   double acc[4] = {0, 0, 0, 0};   // heff, env, eig, vec
+  GemmProfile gemm;
   cudaEvent_t begin(dmrg_ctx* c) {
     cudaEvent_t e = pool.next();
     cudaEventRecord(e, c->stream);
@@ -147,6 +148,7 @@ struct Timing {
     spans.push_back({a, e, cat});
   }
   void flush() {   // call after a stream sync
+    gemm.flush();
     for (const Span& s : spans) {
       float ms = 0;
       cudaEventElapsedTime(&ms, s.a, s.b);
@@ -166,6 +168,7 @@ struct StepOut {
   int m = 0, nmv = 0;
   std::vector<double> D;       // kept singular values, descending
   double heff_flops = 0;
+  int eig_max_n = 0;
 };
 
 struct Piece { int sec, s, off; };
@@ -228,7 +231,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
 
   auto heff = [&](const double* x, double* y) {
     cudaEvent_t th = tm.begin(c);
-    apply_heff(st, iL, hp, x, y, P.precision);
+    apply_heff(st, iL, hp, x, y, P.precision, P.profile ? &tm.gemm : nullptr);
     tm.end(c, th, 0);
     so.nmv += 1;
     so.heff_flops += hp.flops;
@@ -328,15 +331,51 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
     for (const Piece& p : G[g].rows) { gofrow[p.sec * d1 + p.s] = g; rowoff[p.sec * d1 + p.s] = p.off; }
     for (const Piece& p : G[g].cols) coloff[p.sec * d2 + p.s] = p.off;
   }
+  // side = dimension of the density matrix that is diagonalised; other = the summed index
   int64_t mtot = 0, rtot = 0, wtot = 0;
-  for (Group& g : G) {
-    const int side = j > 0 ? g.n : g.np;
+  std::vector<char> small(G.size(), 0);
+  for (int gi = 0; gi < int(G.size()); ++gi) {
+    Group& g = G[gi];
+    const int side = j > 0 ? g.n : g.np, other = j > 0 ? g.np : g.n;
     g.moff = mtot; mtot += int64_t(g.n) * g.np;
     g.roff = rtot; rtot += int64_t(side) * side;
     g.woff = wtot; wtot += side;
+    small[gi] = side > 0 && hestenes_smem(std::max(other, 1), side) <= HESTENES_SMEM_MAX;
   }
-  ensure(c, c->M, std::max<int64_t>(mtot, 1));
-  ensure(c, c->R, std::max<int64_t>(2 * rtot + wtot, 1));
+  std::vector<EigTask> etasks;
+  std::vector<SvdTask> stasks;
+  size_t hsm = 0;
+  for (int gi = 0; gi < int(G.size()); ++gi) {
+    const Group& g = G[gi];
+    const int side = j > 0 ? g.n : g.np, other = j > 0 ? g.np : g.n;
+    if (side == 0) continue;
+    so.eig_max_n = std::max(so.eig_max_n, side);
+    if (small[gi]) {
+      SvdTask t{};
+      t.x_off = g.moff;            // in the M buffer
+      t.v_off = g.roff;            // in the R buffer (same base: see launch below)
+      t.w_off = rtot + g.woff;
+      t.r = other;
+      t.c = side;
+      stasks.push_back(t);
+      hsm = std::max(hsm, hestenes_smem(other, side));
+    } else {
+      EigTask et{};
+      et.a_off = g.roff;
+      et.v_off = g.roff;
+      et.w_off = rtot + g.woff;
+      et.n = side;
+      etasks.push_back(et);
+    }
+  }
+  const int64_t ews = eig_workspace(etasks);
+  // M and R live in one allocation so that the one-sided tasks address X, V and w from one base
+  const int64_t Rbase = std::max<int64_t>(mtot, 1);
+  ensure(c, c->R, Rbase + std::max<int64_t>(rtot + wtot + ews, 1));
+  double* Mp = c->R.p;
+  double* Rp = c->R.p + Rbase;
+  const int64_t nM = Rbase, nR = c->R.n - Rbase;
+  for (SvdTask& t : stasks) { t.v_off += Rbase; t.w_off += Rbase; }
   CopyList gather;
   for (int ka = 0; ka < tl.nl; ++ka)
     for (int s1 = 0; s1 < d1; ++s1)
@@ -344,52 +383,50 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
         const int id = tl.idx(ka, s1, s2);
         const int kd = tl.kd[id];
         if (kd < 0) continue;
-        const Group& g = G[gofrow[ka * d1 + s1]];
-        const int co = coloff[kd * d2 + s2];
-        gather.add(tl.off[id], Bl.dim[ka], g.moff + rowoff[ka * d1 + s1] + int64_t(co) * g.n, g.n,
-                   Bl.dim[ka], Br.dim[kd], 0, 1.0);
+        const int gi = gofrow[ka * d1 + s1];
+        const Group& g = G[gi];
+        const int ro = rowoff[ka * d1 + s1], co = coloff[kd * d2 + s2];
+        if (small[gi] && j > 0)     // X = M^T: rows (s2,kd), columns (ka,s1)
+          gather.add(tl.off[id], Bl.dim[ka], g.moff + co + int64_t(ro) * g.np, g.np, Br.dim[kd],
+                     Bl.dim[ka], 1, 1.0);
+        else                        // X = M: rows (ka,s1), columns (s2,kd)
+          gather.add(tl.off[id], Bl.dim[ka], g.moff + ro + int64_t(co) * g.n, g.n, Bl.dim[ka],
+                     Br.dim[kd], 0, 1.0);
       }
   GemmList grho;
   grho.tA = j < 0;
   grho.tB = j > 0;
-  std::vector<EigTask> esmall, elarge;
-  int nsmall = 0, nlarge = 0;
-  for (const Group& g : G) {
+  for (int gi = 0; gi < int(G.size()); ++gi) {
+    const Group& g = G[gi];
     const int side = j > 0 ? g.n : g.np;
-    if (side == 0) continue;
+    if (side == 0 || small[gi]) continue;
     grho.add(g.roff, side, side, side, 1.0, 0.0);
     const int K2 = j > 0 ? g.np : g.n;
     if (K2 > 0) grho.seg(g.moff, g.n, g.moff, g.n, K2);
-    EigTask et{};
-    et.a_off = g.roff;
-    et.v_off = rtot + g.roff;
-    et.w_off = 2 * rtot + g.woff;
-    et.n = side;
-    if (side <= 100) { esmall.push_back(et); nsmall = std::max(nsmall, side); }
-    else { elarge.push_back(et); nlarge = std::max(nlarge, side); }
   }
   Upload u2;
   u2.put(gather);
   u2.put(grho);
-  const size_t es_off = u2.put(esmall), el_off = u2.put(elarge);
+  const size_t st_off = u2.put(stasks);
   char* db2 = u2.send(c, 1);
-  run_copy(c, gather, db2, psi, n, c->M.p, c->M.n);
-  run_gemm(c, grho, db2, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
-  check_eig(esmall, c->R.n);
-  check_eig(elarge, c->R.n);
+  run_copy(c, gather, db2, psi, n, Mp, nM);
+  run_gemm(c, grho, db2, Mp, nM, Mp, nM, Rp, nR);
+  for (const SvdTask& t : stasks) {
+    const int64_t ex = int64_t(t.r) * t.c - 1, ev = int64_t(t.c) * t.c - 1;
+    if (t.x_off < 0 || t.x_off + ex >= nM || t.v_off + ev >= c->R.n || t.w_off + t.c - 1 >= c->R.n)
+      fail(DMRG_ERR_ARG, "internal plan check failed: one-sided Jacobi task out of bounds");
+  }
   cuda_check(cudaMemsetAsync(c->d_status, 0, sizeof(int), s), "status");
-  launch_jacobi(s, c->R.p, reinterpret_cast<const EigTask*>(db2 + es_off), int(esmall.size()),
-                nsmall, c->d_status);
-  launch_jacobi(s, c->R.p, reinterpret_cast<const EigTask*>(db2 + el_off), int(elarge.size()),
-                nlarge, c->d_status);
+  launch_hestenes(s, c->R.p, reinterpret_cast<const SvdTask*>(db2 + st_off), int(stasks.size()),
+                  hsm, c->d_status);
+  run_eigs(c, Rp, nR, etasks, rtot + wtot, nullptr);
   std::vector<double> lam(std::max<int64_t>(wtot, 1));
-  int jstat = 0;
-  cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + 2 * rtot, sizeof(double) * wtot,
+  int hstat = 0;
+  cuda_check(cudaMemcpyAsync(lam.data(), Rp + rtot, sizeof(double) * wtot,
                              cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
-  cuda_check(cudaMemcpyAsync(&jstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "status");
+  cuda_check(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "status");
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
-  cuda_check(cudaGetLastError(), "eigensolve");
-  if (jstat != 0) fail(DMRG_ERR_CUDA, "Jacobi eigensolver did not converge");
+  if (hstat) fail(DMRG_ERR_CUDA, "one-sided Jacobi did not converge");
 
   std::vector<std::vector<double>> vals(G.size());
   for (int g = 0; g < int(G.size()); ++g) {
@@ -419,7 +456,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   DBuf nA, nB;
   dalloc(c, nA, std::max<int64_t>(nl.size, 1));
   dalloc(c, nB, std::max<int64_t>(nrl.size, 1));
-  CopyList cp;
+  CopyList cpR, cpM;   // sources: eigenvectors (R region) / rotated X (M region)
   GemmList gs;
   if (j > 0) {
     gs.tA = true;
@@ -427,41 +464,56 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
       for (int s1 = 0; s1 < d1; ++s1) {
         const Group& g = G[gofrow[ka * d1 + s1]];
         if (g.keep == 0) continue;
-        cp.add(g.roff + rowoff[ka * d1 + s1], g.n, nl.off[ka * d1 + s1], Bl.dim[ka], Bl.dim[ka],
-               g.keep, 0, 1.0);
+        cpR.add(g.roff + rowoff[ka * d1 + s1], g.n, nl.off[ka * d1 + s1], Bl.dim[ka], Bl.dim[ka],
+                g.keep, 0, 1.0);
       }
-    for (const Group& g : G) {
+    for (int gi = 0; gi < int(G.size()); ++gi) {
+      const Group& g = G[gi];
       if (g.keep == 0) continue;
       for (const Piece& p : g.cols) {   // p.sec = kd, p.s = s2
         if (nrl.kb[g.kc * d2 + p.s] != p.sec) continue;
-        gs.add(nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1.0, 0.0);
-        gs.seg(g.roff, g.n, g.moff + int64_t(p.off) * g.n, g.n, g.n);
+        if (small[gi]) {                // (X V)^T rows = D.V
+          cpM.add(g.moff + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
+                  1.0);
+        } else {
+          gs.add(nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1.0, 0.0);
+          gs.seg(g.roff, g.n, g.moff + int64_t(p.off) * g.n, g.n, g.n);
+        }
       }
     }
   } else {
-    for (const Group& g : G) {
+    for (int gi = 0; gi < int(G.size()); ++gi) {
+      const Group& g = G[gi];
       if (g.keep == 0) continue;
       for (const Piece& p : g.cols) {
         if (nrl.kb[g.kc * d2 + p.s] != p.sec) continue;
-        cp.add(g.roff + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
-               1.0);
+        cpR.add(g.roff + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
+                1.0);
       }
       for (const Piece& p : g.rows) {   // p.sec = ka, p.s = s1
-        gs.add(nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec], g.keep, 1.0, 0.0);
-        if (g.np > 0) gs.seg(g.moff + p.off, g.n, g.roff, g.np, g.np);
+        if (small[gi]) {                // X V columns = U.D
+          cpM.add(g.moff + p.off, g.n, nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec],
+                  g.keep, 0, 1.0);
+        } else {
+          gs.add(nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec], g.keep, 1.0, 0.0);
+          if (g.np > 0) gs.seg(g.moff + p.off, g.n, g.roff, g.np, g.np);
+        }
       }
     }
   }
   Upload u3;
-  u3.put(cp);
+  u3.put(cpR);
+  u3.put(cpM);
   u3.put(gs);
   char* db3 = u3.send(c, 3);
   if (j > 0) {
-    run_copy(c, cp, db3, c->R.p, c->R.n, nA.p, nA.n);
-    run_gemm(c, gs, db3, c->R.p, c->R.n, c->M.p, c->M.n, nB.p, nB.n);
+    run_copy(c, cpR, db3, Rp, nR, nA.p, nA.n);
+    run_copy(c, cpM, db3, Mp, nM, nB.p, nB.n);
+    run_gemm(c, gs, db3, Rp, nR, Mp, nM, nB.p, nB.n);
   } else {
-    run_copy(c, cp, db3, c->R.p, c->R.n, nB.p, nB.n);
-    run_gemm(c, gs, db3, c->M.p, c->M.n, c->R.p, c->R.n, nA.p, nA.n);
+    run_copy(c, cpR, db3, Rp, nR, nB.p, nB.n);
+    run_copy(c, cpM, db3, Mp, nM, nA.p, nA.n);
+    run_gemm(c, gs, db3, Mp, nM, Rp, nR, nA.p, nA.n);
   }
   dfree(c, st->A[iL]);
   dfree(c, st->A[iR]);
@@ -503,6 +555,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     out.n_matvec += so.nmv;
     out.heff_flops += so.heff_flops;
     out.env_flops += ef;
+    out.eig_max_n = std::max(out.eig_max_n, so.eig_max_n);
     if (i == svn_site && j < 0) {
       double S = 0.0;
       for (double x : so.D) {
@@ -528,6 +581,9 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   out.env_seconds = tm.acc[1];
   out.eig_seconds = tm.acc[2];
   out.vec_seconds = tm.acc[3];
+  out.gemm_flops = tm.gemm.flops;
+  out.gemm_seconds = tm.gemm.seconds;
+  out.gemm_launches = tm.gemm.launches;
 }
 
 }  // namespace dmrg

@@ -6,6 +6,8 @@
 // 3-stage cp.async pipeline. Operands may be transposed (NN, NT, TN) so that no permute copies
 // are needed anywhere in the sweep. B200 has no tcgen05 FP64 kind; mma.sync f64 is the FP64
 // tensor-core instruction on sm_100a.
+#include <atomic>
+
 #include "kernels.cuh"
 
 namespace dmrg {
@@ -173,6 +175,7 @@ void launch_variant(cudaStream_t s, const double* A, const double* B, double* C,
   }
   int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
   k_gemm_f64<TA, TB><<<grid, THREADS, SMEM_BYTES, s>>>(A, B, C, tasks, ntasks, segs, total_tiles);
+  count_launch();
 }
 
 }  // namespace
@@ -190,6 +193,10 @@ void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, 
   else
     launch_variant<true, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
 }
+
+static std::atomic<long long> g_launches{0};
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 int device_sm_count() {
   int dev = 0, n = 0;

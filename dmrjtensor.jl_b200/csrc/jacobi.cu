@@ -88,31 +88,40 @@ k_jacobi(double* __restrict__ base, const EigTask* __restrict__ tasks, int in_sm
         sn[k] = s;
       }
       __syncthreads();
-      // rows p, q  <-  J^T A
-      for (int64_t it = tid; it < int64_t(npairs) * n; it += blockDim.x) {
-        const int k = int(it / n), j = int(it % n);
+      // rows p, q  <-  J^T A : warp w owns pairs w, w+nwarps, ..; lanes walk the columns
+      const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+      for (int k = warp; k < npairs; k += nwarps) {
         const int q = qq[k];
-        if (q < 0 || sn[k] == 0.0) continue;
+        const double s = sn[k];
+        if (q < 0 || s == 0.0) continue;
         const int p = pp[k];
-        const double c = cs[k], s = sn[k];
-        const double ap = A[p + int64_t(j) * n], aq = A[q + int64_t(j) * n];
-        A[p + int64_t(j) * n] = c * ap - s * aq;
-        A[q + int64_t(j) * n] = s * ap + c * aq;
+        const double c = cs[k];
+        for (int j = lane; j < n; j += 32) {
+          const double ap = A[p + j * n], aq = A[q + j * n];
+          A[p + j * n] = c * ap - s * aq;
+          A[q + j * n] = s * ap + c * aq;
+        }
       }
       __syncthreads();
-      // columns p, q  <-  A J, V J
-      for (int64_t it = tid; it < int64_t(npairs) * n; it += blockDim.x) {
-        const int k = int(it / n), i = int(it % n);
+      // columns p, q  <-  A J, V J : lanes walk the (contiguous) rows
+      for (int k = warp; k < npairs; k += nwarps) {
         const int q = qq[k];
-        if (q < 0 || sn[k] == 0.0) continue;
+        const double s = sn[k];
+        if (q < 0 || s == 0.0) continue;
         const int p = pp[k];
-        const double c = cs[k], s = sn[k];
-        const double ap = A[i + int64_t(p) * n], aq = A[i + int64_t(q) * n];
-        A[i + int64_t(p) * n] = c * ap - s * aq;
-        A[i + int64_t(q) * n] = s * ap + c * aq;
-        const double vp = V[i + int64_t(p) * n], vq = V[i + int64_t(q) * n];
-        V[i + int64_t(p) * n] = c * vp - s * vq;
-        V[i + int64_t(q) * n] = s * vp + c * vq;
+        const double c = cs[k];
+        double* Ap_ = A + p * n;
+        double* Aq_ = A + q * n;
+        double* Vp_ = V + p * n;
+        double* Vq_ = V + q * n;
+        for (int i = lane; i < n; i += 32) {
+          const double ap = Ap_[i], aq = Aq_[i];
+          Ap_[i] = c * ap - s * aq;
+          Aq_[i] = s * ap + c * aq;
+          const double vp = Vp_[i], vq = Vq_[i];
+          Vp_[i] = c * vp - s * vq;
+          Vq_[i] = s * vp + c * vq;
+        }
       }
       __syncthreads();
     }
@@ -167,6 +176,7 @@ void launch_jacobi(cudaStream_t s, double* base, const EigTask* tasks, int ntask
   const size_t smem = jacobi_smem(max_n, small);
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   k_jacobi<<<ntasks, JAC_THREADS, smem, s>>>(base, tasks, small ? 1 : 0, status);
+  count_launch();
 }
 
 }  // namespace dmrg

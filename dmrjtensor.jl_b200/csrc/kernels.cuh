@@ -58,6 +58,17 @@ struct EigTask {
   int n, pad;
 };
 
+// One-sided Jacobi of X (r x c, column-major at x_off, overwritten by X V sorted): V (c x c) at
+// v_off, eigenvalues |x_i|^2 of X^T X (descending) at w_off.
+struct SvdTask {
+  int64_t x_off, v_off, w_off;
+  int r, c;
+};
+size_t hestenes_smem(int r, int c);
+void launch_hestenes(cudaStream_t s, double* base, const SvdTask* tasks, int ntasks, size_t smem,
+                     int* status);
+constexpr size_t HESTENES_SMEM_MAX = 200 * 1024;
+
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
 
 // Persistent grouped FP64 GEMM (DMMA m8n8k4 tensor-core path).
@@ -84,10 +95,33 @@ void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const doub
 void launch_scale(cudaStream_t s, double* x, int64_t n, double a);
 void launch_zero(cudaStream_t s, double* x, int64_t n);
 
+// Block Jacobi for large blocks (n > 100): padded to N = 16*nb (nb even).
+struct BlockEigGroup {
+  int64_t a_off, w_off;          // caller's matrix (n x n) / eigenvalues (n), as in EigTask
+  int64_t ap_off, vp_off, q_off; // workspace: padded A (N x N), V (N x N), pair rotations
+  int n, N;
+};
+struct BlockEigPlan {
+  const BlockEigGroup* groups;   // device arrays
+  int ngroups;
+  const int2* pairs;             // (group, pair index) for every block pair of a round
+  int npairs;
+  const int4* tiles;             // (group, kind 0 = A tile / 1 = V tile, a, b)
+  int ntiles;
+  int maxN, maxn, max_sweeps;
+};
+int block_eig_padded(int n);
+// Runs the sweeps (host loop with one flag read per sweep). flags/floors: >= ngroups entries.
+void launch_block_jacobi(cudaStream_t s, double* base, const BlockEigPlan& plan, int* flags_dev,
+                         int* flags_host, double* floors_dev, int* sweeps_done);
+
 // Batched cyclic Jacobi: one CTA per task. Overwrites the matrices.
 void launch_jacobi(cudaStream_t s, double* base, const EigTask* tasks, int ntasks, int max_n,
                    int* status);
 
 int device_sm_count();
+// Process-wide count of kernel launches issued by this library.
+void count_launch(int n = 1);
+long long launch_count();
 
 }  // namespace dmrg

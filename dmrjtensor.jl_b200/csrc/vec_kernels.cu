@@ -155,6 +155,7 @@ void launch_mix(cudaStream_t s, const double* in, double* out, const MixTask* ta
   if (total_tiles <= 0) return;
   int grid = total_tiles < 4096 ? total_tiles : 4096;
   k_mix<<<grid, 256, 0, s>>>(in, out, tasks, ntasks, terms, total_tiles);
+  count_launch();
 }
 
 void launch_copy(cudaStream_t s, const double* src, double* dst, const CopyTask* tasks,
@@ -162,12 +163,14 @@ void launch_copy(cudaStream_t s, const double* src, double* dst, const CopyTask*
   if (total_tiles <= 0) return;
   int grid = total_tiles < 4096 ? total_tiles : 4096;
   k_copy<<<grid, 256, 0, s>>>(src, dst, tasks, ntasks, total_tiles);
+  count_launch();
 }
 
 void launch_mdot(cudaStream_t s, const double* X, int64_t ldx, int k, const double* y, int64_t n,
                  double* partial, double* out) {
   k_mdot_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(X, ldx, k, y, n, partial);
   k_reduce_rows<<<k, 256, 0, s>>>(partial, RED_BLOCKS, out);
+  count_launch(2);
 }
 
 void launch_axpby(cudaStream_t s, int64_t n, double a, const double* ap, double asign,
@@ -175,17 +178,20 @@ void launch_axpby(cudaStream_t s, int64_t n, double a, const double* ap, double 
                   int b_recip) {
   if (n <= 0) return;
   k_axpby<<<grid_for(n), RED_THREADS, 0, s>>>(n, a, ap, asign, x, b, bp, bsign, y, b_recip);
+  count_launch();
 }
 
 void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c, double* y,
                  int64_t n) {
   if (n <= 0 || k <= 0) return;
   k_msub<<<grid_for(n), RED_THREADS, 0, s>>>(X, ldx, k, c, y, n);
+  count_launch();
 }
 
 void launch_scale(cudaStream_t s, double* x, int64_t n, double a) {
   if (n <= 0) return;
   k_scale<<<grid_for(n), RED_THREADS, 0, s>>>(x, n, a);
+  count_launch();
 }
 
 void launch_zero(cudaStream_t s, double* x, int64_t n) {

@@ -385,7 +385,7 @@ class DeviceState:
 
 
 def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
-                degen_rtol=0.0, betatest=1e-10, fp64_final=1):
+                degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0):
     p = Params()
     lib().dmrg_params_default(C.byref(p))
     p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)
@@ -393,6 +393,7 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
     p.precision = _lib.PREC[precision] if isinstance(precision, str) else int(precision)
     p.svnbond, p.degen_rtol, p.betatest, p.fp64_final = int(svnbond), float(degen_rtol), \
         float(betatest), int(fp64_final)
+    p.profile = int(profile)
     return p
 
 

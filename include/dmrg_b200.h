@@ -80,7 +80,8 @@ typedef struct dmrg_params {
   double degen_rtol; /* >0: never split a cluster of equal weights at the cut  */
   double betatest;   /* Krylov breakdown threshold, 1e-10 (algs/DMRG.jl:57)     */
   int fp64_final;    /* chosen forms: 1 = re-evaluate the Ritz energy with one FP64 matvec */
-  int reserved[7];
+  int profile;       /* 1 = time every Heff GEMM launch with CUDA events (gemm_* stats)  */
+  int reserved[6];
 } dmrg_params;
 
 /* Per-sweep record (what dmrgcvg prints, algs/DMRG.jl:610-652, plus timings). */
@@ -98,6 +99,10 @@ typedef struct dmrg_sweep_stats {
   double eig_seconds;   /* density-matrix formation + eigensolve + split      */
   double vec_seconds;   /* Lanczos vector operations                          */
   double d_top[8];      /* largest singular values at bond svnbond            */
+  double gemm_flops;    /* profile = 1: algorithmic FLOPs of the Heff GEMM launches */
+  double gemm_seconds;  /* profile = 1: their summed device time                     */
+  int gemm_launches;    /* profile = 1: their number                                  */
+  int eig_max_n;        /* largest density-matrix block of the sweep                  */
 } dmrg_sweep_stats;
 
 /* ---------------------------------------------------------------- context */
@@ -106,6 +111,8 @@ DMRG_API int dmrg_abi_version(void);
 DMRG_API int dmrg_ctx_create(int device, size_t hbm_budget_bytes, dmrg_ctx** out);
 DMRG_API int dmrg_ctx_destroy(dmrg_ctx* ctx);
 DMRG_API const char* dmrg_last_error(const dmrg_ctx* ctx);
+/* Number of kernel launches this library has issued in this process (all contexts). */
+DMRG_API long long dmrg_kernel_launches(void);
 /* Bytes currently allocated on the device by this context, and its peak. */
 DMRG_API int dmrg_ctx_memory(const dmrg_ctx* ctx, size_t* in_use, size_t* peak);
 
@@ -179,6 +186,12 @@ DMRG_API int dmrg_test_gemm(dmrg_ctx* ctx, int transA, int transB, int M, int N,
  * sizes n[i] packed back to back in A; eigenvalues (descending) packed into w and eigenvectors
  * (columns) overwrite A. */
 DMRG_API int dmrg_test_eigh(dmrg_ctx* ctx, int nmat, const int* n, double* A, double* w);
+
+/* One-sided Jacobi of nmat column-major matrices X_i (r[i] x c[i], packed in X): on return X
+ * holds X_i V_i with columns sorted by descending norm, V the c[i] x c[i] rotations (packed),
+ * w the squared column norms (descending) and sweeps[0] the largest sweep count. */
+DMRG_API int dmrg_test_svd(dmrg_ctx* ctx, int nmat, const int* r, const int* c, double* X,
+                           double* V, double* w, int* sweeps);
 
 /* Fills *p with the reference defaults (minm 2, krylov 2, betatest 1e-10, ...). */
 DMRG_API void dmrg_params_default(dmrg_params* p);
