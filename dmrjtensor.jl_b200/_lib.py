@@ -85,6 +85,7 @@ SIGNATURES = {
                                  _DP, C.c_int, _DP, C.c_int]),
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),
     "dmrg_test_svd": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP, _IP]),
+    "dmrg_test_syevt": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP]),
 }
 
 _lib = None

@@ -331,51 +331,56 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
     for (const Piece& p : G[g].rows) { gofrow[p.sec * d1 + p.s] = g; rowoff[p.sec * d1 + p.s] = p.off; }
     for (const Piece& p : G[g].cols) coloff[p.sec * d2 + p.s] = p.off;
   }
-  // side = dimension of the density matrix that is diagonalised; other = the summed index
+  // side = dimension of the density matrix that is diagonalised (rows of M for j>0, columns
+  // for j<0). R buffer: [rho | eigenvalues | d,e,tau | eigenvectors | block-Jacobi workspace].
   int64_t mtot = 0, rtot = 0, wtot = 0;
-  std::vector<char> small(G.size(), 0);
-  for (int gi = 0; gi < int(G.size()); ++gi) {
-    Group& g = G[gi];
-    const int side = j > 0 ? g.n : g.np, other = j > 0 ? g.np : g.n;
+  for (Group& g : G) {
+    const int side = j > 0 ? g.n : g.np;
     g.moff = mtot; mtot += int64_t(g.n) * g.np;
     g.roff = rtot; rtot += int64_t(side) * side;
     g.woff = wtot; wtot += side;
-    small[gi] = side > 0 && hestenes_smem(std::max(other, 1), side) <= HESTENES_SMEM_MAX;
   }
+  const int64_t W0 = rtot, WS0 = rtot + wtot, U0 = rtot + 4 * wtot, J0 = 2 * rtot + 4 * wtot;
   std::vector<EigTask> etasks;
-  std::vector<SvdTask> stasks;
-  size_t hsm = 0;
+  std::vector<TridTask> ttasks;
+  std::vector<int> tgroup;
+  std::vector<int64_t> uoff(G.size(), 0);
+  int tmax = 0;
   for (int gi = 0; gi < int(G.size()); ++gi) {
     const Group& g = G[gi];
-    const int side = j > 0 ? g.n : g.np, other = j > 0 ? g.np : g.n;
+    const int side = j > 0 ? g.n : g.np;
     if (side == 0) continue;
     so.eig_max_n = std::max(so.eig_max_n, side);
-    if (small[gi]) {
-      SvdTask t{};
-      t.x_off = g.moff;            // in the M buffer
-      t.v_off = g.roff;            // in the R buffer (same base: see launch below)
-      t.w_off = rtot + g.woff;
-      t.r = other;
-      t.c = side;
-      stasks.push_back(t);
-      hsm = std::max(hsm, hestenes_smem(other, side));
+    if (side <= SYEVT_NMAX) {
+      TridTask t{};
+      t.a_off = g.roff;
+      t.w_off = W0 + g.woff;
+      t.ws_off = WS0 + 3 * g.woff;
+      t.u_off = U0 + g.roff;
+      t.n = side;
+      ttasks.push_back(t);
+      tgroup.push_back(gi);
+      uoff[gi] = t.u_off;
+      tmax = std::max(tmax, side);
     } else {
       EigTask et{};
       et.a_off = g.roff;
       et.v_off = g.roff;
-      et.w_off = rtot + g.woff;
+      et.w_off = W0 + g.woff;
       et.n = side;
       etasks.push_back(et);
+      uoff[gi] = g.roff;      // block Jacobi returns the eigenvectors in place
     }
   }
   const int64_t ews = eig_workspace(etasks);
-  // M and R live in one allocation so that the one-sided tasks address X, V and w from one base
-  const int64_t Rbase = std::max<int64_t>(mtot, 1);
-  ensure(c, c->R, Rbase + std::max<int64_t>(rtot + wtot + ews, 1));
-  double* Mp = c->R.p;
-  double* Rp = c->R.p + Rbase;
-  const int64_t nM = Rbase, nR = c->R.n - Rbase;
-  for (SvdTask& t : stasks) { t.v_off += Rbase; t.w_off += Rbase; }
+  ensure(c, c->M, std::max<int64_t>(mtot, 1));
+  ensure(c, c->R, std::max<int64_t>(J0 + ews, 1));
+  for (const TridTask& t : ttasks) {
+    const int64_t nn = int64_t(t.n) * t.n;
+    if (t.a_off + nn > c->R.n || t.w_off + t.n > c->R.n || t.ws_off + 3 * t.n > c->R.n ||
+        t.u_off + nn > c->R.n)
+      fail(DMRG_ERR_ARG, "internal plan check failed: tridiagonal eigensolver task");
+  }
   CopyList gather;
   for (int ka = 0; ka < tl.nl; ++ka)
     for (int s1 = 0; s1 < d1; ++s1)
@@ -383,23 +388,17 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
         const int id = tl.idx(ka, s1, s2);
         const int kd = tl.kd[id];
         if (kd < 0) continue;
-        const int gi = gofrow[ka * d1 + s1];
-        const Group& g = G[gi];
-        const int ro = rowoff[ka * d1 + s1], co = coloff[kd * d2 + s2];
-        if (small[gi] && j > 0)     // X = M^T: rows (s2,kd), columns (ka,s1)
-          gather.add(tl.off[id], Bl.dim[ka], g.moff + co + int64_t(ro) * g.np, g.np, Br.dim[kd],
-                     Bl.dim[ka], 1, 1.0);
-        else                        // X = M: rows (ka,s1), columns (s2,kd)
-          gather.add(tl.off[id], Bl.dim[ka], g.moff + ro + int64_t(co) * g.n, g.n, Bl.dim[ka],
-                     Br.dim[kd], 0, 1.0);
+        const Group& g = G[gofrow[ka * d1 + s1]];
+        const int co = coloff[kd * d2 + s2];
+        gather.add(tl.off[id], Bl.dim[ka], g.moff + rowoff[ka * d1 + s1] + int64_t(co) * g.n, g.n,
+                   Bl.dim[ka], Br.dim[kd], 0, 1.0);
       }
   GemmList grho;
   grho.tA = j < 0;
   grho.tB = j > 0;
-  for (int gi = 0; gi < int(G.size()); ++gi) {
-    const Group& g = G[gi];
+  for (const Group& g : G) {
     const int side = j > 0 ? g.n : g.np;
-    if (side == 0 || small[gi]) continue;
+    if (side == 0) continue;
     grho.add(g.roff, side, side, side, 1.0, 0.0);
     const int K2 = j > 0 ? g.np : g.n;
     if (K2 > 0) grho.seg(g.moff, g.n, g.moff, g.n, K2);
@@ -407,26 +406,17 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   Upload u2;
   u2.put(gather);
   u2.put(grho);
-  const size_t st_off = u2.put(stasks);
+  const size_t tt_off = u2.put(ttasks);
   char* db2 = u2.send(c, 1);
-  run_copy(c, gather, db2, psi, n, Mp, nM);
-  run_gemm(c, grho, db2, Mp, nM, Mp, nM, Rp, nR);
-  for (const SvdTask& t : stasks) {
-    const int64_t ex = int64_t(t.r) * t.c - 1, ev = int64_t(t.c) * t.c - 1;
-    if (t.x_off < 0 || t.x_off + ex >= nM || t.v_off + ev >= c->R.n || t.w_off + t.c - 1 >= c->R.n)
-      fail(DMRG_ERR_ARG, "internal plan check failed: one-sided Jacobi task out of bounds");
-  }
-  cuda_check(cudaMemsetAsync(c->d_status, 0, sizeof(int), s), "status");
-  launch_hestenes(s, c->R.p, reinterpret_cast<const SvdTask*>(db2 + st_off), int(stasks.size()),
-                  hsm, c->d_status);
-  run_eigs(c, Rp, nR, etasks, rtot + wtot, nullptr);
+  run_copy(c, gather, db2, psi, n, c->M.p, c->M.n);
+  run_gemm(c, grho, db2, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
+  launch_trid_eigvals(s, c->R.p, reinterpret_cast<const TridTask*>(db2 + tt_off),
+                      int(ttasks.size()), tmax);
+  run_eigs(c, c->R.p, c->R.n, etasks, J0, nullptr);
   std::vector<double> lam(std::max<int64_t>(wtot, 1));
-  int hstat = 0;
-  cuda_check(cudaMemcpyAsync(lam.data(), Rp + rtot, sizeof(double) * wtot,
+  cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + W0, sizeof(double) * wtot,
                              cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
-  cuda_check(cudaMemcpyAsync(&hstat, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "status");
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
-  if (hstat) fail(DMRG_ERR_CUDA, "one-sided Jacobi did not converge");
 
   std::vector<std::vector<double>> vals(G.size());
   for (int g = 0; g < int(G.size()); ++g) {
@@ -449,6 +439,24 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   for (size_t a = 0; a < kept.size(); ++a) so.D[a] = std::sqrt(std::max(kept[a], 0.0));
   so.truncerr = sel.truncerr;
   so.m = int(kept.size());
+  // eigenvectors of the kept states of the tridiagonal-path blocks
+  std::vector<TridTask> vt;
+  int vmax_n = 0, vmax_k = 0;
+  for (size_t a = 0; a < ttasks.size(); ++a) {
+    TridTask t = ttasks[a];
+    t.keep = G[tgroup[a]].keep;
+    if (t.keep == 0) continue;
+    vt.push_back(t);
+    vmax_n = std::max(vmax_n, t.n);
+    vmax_k = std::max(vmax_k, t.keep);
+  }
+  if (!vt.empty()) {
+    Upload uv;
+    const size_t vo = uv.put(vt);
+    char* dbv = uv.send(c, 6);
+    launch_trid_vectors(s, c->R.p, reinterpret_cast<const TridTask*>(dbv + vo), int(vt.size()),
+                        vmax_n, vmax_k);
+  }
 
   // ---------------- split back into the two site tensors (algs/DMRG.jl:389-395, 483-490)
   SiteLayout nl = make_site_layout(Bl, ml.p, C);
@@ -456,29 +464,25 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   DBuf nA, nB;
   dalloc(c, nA, std::max<int64_t>(nl.size, 1));
   dalloc(c, nB, std::max<int64_t>(nrl.size, 1));
-  CopyList cpR, cpM;   // sources: eigenvectors (R region) / rotated X (M region)
+  CopyList cp;
   GemmList gs;
   if (j > 0) {
     gs.tA = true;
     for (int ka = 0; ka < Bl.nsec(); ++ka)
       for (int s1 = 0; s1 < d1; ++s1) {
-        const Group& g = G[gofrow[ka * d1 + s1]];
+        const int gi = gofrow[ka * d1 + s1];
+        const Group& g = G[gi];
         if (g.keep == 0) continue;
-        cpR.add(g.roff + rowoff[ka * d1 + s1], g.n, nl.off[ka * d1 + s1], Bl.dim[ka], Bl.dim[ka],
-                g.keep, 0, 1.0);
+        cp.add(uoff[gi] + rowoff[ka * d1 + s1], g.n, nl.off[ka * d1 + s1], Bl.dim[ka], Bl.dim[ka],
+               g.keep, 0, 1.0);
       }
     for (int gi = 0; gi < int(G.size()); ++gi) {
       const Group& g = G[gi];
       if (g.keep == 0) continue;
       for (const Piece& p : g.cols) {   // p.sec = kd, p.s = s2
         if (nrl.kb[g.kc * d2 + p.s] != p.sec) continue;
-        if (small[gi]) {                // (X V)^T rows = D.V
-          cpM.add(g.moff + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
-                  1.0);
-        } else {
-          gs.add(nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1.0, 0.0);
-          gs.seg(g.roff, g.n, g.moff + int64_t(p.off) * g.n, g.n, g.n);
-        }
+        gs.add(nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1.0, 0.0);
+        gs.seg(uoff[gi], g.n, g.moff + int64_t(p.off) * g.n, g.n, g.n);
       }
     }
   } else {
@@ -487,33 +491,25 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
       if (g.keep == 0) continue;
       for (const Piece& p : g.cols) {
         if (nrl.kb[g.kc * d2 + p.s] != p.sec) continue;
-        cpR.add(g.roff + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
-                1.0);
+        cp.add(uoff[gi] + p.off, g.np, nrl.off[g.kc * d2 + p.s], g.keep, g.keep, Br.dim[p.sec], 1,
+               1.0);
       }
       for (const Piece& p : g.rows) {   // p.sec = ka, p.s = s1
-        if (small[gi]) {                // X V columns = U.D
-          cpM.add(g.moff + p.off, g.n, nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec],
-                  g.keep, 0, 1.0);
-        } else {
-          gs.add(nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec], g.keep, 1.0, 0.0);
-          if (g.np > 0) gs.seg(g.moff + p.off, g.n, g.roff, g.np, g.np);
-        }
+        gs.add(nl.off[p.sec * d1 + p.s], Bl.dim[p.sec], Bl.dim[p.sec], g.keep, 1.0, 0.0);
+        if (g.np > 0) gs.seg(g.moff + p.off, g.n, uoff[gi], g.np, g.np);
       }
     }
   }
   Upload u3;
-  u3.put(cpR);
-  u3.put(cpM);
+  u3.put(cp);
   u3.put(gs);
   char* db3 = u3.send(c, 3);
   if (j > 0) {
-    run_copy(c, cpR, db3, Rp, nR, nA.p, nA.n);
-    run_copy(c, cpM, db3, Mp, nM, nB.p, nB.n);
-    run_gemm(c, gs, db3, Rp, nR, Mp, nM, nB.p, nB.n);
+    run_copy(c, cp, db3, c->R.p, c->R.n, nA.p, nA.n);
+    run_gemm(c, gs, db3, c->R.p, c->R.n, c->M.p, c->M.n, nB.p, nB.n);
   } else {
-    run_copy(c, cpR, db3, Rp, nR, nB.p, nB.n);
-    run_copy(c, cpM, db3, Mp, nM, nA.p, nA.n);
-    run_gemm(c, gs, db3, Mp, nM, Rp, nR, nA.p, nA.n);
+    run_copy(c, cp, db3, c->R.p, c->R.n, nB.p, nB.n);
+    run_gemm(c, gs, db3, c->M.p, c->M.n, c->R.p, c->R.n, nA.p, nA.n);
   }
   dfree(c, st->A[iL]);
   dfree(c, st->A[iR]);

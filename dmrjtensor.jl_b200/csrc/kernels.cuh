@@ -69,6 +69,21 @@ void launch_hestenes(cudaStream_t s, double* base, const SvdTask* tasks, int nta
                      int* status);
 constexpr size_t HESTENES_SMEM_MAX = 200 * 1024;
 
+// Tridiagonal eigensolver for density-matrix blocks with n <= SYEVT_NMAX (syevt.cu).
+constexpr int SYEVT_NMAX = 112;
+struct TridTask {
+  int64_t a_off;   // n x n matrix (column-major, ld n); reflectors are stored in its lower part
+  int64_t w_off;   // n eigenvalues, descending
+  int64_t ws_off;  // 3n workspace: d, e, tau
+  int64_t u_off;   // n x keep eigenvectors (launch 2)
+  int n, keep;
+};
+size_t syevt_smem_vals(int n);
+size_t syevt_smem_vecs(int n, int k);
+void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks, int max_n);
+void launch_trid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
+                         int max_n, int max_k);
+
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
 
 // Persistent grouped FP64 GEMM (DMMA m8n8k4 tensor-core path).

@@ -193,6 +193,11 @@ DMRG_API int dmrg_test_eigh(dmrg_ctx* ctx, int nmat, const int* n, double* A, do
 DMRG_API int dmrg_test_svd(dmrg_ctx* ctx, int nmat, const int* r, const int* c, double* X,
                            double* V, double* w, int* sweeps);
 
+/* Tridiagonal-path eigensolver (n[i] <= 112): all eigenvalues (descending, packed in w) and the
+ * eigenvectors of the k[i] largest (packed n[i] x k[i] column-major in U). A is overwritten. */
+DMRG_API int dmrg_test_syevt(dmrg_ctx* ctx, int nmat, const int* n, const int* k, double* A,
+                             double* w, double* U);
+
 /* Fills *p with the reference defaults (minm 2, krylov 2, betatest 1e-10, ...). */
 DMRG_API void dmrg_params_default(dmrg_params* p);
 

@@ -113,3 +113,49 @@ def test_one_sided_jacobi(dmrgb, ctx, shapes):
         ox += r * c
         ov += c * c
         ow += c
+
+
+def _rho_like(rng, n, kind):
+    if kind == "rank":
+        X = rng.standard_normal((n, max(1, n // 2)))
+        return X @ X.T / n
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    if kind == "deg":        # exact pairs and quadruplets (multiplets) and a null space
+        w = np.zeros(n)
+        m = n // 3
+        w[:2 * m:2] = np.exp(-np.arange(m))
+        w[1:2 * m:2] = np.exp(-np.arange(m))
+    else:                    # 16 decades of decay, like a converged Schmidt spectrum
+        w = 10.0 ** (-np.arange(n) * 16.0 / n)
+    A = (Q * w) @ Q.T
+    return 0.5 * (A + A.T)
+
+
+@pytest.mark.parametrize("case", [[(66, "rank", 40), (1, "rank", 1), (2, "rank", 2), (3, "rank", 1)],
+                                  [(66, "deg", 50), (90, "deg", 60)],
+                                  [(112, "decay", 100), (40, "decay", 40)]])
+def test_tridiagonal_eigensolver(dmrgb, ctx, case):
+    """All eigenvalues within 2e-14 ||A||; the k kept eigenvectors orthonormal to 1e-13 and with
+    residual ||A u - lambda u|| <= 1e-12 ||A|| (the truncation's tolerance needs)."""
+    rng = np.random.default_rng(len(case))
+    mats = [_rho_like(rng, n, kind) for n, kind, _ in case]
+    ns = [n for n, _, _ in case]
+    ks = [k for _, _, k in case]
+    A = np.concatenate([np.asfortranarray(M).ravel(order="F") for M in mats])
+    w = np.zeros(sum(ns))
+    U = np.zeros(sum(n * k for n, k in zip(ns, ks)))
+    code = dmrgb.lib().dmrg_test_syevt(ctx.h, len(ns), (C.c_int * len(ns))(*ns),
+                                       (C.c_int * len(ks))(*ks), A.ctypes.data_as(DP),
+                                       w.ctypes.data_as(DP), U.ctypes.data_as(DP))
+    assert code == 0, dmrgb.lib().dmrg_last_error(ctx.h)
+    ow = ou = 0
+    for M, n, k in zip(mats, ns, ks):
+        lam = w[ow:ow + n]
+        ref = np.sort(np.linalg.eigvalsh(M))[::-1]
+        nrm = max(np.linalg.norm(M, 2), 1e-300)
+        assert np.max(np.abs(lam - ref)) < 2e-14 * nrm
+        Uk = U[ou:ou + n * k].reshape((n, k), order="F")
+        assert np.max(np.abs(Uk.T @ Uk - np.eye(k))) < 1e-13
+        assert np.max(np.abs(M @ Uk - Uk * lam[:k])) < 1e-12 * nrm
+        ow += n
+        ou += n * k
