@@ -78,6 +78,7 @@ SIGNATURES = {
     "dmrg_rupdate": (C.c_int, [_P, _P, C.c_int]),
     "dmrg_env_get": (C.c_int, [_P, C.c_int, C.c_int, _DP, _IP]),
     "dmrg_heff_apply": (C.c_int, [_P, _P, C.c_int, _DP, _DP, C.c_int]),
+    "dmrg_heff_apply_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
     "dmrg_twosite_dims": (C.c_int, [_P, _P, C.c_int, _IP]),
     "dmrg_sweep": (C.c_int, [_P, _P, C.POINTER(Params), C.POINTER(SweepStats)]),
     "dmrg_params_default": (None, [C.POINTER(Params)]),

@@ -607,6 +607,20 @@ int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* p
   });
 }
 
+int dmrg_heff_apply_noalloc(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
+                            double* psi_out, int precision) {
+  if (!st) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    if (mpo != st->mpo) fail(DMRG_ERR_ARG, "state was uploaded with a different MPO");
+    if (iL < 0 || iL + 1 >= st->L || !psi_in || !psi_out) fail(DMRG_ERR_ARG, "bad arguments");
+    if (precision != DMRG_PREC_FP64) fail(DMRG_ERR_ARG, "dmrg_heff_apply_noalloc computes in FP64");
+    if (!st->Lvalid[iL] || !st->Rvalid[iL + 1]) fail(DMRG_ERR_STATE, "environments not built");
+    set_device(c);
+    heff_apply_noalloc(st, iL, psi_in, psi_out);
+  });
+}
+
 int dmrg_sweep(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_sweep_stats* out) {
   if (!st) return DMRG_ERR_ARG;
   dmrg_ctx* c = st->ctx;

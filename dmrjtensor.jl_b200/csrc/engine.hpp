@@ -258,6 +258,9 @@ void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot);
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
                 int precision, GemmProfile* prof = nullptr);
 
+// Heff with every intermediate in the library's fixed device array (noalloc.cu).
+void heff_apply_noalloc(dmrg_state* st, int iL, const double* in_dev, double* out_dev);
+
 void env_boundaries(dmrg_state* st);
 void lupdate(dmrg_state* st, int i, double* flops);
 void rupdate(dmrg_state* st, int i, double* flops);

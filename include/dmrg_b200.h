@@ -169,6 +169,18 @@ DMRG_API int dmrg_env_get(dmrg_state* st, int site, int left, double* out, int* 
  * Uses Lenv[iL] and Renv[iL+1]. precision: enum dmrg_precision. */
 DMRG_API int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
                     double* psi_out, int precision);
+/* Same product as dmrg_heff_apply for callers that cannot allocate device memory at this point
+ * (for example a host framework whose caching allocator already owns all free HBM, or a solver
+ * loop that must not call the allocator). No reference counterpart: the reference allocates every
+ * intermediate itself. psi_in and psi_out are DEVICE pointers to dense-equivalent
+ * [ml, d1, d2, mr] column-major vectors; every intermediate lives in one fixed device array inside
+ * the library (9 MiB per GPU that loads the library, kept until exit), limited to 2^20 doubles of
+ * vector/intermediate data and 1 MiB of task descriptors: larger two-site spaces are rejected with
+ * DMRG_ERR_BUDGET. Nothing is allocated, no cudaMalloc/cudaFree is called. The first call on a
+ * device looks up the array's device address, so make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race. Returns after the result is written. */
+DMRG_API int dmrg_heff_apply_noalloc(dmrg_state* st, const dmrg_mpo* mpo, int iL,
+                                     const double* psi_in, double* psi_out, int precision);
 /* Dense-equivalent dims of the two-site space at (iL, iL+1): dims[4] = {ml, d1, d2, mr}. */
 DMRG_API int dmrg_twosite_dims(const dmrg_state* st, const dmrg_mpo* mpo, int iL, int* dims);
 
