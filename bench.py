@@ -251,6 +251,21 @@ def dist_setup():
     return world, rank, local, pg
 
 
+def reduce_max(dist, x):
+    """Max of a float over all ranks (the slowest replica sets the whole-job time)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(world, steps, tmax):
+    """Whole-job throughput of N independent replicas: N * K sweeps in the slowest rank's time."""
+    return world * steps / tmax
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -304,13 +319,8 @@ def run_ours(args, world, rank, local, dist):
     launches = pkg.kernel_launches() - n0
     clocks = sampler.stop() if rank == 0 else None
     dev_s = sum(s["seconds"] for s in stats)
-    tmax = dev_s
-    if dist:
-        import torch
-        t = torch.tensor([dev_s], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tmax = float(t.item())
-    value = world * args.steps / tmax
+    tmax = reduce_max(dist, dev_s)
+    value = aggregate_value(world, args.steps, tmax)
     heff_flops = sum(s["heff_flops"] for s in stats) / args.steps
     heff_sec = sum(s["heff_seconds"] for s in stats) / args.steps
     sweep_s = dev_s / args.steps
