@@ -166,6 +166,7 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
     if (s.ev) cudaEventDestroy(s.ev);
   }
   cudaStreamSynchronize(c->stream);
+  for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   cudaFree(c->d_scal);
   cudaFree(c->d_partial);
   cudaFree(c->d_status);

@@ -151,6 +151,7 @@ struct dmrg_ctx {
   int* d_status = nullptr;
   double* h_scal = nullptr;      // pinned mirror of d_scal
   cudaEvent_t ev[8] = {};
+  std::vector<cudaEvent_t> tev;  // phase-timing events, reused across sweeps
   int max_groups = 4096;
   int* d_flags = nullptr;        // block-Jacobi per-group flags
   int* h_flags = nullptr;        // pinned

@@ -15,64 +15,6 @@
 namespace dmrg {
 namespace {
 
-// Small dense symmetric eigenproblem on the host (Krylov tridiagonal, k <= 16): cyclic Jacobi,
-// eigenvalues ascending, eigenvectors in the columns of V (column-major n x n).
-void host_syev(int n, std::vector<double> A, std::vector<double>& w, std::vector<double>& V) {
-  V.assign(size_t(n) * n, 0.0);
-  for (int i = 0; i < n; ++i) V[i + i * n] = 1.0;
-  for (int sweep = 0; sweep < 100; ++sweep) {
-    double off = 0.0;
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) off += A[p + q * n] * A[p + q * n];
-    if (off < 1e-300) break;
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = A[p + q * n];
-        if (std::fabs(apq) < 1e-300) continue;
-        const double theta = (A[q + q * n] - A[p + p * n]) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < n; ++k) {  // rows
-          const double ap = A[p + k * n], aq = A[q + k * n];
-          A[p + k * n] = c * ap - s * aq;
-          A[q + k * n] = s * ap + c * aq;
-        }
-        for (int k = 0; k < n; ++k) {  // columns
-          const double ap = A[k + p * n], aq = A[k + q * n];
-          A[k + p * n] = c * ap - s * aq;
-          A[k + q * n] = s * ap + c * aq;
-          const double vp = V[k + p * n], vq = V[k + q * n];
-          V[k + p * n] = c * vp - s * vq;
-          V[k + q * n] = s * vp + c * vq;
-        }
-      }
-  }
-  std::vector<int> ord(n);
-  for (int i = 0; i < n; ++i) ord[i] = i;
-  std::stable_sort(ord.begin(), ord.end(),
-                   [&](int a, int b) { return A[a + a * n] < A[b + b * n]; });
-  w.resize(n);
-  std::vector<double> Vs(size_t(n) * n);
-  for (int k = 0; k < n; ++k) {
-    w[k] = A[ord[k] + ord[k] * n];
-    for (int i = 0; i < n; ++i) Vs[i + k * n] = V[i + ord[k] * n];
-  }
-  V.swap(Vs);
-}
-
-// Device scalars: value written by a reduction at d_scal[slot], read back synchronously.
-double read_scalar(dmrg_ctx* c, int slot) {
-  cuda_check(cudaMemcpyAsync(c->h_scal + slot, c->d_scal + slot, sizeof(double),
-                             cudaMemcpyDeviceToHost, c->stream), "scalar D2H");
-  cuda_check(cudaStreamSynchronize(c->stream), "scalar sync");
-  return c->h_scal[slot];
-}
-
-double dot_dev(dmrg_ctx* c, const double* x, const double* y, int64_t n, int slot = 0) {
-  launch_mdot(c->stream, x, 0, 1, y, n, c->d_partial, c->d_scal + slot);
-  return read_scalar(c, slot);
-}
-
 // Same rule as oracle/qtensor.py select_kept (global over all groups).
 struct Sel {
   std::vector<int> keep;
@@ -116,46 +58,40 @@ Sel select_kept(const std::vector<std::vector<double>>& vals, int maxm, int minm
   return s;
 }
 
-struct EvPool {
-  std::vector<cudaEvent_t> ev;
-  std::vector<std::pair<int, int>> pairs;   // (start idx, category)
-  int used = 0;
-  cudaEvent_t next() {
-    if (used == int(ev.size())) {
-      cudaEvent_t e;
-      cuda_check(cudaEventCreate(&e), "event create");
-      ev.push_back(e);
-    }
-    return ev[used++];
-  }
-  ~EvPool() { for (auto e : ev) cudaEventDestroy(e); }
-};
-
+// Phase timing with CUDA events from the context's persistent pool (profile != 0 only). Events
+// are read once, after the sweep's final synchronisation.
 struct Timing {
-  EvPool pool;
-  struct Span { cudaEvent_t a, b; int cat; };
+  dmrg_ctx* c;
+  bool on;
+  int used = 0;
+  struct Span { int a, b, cat; };
   std::vector<Span> spans;
   double acc[4] = {0, 0, 0, 0};   // heff, env, eig, vec
   GemmProfile gemm;
-  cudaEvent_t begin(dmrg_ctx* c) {
-    cudaEvent_t e = pool.next();
-    cudaEventRecord(e, c->stream);
-    return e;
+  Timing(dmrg_ctx* ctx, bool enabled) : c(ctx), on(enabled) {}
+  int record() {
+    if (used == int(c->tev.size())) {
+      cudaEvent_t e;
+      cuda_check(cudaEventCreate(&e), "event create");
+      c->tev.push_back(e);
+    }
+    cuda_check(cudaEventRecord(c->tev[used], c->stream), "event record");
+    return used++;
   }
-  void end(dmrg_ctx* c, cudaEvent_t a, int cat) {
-    cudaEvent_t e = pool.next();
-    cudaEventRecord(e, c->stream);
-    spans.push_back({a, e, cat});
+  cudaEvent_t event(int i) const { return c->tev[i]; }
+  int begin() { return on ? record() : -1; }
+  void end(int a, int cat) {
+    if (on && a >= 0) spans.push_back({a, record(), cat});
   }
   void flush() {   // call after a stream sync
     gemm.flush();
-    for (const Span& s : spans) {
+    for (const Span& sp : spans) {
       float ms = 0;
-      cudaEventElapsedTime(&ms, s.a, s.b);
-      acc[s.cat] += ms * 1e-3;
+      cudaEventElapsedTime(&ms, c->tev[sp.a], c->tev[sp.b]);
+      acc[sp.cat] += ms * 1e-3;
     }
     spans.clear();
-    pool.used = 0;
+    used = 0;
   }
 };
 
@@ -191,11 +127,13 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   const int d1 = ml.d, d2 = mr.d;
   if (!st->Lvalid[iL] || !st->Rvalid[iR]) fail(DMRG_ERR_STATE, "environments are not built");
 
-  // psi[iL] (j>0) or psi[iR] (j<0) /= norm  (algs/DMRG.jl:365-369)
-  cudaEvent_t tv = tm.begin(c);
+  // psi[iL] (j>0) or psi[iR] (j<0) /= norm  (algs/DMRG.jl:365-369); the squared norm stays on
+  // the device
+  int tv = tm.begin();
   const int ic = j > 0 ? iL : iR;
-  const double nr = std::sqrt(dot_dev(c, st->A[ic].p, st->A[ic].p, st->lay[ic].size));
-  if (nr > 0) launch_scale(s, st->A[ic].p, st->lay[ic].size, 1.0 / nr);
+  launch_mdot(s, st->A[ic].p, 0, 1, st->A[ic].p, st->lay[ic].size, c->d_partial,
+              c->d_scal + lz::NRM);
+  launch_scale_rsqrt(s, st->A[ic].p, st->lay[ic].size, c->d_scal + lz::NRM);
 
   HeffPlan hp;
   plan_heff(st, iL, hp);
@@ -227,87 +165,68 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   double* K = c->K.p;
   double* H = c->H.p;
   run_gemm(c, gaa, hp.dbase, st->A[iL].p, st->A[iL].n, st->A[iR].p, st->A[iR].n, K, n);
-  tm.end(c, tv, 3);
+  tm.end(tv, 3);
 
   auto heff = [&](const double* x, double* y) {
-    cudaEvent_t th = tm.begin(c);
+    const int th = tm.begin();
     apply_heff(st, iL, hp, x, y, P.precision, P.profile ? &tm.gemm : nullptr);
-    tm.end(c, th, 0);
+    tm.end(th, 0);
     so.nmv += 1;
     so.heff_flops += hp.flops;
   };
 
-  double E = 0.0;
-  const double* psi = K;
+  // Krylov solve with every scalar in device memory (slots lz::*): no host round trip; a
+  // breakdown (beta <= betatest) zeroes the remaining Krylov vectors instead of ending the loop,
+  // and the Ritz step uses only the active ones. The energy is read back with the eigenvalues.
+  double* scal = c->d_scal;
   if (P.krylov <= 2) {
     // simplelanczos (algs/DMRG.jl:57-90): H is applied to AA before its normalisation
     heff(K, H);
-    tv = tm.begin(c);
-    const double nAA = std::sqrt(dot_dev(c, K, K, n));
-    launch_scale(s, K, n, 1.0 / nAA);
-    const double a1 = dot_dev(c, K, H, n);
-    launch_axpby(s, n, -a1, nullptr, 0, K, 1.0, nullptr, 0, H, 0);
-    const double b1 = std::sqrt(dot_dev(c, H, H, n));
-    tm.end(c, tv, 3);
-    if (b1 > P.betatest) {
-      double* K1 = K + n;
-      launch_axpby(s, n, 1.0 / b1, nullptr, 0, H, 0.0, nullptr, 0, K1, 0);
-      heff(K1, H);
-      const double a2 = dot_dev(c, K1, H, n);
-      std::vector<double> w, V;
-      host_syev(2, {a1, b1, b1, a2}, w, V);
-      E = w[0];
-      launch_axpby(s, n, V[0], nullptr, 0, K, 0.0, nullptr, 0, H, 0);
-      launch_axpby(s, n, V[1], nullptr, 0, K1, 1.0, nullptr, 0, H, 0);
-      psi = H;
-    } else {
-      E = a1;
-      psi = K;
-    }
+    tv = tm.begin();
+    launch_dot2(s, K, H, n, c->d_partial, scal + lz::KK);
+    launch_lanczos2_orth(s, K, H, n, scal, c->d_partial);   // K /= |K|, H -= a1 K, |H|^2
+    double* K1 = K + n;
+    launch_next_vector(s, H, K1, n, scal, 0, P.betatest);
+    tm.end(tv, 3);
+    heff(K1, H);
+    tv = tm.begin();
+    launch_mdot(s, K1, 0, 1, H, n, c->d_partial, scal + lz::ALPHA + 1);
+    launch_ritz(s, scal, 2);
+    launch_lincomb(s, K, n, 2, scal + lz::COEF, H, n);
+    tm.end(tv, 3);
   } else {
-    tv = tm.begin(c);
-    const double nAA = std::sqrt(dot_dev(c, K, K, n));
-    launch_scale(s, K, n, 1.0 / nAA);
-    tm.end(c, tv, 3);
-    std::vector<double> al, be;
+    tv = tm.begin();
+    launch_mdot(s, K, 0, 1, K, n, c->d_partial, scal + lz::KK);
+    launch_scale_rsqrt(s, K, n, scal + lz::KK);
+    tm.end(tv, 3);
     for (int jj = 0; jj < kdim; ++jj) {
       double* Kj = K + int64_t(jj) * n;
       heff(Kj, H);
-      tv = tm.begin(c);
-      const double a = dot_dev(c, Kj, H, n);
-      al.push_back(a);
-      if (jj == kdim - 1) { tm.end(c, tv, 3); break; }
-      launch_axpby(s, n, -a, nullptr, 0, Kj, 1.0, nullptr, 0, H, 0);
-      if (jj > 0) launch_axpby(s, n, -be[jj - 1], nullptr, 0, Kj - n, 1.0, nullptr, 0, H, 0);
+      tv = tm.begin();
+      launch_mdot(s, Kj, 0, 1, H, n, c->d_partial, scal + lz::ALPHA + jj);
+      if (jj == kdim - 1) { tm.end(tv, 3); break; }
+      launch_axpby(s, n, 0.0, scal + lz::ALPHA + jj, -1.0, Kj, 1.0, nullptr, 0, H, 0);
+      if (jj > 0)
+        launch_axpby(s, n, 0.0, scal + lz::BETA + jj - 1, -1.0, Kj - n, 1.0, nullptr, 0, H, 0);
       for (int pass = 0; pass < 2; ++pass) {   // full re-orthogonalisation (CGS2)
-        launch_mdot(s, K, n, jj + 1, H, n, c->d_partial, c->d_scal);
-        launch_msub(s, K, n, jj + 1, c->d_scal, H, n);
+        launch_mdot(s, K, n, jj + 1, H, n, c->d_partial, scal + lz::CGS);
+        launch_msub(s, K, n, jj + 1, scal + lz::CGS, H, n);
       }
-      const double b = std::sqrt(dot_dev(c, H, H, n));
-      tm.end(c, tv, 3);
-      if (b <= P.betatest) break;
-      be.push_back(b);
-      launch_axpby(s, n, 1.0 / b, nullptr, 0, H, 0.0, nullptr, 0, K + int64_t(jj + 1) * n, 0);
+      launch_mdot(s, H, 0, 1, H, n, c->d_partial, scal + lz::B2 + jj);
+      launch_next_vector(s, H, K + int64_t(jj + 1) * n, n, scal, jj, P.betatest);
+      tm.end(tv, 3);
     }
-    const int m = int(al.size());
-    std::vector<double> T(size_t(m) * m, 0.0), w, V;
-    for (int a = 0; a < m; ++a) {
-      T[a + a * m] = al[a];
-      if (a + 1 < m) T[a + (a + 1) * m] = T[a + 1 + a * m] = be[a];
-    }
-    host_syev(m, T, w, V);
-    E = w[0];
-    for (int a = 0; a < m; ++a) c->h_scal[32 + a] = -V[a];
-    cuda_check(cudaMemcpyAsync(c->d_scal + 32, c->h_scal + 32, sizeof(double) * m,
-                               cudaMemcpyHostToDevice, s), "ritz coefficients");
-    launch_zero(s, H, n);
-    launch_msub(s, K, n, m, c->d_scal + 32, H, n);
-    psi = H;
+    tv = tm.begin();
+    launch_ritz(s, scal, kdim);
+    launch_lincomb(s, K, n, kdim, scal + lz::COEF, H, n);
+    tm.end(tv, 3);
   }
-  so.energy = E;
+  const double* psi = H;
+  cuda_check(cudaMemcpyAsync(c->h_scal + lz::EN, scal + lz::EN, sizeof(double),
+                             cudaMemcpyDeviceToHost, s), "energy D2H");
 
   // ---------------- reduced density matrix per centre-charge group (algs/DMRG.jl:425-429)
-  cudaEvent_t te = tm.begin(c);
+  const int te = tm.begin();
   std::map<QN, Group> gm;
   for (int ka = 0; ka < Bl.nsec(); ++ka)
     for (int s1 = 0; s1 < d1; ++s1) {
@@ -417,6 +336,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + W0, sizeof(double) * wtot,
                              cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
+  so.energy = c->h_scal[lz::EN];
 
   std::vector<std::vector<double>> vals(G.size());
   for (int g = 0; g < int(G.size()); ++g) {
@@ -519,7 +439,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
   st->lay[iR] = nrl;
   st->bond[iL + 1] = C;
   if (j > 0) st->Rvalid[iL] = 0; else st->Lvalid[iL + 1] = 0;
-  tm.end(c, te, 2);
+  tm.end(te, 2);
 }
 
 }  // namespace
@@ -532,19 +452,18 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   std::memset(&out, 0, sizeof(out));
   const int svn = P.svnbond > 0 ? P.svnbond : (L + 1) / 2;
   const int svn_site = std::min(std::max(2, svn + 1), L) - 1;   // 0-based i of SvNcheck!
-  Timing tm;
-  cudaEvent_t t0 = tm.pool.next(), t1 = tm.pool.next();
-  cudaEventRecord(t0, c->stream);
+  Timing tm(c, P.profile != 0);
+  const int t0 = tm.record();
   int j = st->dir;
   for (int ns = 0; ns < 2 * (L - 1); ++ns) {
     const int i = st->oc;
     const int iL = j > 0 ? i : i - 1, iR = j > 0 ? i + 1 : i;
     StepOut so;
     twostep(st, P, j, iL, iR, tm, so);
-    cudaEvent_t tenv = tm.begin(c);
+    const int tenv = tm.begin();
     double ef = 0.0;
     if (j > 0) lupdate(st, i, &ef); else rupdate(st, i, &ef);
-    tm.end(c, tenv, 1);
+    tm.end(tenv, 1);
     out.energy = so.energy;
     out.max_truncerr = std::max(out.max_truncerr, so.truncerr);
     out.biggest_m = std::max(out.biggest_m, so.m);
@@ -563,16 +482,14 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     }
     st->oc += j;
     if ((st->oc == L - 1 && j > 0) || (st->oc == 0 && j < 0)) j = -j;
-    cuda_check(cudaStreamSynchronize(c->stream), "step sync");
-    tm.flush();
-    tm.pool.used = 2;
   }
   st->dir = j;
-  cudaEventRecord(t1, c->stream);
-  cuda_check(cudaEventSynchronize(t1), "sweep sync");
+  const int t1 = tm.record();
+  cuda_check(cudaEventSynchronize(tm.event(t1)), "sweep sync");
   float ms = 0;
-  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventElapsedTime(&ms, tm.event(t0), tm.event(t1));
   out.seconds = ms * 1e-3;
+  tm.flush();
   out.heff_seconds = tm.acc[0];
   out.env_seconds = tm.acc[1];
   out.eig_seconds = tm.acc[2];

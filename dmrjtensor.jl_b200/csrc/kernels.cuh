@@ -110,6 +110,37 @@ void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const doub
 void launch_scale(cudaStream_t s, double* x, int64_t n, double a);
 void launch_zero(cudaStream_t s, double* x, int64_t n);
 
+// Device-resident Krylov scalars: slots of the context's 256-double scalar array. The Krylov
+// solve of a bond step runs without host round trips; the host reads only the energy (EN).
+namespace lz {
+constexpr int CGS = 0;      // [0, 16): Gram-Schmidt coefficients
+constexpr int KK = 16;      // <K,K>      (KK and KH adjacent: written by one dot2)
+constexpr int KH = 17;      // <K,HK>
+constexpr int NRM = 18;     // squared norm of the centre site tensor
+constexpr int EN = 19;      // Ritz energy
+constexpr int COEF = 32;    // [32, 48): Ritz vector coefficients
+constexpr int ALPHA = 48;   // [48, 64): alpha_j
+constexpr int B2 = 64;      // [64, 80): |r_j|^2
+constexpr int BETA = 80;    // [80, 96): beta_j (0 after a breakdown)
+constexpr int ACT = 96;     // [96, 113): 1 while K_j is an active Krylov vector
+}  // namespace lz
+// x *= 1/sqrt(*nrm2) when *nrm2 > 0
+void launch_scale_rsqrt(cudaStream_t s, double* x, int64_t n, const double* nrm2);
+// out[0] = <x,x>, out[1] = <x,y>
+void launch_dot2(cudaStream_t s, const double* x, const double* y, int64_t n, double* partial,
+                 double* out);
+// reference 2-vector step: K /= |K|, H -= a1 K, s[ALPHA] = a1, s[B2] = <H,H>
+void launch_lanczos2_orth(cudaStream_t s, double* K, double* H, int64_t n, double* scal,
+                          double* partial);
+// K_{j+1} = H / beta_j, or 0 after a breakdown (beta_j <= betatest)
+void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, double* scal,
+                        int j, double betatest);
+// lowest Ritz pair of the Krylov tridiagonal: s[EN], s[COEF + j]
+void launch_ritz(cudaStream_t s, double* scal, int kdim);
+// y = sum_j c[j] X_j, j < k
+void launch_lincomb(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c,
+                    double* y, int64_t n);
+
 // Block Jacobi for large blocks (n > 100): padded to N = 16*nb (nb even).
 struct BlockEigGroup {
   int64_t a_off, w_off;          // caller's matrix (n x n) / eigenvalues (n), as in EigTask

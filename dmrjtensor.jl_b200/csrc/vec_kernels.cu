@@ -141,6 +141,157 @@ __global__ void k_scale(double* x, int64_t n, double a) {
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) x[i] *= a;
 }
 
+// x *= 1/sqrt(*nrm2) when *nrm2 > 0 (normalisation by a device-resident squared norm)
+__global__ void k_scale_rsqrt(double* x, int64_t n, const double* nrm2) {
+  const double v = *nrm2;
+  const double a = (v > 0.0) ? 1.0 / sqrt(v) : 1.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) x[i] *= a;
+}
+
+// partial rows 0/1: this block's share of <x,x> and <x,y>
+__global__ void k_dot2_partial(const double* __restrict__ x, const double* __restrict__ y,
+                               int64_t n, double* partial) {
+  double sxx = 0.0, sxy = 0.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double xv = x[i];
+    sxx += xv * xv;
+    sxy += xv * y[i];
+  }
+  __shared__ double red[2][RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  sxx = warp_sum(sxx);
+  sxy = warp_sum(sxy);
+  if (lane == 0) { red[0][wid] = sxx; red[1][wid] = sxy; }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double s = 0.0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) s += red[threadIdx.x][w];
+    partial[threadIdx.x * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// First half of the reference 2-vector Krylov step, from s[KK] = <K,K> and s[KH] = <K,HK>:
+// K <- K / |K|, a1 = <K,HK> / |K| (stored at s[ALPHA]), H <- H - a1 K, and this block's share
+// of <H,H> in partial row 0.
+__global__ void k_lanczos2_orth(double* K, double* H, int64_t n, double* s, double* partial) {
+  const double nn = sqrt(s[lz::KK]);
+  const double inv = 1.0 / nn;
+  const double a1 = s[lz::KH] / nn;
+  double shh = 0.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double k = K[i] * inv;
+    const double h = H[i] - a1 * k;
+    K[i] = k;
+    H[i] = h;
+    shh += h * h;
+  }
+  __shared__ double red[RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  shh = warp_sum(shh);
+  if (lane == 0) red[wid] = shh;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += red[w];
+    partial[blockIdx.x] = t;
+    if (blockIdx.x == 0) s[lz::ALPHA] = a1;
+  }
+}
+
+// Next Krylov vector K_{j+1} = H / beta_j with beta_j = sqrt(s[B2+j]), or 0 once the recursion
+// has broken down (beta_j <= betatest, or an earlier breakdown: s[ACT+j] == 0). Every thread
+// takes the decision from the same read-only inputs; thread 0 records beta_j (0 on breakdown)
+// and the activity of K_{j+1}.
+__global__ void k_next_vector(const double* __restrict__ H, double* __restrict__ Kn, int64_t n,
+                              double* s, int j, double betatest) {
+  const bool act = (j == 0) || (s[lz::ACT + j] != 0.0);
+  const double b = sqrt(s[lz::B2 + j]);
+  const bool ok = act && (b > betatest);
+  const double r = ok ? 1.0 / b : 0.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    Kn[i] = ok ? r * H[i] : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s[lz::BETA + j] = ok ? b : 0.0;
+    s[lz::ACT + j + 1] = ok ? 1.0 : 0.0;
+  }
+}
+
+// Ritz step of the Krylov solve, one warp: T = tridiag(alpha, beta) of the m active vectors
+// (m = 1 + number of leading non-zero beta_j, at most kdim), cyclic Jacobi (same rotation order
+// and thresholds as a serial cyclic Jacobi: lanes own the rows/columns of one rotation), lowest
+// eigenvalue -> s[EN], its eigenvector -> s[COEF + j] (0 for j >= m).
+__global__ void k_ritz(double* s, int kdim) {
+  __shared__ double A[MAXK * MAXK], V[MAXK * MAXK];
+  const int lane = threadIdx.x;
+  int m = 1;
+  while (m < kdim && s[lz::BETA + m - 1] > 0.0) ++m;
+  for (int e = lane; e < m * m; e += 32) {
+    const int r = e % m, c = e / m;
+    double v = 0.0;
+    if (r == c) v = s[lz::ALPHA + r];
+    else if (r == c + 1) v = s[lz::BETA + c];
+    else if (c == r + 1) v = s[lz::BETA + r];
+    A[e] = v;
+    V[e] = (r == c) ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) off += A[p + q * m] * A[p + q * m];
+    if (off < 1e-300) break;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = A[p + q * m];
+        if (fabs(apq) < 1e-300) continue;
+        const double theta = (A[q + q * m] - A[p + p * m]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+        __syncwarp();
+        if (lane < m) {   // rows p, q
+          const double ap = A[p + lane * m], aq = A[q + lane * m];
+          A[p + lane * m] = c * ap - sn * aq;
+          A[q + lane * m] = sn * ap + c * aq;
+        }
+        __syncwarp();
+        if (lane < m) {   // columns p, q
+          const double ap = A[lane + p * m], aq = A[lane + q * m];
+          A[lane + p * m] = c * ap - sn * aq;
+          A[lane + q * m] = sn * ap + c * aq;
+          const double vp = V[lane + p * m], vq = V[lane + q * m];
+          V[lane + p * m] = c * vp - sn * vq;
+          V[lane + q * m] = sn * vp + c * vq;
+        }
+        __syncwarp();
+      }
+  }
+  int o = 0;
+  for (int k = 1; k < m; ++k)
+    if (A[k + k * m] < A[o + o * m]) o = k;   // lowest; ties keep the lower index
+  if (lane == 0) s[lz::EN] = A[o + o * m];
+  for (int k = lane; k < kdim; k += 32) s[lz::COEF + k] = (k < m) ? V[k + o * m] : 0.0;
+}
+
+// y = sum_j c[j] * X_j (y not read), j < k, c in device memory
+__global__ void k_lincomb(const double* __restrict__ X, int64_t ldx, int k,
+                          const double* __restrict__ c, double* __restrict__ y, int64_t n) {
+  double cc[MAXK];
+#pragma unroll
+  for (int j = 0; j < MAXK; ++j) cc[j] = j < k ? c[j] : 0.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double v = cc[0] * X[i];
+#pragma unroll
+    for (int j = 1; j < MAXK; ++j)
+      if (j < k) v += cc[j] * X[j * ldx + i];
+    y[i] = v;
+  }
+}
+
 int grid_for(int64_t n) {
   int64_t b = (n + RED_THREADS - 1) / RED_THREADS;
   if (b > 4 * RED_BLOCKS) b = 4 * RED_BLOCKS;
@@ -191,6 +342,44 @@ void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const doub
 void launch_scale(cudaStream_t s, double* x, int64_t n, double a) {
   if (n <= 0) return;
   k_scale<<<grid_for(n), RED_THREADS, 0, s>>>(x, n, a);
+  count_launch();
+}
+
+void launch_scale_rsqrt(cudaStream_t s, double* x, int64_t n, const double* nrm2) {
+  if (n <= 0) return;
+  k_scale_rsqrt<<<grid_for(n), RED_THREADS, 0, s>>>(x, n, nrm2);
+  count_launch();
+}
+
+void launch_dot2(cudaStream_t s, const double* x, const double* y, int64_t n, double* partial,
+                 double* out) {
+  k_dot2_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, y, n, partial);
+  k_reduce_rows<<<2, 256, 0, s>>>(partial, RED_BLOCKS, out);
+  count_launch(2);
+}
+
+void launch_lanczos2_orth(cudaStream_t s, double* K, double* H, int64_t n, double* scal,
+                          double* partial) {
+  k_lanczos2_orth<<<RED_BLOCKS, RED_THREADS, 0, s>>>(K, H, n, scal, partial);
+  k_reduce_rows<<<1, 256, 0, s>>>(partial, RED_BLOCKS, scal + lz::B2);
+  count_launch(2);
+}
+
+void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, double* scal,
+                        int j, double betatest) {
+  k_next_vector<<<grid_for(n), RED_THREADS, 0, s>>>(H, Kn, n, scal, j, betatest);
+  count_launch();
+}
+
+void launch_ritz(cudaStream_t s, double* scal, int kdim) {
+  k_ritz<<<1, 32, 0, s>>>(scal, kdim);
+  count_launch();
+}
+
+void launch_lincomb(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c,
+                    double* y, int64_t n) {
+  if (n <= 0 || k <= 0) return;
+  k_lincomb<<<grid_for(n), RED_THREADS, 0, s>>>(X, ldx, k, c, y, n);
   count_launch();
 }
 
