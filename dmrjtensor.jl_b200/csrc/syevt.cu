@@ -1,69 +1,124 @@
 // syevt.cu -- density-matrix eigensolver for blocks up to SYEVT_NMAX: Householder
-// tridiagonalisation, bisection, inverse iteration, re-orthogonalisation, back-transformation.
+// tridiagonalisation, multisection, inverse iteration, re-orthogonalisation, back-transformation.
+// One CTA per block; every phase is laid out for latency (few block barriers, no dependent
+// shared- or local-memory loads on the arithmetic chains), since the blocks are small.
 //
-// Launch 1 (k_trid_eigvals), one CTA per block, matrix in shared memory:
-//   * A = Q T Q^T by n-2 Householder reflectors (lower form, LAPACK dsytd2 order); the reflector
-//     vectors are written into the strictly lower part of the caller's matrix, d/e/tau into a
-//     small per-block workspace;
-//   * all eigenvalues of T by bisection to an absolute width of 4 eps ||T|| (one thread per
-//     eigenvalue), with a division-free Sturm count (see sturm_below).
+// Launch 1 (k_trid_eigvals), matrix in shared memory:
+//   * A = Q T Q^T by n-2 Householder reflectors (lower form, LAPACK dsytd2 order). Per step two
+//     block barriers: B v (two threads per row), then the rank-2 update, during which warp 0
+//     updates the next pivot column first and builds the next reflector (look-ahead). The
+//     reflector vectors are written into the strictly lower part of the caller's matrix, d/e/tau
+//     into a small per-block workspace;
+//   * all eigenvalues of T by trisection (two threads per eigenvalue, two Sturm counts per
+//     step) to an absolute width of 8.9e-16 ||T||, with a division-free Sturm count (see
+//     sturm_below).
 // The host then truncates globally and asks for the top-k vectors of each block.
-// Launch 2 (k_trid_vectors), one CTA per block:
-//   * eigenvectors of T by inverse iteration on (T - lambda I) with partial-pivoting LU (three
-//     iterations from a fixed pseudo-random start). Eigenvalues closer than 1e-10 ||T|| form a
-//     cluster whose members are re-orthogonalised against each other at every iteration; kept
-//     eigenvalues below 1e-13 ||T|| (numerically zero) get an orthonormal completion instead;
-//   * two passes of classical Gram-Schmidt over the k vectors (largest eigenvalue first);
-//   * back-transformation U = Q Z with the stored reflectors.
+// Launch 2 (k_trid_vectors):
+//   * eigenvectors of T by inverse iteration on (T - lambda I) with partial-pivoting LU, one
+//     thread per vector (three iterations from a fixed pseudo-random start; factors in shared
+//     memory). Vectors of (nearly) equal eigenvalues come out as independent vectors of their
+//     common eigenspace; kept eigenvalues below 1e-13 ||T|| (numerically zero) start from the
+//     pseudo-random vector alone (an orthonormal completion after the next step);
+//   * Cholesky QR over the k vectors (largest eigenvalue first), a second pass unless the Gram
+//     matrix was already within 1e-3/k of the identity; two passes of classical Gram-Schmidt
+//     with restarts instead if a Cholesky pivot shows nearly dependent vectors;
+//   * back-transformation U = Q Z with the stored reflectors, in blocks of 8 (compact WY form
+//     I - V T V^T, LAPACK dlarft order).
 #include "kernels.cuh"
 
 namespace dmrg {
 namespace {
 
-constexpr int TE_THREADS = 256;
+constexpr int TE_THREADS = 256;   // 8 warps; two threads per row / per eigenvalue (n <= 128)
+constexpr int TV_THREADS = 256;
+constexpr int BT_NB = 8;          // reflectors per back-transformation block
+constexpr unsigned FULL = 0xffffffffu;
+constexpr size_t SMEM_LIMIT = 227 * 1024;
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
   return v;
 }
 
-// block-wide sum; red has >= 32 entries; all threads get the result
-__device__ double bsum(double v, double* red) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  v = wsum(v);
-  __syncthreads();
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double t = 0.0;
-  const int nw = blockDim.x >> 5;
-  for (int i = 0; i < nw; ++i) t += red[i];
-  return t;
+// Scales the pair (D, Dm1) by the power of two that brings the larger magnitude into [1, 2):
+// exact, keeps the signs, and needs only exponent-field arithmetic.
+__device__ __forceinline__ void rescale_pair(double& D, double& Dm1) {
+  const double mx = fmax(fabs(D), fabs(Dm1));
+  const int fld = (__double2hiint(mx) >> 20) & 0x7ff;
+  if (fld != 0 && fld != 0x7ff) {
+    const int ex = min(fld - 1023, 1022);
+    const double sc = __hiloint2double((1023 - ex) << 20, 0);
+    D *= sc;
+    Dm1 *= sc;
+  }
 }
 
-// Number of eigenvalues of T(d,e) strictly below x: sign changes of the leading minors
-// D_j = (d_j - x) D_{j-1} - e_{j-1}^2 D_{j-2}. Only one FMA per step sits on the dependent chain
-// (the products with the previous minor and d_j - x are off it); an exact zero minor counts with
-// the sign opposite to its predecessor; every 8 steps the pair is renormalised by a power of two.
-__device__ int sturm_below(const double* d, const double* e2, int n, double x) {
+// One step of the Sturm sequence: D_j = (d_j - x) D_{j-1} - e_{j-1}^2 D_{j-2}. Only the FMA is
+// on the dependent chain (the product with D_{j-2} is available a step earlier). An exact zero
+// minor counts with the sign opposite to its predecessor.
+__device__ __forceinline__ void sturm_step(double dx, double ee, double& D, double& Dm1, bool& neg,
+                                           int& c) {
+  const double Dn = fma(dx, D, -ee * Dm1);
+  const bool ng = (Dn == 0.0) ? !neg : (Dn < 0.0);
+  c += (ng != neg) ? 1 : 0;
+  neg = ng;
+  Dm1 = D;
+  D = Dn;
+}
+
+// Number of eigenvalues of T(d,e) strictly below x (sign changes of the leading minors).
+// Unrolled by 8 with the loads of each group issued first, then one exact rescale per group.
+__device__ int sturm_below(const double* __restrict__ d, const double* __restrict__ e2, int n,
+                           double x) {
   double Dm1 = 1.0, D = d[0] - x;
-  int c = (D < 0) ? 1 : 0;
-  bool neg = D < 0;
-  for (int j = 1; j < n; ++j) {
-    const double Dn = fma(d[j] - x, D, -e2[j - 1] * Dm1);
-    const bool ng = (Dn == 0.0) ? !neg : (Dn < 0);
-    c += (ng != neg) ? 1 : 0;
-    neg = ng;
-    Dm1 = D;
-    D = Dn;
-    if ((j & 7) == 0) {
-      const double mx = fmax(fabs(D), fabs(Dm1));
-      const int ex = (mx > 0.0) ? ilogb(mx) : 0;
-      D = scalbn(D, -ex);
-      Dm1 = scalbn(Dm1, -ex);
+  bool neg = D < 0.0;
+  int c = neg ? 1 : 0;
+  int j = 1;
+  for (; j + 8 <= n; j += 8) {
+    double dx[8], ee[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      dx[q] = d[j + q] - x;
+      ee[q] = e2[j + q - 1];
     }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sturm_step(dx[q], ee[q], D, Dm1, neg, c);
+    rescale_pair(D, Dm1);
   }
+  for (; j < n; ++j) sturm_step(d[j] - x, e2[j - 1], D, Dm1, neg, c);
   return c;
+}
+
+// Householder reflector of column k (one warp): x = A[k+1:n, k], H = I - tau v v^T with v[0] = 1
+// and H x = beta e_1. Writes v (length n-k-1) to vout, stores v[1:] in place below the
+// subdiagonal, and records d[k] = A[k,k], e[k] = beta, tau[k].
+__device__ void householder_col(double* __restrict__ A, int n, int k, double* __restrict__ vout,
+                                double* d, double* e, double* tau, int lane) {
+  const int m = n - k - 1;
+  double* col = A + k * n + k + 1;
+  double part = 0.0;
+  for (int i = 1 + lane; i < m; i += 32) part += col[i] * col[i];
+  const double xn2 = wsum(part);
+  const double alpha = col[0];
+  double t, sc, beta;
+  if (xn2 == 0.0) {
+    t = 0.0; sc = 0.0; beta = alpha;
+  } else {
+    beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    t = (beta - alpha) / beta;
+    sc = 1.0 / (alpha - beta);
+  }
+  for (int i = lane; i < m; i += 32) {
+    const double vi = (i == 0) ? 1.0 : col[i] * sc;
+    vout[i] = vi;
+    if (i > 0) col[i] = vi;
+  }
+  if (lane == 0) {
+    e[k] = beta;
+    tau[k] = t;
+    d[k] = A[k + k * n];
+  }
 }
 
 __global__ void __launch_bounds__(TE_THREADS)
@@ -73,81 +128,79 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
   if (n <= 0) return;
   extern __shared__ double sm[];
   double* A = sm;               // n x n
-  double* v = A + n * n;        // n
-  double* p = v + n;            // n
+  double* vb = A + n * n;       // 2 x n: reflector of this step / of the next
+  double* p = vb + 2 * n;       // n
   double* d = p + n;            // n
   double* e = d + n;            // n
   double* e2 = e + n;           // n
   double* tau = e2 + n;         // n
-  __shared__ double red[32];
-  __shared__ double s_tau, s_scale, s_beta, s_K;
-  const int tid = threadIdx.x;
+  __shared__ double s_lo, s_hi;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   double* Ag = base + tk.a_off;
   for (int x = tid; x < n * n; x += blockDim.x) A[x] = Ag[x];
   __syncthreads();
+  if (n >= 3 && warp == 0) householder_col(A, n, 0, vb, d, e, tau, lane);
+  __syncthreads();
   for (int k = 0; k + 2 < n; ++k) {
-    const int m = n - k - 1;              // length of x = A[k+1:n, k]
-    const double* col = A + k * n + k + 1;
-    double part = 0.0;
-    for (int i = 1 + tid; i < m; i += blockDim.x) part += col[i] * col[i];
-    const double xn2 = bsum(part, red);
-    if (tid == 0) {
-      const double alpha = col[0];
-      if (xn2 == 0.0) {
-        s_tau = 0.0; s_beta = alpha; s_scale = 0.0;
-      } else {
-        const double beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-        s_tau = (beta - alpha) / beta;
-        s_scale = 1.0 / (alpha - beta);
-        s_beta = beta;
+    const int m = n - k - 1;
+    const double* v = vb + (k & 1) * n;
+    double* vn = vb + ((k + 1) & 1) * n;
+    const double t = tau[k];
+    double* B = A + (k + 1) * n + (k + 1);     // trailing matrix B[i + j*n], i, j < m
+    {   // p = t B v: two threads per row (row i, half h of the columns), rows of B contiguous
+      const int i = warp * 16 + (lane >> 1), h = lane & 1;
+      const int jh = (m + 1) >> 1;
+      const int j0 = h ? jh : 0, j1 = h ? m : jh;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      if (i < m) {
+        const double* Bi = B + i;
+        int j = j0;
+        for (; j + 4 <= j1; j += 4) {
+          s0 += Bi[j * n] * v[j];
+          s1 += Bi[(j + 1) * n] * v[j + 1];
+          s2 += Bi[(j + 2) * n] * v[j + 2];
+          s3 += Bi[(j + 3) * n] * v[j + 3];
+        }
+        for (; j < j1; ++j) s0 += Bi[j * n] * v[j];
       }
-      e[k] = s_beta;
-      tau[k] = s_tau;
-      d[k] = A[k + k * n];
+      double s = (s0 + s1) + (s2 + s3);
+      s += __shfl_xor_sync(FULL, s, 1);
+      if (i < m && h == 0) p[i] = t * s;
     }
     __syncthreads();
-    const double t = s_tau, sc = s_scale;
-    for (int i = tid; i < m; i += blockDim.x) v[i] = (i == 0) ? 1.0 : col[i] * sc;
-    __syncthreads();
-    if (t != 0.0) {
-      // p = t * B v, B = A[k+1:, k+1:] symmetric: p_i = sum_j B[j,i] v_j (contiguous column),
-      // 8 lanes per column so that 32 columns reduce in parallel
-      {
-        const int g8 = tid >> 3, l8 = tid & 7, ng8 = blockDim.x >> 3;
-        for (int ib = 0; ib < m; ib += ng8) {     // uniform trip count: shuffles stay convergent
-          const int i = ib + g8;
-          double s = 0.0;
-          if (i < m) {
-            const double* colB = A + (k + 1 + i) * n + (k + 1);
-            for (int j = l8; j < m; j += 8) s += colB[j] * v[j];
-          }
-          s += __shfl_xor_sync(0xffffffffu, s, 4, 8);
-          s += __shfl_xor_sync(0xffffffffu, s, 2, 8);
-          s += __shfl_xor_sync(0xffffffffu, s, 1, 8);
-          if (i < m && l8 == 0) p[i] = t * s;
+    // K = p.v (every warp identically), w = p - (t K / 2) v; B -= v w^T + w v^T
+    double kp = 0.0;
+    for (int i = lane; i < m; i += 32) kp += p[i] * v[i];
+    kp = wsum(kp);
+    const double hk = 0.5 * t * kp;
+    if (warp == 0) {
+      // pivot column (column 0 of B, all rows), then the next reflector from it
+      const double w0 = p[0] - hk * v[0];
+      for (int i = lane; i < m; i += 32) {
+        const double wi = p[i] - hk * v[i];
+        B[i] -= v[i] * w0 + wi * v[0];
+      }
+      __syncwarp();
+      if (k + 3 < n) householder_col(A, n, k + 1, vn, d, e, tau, lane);
+    } else {
+      // columns 1..m-1, rows 1..m-1 (row 0 of B is never read again)
+      double vi[4], wi[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = 1 + lane + 32 * r;
+        vi[r] = (i < m) ? v[i] : 0.0;
+        wi[r] = (i < m) ? p[i] - hk * v[i] : 0.0;
+      }
+      for (int j = warp; j < m; j += nw - 1) {
+        const double vj = v[j], wj = p[j] - hk * v[j];
+        double* col = B + j * n;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = 1 + lane + 32 * r;
+          if (i < m) col[i] -= vi[r] * wj + wi[r] * vj;
         }
       }
-      __syncthreads();
-      double kp = 0.0;
-      for (int i = tid; i < m; i += blockDim.x) kp += p[i] * v[i];
-      const double K = bsum(kp, red);
-      if (tid == 0) s_K = 0.5 * t * K;
-      __syncthreads();
-      const double hk = s_K;
-      for (int i = tid; i < m; i += blockDim.x) p[i] -= hk * v[i];   // p becomes w
-      __syncthreads();
-      {
-        const int lane = tid & 31, wp = tid >> 5, nw = blockDim.x >> 5;
-        for (int j = wp; j < m; j += nw) {
-          double* colB = A + (k + 1 + j) * n + (k + 1);
-          const double vj = v[j], pj = p[j];
-          for (int i = lane; i < m; i += 32) colB[i] -= v[i] * pj + p[i] * vj;
-        }
-      }
-      __syncthreads();
     }
-    // keep the reflector (v[1:]) in the now-unused column below the subdiagonal
-    for (int i = 1 + tid; i < m; i += blockDim.x) A[k * n + k + 1 + i] = v[i];
     __syncthreads();
   }
   if (tid == 0) {
@@ -169,33 +222,52 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
     ws[n + i] = e[i];
     ws[2 * n + i] = tau[i];
   }
-  __syncthreads();
-  // Gershgorin interval
-  __shared__ double s_lo, s_hi;
-  if (tid == 0) {
+  if (warp == 0) {   // Gershgorin interval
     double lo = 1e300, hi = -1e300;
-    for (int i = 0; i < n; ++i) {
+    for (int i = lane; i < n; i += 32) {
       const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
       lo = fmin(lo, d[i] - r);
       hi = fmax(hi, d[i] + r);
     }
-    const double pad = 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300;
-    s_lo = lo - pad;
-    s_hi = hi + pad;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(FULL, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(FULL, hi, o));
+    }
+    if (lane == 0) {
+      const double pad = 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300;
+      s_lo = lo - pad;
+      s_hi = hi + pad;
+    }
   }
   __syncthreads();
+  // trisection: threads 2i and 2i+1 count at the two interior points of eigenvalue i's interval
   const double tn = fmax(fabs(s_lo), fabs(s_hi));
-  double* W = base + tk.w_off;
-  for (int i = tid; i < n; i += blockDim.x) {       // i-th largest = (n-1-i)-th smallest
-    const int target = n - 1 - i;
-    double a = s_lo, b = s_hi;
-    for (int it = 0; it < 128; ++it) {
-      const double mid = 0.5 * (a + b);
-      if (b - a <= 8.9e-16 * tn || mid == a || mid == b) break;   // converged / no progress
-      if (sturm_below(d, e2, n, mid) > target) b = mid; else a = mid;
+  const double tol = 8.9e-16 * tn;
+  const int ei = tid >> 1, h = tid & 1;
+  const int target = n - 1 - ei;           // i-th largest = (n-1-i)-th smallest
+  bool done = ei >= n;
+  double a = s_lo, b = s_hi;
+  for (int it = 0; it < 200; ++it) {       // width / 3 per step: ~32 steps
+    if (__all_sync(FULL, done)) break;
+    double x0 = 0.0, x1 = 0.0;
+    bool below = false;
+    if (!done) {
+      const double w = b - a;
+      x0 = a + w * (1.0 / 3.0);
+      x1 = a + w * (2.0 / 3.0);
+      if (w <= tol || !(a < x0 && x0 < x1 && x1 < b)) done = true;   // converged / no progress
+      else below = sturm_below(d, e2, n, h ? x1 : x0) > target;
     }
-    W[i] = 0.5 * (a + b);
+    const bool other = __shfl_xor_sync(FULL, below, 1);
+    if (!done) {
+      const bool r0 = h ? other : below, r1 = h ? below : other;
+      if (r0) b = x0;
+      else if (r1) { a = x0; b = x1; }
+      else a = x1;
+    }
   }
+  if (h == 0 && ei < n) base[tk.w_off + ei] = 0.5 * (a + b);
 }
 
 // pseudo-random start vector entry (fixed: results are reproducible)
@@ -205,194 +277,411 @@ __device__ __forceinline__ double prand(int i, int j) {
   return (double(h) / 4294967296.0) - 0.5;
 }
 
-// One thread: z <- (T - lam I)^{-1} z three times with re-orthogonalisation against Zc columns
-// [c0, col) (a cluster), using partial-pivoting LU held in local arrays.
-__device__ void inverse_iteration(const double* d, const double* e, int n, double lam,
-                                  double* Z, int col, int c0, double tn) {
-  constexpr int NM = SYEVT_NMAX;
-  double u0[NM], u1[NM], u2[NM], l[NM];
-  int piv[NM];
-  // factor (T - lam I) = P L U with U having two superdiagonals
-  double pert = 2.2e-16 * tn;
+// block-wide sum; red has >= 32 entries; all threads get the result
+__device__ double bsum(double v, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = wsum(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int i = 0; i < nw; ++i) t += red[i];
+  return t;
+}
+
+// LU factors of one solver thread in shared memory: element k at [k * stride] (threads
+// interleaved, so that neighbouring threads touch neighbouring words).
+struct LUSlot {
+  double *u0, *u1, *u2, *l;
+  int* piv;
+  int stride;
+};
+
+// One thread: z <- (T - lam I)^{-1} z three times, z = column col of the row-major Z (leading
+// dimension ldz). The solves run in groups of 8 steps whose loads are issued first, so that only
+// the arithmetic recurrence is on the dependent chain.
+__device__ void inverse_iteration(const double* __restrict__ d, const double* __restrict__ e, int n,
+                                  double lam, double* Z, int ldz, int col, double tn, LUSlot f) {
+  const int S = f.stride;
+  // factor (T - lam I) = P L U with U having two superdiagonals; u0 keeps reciprocal pivots
+  const double pert = 2.2e-16 * tn;
   double dk = d[0] - lam, ek = n > 1 ? e[0] : 0.0;
-  for (int k = 0; k < n; ++k) {
-    if (k == n - 1) {
-      u0[k] = dk; u1[k] = 0.0; u2[k] = 0.0; piv[k] = 0;
-      break;
-    }
+  for (int k = 0; k + 1 < n; ++k) {
     const double sub = e[k];                  // T(k+1, k)
     const double dn = d[k + 1] - lam;
     const double en = (k + 2 < n) ? e[k + 1] : 0.0;
     if (fabs(dk) >= fabs(sub)) {              // no swap
-      const double piv_v = (dk == 0.0) ? pert : dk;
-      u0[k] = piv_v; u1[k] = ek; u2[k] = 0.0; piv[k] = 0;
-      l[k] = sub / piv_v;
-      dk = dn - l[k] * ek;
+      const double r = 1.0 / ((dk == 0.0) ? pert : dk);
+      const double lk = sub * r;
+      f.u0[k * S] = r; f.u1[k * S] = ek; f.u2[k * S] = 0.0; f.piv[k * S] = 0; f.l[k * S] = lk;
+      dk = dn - lk * ek;
       ek = en;
     } else {                                  // swap rows k and k+1
-      u0[k] = sub; u1[k] = dn; u2[k] = en; piv[k] = 1;
-      l[k] = dk / sub;
-      dk = ek - l[k] * dn;
-      ek = -l[k] * en;
+      const double r = 1.0 / sub;
+      const double lk = dk * r;
+      f.u0[k * S] = r; f.u1[k * S] = dn; f.u2[k * S] = en; f.piv[k * S] = 1; f.l[k * S] = lk;
+      dk = ek - lk * dn;
+      ek = -lk * en;
     }
   }
-  if (u0[n - 1] == 0.0) u0[n - 1] = pert;
-  for (int k = 0; k < n; ++k) u0[k] = 1.0 / u0[k];   // store reciprocals: the solves multiply
-  double* z = Z + int64_t(col) * n;
+  f.u0[(n - 1) * S] = 1.0 / ((dk == 0.0) ? pert : dk);
+  f.u1[(n - 1) * S] = 0.0; f.u2[(n - 1) * S] = 0.0; f.piv[(n - 1) * S] = 0;
+  double* z = Z + col;                        // z[r] at z[r * ldz]
   for (int it = 0; it < 3; ++it) {
-    // solve P L y = z
-    for (int k = 0; k + 1 < n; ++k) {
-      if (piv[k]) { const double t = z[k]; z[k] = z[k + 1]; z[k + 1] = t; }
-      z[k + 1] -= l[k] * z[k];
+    // solve P L y = z; z[k] is carried in a register. Loads of a group precede its stores, and
+    // every store goes below the indices still to be loaded.
+    double zk = z[0];
+    int k = 0;
+    for (; k + 8 < n; k += 8) {
+      double zz[8], ll[8];
+      int pp[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        zz[q] = z[(k + 1 + q) * ldz];
+        ll[q] = f.l[(k + q) * S];
+        pp[q] = f.piv[(k + q) * S];
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        double zn = zz[q];
+        if (pp[q]) { const double tt = zk; zk = zn; zn = tt; }
+        zn -= ll[q] * zk;
+        z[(k + q) * ldz] = zk;
+        zk = zn;
+      }
     }
-    // solve U x = y
-    for (int k = n - 1; k >= 0; --k) {
-      double s = z[k];
-      if (k + 1 < n) s -= u1[k] * z[k + 1];
-      if (k + 2 < n) s -= u2[k] * z[k + 2];
-      z[k] = s * u0[k];
+    for (; k + 1 < n; ++k) {
+      double zn = z[(k + 1) * ldz];
+      if (f.piv[k * S]) { const double tt = zk; zk = zn; zn = tt; }
+      zn -= f.l[k * S] * zk;
+      z[k * ldz] = zk;
+      zk = zn;
     }
-    for (int c = c0; c < col; ++c) {          // cluster re-orthogonalisation
-      const double* y = Z + int64_t(c) * n;
-      double dot = 0.0;
-      for (int i = 0; i < n; ++i) dot += y[i] * z[i];
-      for (int i = 0; i < n; ++i) z[i] -= dot * y[i];
+    z[(n - 1) * ldz] = zk;
+    // solve U x = y (x[k+1], x[k+2] carried in registers)
+    double x1 = 0.0, x2 = 0.0;
+    k = n - 1;
+    for (; k >= 7; k -= 8) {
+      double zz[8], a0[8], a1[8], a2[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        zz[q] = z[(k - q) * ldz];
+        a0[q] = f.u0[(k - q) * S];
+        a1[q] = f.u1[(k - q) * S];
+        a2[q] = f.u2[(k - q) * S];
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double xk = (zz[q] - a1[q] * x1 - a2[q] * x2) * a0[q];
+        z[(k - q) * ldz] = xk;
+        x2 = x1;
+        x1 = xk;
+      }
     }
-    double nr = 0.0;
-    for (int i = 0; i < n; ++i) nr += z[i] * z[i];
-    nr = sqrt(nr);
-    if (nr == 0.0) { for (int i = 0; i < n; ++i) z[i] = prand(i, col + 7 * it); continue; }
-    for (int i = 0; i < n; ++i) z[i] /= nr;
+    for (; k >= 0; --k) {
+      const double xk = (z[k * ldz] - f.u1[k * S] * x1 - f.u2[k * S] * x2) * f.u0[k * S];
+      z[k * ldz] = xk;
+      x2 = x1;
+      x1 = xk;
+    }
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int i = 0;
+    for (; i + 4 <= n; i += 4) {
+      s0 += z[i * ldz] * z[i * ldz];
+      s1 += z[(i + 1) * ldz] * z[(i + 1) * ldz];
+      s2 += z[(i + 2) * ldz] * z[(i + 2) * ldz];
+      s3 += z[(i + 3) * ldz] * z[(i + 3) * ldz];
+    }
+    for (; i < n; ++i) s0 += z[i * ldz] * z[i * ldz];
+    const double nr = sqrt((s0 + s1) + (s2 + s3));
+    if (nr == 0.0) {
+      for (int r = 0; r < n; ++r) z[r * ldz] = prand(r, col + 7 * it);
+      continue;
+    }
+    const double inv = 1.0 / nr;
+    for (int r = 0; r < n; ++r) z[r * ldz] *= inv;
   }
 }
 
-__global__ void __launch_bounds__(TE_THREADS)
-k_trid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks) {
+// Shared-memory layout of k_trid_vectors (doubles first, then ints).
+__host__ __device__ size_t vec_union_doubles(int n, int k, int nslot) {
+  size_t u = size_t(4) * nslot * n;
+  if (size_t(k) * k > u) u = size_t(k) * k;
+  if (size_t(n) * n > u) u = size_t(n) * n;
+  return u;
+}
+__host__ __device__ size_t vec_layout_bytes(int n, int k, int nslot) {
+  const int ldz = k | 1;
+  const int nblk = n >= 3 ? (n - 2 + BT_NB - 1) / BT_NB : 0;
+  const size_t dbl = 2 * size_t(n) + size_t(n) * ldz + size_t(BT_NB) * k + size_t(nblk) * 64 +
+                     8 * 64 + 2 * size_t(k) + vec_union_doubles(n, k, nslot);
+  return sizeof(double) * dbl + sizeof(int) * size_t(nslot) * n + 64;
+}
+
+__global__ void __launch_bounds__(TV_THREADS)
+k_trid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks, int nslot) {
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n, kk = tk.keep;
   if (n <= 0 || kk <= 0) return;
+  const int ldz = kk | 1;                 // odd row stride
+  const int nblk = n >= 3 ? (n - 2 + BT_NB - 1) / BT_NB : 0;
   extern __shared__ double sm[];
-  double* Z = sm;                 // n x kk (columns = vectors of T, then of A)
-  double* d = Z + n * kk;         // n
-  double* e = d + n;              // n
-  double* y = e + n;              // kk (dot products)
-  int* cl = reinterpret_cast<int*>(y + kk);   // cluster start of each kept index
+  double* d = sm;                         // n
+  double* e = d + n;                      // n
+  double* Z = e + n;                      // n x ldz: vector q of row r at Z[r*ldz + q]
+  double* Y = Z + n * ldz;                // BT_NB x kk
+  double* Tb = Y + BT_NB * kk;            // nblk x 64: T factor of each reflector block
+  double* Sw = Tb + nblk * 64;            // 8 warps x 64: reflector Gram entries
+  double* rinv = Sw + 8 * 64;             // kk: 1 / Cholesky pivot
+  double* sq = rinv + kk;                 // kk: sqrt(Cholesky pivot)
+  double* Un = sq + kk;                   // LU factors (nslot threads) | Gram matrix | reflectors
+  int* piv = reinterpret_cast<int*>(Un + vec_union_doubles(n, kk, nslot));
   __shared__ double red[32];
   __shared__ double s_tn;
-  const int tid = threadIdx.x;
+  __shared__ int s_flag, s_need2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double* ws = base + tk.ws_off;
   const double* W = base + tk.w_off;
+  const double* Ag = base + tk.a_off;
+  const double* tau = ws + 2 * n;
   for (int i = tid; i < n; i += blockDim.x) { d[i] = ws[i]; e[i] = ws[n + i]; }
-  if (tid == 0) {
+  if (warp == 0) {
     double tn = 0.0;
-    for (int i = 0; i < n; ++i) tn = fmax(tn, fabs(W[i]));
-    s_tn = fmax(tn, 1e-300);
-    // clusters among the kept eigenvalues (descending): gap <= 1e-10 ||T||
-    int c0 = 0;
-    cl[0] = 0;
-    for (int i = 1; i < kk; ++i) {
-      if (W[i - 1] - W[i] > 1e-10 * s_tn) c0 = i;
-      cl[i] = c0;
+    for (int i = lane; i < n; i += 32) tn = fmax(tn, fabs(W[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tn = fmax(tn, __shfl_xor_sync(FULL, tn, o));
+    if (lane == 0) {
+      s_tn = fmax(tn, 1e-300);
+      s_flag = 0;
+      s_need2 = 0;
     }
   }
   __syncthreads();
   const double tn = s_tn;
-  // each cluster is handled by the thread of its first member, members in order
-  for (int i = tid; i < kk; i += blockDim.x) {
-    if (cl[i] != i) continue;
-    int j = i;
-    while (j < kk && cl[j] == i) {
-      double* z = Z + int64_t(j) * n;
-      for (int r = 0; r < n; ++r) z[r] = prand(r, j);
-      if (W[j] > 1e-13 * tn) inverse_iteration(d, e, n, W[j], Z, j, i, tn);
-      ++j;
+  // ---- inverse iteration: one thread per kept vector, nslot vectors at a time. Vectors of
+  // (nearly) equal eigenvalues come out as independent vectors of their common eigenspace and
+  // are separated by the orthogonalisation below.
+  for (int b0 = 0; b0 < kk; b0 += nslot) {
+    const int j = b0 + tid;
+    if (tid < nslot && j < kk) {
+      LUSlot f{Un + tid, Un + int64_t(nslot) * n + tid, Un + int64_t(2) * nslot * n + tid,
+               Un + int64_t(3) * nslot * n + tid, piv + tid, nslot};
+      for (int r = 0; r < n; ++r) Z[r * ldz + j] = prand(r, j);
+      if (W[j] > 1e-13 * tn) inverse_iteration(d, e, n, W[j], Z, ldz, j, tn, f);
     }
+    __syncthreads();
+  }
+  // ---- Cholesky QR: G = Z^T Z = R^T R, Z <- Z R^{-1}; a second pass when G was not already
+  // within 1e-3/k of the identity
+  double* G = Un;                         // kk x kk row-major, upper triangle
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int x = tid; x < kk * kk; x += blockDim.x) {
+      const int p = x / kk, q = x - p * kk;
+      if (p > q) continue;
+      double s0 = 0.0, s1 = 0.0;
+      int r = 0;
+      for (; r + 2 <= n; r += 2) {
+        s0 += Z[r * ldz + p] * Z[r * ldz + q];
+        s1 += Z[(r + 1) * ldz + p] * Z[(r + 1) * ldz + q];
+      }
+      if (r < n) s0 += Z[r * ldz + p] * Z[r * ldz + q];
+      const double g = s0 + s1;
+      G[p * kk + q] = g;
+      if (pass == 0 && fabs(g - (p == q ? 1.0 : 0.0)) > 1e-3 / kk) s_need2 = 1;
+    }
+    __syncthreads();
+    for (int j = 0; j < kk; ++j) {        // outer-product elimination, row j is read-only here
+      const double gjj = G[j * kk + j];
+      if (!(gjj > 1e-8) && tid == 0) s_flag = 1;   // nearly dependent: Gram-Schmidt instead
+      const double inv = 1.0 / fmax(gjj, 1e-300);
+      const int t = kk - j - 1;
+      for (int x = tid; x < t * t; x += blockDim.x) {
+        const int p = j + 1 + x / t, q = j + 1 + x % t;
+        if (p <= q) G[p * kk + q] -= G[j * kk + p] * G[j * kk + q] * inv;
+      }
+      __syncthreads();
+    }
+    for (int q = tid; q < kk; q += blockDim.x) {
+      const double g = fmax(G[q * kk + q], 1e-300);
+      rinv[q] = 1.0 / g;
+      sq[q] = sqrt(g);
+    }
+    __syncthreads();
+    if (s_flag) break;
+    for (int r = tid; r < n; r += blockDim.x) {   // row r: y R' = z with y_q = x_q / sqrt(g_q)
+      double* zr = Z + r * ldz;
+      for (int q = 0; q < kk; ++q) {
+        double s0 = zr[q], s1 = 0.0;
+        int p = 0;
+        for (; p + 2 <= q; p += 2) {
+          s0 -= zr[p] * G[p * kk + q];
+          s1 -= zr[p + 1] * G[(p + 1) * kk + q];
+        }
+        if (p < q) s0 -= zr[p] * G[p * kk + q];
+        zr[q] = (s0 + s1) * rinv[q];
+      }
+      for (int q = 0; q < kk; ++q) zr[q] *= sq[q];
+    }
+    __syncthreads();
+    if (!s_need2) break;
+  }
+  if (s_flag) {
+    // two passes of classical Gram-Schmidt, largest eigenvalue first, with fresh starts for
+    // vectors that lie (numerically) in the span of the previous ones
+    int attempt = 0;
+    for (int c = 0; c < kk; ++c) {
+      for (int pass = 0; pass < 2; ++pass) {
+        {
+          const int g8 = tid >> 3, l8 = tid & 7, ng8 = blockDim.x >> 3;
+          for (int qb = 0; qb < c; qb += ng8) {   // uniform trip count: shuffles stay convergent
+            const int q = qb + g8;
+            double s = 0.0;
+            if (q < c)
+              for (int r = l8; r < n; r += 8) s += Z[r * ldz + q] * Z[r * ldz + c];
+            s += __shfl_xor_sync(FULL, s, 4, 8);
+            s += __shfl_xor_sync(FULL, s, 2, 8);
+            s += __shfl_xor_sync(FULL, s, 1, 8);
+            if (q < c && l8 == 0) Y[q] = s;
+          }
+        }
+        __syncthreads();
+        for (int r = tid; r < n; r += blockDim.x) {
+          double s = Z[r * ldz + c];
+          for (int q = 0; q < c; ++q) s -= Y[q] * Z[r * ldz + q];
+          Z[r * ldz + c] = s;
+        }
+        __syncthreads();
+      }
+      double part = 0.0;
+      for (int r = tid; r < n; r += blockDim.x) part += Z[r * ldz + c] * Z[r * ldz + c];
+      const double nr = sqrt(bsum(part, red));
+      if (nr < 1e-8 && attempt < 8) {   // block-wide value: every thread takes the same branch
+        ++attempt;
+        for (int r = tid; r < n; r += blockDim.x) Z[r * ldz + c] = prand(r, c + 1000 * attempt);
+        __syncthreads();
+        --c;
+        continue;
+      }
+      attempt = 0;
+      for (int r = tid; r < n; r += blockDim.x) Z[r * ldz + c] /= fmax(nr, 1e-300);
+      __syncthreads();
+    }
+  }
+  // ---- back-transformation U = H_0 H_1 ... H_{n-3} Z in blocks of BT_NB reflectors:
+  // H_k0 ... H_k0+nb-1 = I - V T V^T (T upper triangular, forward order). The reflectors are
+  // staged in shared memory (column k holds v_k below its implicit unit entry at row k+1).
+  double* V = Un;
+  for (int x = tid; x < n * n; x += blockDim.x) V[x] = Ag[x];
+  __syncthreads();
+  for (int bb = warp; bb < nblk; bb += 8) {
+    const int k0 = bb * BT_NB, nb = min(BT_NB, n - 2 - k0);
+    double* S = Sw + warp * 64;
+    if (lane < 28) {                      // S[c][i] = v_c . v_i, c < i
+      int c = 0, i = 0, x = lane;
+      for (int cc = 0; cc < BT_NB; ++cc) {
+        const int cnt = BT_NB - 1 - cc;
+        if (x < cnt) { c = cc; i = cc + 1 + x; break; }
+        x -= cnt;
+      }
+      if (i < nb) {
+        const int kc = k0 + c, ki = k0 + i;
+        const double* vc = V + kc * n;
+        const double* vi = V + ki * n;
+        double s0 = vc[ki + 1], s1 = 0.0;      // v_i[ki+1] = 1
+        int r = ki + 2;
+        for (; r + 2 <= n; r += 2) { s0 += vc[r] * vi[r]; s1 += vc[r + 1] * vi[r + 1]; }
+        if (r < n) s0 += vc[r] * vi[r];
+        S[c * 8 + i] = s0 + s1;
+      }
+    }
+    __syncwarp();
+    if (lane < nb) {                      // row a of T: T[a][i] = -tau_i sum_{c=a}^{i-1} T[a][c] S[c][i]
+      const int a = lane;
+      double Tr[BT_NB];
+#pragma unroll
+      for (int i = 0; i < BT_NB; ++i) {
+        double v = 0.0;
+        if (i == a) {
+          v = tau[k0 + a];
+        } else if (i > a && i < nb) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < BT_NB; ++c)
+            if (c >= a && c < i) s += Tr[c] * S[c * 8 + i];
+          v = -tau[k0 + i] * s;
+        }
+        Tr[i] = v;
+      }
+#pragma unroll
+      for (int i = 0; i < BT_NB; ++i) Tb[bb * 64 + a * 8 + i] = Tr[i];
+    }
+    __syncwarp();
   }
   __syncthreads();
-  // two passes of classical Gram-Schmidt, largest eigenvalue first
-  int attempt = 0;
-  for (int c = 0; c < kk; ++c) {
-    double* z = Z + int64_t(c) * n;
-    for (int pass = 0; pass < 2; ++pass) {
-      {
-        const int g8 = tid >> 3, l8 = tid & 7, ng8 = blockDim.x >> 3;
-        for (int qb = 0; qb < c; qb += ng8) {     // uniform trip count
-          const int q = qb + g8;
-          double s = 0.0;
-          if (q < c) {
-            const double* zq = Z + int64_t(q) * n;
-            for (int r = l8; r < n; r += 8) s += zq[r] * z[r];
-          }
-          s += __shfl_xor_sync(0xffffffffu, s, 4, 8);
-          s += __shfl_xor_sync(0xffffffffu, s, 2, 8);
-          s += __shfl_xor_sync(0xffffffffu, s, 1, 8);
-          if (q < c && l8 == 0) y[q] = s;
-        }
-      }
-      __syncthreads();
-      for (int r = tid; r < n; r += blockDim.x) {
-        double s = z[r];
-        for (int q = 0; q < c; ++q) s -= y[q] * Z[int64_t(q) * n + r];
-        z[r] = s;
-      }
-      __syncthreads();
-    }
-    double part = 0.0;
-    for (int r = tid; r < n; r += blockDim.x) part += z[r] * z[r];
-    const double nr = sqrt(bsum(part, red));
-    if (nr < 1e-8 && attempt < 8) {   // (numerically) in the span already: another start
-      ++attempt;
-      for (int r = tid; r < n; r += blockDim.x) z[r] = prand(r, c + 1000 * attempt);
-      __syncthreads();
-      --c;   // redo this column (every thread takes the same branch: nr is block-wide)
-      continue;
-    }
-    attempt = 0;
-    for (int r = tid; r < n; r += blockDim.x) z[r] /= fmax(nr, 1e-300);
-    __syncthreads();
-  }
-  // back-transformation with the reflectors H_k = I - tau_k v_k v_k^T (rows k+1..n-1)
-  const double* Ag = base + tk.a_off;
-  const double* tau = ws + 2 * n;
-  for (int k = n - 3; k >= 0; --k) {
-    const double t = tau[k];
-    if (t == 0.0) continue;
-    const int m = n - k - 1;
-    const double* vk = Ag + k * n + k + 1;    // vk[0] = 1 implicitly
-    const int lane = tid & 31, wp = tid >> 5, nw = blockDim.x >> 5;
-    {
-      const int g8 = tid >> 3, l8 = tid & 7, ng8 = blockDim.x >> 3;
-      for (int qb = 0; qb < kk; qb += ng8) {       // uniform trip count: shuffles stay convergent
+  for (int bb = nblk - 1; bb >= 0; --bb) {
+    const int k0 = bb * BT_NB, nb = min(BT_NB, n - 2 - k0);
+    const double* T = Tb + bb * 64;
+    {   // Y = T (V^T Z): 8-lane groups, lane a = reflector, group = vector q
+      const int g8 = tid >> 3, a = tid & 7, ng8 = blockDim.x >> 3;
+      for (int qb = 0; qb < kk; qb += ng8) {      // uniform trip count: shuffles stay convergent
         const int q = qb + g8;
-        double s = 0.0;
-        if (q < kk) {
-          const double* zq = Z + int64_t(q) * n + k + 1;
-          for (int r = l8; r < m; r += 8) s += (r == 0 ? 1.0 : vk[r]) * zq[r];
+        double y = 0.0;
+        if (q < kk && a < nb) {
+          const int k = k0 + a;
+          const double* vk = V + k * n;
+          double s0 = Z[(k + 1) * ldz + q], s1 = 0.0;
+          int r = k + 2;
+          for (; r + 2 <= n; r += 2) {
+            s0 += vk[r] * Z[r * ldz + q];
+            s1 += vk[r + 1] * Z[(r + 1) * ldz + q];
+          }
+          if (r < n) s0 += vk[r] * Z[r * ldz + q];
+          y = s0 + s1;
         }
-        s += __shfl_xor_sync(0xffffffffu, s, 4, 8);
-        s += __shfl_xor_sync(0xffffffffu, s, 2, 8);
-        s += __shfl_xor_sync(0xffffffffu, s, 1, 8);
-        if (q < kk && l8 == 0) y[q] = t * s;
+        double y2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < BT_NB; ++c) {
+          const double yc = __shfl_sync(FULL, y, c, 8);
+          if (c >= a && c < nb) y2 += T[a * 8 + c] * yc;
+        }
+        if (q < kk && a < nb) Y[a * kk + q] = y2;
       }
     }
     __syncthreads();
-    for (int q = wp; q < kk; q += nw) {
-      double* zq = Z + int64_t(q) * n + k + 1;
-      const double yq = y[q];
-      for (int r = lane; r < m; r += 32) zq[r] -= (r == 0 ? 1.0 : vk[r]) * yq;
+    const int r0 = k0 + 1, nr = n - r0;         // Z -= V Y on rows r0..n-1
+    for (int x = tid; x < nr * kk; x += blockDim.x) {
+      const int rr = x / kk, q = x - rr * kk, r = r0 + rr;
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < BT_NB; ++a) {
+        if (a < nb) {
+          const int k = k0 + a;
+          const double va = (r == k + 1) ? 1.0 : (r > k + 1 ? V[k * n + r] : 0.0);
+          s += va * Y[a * kk + q];
+        }
+      }
+      Z[r * ldz + q] -= s;
     }
     __syncthreads();
   }
   double* U = base + tk.u_off;
-  for (int x = tid; x < n * kk; x += blockDim.x) U[x] = Z[x];
+  for (int x = tid; x < n * kk; x += blockDim.x) {
+    const int q = x / n, r = x - q * n;
+    U[x] = Z[r * ldz + q];
+  }
+}
+
+int vec_slots(int max_n, int max_k) {
+  int nslot = max_k;
+  while (nslot > 1 && vec_layout_bytes(max_n, max_k, nslot) > SMEM_LIMIT) --nslot;
+  return nslot;
 }
 
 }  // namespace
 
 size_t syevt_smem_vals(int n) { return sizeof(double) * (size_t(n) * n + 7 * size_t(n)) + 64; }
-size_t syevt_smem_vecs(int n, int k) {
-  return sizeof(double) * (size_t(n) * k + 2 * size_t(n) + k) + sizeof(int) * size_t(k) + 64;
-}
+size_t syevt_smem_vecs(int n, int k) { return vec_layout_bytes(n, k, vec_slots(n, k)); }
 
 void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks, int max_n) {
   if (ntasks <= 0) return;
@@ -405,9 +694,10 @@ void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, in
 void launch_trid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
                          int max_n, int max_k) {
   if (ntasks <= 0) return;
-  const size_t sm = syevt_smem_vecs(max_n, max_k);
+  const int nslot = vec_slots(max_n, max_k);
+  const size_t sm = vec_layout_bytes(max_n, max_k, nslot);
   cudaFuncSetAttribute(k_trid_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-  k_trid_vectors<<<ntasks, TE_THREADS, sm, s>>>(base, tasks);
+  k_trid_vectors<<<ntasks, TV_THREADS, sm, s>>>(base, tasks, nslot);
   count_launch();
 }
 
