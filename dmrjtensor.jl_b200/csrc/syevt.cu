@@ -30,6 +30,7 @@ namespace dmrg {
 namespace {
 
 constexpr int TE_THREADS = 256;   // 8 warps; two threads per row / per eigenvalue (n <= 128)
+static_assert(TE_THREADS == 256, "the Householder step sums exactly 8 per-warp shares");
 constexpr int TV_THREADS = 256;
 constexpr int BT_NB = 8;          // reflectors per back-transformation block
 constexpr unsigned FULL = 0xffffffffu;
@@ -41,8 +42,8 @@ __device__ __forceinline__ double wsum(double v) {
   return v;
 }
 
-// Scales the pair (D, Dm1) by the power of two that brings the larger magnitude into [1, 2):
-// exact, keeps the signs, and needs only exponent-field arithmetic.
+// Scales a pair by the power of two that brings the larger magnitude into [1, 2): exact, keeps
+// the signs, and needs only exponent-field arithmetic.
 __device__ __forceinline__ void rescale_pair(double& D, double& Dm1) {
   const double mx = fmax(fabs(D), fabs(Dm1));
   const int fld = (__double2hiint(mx) >> 20) & 0x7ff;
@@ -54,39 +55,49 @@ __device__ __forceinline__ void rescale_pair(double& D, double& Dm1) {
   }
 }
 
-// One step of the Sturm sequence: D_j = (d_j - x) D_{j-1} - e_{j-1}^2 D_{j-2}. Only the FMA is
-// on the dependent chain (the product with D_{j-2} is available a step earlier). An exact zero
-// minor counts with the sign opposite to its predecessor.
-__device__ __forceinline__ void sturm_step(double dx, double ee, double& D, double& Dm1, bool& neg,
-                                           int& c) {
-  const double Dn = fma(dx, D, -ee * Dm1);
-  const bool ng = (Dn == 0.0) ? !neg : (Dn < 0.0);
-  c += (ng != neg) ? 1 : 0;
-  neg = ng;
-  Dm1 = D;
-  D = Dn;
-}
-
-// Number of eigenvalues of T(d,e) strictly below x (sign changes of the leading minors).
-// Unrolled by 8 with the loads of each group issued first, then one exact rescale per group.
+// Number of eigenvalues of T(d,e) strictly below x: sign changes of the leading minors
+// D_j = (d_j - x) D_{j-1} - e_{j-1}^2 D_{j-2}. The carried pair is (D_{j-1}, t_j) with
+// t_j = -e_{j-1}^2 D_{j-2}: each step is one FMA for D_j and one product t_{j+1} from D_{j-1}, two
+// independent operations, so only the FMA is on the dependent chain. Groups of 8 steps load
+// first, count signs after the group (an exact zero minor counts with the sign opposite to its
+// predecessor), then rescale the pair by a power of two.
 __device__ int sturm_below(const double* __restrict__ d, const double* __restrict__ e2, int n,
                            double x) {
-  double Dm1 = 1.0, D = d[0] - x;
+  double D = d[0] - x;
+  double t = -e2[0];                      // t_1 = -e_0^2 D_{-1}, D_{-1} = 1
   bool neg = D < 0.0;
   int c = neg ? 1 : 0;
   int j = 1;
   for (; j + 8 <= n; j += 8) {
-    double dx[8], ee[8];
+    double dx[8], ee[8], Ds[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       dx[q] = d[j + q] - x;
-      ee[q] = e2[j + q - 1];
+      ee[q] = e2[j + q];                  // e2[n-1] = 0: the last product is unused
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) sturm_step(dx[q], ee[q], D, Dm1, neg, c);
-    rescale_pair(D, Dm1);
+    for (int q = 0; q < 8; ++q) {
+      const double Dn = fma(dx[q], D, t);
+      t = -ee[q] * D;
+      D = Dn;
+      Ds[q] = Dn;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const bool ng = (Ds[q] == 0.0) ? !neg : (Ds[q] < 0.0);
+      c += (ng != neg) ? 1 : 0;
+      neg = ng;
+    }
+    rescale_pair(D, t);
   }
-  for (; j < n; ++j) sturm_step(d[j] - x, e2[j - 1], D, Dm1, neg, c);
+  for (; j < n; ++j) {
+    const double Dn = fma(d[j] - x, D, t);
+    t = -e2[j] * D;
+    D = Dn;
+    const bool ng = (Dn == 0.0) ? !neg : (Dn < 0.0);
+    c += (ng != neg) ? 1 : 0;
+    neg = ng;
+  }
   return c;
 }
 
@@ -135,6 +146,7 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
   double* e2 = e + n;           // n
   double* tau = e2 + n;         // n
   __shared__ double s_lo, s_hi;
+  __shared__ double kw[TE_THREADS / 32];   // per-warp shares of K
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   double* Ag = base + tk.a_off;
   for (int x = tid; x < n * n; x += blockDim.x) A[x] = Ag[x];
@@ -147,7 +159,8 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
     double* vn = vb + ((k + 1) & 1) * n;
     const double t = tau[k];
     double* B = A + (k + 1) * n + (k + 1);     // trailing matrix B[i + j*n], i, j < m
-    {   // p = t B v: two threads per row (row i, half h of the columns), rows of B contiguous
+    {   // p = t B v: two threads per row (row i, half h of the columns; rows of B are read along
+        // consecutive i, conflict-free), and this warp's share of K = p.v
       const int i = warp * 16 + (lane >> 1), h = lane & 1;
       const int jh = (m + 1) >> 1;
       const int j0 = h ? jh : 0, j1 = h ? m : jh;
@@ -155,35 +168,85 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
       if (i < m) {
         const double* Bi = B + i;
         int j = j0;
-        for (; j + 4 <= j1; j += 4) {
-          s0 += Bi[j * n] * v[j];
-          s1 += Bi[(j + 1) * n] * v[j + 1];
-          s2 += Bi[(j + 2) * n] * v[j + 2];
-          s3 += Bi[(j + 3) * n] * v[j + 3];
+        for (; j + 8 <= j1; j += 8) {
+          double bb[8], ww[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) { bb[q] = Bi[(j + q) * n]; ww[q] = v[j + q]; }
+          s0 += bb[0] * ww[0]; s1 += bb[1] * ww[1]; s2 += bb[2] * ww[2]; s3 += bb[3] * ww[3];
+          s0 += bb[4] * ww[4]; s1 += bb[5] * ww[5]; s2 += bb[6] * ww[6]; s3 += bb[7] * ww[7];
         }
         for (; j < j1; ++j) s0 += Bi[j * n] * v[j];
       }
-      double s = (s0 + s1) + (s2 + s3);
-      s += __shfl_xor_sync(FULL, s, 1);
-      if (i < m && h == 0) p[i] = t * s;
+      double sv = (s0 + s1) + (s2 + s3);
+      sv += __shfl_xor_sync(FULL, sv, 1);
+      double kpart = 0.0;
+      if (i < m && h == 0) {
+        const double pi = t * sv;
+        p[i] = pi;
+        kpart = pi * v[i];
+      }
+      kpart = wsum(kpart);
+      if (lane == 0) kw[warp] = kpart;
     }
     __syncthreads();
-    // K = p.v (every warp identically), w = p - (t K / 2) v; B -= v w^T + w v^T
-    double kp = 0.0;
-    for (int i = lane; i < m; i += 32) kp += p[i] * v[i];
-    kp = wsum(kp);
-    const double hk = 0.5 * t * kp;
+    // K = p.v, w = p - (t K / 2) v; B -= v w^T + w v^T
+    const double K = ((kw[0] + kw[1]) + (kw[2] + kw[3])) + ((kw[4] + kw[5]) + (kw[6] + kw[7]));
+    const double hk = 0.5 * t * K;
     if (warp == 0) {
-      // pivot column (column 0 of B, all rows), then the next reflector from it
-      const double w0 = p[0] - hk * v[0];
-      for (int i = lane; i < m; i += 32) {
-        const double wi = p[i] - hk * v[i];
-        B[i] -= v[i] * w0 + wi * v[0];
+      // pivot column (column 0 of B, all rows; c[r] = its row lane + 32 r), then the next
+      // reflector from it, without a round trip through shared memory
+      const double v0 = v[0];
+      const double w0 = p[0] - hk * v0;
+      double c[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = lane + 32 * r;
+        double vi = 0.0, pi = 0.0, bi = 0.0;
+        if (i < m) { vi = v[i]; pi = p[i]; bi = B[i]; }
+        const double wi = pi - hk * vi;
+        c[r] = bi - (vi * w0 + wi * v0);
       }
-      __syncwarp();
-      if (k + 3 < n) householder_col(A, n, k + 1, vn, d, e, tau, lane);
+      if (k + 3 < n) {
+        // column k+1 of A: d[k+1] = c(0), alpha = c(1), x tail = c(2..m-1)
+        double part = 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = lane + 32 * r;
+          if (i >= 2 && i < m) part += c[r] * c[r];
+        }
+        const double xn2 = wsum(part);
+        const double alpha = __shfl_sync(FULL, c[0], 1);
+        double tn, sc, beta;
+        if (xn2 == 0.0) {
+          tn = 0.0; sc = 0.0; beta = alpha;
+        } else {
+          beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+          tn = (beta - alpha) / beta;
+          sc = 1.0 / (alpha - beta);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = lane + 32 * r;
+          if (i >= 1 && i < m) {
+            const double vi = (i == 1) ? 1.0 : c[r] * sc;
+            vn[i - 1] = vi;
+            if (i >= 2) B[i] = vi;             // reflector tail, below the subdiagonal
+          }
+        }
+        if (lane == 0) {
+          d[k + 1] = c[0];
+          e[k + 1] = beta;
+          tau[k + 1] = tn;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = lane + 32 * r;
+          if (i < m) B[i] = c[r];
+        }
+      }
     } else {
-      // columns 1..m-1, rows 1..m-1 (row 0 of B is never read again)
+      // columns 1..m-1, rows 1..m-1 (row 0 of B is never read again), two columns at a time
       double vi[4], wi[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -191,13 +254,29 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
         vi[r] = (i < m) ? v[i] : 0.0;
         wi[r] = (i < m) ? p[i] - hk * v[i] : 0.0;
       }
-      for (int j = warp; j < m; j += nw - 1) {
-        const double vj = v[j], wj = p[j] - hk * v[j];
+      const int ow = nw - 1;
+      for (int j = warp; j < m; j += 2 * ow) {
+        const int j2 = j + ow;
+        const bool two = j2 < m;
+        const double vj = v[j], wj = p[j] - hk * vj;
+        const double vj2 = two ? v[j2] : 0.0;
+        const double wj2 = two ? p[j2] - hk * vj2 : 0.0;
         double* col = B + j * n;
+        double* col2 = B + j2 * n;
+        double b1[4], b2[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
           const int i = 1 + lane + 32 * r;
-          if (i < m) col[i] -= vi[r] * wj + wi[r] * vj;
+          b1[r] = (i < m) ? col[i] : 0.0;
+          b2[r] = (two && i < m) ? col2[i] : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = 1 + lane + 32 * r;
+          if (i < m) {
+            col[i] = b1[r] - (vi[r] * wj + wi[r] * vj);
+            if (two) col2[i] = b2[r] - (vi[r] * wj2 + wi[r] * vj2);
+          }
         }
       }
     }
@@ -630,14 +709,16 @@ k_trid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks, in
         if (q < kk && a < nb) {
           const int k = k0 + a;
           const double* vk = V + k * n;
-          double s0 = Z[(k + 1) * ldz + q], s1 = 0.0;
+          double s0 = Z[(k + 1) * ldz + q], s1 = 0.0, s2 = 0.0, s3 = 0.0;
           int r = k + 2;
-          for (; r + 2 <= n; r += 2) {
-            s0 += vk[r] * Z[r * ldz + q];
-            s1 += vk[r + 1] * Z[(r + 1) * ldz + q];
+          for (; r + 4 <= n; r += 4) {
+            double vv[4], zz[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) { vv[u] = vk[r + u]; zz[u] = Z[(r + u) * ldz + q]; }
+            s0 += vv[0] * zz[0]; s1 += vv[1] * zz[1]; s2 += vv[2] * zz[2]; s3 += vv[3] * zz[3];
           }
-          if (r < n) s0 += vk[r] * Z[r * ldz + q];
-          y = s0 + s1;
+          for (; r < n; ++r) s0 += vk[r] * Z[r * ldz + q];
+          y = (s0 + s1) + (s2 + s3);
         }
         double y2 = 0.0;
 #pragma unroll
@@ -649,19 +730,39 @@ k_trid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks, in
       }
     }
     __syncthreads();
-    const int r0 = k0 + 1, nr = n - r0;         // Z -= V Y on rows r0..n-1
-    for (int x = tid; x < nr * kk; x += blockDim.x) {
-      const int rr = x / kk, q = x - rr * kk, r = r0 + rr;
-      double s = 0.0;
+    // Z -= V Y on rows r0..n-1: a thread owns row r (its reflector entries in registers) and
+    // the vectors q = g, g + G, ... of its group g
+    const int r0 = k0 + 1, nr = n - r0;
+    const int G = max(1, int(blockDim.x) / nr);
+    if (tid < G * nr) {
+      const int g = tid / nr, r = r0 + (tid - g * nr);
+      double va[BT_NB];
 #pragma unroll
       for (int a = 0; a < BT_NB; ++a) {
-        if (a < nb) {
-          const int k = k0 + a;
-          const double va = (r == k + 1) ? 1.0 : (r > k + 1 ? V[k * n + r] : 0.0);
-          s += va * Y[a * kk + q];
-        }
+        const int k = k0 + a;
+        va[a] = (a >= nb) ? 0.0 : (r == k + 1) ? 1.0 : (r > k + 1 ? V[k * n + r] : 0.0);
       }
-      Z[r * ldz + q] -= s;
+      double* zr = Z + r * ldz;
+      int q = g;
+      for (; q + G < kk; q += 2 * G) {
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int a = 0; a < BT_NB; ++a) {
+          if (a < nb) {
+            s0 += va[a] * Y[a * kk + q];
+            s1 += va[a] * Y[a * kk + q + G];
+          }
+        }
+        zr[q] -= s0;
+        zr[q + G] -= s1;
+      }
+      if (q < kk) {
+        double s0 = 0.0;
+#pragma unroll
+        for (int a = 0; a < BT_NB; ++a)
+          if (a < nb) s0 += va[a] * Y[a * kk + q];
+        zr[q] -= s0;
+      }
     }
     __syncthreads();
   }
