@@ -221,8 +221,9 @@ __global__ void k_next_vector(const double* __restrict__ H, double* __restrict__
 }
 
 // Ritz step of the Krylov solve, one warp: T = tridiag(alpha, beta) of the m active vectors
-// (m = 1 + number of leading non-zero beta_j, at most kdim), cyclic Jacobi (same rotation order
-// and thresholds as a serial cyclic Jacobi: lanes own the rows/columns of one rotation), lowest
+// (m = 1 + number of leading non-zero beta_j, at most kdim), cyclic Jacobi (serial rotation
+// order; lanes own the rows/columns of one rotation) until the off-diagonal is at the rounding
+// level of the diagonal, lowest
 // eigenvalue -> s[EN], its eigenvector -> s[COEF + j] (0 for j >= m).
 __global__ void k_ritz(double* s, int kdim) {
   __shared__ double A[MAXK * MAXK], V[MAXK * MAXK];
@@ -240,10 +241,12 @@ __global__ void k_ritz(double* s, int kdim) {
   }
   __syncwarp();
   for (int sweep = 0; sweep < 100; ++sweep) {
-    double off = 0.0;
-    for (int p = 0; p < m; ++p)
+    double off = 0.0, dg = 0.0;
+    for (int p = 0; p < m; ++p) {
+      dg += A[p + p * m] * A[p + p * m];
       for (int q = p + 1; q < m; ++q) off += A[p + q * m] * A[p + q * m];
-    if (off < 1e-300) break;
+    }
+    if (off < 1e-300 || off <= 1e-32 * dg) break;   // off-diagonal at the rounding level
     for (int p = 0; p < m; ++p)
       for (int q = p + 1; q < m; ++q) {
         const double apq = A[p + q * m];
