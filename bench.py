@@ -249,6 +249,47 @@ def oracle_sample(sectors, krylov, nsteps=2, seed=0):
     return t_step, est, desc
 
 
+def run_serving(pkg, device, nreq, rate=20.0, slots=8, seed=5):
+    """Serving workload (transverse-field Ising chains, Poisson arrivals): requests are submitted
+    at their arrival times to a server with `slots` concurrent solves and a 150 GB budget;
+    returns solves/s over the whole run (first arrival to last completion) and the latency
+    percentiles (submit to completion)."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, nreq)
+    hs = rng.uniform(0.5, 1.5, nreq)
+    Ls = rng.choice([16, 32, 64, 128], nreq)
+    ms = rng.choice([64, 128, 256, 512], nreq)
+    reqs = []
+    for h, L, m in zip(hs, Ls, ms):
+        mpo = pkg.makeMPO(pkg.tfiMPO(h=float(h)), 2, int(L))
+        psi = pkg.MPS([np.full((1, 2, 1), 1 / math.sqrt(2)) for _ in range(int(L))], oc=0)
+        reqs.append((psi, mpo, int(m)))
+    lat = []
+    with pkg.Server(device=device, slots=slots, hbm_budget=150 * 10**9) as srv:
+        t0 = time.perf_counter()
+        tick = []
+        arrival = t0
+        for (psi, mpo, m), g in zip(reqs, gaps):
+            arrival += g
+            now = time.perf_counter()
+            if arrival > now:
+                time.sleep(arrival - now)
+            tick.append((srv.submit(psi, mpo, m=m, sweeps=6, cutoff=CUTOFF), time.perf_counter()))
+        for t, ts in tick:
+            st = srv.poll(t, -1)
+            if st["status"] != 2:
+                raise RuntimeError(f"served solve failed: {st}")
+            lat.append(st["queue_seconds"] + st["run_seconds"])
+        t1 = time.perf_counter()
+    lat.sort()
+    pct = lambda q: lat[min(len(lat) - 1, int(math.ceil(q * len(lat))) - 1)]
+    return {"workload": "TFI chains, h~U[0.5,1.5], L in {16,32,64,128}, maxm in {64,128,256,512}, "
+                        "6 sweeps, cutoff 1e-10, |+...+> start, Poisson arrivals",
+            "requests": nreq, "arrival_rate_per_s": rate, "slots": slots,
+            "solves_per_s": nreq / (t1 - t0), "p50_latency_s": pct(0.50),
+            "p99_latency_s": pct(0.99), "mean_latency_s": statistics.mean(lat)}
+
+
 def cpu_threads():
     try:
         import threadpoolctl
@@ -375,6 +416,7 @@ def run_ours(args, world, rank, local, dist):
         e2e = {"value": 1.0 / statistics.mean(e2e_times), "unit": "sweeps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "seconds_per_step": statistics.mean(e2e_times)}
+    serving = run_serving(pkg, local, args.serve_requests) if args.serve_requests > 0 else None
     if rank != 0:
         return
     peak = fp64_gemm_peak(local)
@@ -419,6 +461,7 @@ def run_ours(args, world, rank, local, dist):
         "clocks": clocks,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "serving": serving,
     }
     print(json.dumps(out))
 
@@ -436,6 +479,8 @@ def main():
     ap.add_argument("--dump-sectors", default=None)
     ap.add_argument("--steps-ref", type=int, default=2)
     ap.add_argument("--warmup-ref", type=int, default=1)
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests of the serving measurement (0: skip it)")
     ap.add_argument("--ramp-sweeps", type=int, default=None,
                     help="untimed ramp sweeps before the timed ones (default: the full 11-sweep "
                          "ramp); fewer only for profiler runs")

@@ -10,6 +10,7 @@ from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heise
                      heisenbergMPO, hubbardMPO, makeMPO, spinOps, tfiMPO)
 from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
                     default_context, dmrg, make_params, makeEnv, neelMPS, product_MPS, randMPS)
+from .serving import Server, ServerError
 
 
 
@@ -24,4 +25,5 @@ __all__ = [
     "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
     "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",
     "default_context", "dmrg", "make_params", "makeEnv", "neelMPS", "product_MPS", "randMPS",
+    "Server", "ServerError",
 ]

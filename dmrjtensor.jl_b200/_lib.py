@@ -41,6 +41,33 @@ class SweepStats(C.Structure):
         return d
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("slots", C.c_int), ("hbm_budget_bytes", C.c_size_t),
+                ("reserved", C.c_int * 8)]
+
+
+class Request(C.Structure):
+    _fields_ = [("L", C.c_int), ("nsym", C.c_int),
+                ("d", C.POINTER(C.c_int)), ("wl", C.POINTER(C.c_int)), ("wr", C.POINTER(C.c_int)),
+                ("W", C.POINTER(C.POINTER(C.c_double))), ("phys_qn", C.POINTER(C.POINTER(C.c_int))),
+                ("ml", C.POINTER(C.c_int)), ("mr", C.POINTER(C.c_int)),
+                ("A", C.POINTER(C.POINTER(C.c_double))), ("oc", C.c_int), ("sweeps", C.c_int),
+                ("params", Params)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("error", C.c_int), ("energy", C.c_double),
+                ("max_truncerr", C.c_double), ("entropy", C.c_double), ("biggest_m", C.c_int),
+                ("sweeps_done", C.c_int), ("queue_seconds", C.c_double),
+                ("run_seconds", C.c_double), ("footprint_bytes", C.c_size_t)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class DmrgError(RuntimeError):
     """Raised for every non-zero status returned by the library."""
 
@@ -87,6 +114,13 @@ SIGNATURES = {
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),
     "dmrg_test_svd": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP, _IP]),
     "dmrg_test_syevt": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP]),
+    "dmrg_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_P)]),
+    "dmrg_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "dmrg_server_poll": (C.c_int, [_P, C.c_longlong, C.c_int, C.POINTER(Result)]),
+    "dmrg_server_fetch_site": (C.c_int, [_P, C.c_longlong, C.c_int, _DP, _IP, _IP, _IP, _IP]),
+    "dmrg_server_release": (C.c_int, [_P, C.c_longlong]),
+    "dmrg_server_destroy": (C.c_int, [_P]),
+    "dmrg_server_last_error": (C.c_char_p, [_P]),
 }
 
 _lib = None

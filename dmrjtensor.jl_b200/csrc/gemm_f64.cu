@@ -7,6 +7,9 @@
 // are needed anywhere in the sweep. B200 has no tcgen05 FP64 kind; mma.sync f64 is the FP64
 // tensor-core instruction on sm_100a.
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "kernels.cuh"
 
@@ -167,12 +170,7 @@ template <bool TA, bool TB>
 void launch_variant(cudaStream_t s, const double* A, const double* B, double* C,
                     const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
                     int grid_cap) {
-  static bool configured = false;  // attribute is per device function; idempotent
-  if (!configured) {
-    cudaFuncSetAttribute(k_gemm_f64<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(SMEM_BYTES));
-    configured = true;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_f64<TA, TB>), SMEM_BYTES);
   int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
   k_gemm_f64<TA, TB><<<grid, THREADS, SMEM_BYTES, s>>>(A, B, C, tasks, ntasks, segs, total_tiles);
   count_launch();
@@ -192,6 +190,22 @@ void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, 
     launch_variant<true, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
   else
     launch_variant<true, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+}
+
+// Raises (never lowers) the dynamic shared-memory limit of a kernel on the current device. The
+// limit is a property of the kernel shared by every host thread, so launchers on different
+// threads (one context each) must never lower it below what another thread launches with.
+void raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> cur;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& c = cur[{dev, func}];
+  if (bytes > c &&
+      cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) ==
+          cudaSuccess)
+    c = bytes;
 }
 
 static std::atomic<long long> g_launches{0};

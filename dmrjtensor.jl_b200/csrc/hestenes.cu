@@ -135,7 +135,7 @@ size_t hestenes_smem(int r, int c) {
 void launch_hestenes(cudaStream_t s, double* base, const SvdTask* tasks, int ntasks,
                      size_t smem, int* status) {
   if (ntasks <= 0) return;
-  cudaFuncSetAttribute(k_hestenes, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  raise_smem_limit(reinterpret_cast<const void*>(k_hestenes), smem);
   k_hestenes<<<ntasks, HJ_THREADS, smem, s>>>(base, tasks, status);
   count_launch();
 }

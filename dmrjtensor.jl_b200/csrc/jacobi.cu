@@ -174,7 +174,7 @@ void launch_jacobi(cudaStream_t s, double* base, const EigTask* tasks, int ntask
   if (ntasks <= 0) return;
   const bool small = max_n <= 100;
   const size_t smem = jacobi_smem(max_n, small);
-  cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  raise_smem_limit(reinterpret_cast<const void*>(k_jacobi), smem);
   k_jacobi<<<ntasks, JAC_THREADS, smem, s>>>(base, tasks, small ? 1 : 0, status);
   count_launch();
 }

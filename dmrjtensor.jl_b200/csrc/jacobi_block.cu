@@ -325,12 +325,8 @@ void launch_block_jacobi(cudaStream_t s, double* base, const BlockEigPlan& pl, i
   k_bj_init<<<dim3(64, ng), 256, 0, s>>>(base, pl.groups, ng);
   k_bj_norm<<<ng, 512, 0, s>>>(base, pl.groups, floors_dev);
   count_launch(2);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_bj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(UPD_SMEM));
-    cudaFuncSetAttribute(k_bj_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SOLVE_SMEM));
-    attr = true;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_bj_update), UPD_SMEM);
+  raise_smem_limit(reinterpret_cast<const void*>(k_bj_solve), SOLVE_SMEM);
   const int nbmax = pl.maxN / B;
   int sw = 0;
   for (; sw < pl.max_sweeps; ++sw) {
@@ -351,7 +347,7 @@ void launch_block_jacobi(cudaStream_t s, double* base, const BlockEigPlan& pl, i
   }
   if (sweeps_done) *sweeps_done = sw;
   size_t fs = sizeof(double) * pl.maxn + sizeof(int) * pl.maxn;
-  cudaFuncSetAttribute(k_bj_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fs));
+  raise_smem_limit(reinterpret_cast<const void*>(k_bj_finish), fs);
   k_bj_finish<<<ng, 512, fs, s>>>(base, pl.groups);
   count_launch();
 }

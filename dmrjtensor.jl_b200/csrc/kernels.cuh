@@ -166,6 +166,9 @@ void launch_jacobi(cudaStream_t s, double* base, const EigTask* tasks, int ntask
                    int* status);
 
 int device_sm_count();
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the current device; safe when
+// several host threads launch the same kernel with different sizes.
+void raise_smem_limit(const void* func, size_t bytes);
 // Process-wide count of kernel launches issued by this library.
 void count_launch(int n = 1);
 long long launch_count();

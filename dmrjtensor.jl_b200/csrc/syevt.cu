@@ -787,7 +787,7 @@ size_t syevt_smem_vecs(int n, int k) { return vec_layout_bytes(n, k, vec_slots(n
 void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks, int max_n) {
   if (ntasks <= 0) return;
   const size_t sm = syevt_smem_vals(max_n);
-  cudaFuncSetAttribute(k_trid_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+  raise_smem_limit(reinterpret_cast<const void*>(k_trid_eigvals), sm);
   k_trid_eigvals<<<ntasks, TE_THREADS, sm, s>>>(base, tasks);
   count_launch();
 }
@@ -797,7 +797,7 @@ void launch_trid_vectors(cudaStream_t s, double* base, const TridTask* tasks, in
   if (ntasks <= 0) return;
   const int nslot = vec_slots(max_n, max_k);
   const size_t sm = vec_layout_bytes(max_n, max_k, nslot);
-  cudaFuncSetAttribute(k_trid_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+  raise_smem_limit(reinterpret_cast<const void*>(k_trid_vectors), sm);
   k_trid_vectors<<<ntasks, TV_THREADS, sm, s>>>(base, tasks, nslot);
   count_launch();
 }

@@ -213,6 +213,73 @@ DMRG_API int dmrg_test_syevt(dmrg_ctx* ctx, int nmat, const int* n, const int* k
 /* Fills *p with the reference defaults (minm 2, krylov 2, betatest 1e-10, ...). */
 DMRG_API void dmrg_params_default(dmrg_params* p);
 
+/* ---------------------------------------------------------------- serving
+ * Many independent ground-state solves on one GPU: each request is what one call of
+ * dmrg(psi, mpo; m, minm, sweeps, cutoff) computes (algs/DMRG.jl:549-588), submitted
+ * asynchronously. The server runs up to `slots` solves at once, one host worker thread and one
+ * context (CUDA stream) each, so that the latency-bound bond steps of different solves overlap on
+ * the GPU; a request starts as soon as a slot is free and its worst-case device footprint fits
+ * in what the running solves leave of `hbm_budget_bytes` (continuous admission, first come first
+ * served). A solve's results do not depend on the other solves running beside it. */
+typedef struct dmrg_server dmrg_server;
+
+typedef struct dmrg_server_config {
+  int device;
+  int slots;                 /* concurrent solves, >= 1 */
+  size_t hbm_budget_bytes;   /* 0: no budget (slots alone limit admission) */
+  int reserved[8];
+} dmrg_server_config;
+
+/* One solve. Same arrays and conventions as dmrg_mpo_upload / dmrg_mps_upload (dense-equivalent
+ * column-major tensors, physical charges per site or NULL for nsym = 0, bond labels derived).
+ * The server copies everything during dmrg_server_submit. */
+typedef struct dmrg_request {
+  int L, nsym;
+  const int* d;                      /* [L] physical dimensions */
+  const int* wl; const int* wr;      /* [L] MPO bond dimensions */
+  const double* const* W;            /* [L] MPO sites [wl, d, d, wr] */
+  const int* const* phys_qn;         /* [L] d*nsym charges, or NULL when nsym = 0 */
+  const int* ml; const int* mr;      /* [L] MPS bond dimensions */
+  const double* const* A;            /* [L] MPS sites [ml, d, mr] */
+  int oc;                            /* 0-based orthogonality centre */
+  int sweeps;
+  dmrg_params params;
+} dmrg_request;
+
+enum dmrg_request_status {
+  DMRG_REQ_QUEUED = 0, DMRG_REQ_RUNNING = 1, DMRG_REQ_DONE = 2, DMRG_REQ_FAILED = 3
+};
+
+typedef struct dmrg_result {
+  int status;                 /* enum dmrg_request_status */
+  int error;                  /* dmrg_status of a failed solve */
+  double energy;              /* last bond step of the last sweep (what dmrg returns) */
+  double max_truncerr;        /* of the last sweep */
+  double entropy;             /* of the last sweep, bond SvNbond */
+  int biggest_m;
+  int sweeps_done;
+  double queue_seconds;       /* submit -> start */
+  double run_seconds;         /* start -> done (upload, sweeps, download) */
+  size_t footprint_bytes;     /* admission estimate */
+} dmrg_result;
+
+DMRG_API int dmrg_server_create(const dmrg_server_config* cfg, dmrg_server** out);
+/* Copies the request and queues it; *ticket identifies it. Rejects (DMRG_ERR_BUDGET) a request
+ * whose footprint alone exceeds the budget. */
+DMRG_API int dmrg_server_submit(dmrg_server* s, const dmrg_request* req, long long* ticket);
+/* Status and statistics of a ticket, waiting up to wait_ms milliseconds for it to finish
+ * (0: no wait, < 0: until it finishes). */
+DMRG_API int dmrg_server_poll(dmrg_server* s, long long ticket, int wait_ms, dmrg_result* out);
+/* Final MPS site of a finished ticket, dense-equivalent [ml, d, mr] in the grouped bond order
+ * (out NULL: sizes only), as dmrg_mps_download; *oc receives the final centre when non-NULL. */
+DMRG_API int dmrg_server_fetch_site(dmrg_server* s, long long ticket, int site, double* out,
+                                    int* ml, int* d, int* mr, int* oc);
+/* Forgets a finished ticket (its host copy of the final MPS). */
+DMRG_API int dmrg_server_release(dmrg_server* s, long long ticket);
+/* Finishes the queued and running solves, then stops the workers. */
+DMRG_API int dmrg_server_destroy(dmrg_server* s);
+DMRG_API const char* dmrg_server_last_error(const dmrg_server* s);
+
 #ifdef __cplusplus
 }
 #endif
