@@ -143,6 +143,7 @@ int dmrg_ctx_create(int device, size_t hbm_budget_bytes, dmrg_ctx** out) {
       cuda_check(cudaMalloc(&c->d_scal, 256 * sizeof(double)), "scalars");
       cuda_check(cudaMalloc(&c->d_partial, 16 * 296 * sizeof(double)), "partials");
       cuda_check(cudaMalloc(&c->d_status, 16 * sizeof(int)), "status");
+      cuda_check(cudaMemset(c->d_status, 0, 16 * sizeof(int)), "status clear");
       cuda_check(cudaMallocHost(&c->h_scal, 256 * sizeof(double)), "pinned scalars");
       cuda_check(cudaMalloc(&c->d_flags, c->max_groups * sizeof(int)), "flags");
       cuda_check(cudaMallocHost(&c->h_flags, c->max_groups * sizeof(int)), "pinned flags");
@@ -568,7 +569,7 @@ int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* p
     set_device(c);
     HeffPlan hp;
     plan_heff(st, iL, hp);
-    upload_heff(c, hp, 0);
+    upload_heff(c, hp, 0, precision);
     const TwoLayout& tl = hp.tl;
     const Bond& Bl = st->bond[iL];
     const Bond& Br = st->bond[iL + 2];
@@ -595,6 +596,7 @@ int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* p
     cuda_check(cudaMemcpyAsync(h.data(), c->H.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
                                c->stream), "psi download");
     cuda_check(cudaStreamSynchronize(c->stream), "heff sync");
+    check_mma_status(c);
     std::fill(psi_out, psi_out + size_t(ml) * d1 * d2 * mr, 0.0);
     for (int ka = 0; ka < tl.nl; ++ka)
       for (int s1 = 0; s1 < d1; ++s1)

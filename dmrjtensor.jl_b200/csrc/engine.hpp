@@ -112,10 +112,13 @@ struct GemmList {
   int tiles = 0;
   double flops = 0;
   size_t t_off = 0, s_off = 0;  // byte offsets inside the uploaded slot
+  int bm = GEMM_BM;              // tile rows the tile counts refer to
   void clear() { tasks.clear(); segs.clear(); tiles = 0; flops = 0; }
   void add(int64_t c_off, int ldc, int M, int N, double alpha, double beta);
   void seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K);
 };
+// The same products tiled for the split-precision kernel (TF32_TILE_M x GEMM_BN tiles).
+GemmList retile(const GemmList& g, int bm);
 
 struct MixList {
   std::vector<MixTask> tasks;
@@ -225,6 +228,9 @@ struct Upload {
 // device fault.
 void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
               const double* B, int64_t nB, double* C, int64_t nC);
+// The same list on the split-precision (3xTF32, tcgen05) kernel; the list must be retiled.
+void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
+                    const double* B, int64_t nB, double* C, int64_t nC);
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,
              double* out, int64_t nout);
 void run_copy(dmrg_ctx* c, const CopyList& l, char* dbase, const double* src, int64_t nsrc,
@@ -248,14 +254,22 @@ struct GemmProfile {
 struct HeffPlan {
   TwoLayout tl;
   GemmList g1, g3;
+  GemmList g1t, g3t;             // retiled copies for the split-precision kernel (when used)
+  bool split = false;
   MixList mix;
   int64_t x_size = 0, y_size = 0;
   double flops = 0;
   char* dbase = nullptr;
 };
 void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp);
-void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot);
+// Uploads the Heff task lists; with precision DMRG_PREC_3XTF32 also the retiled copies.
+void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision = DMRG_PREC_FP64);
+// Adds the retiled split-precision lists to a plan (before its upload).
+void prepare_split(HeffPlan& hp);
 // y = Heff x for vectors in the tl layout (device pointers).
+// Fails (DMRG_ERR_TIMEOUT) if a split-precision GEMM reported an MMA wait that gave up since the
+// last check, and clears the flag. Synchronous read; call after a stream synchronisation.
+void check_mma_status(dmrg_ctx* c);
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
                 int precision, GemmProfile* prof = nullptr);
 

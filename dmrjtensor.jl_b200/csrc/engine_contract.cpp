@@ -94,11 +94,32 @@ void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp) {
   hp.flops = hp.g1.flops + hp.g3.flops + hp.mix.flops;
 }
 
-void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot) {
+void check_mma_status(dmrg_ctx* c) {
+  int flag = 0;
+  cuda_check(cudaMemcpy(&flag, c->d_status + STATUS_MMA, sizeof(int), cudaMemcpyDeviceToHost),
+             "MMA status");
+  if (flag != 0) {
+    cudaMemset(c->d_status + STATUS_MMA, 0, sizeof(int));
+    fail(DMRG_ERR_TIMEOUT, "split-precision GEMM: a tensor-core MMA completion wait gave up");
+  }
+}
+
+void prepare_split(HeffPlan& hp) {
+  hp.g1t = retile(hp.g1, TF32_TILE_M);
+  hp.g3t = retile(hp.g3, TF32_TILE_M);
+  hp.split = true;
+}
+
+void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision) {
+  if (precision == DMRG_PREC_3XTF32 && !hp.split) prepare_split(hp);
   Upload u;
   u.put(hp.g1);
   u.put(hp.mix);
   u.put(hp.g3);
+  if (hp.split) {
+    u.put(hp.g1t);
+    u.put(hp.g3t);
+  }
   hp.dbase = u.send(c, slot);
 }
 
@@ -130,17 +151,28 @@ GemmProfile::~GemmProfile() { for (auto e : pool) cudaEventDestroy(e); }
 
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
                 int precision, GemmProfile* prof) {
-  (void)precision;
   dmrg_ctx* c = st->ctx;
   ensure(c, c->X, std::max<int64_t>(hp.x_size, 1));
   ensure(c, c->Y, std::max<int64_t>(hp.y_size, 1));
   const int64_t n = hp.tl.size;
+  // split form: the two GEMM steps on the tensor-core 3xTF32 kernel; the MPO mixing stays FP64
+  const bool split = precision == DMRG_PREC_3XTF32;
+  if (split && !hp.split) fail(DMRG_ERR_STATE, "split-precision Heff lists were not uploaded");
+  if (precision != DMRG_PREC_FP64 && !split)
+    fail(DMRG_ERR_ARG, "precision: only FP64 and 3xTF32 Heff forms are built");
   if (prof) prof->begin(c->stream, hp.g1.flops);
-  run_gemm(c, hp.g1, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
+  if (split)
+    run_gemm_split(c, hp.g1t, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
+  else
+    run_gemm(c, hp.g1, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
   if (prof) prof->end(c->stream);
   run_mix(c, hp.mix, hp.dbase, c->X.p, c->X.n, c->Y.p, c->Y.n);
   if (prof) prof->begin(c->stream, hp.g3.flops);
-  run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n, y, n);
+  if (split)
+    run_gemm_split(c, hp.g3t, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n,
+                   y, n);
+  else
+    run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n, y, n);
   if (prof) prof->end(c->stream);
 }
 

@@ -214,13 +214,30 @@ void GemmList::add(int64_t c_off, int ldc, int M, int N, double alpha, double be
   t.N = N;
   t.seg0 = int(segs.size());
   t.nseg = 0;
-  t.tiles_m = (M + GEMM_BM - 1) / GEMM_BM;
+  t.tiles_m = (M + bm - 1) / bm;
   t.tile0 = tiles;
   t.alpha = alpha;
   t.beta = beta;
   if (M <= 0 || N <= 0) { t.tiles_m = 0; }
   tiles += t.tiles_m * ((N + GEMM_BN - 1) / GEMM_BN);
   tasks.push_back(t);
+}
+
+GemmList retile(const GemmList& g, int bm) {
+  GemmList r;
+  r.tA = g.tA;
+  r.tB = g.tB;
+  r.bm = bm;
+  r.segs = g.segs;
+  r.flops = g.flops;
+  r.tasks = g.tasks;
+  r.tiles = 0;
+  for (GemmTask& t : r.tasks) {
+    t.tiles_m = (t.M <= 0 || t.N <= 0) ? 0 : (t.M + bm - 1) / bm;
+    t.tile0 = r.tiles;
+    r.tiles += t.tiles_m * ((t.N + GEMM_BN - 1) / GEMM_BN);
+  }
+  return r;
 }
 
 void GemmList::seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K) {
@@ -323,9 +340,31 @@ void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int6
       if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
     }
   }
+  if (g.bm != GEMM_BM) bad_plan("gemm tiling");
   launch_gemm_f64(c->stream, g.tA, g.tB, A, B, C,
                   reinterpret_cast<const GemmTask*>(dbase + g.t_off), int(g.tasks.size()),
                   reinterpret_cast<const GemmSeg*>(dbase + g.s_off), g.tiles, c->nsm * 4);
+}
+
+void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
+                    const double* B, int64_t nB, double* C, int64_t nC) {
+  if (g.tiles == 0) return;
+  if (g.bm != TF32_TILE_M) bad_plan("split gemm tiling");
+  for (const GemmTask& t : g.tasks) {
+    if (t.M <= 0 || t.N <= 0) continue;
+    if (t.ldc < t.M || !in_range(t.c_off, (t.M - 1) + int64_t(t.N - 1) * t.ldc, nC)) bad_plan("gemm C");
+    for (int q = 0; q < t.nseg; ++q) {
+      const GemmSeg& s = g.segs[t.seg0 + q];
+      const int64_t ea = g.tA ? (s.K - 1) + int64_t(t.M - 1) * s.lda : (t.M - 1) + int64_t(s.K - 1) * s.lda;
+      const int64_t eb = g.tB ? (t.N - 1) + int64_t(s.K - 1) * s.ldb : (s.K - 1) + int64_t(t.N - 1) * s.ldb;
+      if (s.lda < (g.tA ? s.K : t.M) || !in_range(s.a_off, ea, nA)) bad_plan("gemm A");
+      if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
+    }
+  }
+  launch_gemm_tf32x3(c->stream, g.tA, g.tB, A, B, C,
+                     reinterpret_cast<const GemmTask*>(dbase + g.t_off), int(g.tasks.size()),
+                     reinterpret_cast<const GemmSeg*>(dbase + g.s_off), g.tiles, c->nsm * 3,
+                     c->d_status + STATUS_MMA);
 }
 
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,

@@ -115,8 +115,8 @@ struct Group {
   int64_t moff = 0, roff = 0, woff = 0;
 };
 
-void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing& tm,
-             StepOut& so) {
+void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool final_step,
+             Timing& tm, StepOut& so) {
   dmrg_ctx* c = st->ctx;
   cudaStream_t s = c->stream;
   const MPOSite& ml = st->mpo->site[iL];
@@ -152,11 +152,17 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
         if (kc >= 0 && lb.kb[kc * d2 + s2] == kd)
           gaa.seg(la.off[ka * d1 + s1], Bl.dim[ka], lb.off[kc * d2 + s2], Bc.dim[kc], Bc.dim[kc]);
       }
+  const bool split = P.precision == DMRG_PREC_3XTF32;
+  if (split) prepare_split(hp);
   Upload u;
   u.put(hp.g1);
   u.put(hp.mix);
   u.put(hp.g3);
   u.put(gaa);
+  if (hp.split) {
+    u.put(hp.g1t);
+    u.put(hp.g3t);
+  }
   hp.dbase = u.send(c, 0);
   const int64_t n = tl.size;
   const int kdim = std::max(2, std::min(P.krylov, 16));
@@ -222,8 +228,24 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
     tm.end(tv, 3);
   }
   const double* psi = H;
+  // split form, last bond step of the sweep: the reported energy is the FP64 Rayleigh quotient
+  // <psi|H|psi>/<psi|psi> of the Ritz vector (one FP64 matvec; the Krylov vectors are free now)
+  const bool fp64_energy = split && P.fp64_final && final_step;
+  if (fp64_energy) {
+    const int th = tm.begin();
+    apply_heff(st, iL, hp, H, K, DMRG_PREC_FP64, nullptr);
+    tm.end(th, 0);
+    so.nmv += 1;
+    so.heff_flops += hp.flops;
+    launch_dot2(s, H, K, n, c->d_partial, scal + lz::KK);
+    cuda_check(cudaMemcpyAsync(c->h_scal + lz::KK, scal + lz::KK, 2 * sizeof(double),
+                               cudaMemcpyDeviceToHost, s), "Rayleigh quotient D2H");
+  }
   cuda_check(cudaMemcpyAsync(c->h_scal + lz::EN, scal + lz::EN, sizeof(double),
                              cudaMemcpyDeviceToHost, s), "energy D2H");
+  if (split)   // timeout flag of the split GEMMs, read back with the energy (bytes of slot 20)
+    cuda_check(cudaMemcpyAsync(c->h_scal + 20, c->d_status + STATUS_MMA, sizeof(int),
+                               cudaMemcpyDeviceToHost, s), "MMA status D2H");
 
   // ---------------- reduced density matrix per centre-charge group (algs/DMRG.jl:425-429)
   const int te = tm.begin();
@@ -337,6 +359,15 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, Timing
                              cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
   so.energy = c->h_scal[lz::EN];
+  if (fp64_energy && c->h_scal[lz::KK] > 0) so.energy = c->h_scal[lz::KH] / c->h_scal[lz::KK];
+  if (split) {
+    int flag = 0;
+    std::memcpy(&flag, c->h_scal + 20, sizeof(int));
+    if (flag != 0) {
+      cudaMemsetAsync(c->d_status + STATUS_MMA, 0, sizeof(int), s);
+      fail(DMRG_ERR_TIMEOUT, "split-precision GEMM: a tensor-core MMA completion wait gave up");
+    }
+  }
 
   std::vector<std::vector<double>> vals(G.size());
   for (int g = 0; g < int(G.size()); ++g) {
@@ -459,7 +490,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     const int i = st->oc;
     const int iL = j > 0 ? i : i - 1, iR = j > 0 ? i + 1 : i;
     StepOut so;
-    twostep(st, P, j, iL, iR, tm, so);
+    twostep(st, P, j, iL, iR, ns == 2 * (L - 1) - 1, tm, so);
     const int tenv = tm.begin();
     double ef = 0.0;
     if (j > 0) lupdate(st, i, &ef); else rupdate(st, i, &ef);
