@@ -290,6 +290,29 @@ def run_serving(pkg, device, nreq, rate=20.0, slots=8, seed=5):
             "p99_latency_s": pct(0.99), "mean_latency_s": statistics.mean(lat)}
 
 
+def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
+    """Heff at the dense-equivalent size of the headline workload at maxm 1024 (dense random MPS,
+    bond dimension 1024 either side of the centre bond): device time per application in the plain
+    FP64 form and the 3xTF32 tensor-core form, algorithmic TFLOP/s of each."""
+    import ctypes as C
+    lib = pkg.lib()
+    mpo = pkg.makeMPO(pkg.heisenbergMPO, 2, L)
+    iL = L // 2 - 1
+    psi = pkg.randMPS(2, L, m, seed=1, oc=iL)
+    dev = pkg.DeviceState(psi, mpo.device(ctx))
+    dev.env_build()
+    out = {"workload": f"dense Heisenberg L={L}, random MPS with m={m} at bond {iL + 1} "
+                       f"(two-site vector {m}x2x2x{m}); Heff at sites {iL},{iL + 1}"}
+    for name, code in (("fp64", 0), ("3xtf32", 1)):
+        sec, fl = C.c_double(), C.c_double()
+        pkg._lib.check(lib.dmrg_test_heff_time(dev.h, dev.dmpo.h, iL, code, reps, C.byref(sec),
+                                               C.byref(fl)), ctx.h)
+        out["flops_per_apply"] = fl.value
+        out[name] = {"seconds": sec.value, "tflops": fl.value / sec.value / 1e12}
+    out["speedup_3xtf32"] = out["fp64"]["seconds"] / out["3xtf32"]["seconds"]
+    return out
+
+
 def cpu_threads():
     try:
         import threadpoolctl
@@ -437,6 +460,7 @@ def run_ours(args, world, rank, local, dist):
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "seconds_per_step": statistics.mean(e2e_times)}
     serving = run_serving(pkg, local, args.serve_requests) if args.serve_requests > 0 else None
+    heff_large = heff_forms(pkg, ctx) if args.chosen else None
     if rank != 0:
         return
     peak = fp64_gemm_peak(local)
@@ -483,6 +507,7 @@ def run_ours(args, world, rank, local, dist):
         "cpu_baseline": cpu,
         "serving": serving,
         "chosen": chosen,
+        "heff_forms_m1024": heff_large,
     }
     print(json.dumps(out))
 

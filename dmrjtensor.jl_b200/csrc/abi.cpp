@@ -610,6 +610,40 @@ int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* p
   });
 }
 
+int dmrg_test_heff_time(dmrg_state* st, const dmrg_mpo* mpo, int iL, int precision, int reps,
+                        double* seconds, double* flops) {
+  if (!st) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    if (mpo != st->mpo) fail(DMRG_ERR_ARG, "state was uploaded with a different MPO");
+    if (iL < 0 || iL + 1 >= st->L || reps < 1 || !seconds) fail(DMRG_ERR_ARG, "bad arguments");
+    if (!st->Lvalid[iL] || !st->Rvalid[iL + 1]) fail(DMRG_ERR_STATE, "environments not built");
+    set_device(c);
+    HeffPlan hp;
+    plan_heff(st, iL, hp);
+    upload_heff(c, hp, 0, precision);
+    const int64_t n = std::max<int64_t>(hp.tl.size, 1);
+    ensure(c, c->K, n);
+    ensure(c, c->H, n);
+    cuda_check(cudaMemsetAsync(c->K.p, 0, size_t(n) * sizeof(double), c->stream), "vector");
+    apply_heff(st, iL, hp, c->K.p, c->H.p, precision);   // warm-up
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps; ++r) apply_heff(st, iL, hp, c->K.p, c->H.p, precision);
+    cudaEventRecord(e1, c->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_mma_status(c);
+    *seconds = ms * 1e-3 / reps;
+    if (flops) *flops = hp.flops;
+  });
+}
+
 int dmrg_heff_apply_noalloc(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
                             double* psi_out, int precision) {
   if (!st) return DMRG_ERR_ARG;

@@ -30,6 +30,7 @@ constexpr uint32_t TMEM_COLS = 64;               // FP32 accumulator 128 lanes x
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(TBN >> 3) << 17) |
                            (uint32_t(TBM >> 4) << 24);
 constexpr long long WAIT_LIMIT = 1ll << 22;      // try_wait rounds before giving up
+constexpr int A_QUADS = TBM * TBK / 4 / TT, B_QUADS = TBN * TBK / 4 / TT;   // per thread
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -118,10 +119,6 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
   const uint32_t raw = smem_u32(smraw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* sp = smraw + (base - raw);
-  float* Ahi = reinterpret_cast<float*>(sp);
-  float* Alo = reinterpret_cast<float*>(sp + A_BYTES);
-  float* Bhi = reinterpret_cast<float*>(sp + 2 * A_BYTES);
-  float* Blo = reinterpret_cast<float*>(sp + 2 * A_BYTES + B_BYTES);
   const uint32_t aH = base, aL = base + A_BYTES, bH = base + 2 * A_BYTES,
                  bL = base + 2 * A_BYTES + B_BYTES;
   const uint32_t mb = smem_u32(&mbar);
@@ -150,62 +147,113 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
     const GemmTask tk = tasks[lo];
     const int local = tile - tk.tile0;
     const int m0 = (local % tk.tiles_m) * TBM, n0 = (local / tk.tiles_m) * TBN;
+    // K chunks of this tile, over all its segments: (segment q, offset k0). Each thread owns
+    // the elements tid + TT i of a chunk: loaded into registers in one batch (the next chunk's
+    // loads are issued while the current chunk's MMAs run), then split into the staged tiles.
     bool issued = false;
-    for (int q = 0; q < tk.nseg; ++q) {
-      const GemmSeg sg = segs[tk.seg0 + q];
-      for (int k0 = 0; k0 < sg.K; k0 += TBK) {
-        // stage op(A)[m0:m0+128, k0:k0+32] and op(B)[k0:k0+32, n0:n0+64] (rows = N), split
-        for (int e = tid; e < TBM * TBK; e += TT) {
-          const int r = TA ? e / TBK : e % TBM, k = TA ? e % TBK : e / TBM;
-          const int gr = m0 + r, gk = k0 + k;
-          double x = 0.0;
-          if (gr < tk.M && gk < sg.K)
-            x = TA ? A[sg.a_off + gk + int64_t(gr) * sg.lda] : A[sg.a_off + gr + int64_t(gk) * sg.lda];
-          float h, l;
-          split(x, h, l);
-          const int o = soff(TBM, r, k) >> 2;
-          Ahi[o] = h;
-          Alo[o] = l;
+    int q = 0, k0 = 0;
+    while (q < tk.nseg && segs[tk.seg0 + q].K <= 0) ++q;
+    // quads: 4 consecutive K elements of one row (one 16-byte unit of the staged layout);
+    // the thread-to-quad map keeps the global loads coalesced along the contiguous dimension
+    double ra[A_QUADS][4], rb[B_QUADS][4];
+    auto a_quad = [&](int i, int& r, int& kq) {
+      const int e = tid + TT * i;
+      if (TA) { r = e >> 3; kq = e & 7; } else { r = e % TBM; kq = e / TBM; }
+    };
+    auto b_quad = [&](int i, int& c, int& kq) {
+      const int e = tid + TT * i;
+      if (TB) { c = e % TBN; kq = e / TBN; } else { c = e >> 3; kq = e & 7; }
+    };
+    auto load_chunk = [&](int qq, int kk0) {
+      const GemmSeg sg = segs[tk.seg0 + qq];
+#pragma unroll
+      for (int i = 0; i < A_QUADS; ++i) {
+        int r, kq;
+        a_quad(i, r, kq);
+        const int gr = m0 + r;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int gk = kk0 + 4 * kq + j;
+          ra[i][j] = (gr < tk.M && gk < sg.K)
+                         ? (TA ? A[sg.a_off + gk + int64_t(gr) * sg.lda] : A[sg.a_off + gr + int64_t(gk) * sg.lda])
+                         : 0.0;
         }
-        for (int e = tid; e < TBN * TBK; e += TT) {
-          const int c = TB ? e % TBN : e / TBK, k = TB ? e / TBN : e % TBK;
-          const int gc = n0 + c, gk = k0 + k;
-          double x = 0.0;
-          if (gc < tk.N && gk < sg.K)
-            x = TB ? B[sg.b_off + gc + int64_t(gk) * sg.ldb] : B[sg.b_off + gk + int64_t(gc) * sg.ldb];
-          float h, l;
-          split(x, h, l);
-          const int o = soff(TBN, c, k) >> 2;
-          Bhi[o] = h;
-          Blo[o] = l;
-        }
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-          const int ks = min(TBK, sg.K - k0);
-          for (int s = 0; s * 8 < ks; ++s) {
-            const uint64_t dah = sdesc(aH + s * (TBM * 32)), dal = sdesc(aL + s * (TBM * 32));
-            const uint64_t dbh = sdesc(bH + s * (TBN * 32)), dbl = sdesc(bL + s * (TBN * 32));
-            mma_tf32(tmem, dah, dbh, issued ? 1u : 0u);
-            issued = true;
-            mma_tf32(tmem, dah, dbl, 1u);
-            mma_tf32(tmem, dal, dbh, 1u);
-          }
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
-                       :: "r"(mb) : "memory");
-        }
-        issued = true;   // every thread: the accumulator holds this tile's partial sum
-        // the MMAs read the staged tiles: wait until they have completed (bounded)
-        long long it = 0;
-        bool late = false;
-        while (!mbar_try(mb, phase)) {
-          if (++it > WAIT_LIMIT) { late = true; break; }
-        }
-        phase ^= 1u;
-        failed = __syncthreads_or(late) != 0;   // the same decision in every thread
-        if (failed) break;
       }
+#pragma unroll
+      for (int i = 0; i < B_QUADS; ++i) {
+        int c, kq;
+        b_quad(i, c, kq);
+        const int gc = n0 + c;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int gk = kk0 + 4 * kq + j;
+          rb[i][j] = (gc < tk.N && gk < sg.K)
+                         ? (TB ? B[sg.b_off + gc + int64_t(gk) * sg.ldb] : B[sg.b_off + gk + int64_t(gc) * sg.ldb])
+                         : 0.0;
+        }
+      }
+    };
+    if (q < tk.nseg) load_chunk(q, k0);
+    while (q < tk.nseg) {
+      const int ks = min(TBK, segs[tk.seg0 + q].K - k0);
+#pragma unroll
+      for (int i = 0; i < A_QUADS; ++i) {
+        int r, kq;
+        a_quad(i, r, kq);
+        float4 h, l;
+        split(ra[i][0], h.x, l.x);
+        split(ra[i][1], h.y, l.y);
+        split(ra[i][2], h.z, l.z);
+        split(ra[i][3], h.w, l.w);
+        const int o = soff(TBM, r, 4 * kq);
+        *reinterpret_cast<float4*>(sp + o) = h;
+        *reinterpret_cast<float4*>(sp + A_BYTES + o) = l;
+      }
+#pragma unroll
+      for (int i = 0; i < B_QUADS; ++i) {
+        int c, kq;
+        b_quad(i, c, kq);
+        float4 h, l;
+        split(rb[i][0], h.x, l.x);
+        split(rb[i][1], h.y, l.y);
+        split(rb[i][2], h.z, l.z);
+        split(rb[i][3], h.w, l.w);
+        const int o = soff(TBN, c, 4 * kq);
+        *reinterpret_cast<float4*>(sp + 2 * A_BYTES + o) = h;
+        *reinterpret_cast<float4*>(sp + 2 * A_BYTES + B_BYTES + o) = l;
+      }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        for (int st = 0; st * 8 < ks; ++st) {
+          const uint64_t dah = sdesc(aH + st * (TBM * 32)), dal = sdesc(aL + st * (TBM * 32));
+          const uint64_t dbh = sdesc(bH + st * (TBN * 32)), dbl = sdesc(bL + st * (TBN * 32));
+          mma_tf32(tmem, dah, dbh, issued ? 1u : 0u);
+          issued = true;
+          mma_tf32(tmem, dah, dbl, 1u);
+          mma_tf32(tmem, dal, dbh, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                     :: "r"(mb) : "memory");
+      }
+      issued = true;   // every thread: the accumulator holds this tile's partial sum
+      // next chunk coordinates; its loads go out while the MMAs run
+      k0 += TBK;
+      if (k0 >= segs[tk.seg0 + q].K) {
+        k0 = 0;
+        ++q;
+        while (q < tk.nseg && segs[tk.seg0 + q].K <= 0) ++q;
+      }
+      if (q < tk.nseg) load_chunk(q, k0);
+      // the MMAs read the staged tiles: wait until they have completed (bounded)
+      long long it = 0;
+      bool late = false;
+      while (!mbar_try(mb, phase)) {
+        if (++it > WAIT_LIMIT) { late = true; break; }
+      }
+      phase ^= 1u;
+      failed = __syncthreads_or(late) != 0;   // the same decision in every thread
       if (failed) break;
     }
     if (failed) break;

@@ -61,7 +61,7 @@ enum dmrg_status {
 enum dmrg_precision {
   DMRG_PREC_FP64 = 0,    /* plain form: every contraction in FP64 (DMMA) */
   DMRG_PREC_3XTF32 = 1,  /* chosen form: Heff contractions as 3 TF32 tensor-core products */
-  DMRG_PREC_BF16X9 = 2   /* chosen form: Heff contractions as 9 BF16 tensor-core products */
+  DMRG_PREC_BF16X9 = 2   /* reserved (9 BF16 products): not built, rejected with DMRG_ERR_ARG */
 };
 
 typedef struct dmrg_ctx dmrg_ctx;
@@ -209,6 +209,12 @@ DMRG_API int dmrg_test_svd(dmrg_ctx* ctx, int nmat, const int* r, const int* c, 
  * eigenvectors of the k[i] largest (packed n[i] x k[i] column-major in U). A is overwritten. */
 DMRG_API int dmrg_test_syevt(dmrg_ctx* ctx, int nmat, const int* n, const int* k, double* A,
                              double* w, double* U);
+
+/* Device time of the two-site Heff at (iL, iL+1) in the given precision: `reps` applications to
+ * a device-resident vector timed with CUDA events on the context's stream (no host copies).
+ * *seconds = time per application, *flops = its algorithmic FLOPs (block GEMMs + MPO mixing). */
+DMRG_API int dmrg_test_heff_time(dmrg_state* st, const dmrg_mpo* mpo, int iL, int precision,
+                                 int reps, double* seconds, double* flops);
 
 /* Fills *p with the reference defaults (minm 2, krylov 2, betatest 1e-10, ...). */
 DMRG_API void dmrg_params_default(dmrg_params* p);

@@ -71,3 +71,16 @@ def test_split_dense_lanczos_k(dmrgb, ctx):
     ref = ed.sparse_ground_energy(om.make_mpo([om.heisenberg_bulk()] * L, 2))
     assert abs(e["3xtf32"] - e["fp64"]) <= 1e-8
     assert abs(e["3xtf32"] - ref) <= 1e-8 * abs(ref)
+
+
+def test_heff_timing_hook_reports_both_forms(dmrgb, ctx):
+    psi = dmrgb.randMPS(2, 12, 64, seed=5, oc=5)
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, 12)
+    Lenv, _ = dmrgb.makeEnv(psi, mpo, ctx=ctx)
+    dev = Lenv.dev
+    for prec in (0, 1):
+        sec, fl = C.c_double(), C.c_double()
+        assert dmrgb.lib().dmrg_test_heff_time(dev.h, dev.dmpo.h, 5, prec, 3, C.byref(sec),
+                                               C.byref(fl)) == 0
+        assert sec.value > 0 and fl.value > 0
+    assert dmrgb.lib().dmrg_test_heff_time(dev.h, dev.dmpo.h, 5, 2, 1, C.byref(sec), None) == 1
