@@ -82,7 +82,9 @@ void run_eigs(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<EigTas
     pl.maxn = maxn;
     pl.max_sweeps = 30;
     int sw = 0;
+    cuda_check(cudaGetLastError(), "block Jacobi set-up");
     launch_block_jacobi(c->stream, base, pl, c->d_flags, c->h_flags, c->d_floors, &sw);
+    cuda_check(cudaGetLastError(), "block Jacobi");
     if (sweeps) *sweeps = sw;
     if (sw >= pl.max_sweeps) fail(DMRG_ERR_CUDA, "block Jacobi eigensolver did not converge");
   }

@@ -134,6 +134,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   launch_mdot(s, st->A[ic].p, 0, 1, st->A[ic].p, st->lay[ic].size, c->d_partial,
               c->d_scal + lz::NRM);
   launch_scale_rsqrt(s, st->A[ic].p, st->lay[ic].size, c->d_scal + lz::NRM);
+  cuda_check(cudaGetLastError(), "centre normalisation");
 
   HeffPlan hp;
   plan_heff(st, iL, hp);
@@ -171,11 +172,13 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   double* K = c->K.p;
   double* H = c->H.p;
   run_gemm(c, gaa, hp.dbase, st->A[iL].p, st->A[iL].n, st->A[iR].p, st->A[iR].n, K, n);
+  cuda_check(cudaGetLastError(), "two-site tensor");
   tm.end(tv, 3);
 
   auto heff = [&](const double* x, double* y) {
     const int th = tm.begin();
     apply_heff(st, iL, hp, x, y, P.precision, P.profile ? &tm.gemm : nullptr);
+    cuda_check(cudaGetLastError(), "Heff");
     tm.end(th, 0);
     so.nmv += 1;
     so.heff_flops += hp.flops;
@@ -193,6 +196,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     launch_lanczos2_orth(s, K, H, n, scal, c->d_partial);   // K /= |K|, H -= a1 K, |H|^2
     double* K1 = K + n;
     launch_next_vector(s, H, K1, n, scal, 0, P.betatest);
+    cuda_check(cudaGetLastError(), "Krylov vector");
     tm.end(tv, 3);
     heff(K1, H);
     tv = tm.begin();
@@ -227,6 +231,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     launch_lincomb(s, K, n, kdim, scal + lz::COEF, H, n);
     tm.end(tv, 3);
   }
+  cuda_check(cudaGetLastError(), "Krylov step");
   const double* psi = H;
   // split form, last bond step of the sweep: the reported energy is the FP64 Rayleigh quotient
   // <psi|H|psi>/<psi|psi> of the Ritz vector (one FP64 matvec; the Krylov vectors are free now)
@@ -353,6 +358,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   run_gemm(c, grho, db2, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
   launch_trid_eigvals(s, c->R.p, reinterpret_cast<const TridTask*>(db2 + tt_off),
                       int(ttasks.size()), tmax);
+  cuda_check(cudaGetLastError(), "density matrix and eigenvalue launch");
   run_eigs(c, c->R.p, c->R.n, etasks, J0, nullptr);
   std::vector<double> lam(std::max<int64_t>(wtot, 1));
   cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + W0, sizeof(double) * wtot,
@@ -401,6 +407,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     vmax_n = std::max(vmax_n, t.n);
     vmax_k = std::max(vmax_k, t.keep);
   }
+  cuda_check(cudaGetLastError(), "eigenvalue download");
   if (!vt.empty()) {
     Upload uv;
     const size_t vo = uv.put(vt);
@@ -410,6 +417,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   }
 
   // ---------------- split back into the two site tensors (algs/DMRG.jl:389-395, 483-490)
+  cuda_check(cudaGetLastError(), "eigenvectors");
   SiteLayout nl = make_site_layout(Bl, ml.p, C);
   SiteLayout nrl = make_site_layout(C, mr.p, Br);
   DBuf nA, nB;
@@ -455,13 +463,17 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   u3.put(cp);
   u3.put(gs);
   char* db3 = u3.send(c, 3);
+  cuda_check(cudaGetLastError(), "split upload");
   if (j > 0) {
     run_copy(c, cp, db3, c->R.p, c->R.n, nA.p, nA.n);
+    cuda_check(cudaGetLastError(), "split copy");
     run_gemm(c, gs, db3, c->R.p, c->R.n, c->M.p, c->M.n, nB.p, nB.n);
   } else {
     run_copy(c, cp, db3, c->R.p, c->R.n, nB.p, nB.n);
+    cuda_check(cudaGetLastError(), "split copy");
     run_gemm(c, gs, db3, c->M.p, c->M.n, c->R.p, c->R.n, nA.p, nA.n);
   }
+  cuda_check(cudaGetLastError(), "split");
   dfree(c, st->A[iL]);
   dfree(c, st->A[iR]);
   st->A[iL] = nA;
@@ -494,6 +506,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     const int tenv = tm.begin();
     double ef = 0.0;
     if (j > 0) lupdate(st, i, &ef); else rupdate(st, i, &ef);
+    cuda_check(cudaGetLastError(), "environment update");
     tm.end(tenv, 1);
     out.energy = so.energy;
     out.max_truncerr = std::max(out.max_truncerr, so.truncerr);

@@ -34,7 +34,9 @@ static_assert(TE_THREADS == 256, "the Householder step sums exactly 8 per-warp s
 constexpr int TV_THREADS = 256;
 constexpr int BT_NB = 8;          // reflectors per back-transformation block
 constexpr unsigned FULL = 0xffffffffu;
-constexpr size_t SMEM_LIMIT = 227 * 1024;
+// dynamic shared memory per CTA: the 227 KB opt-in maximum less room for the kernels' static
+// shared memory (the dynamic limit of a kernel is the maximum minus its static part)
+constexpr size_t SMEM_LIMIT = 227 * 1024 - 1024;
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
