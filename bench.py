@@ -490,6 +490,8 @@ def run_ours(args, world, rank, local, dist):
         "phase_seconds_profiled_sweep": {k: prof[k] for k in
                                          ("seconds", "heff_seconds", "env_seconds",
                                           "eig_seconds", "vec_seconds")},
+        "host_seconds_per_step": statistics.mean(s["host_seconds"] for s in stats),
+        "host_wait_seconds_per_step": statistics.mean(s["wait_seconds"] for s in stats),
         "eig_max_n": max(s["eig_max_n"] for s in stats),
         "n_matvec_per_sweep": stats[-1]["n_matvec"],
         "setup_seconds_ramp": t_setup,

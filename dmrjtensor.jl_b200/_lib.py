@@ -33,7 +33,8 @@ class SweepStats(C.Structure):
                 ("env_flops", C.c_double), ("env_seconds", C.c_double),
                 ("eig_seconds", C.c_double), ("vec_seconds", C.c_double),
                 ("d_top", C.c_double * 8), ("gemm_flops", C.c_double),
-                ("gemm_seconds", C.c_double), ("gemm_launches", C.c_int), ("eig_max_n", C.c_int)]
+                ("gemm_seconds", C.c_double), ("gemm_launches", C.c_int), ("eig_max_n", C.c_int),
+                ("host_seconds", C.c_double), ("wait_seconds", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "d_top"}

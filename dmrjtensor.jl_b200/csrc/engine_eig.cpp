@@ -18,6 +18,8 @@ int64_t eig_workspace(const std::vector<EigTask>& tasks) {
 
 void run_eigs(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<EigTask>& tasks,
               int64_t ws_off, int* sweeps) {
+  if (sweeps) *sweeps = 0;
+  if (tasks.empty()) return;   // nothing to solve: no status read, no synchronisation
   std::vector<EigTask> small;
   std::vector<BlockEigGroup> big;
   int nsmall = 0, maxN = 0, maxn = 0;

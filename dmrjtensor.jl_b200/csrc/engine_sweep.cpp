@@ -7,6 +7,7 @@
 // truncation on the host from the downloaded eigenvalues, split back into the two site tensors
 // (copies + one grouped GEMM), then the environment update of the site left behind.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <map>
 
@@ -100,7 +101,7 @@ struct Timing {
 namespace {
 
 struct StepOut {
-  double energy = 0, truncerr = 0;
+  double energy = 0, truncerr = 0, wait = 0;
   int m = 0, nmv = 0;
   std::vector<double> D;       // kept singular values, descending
   double heff_flops = 0;
@@ -363,7 +364,9 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   std::vector<double> lam(std::max<int64_t>(wtot, 1));
   cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + W0, sizeof(double) * wtot,
                              cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
+  const auto w0 = std::chrono::steady_clock::now();
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
+  so.wait = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   so.energy = c->h_scal[lz::EN];
   if (fp64_energy && c->h_scal[lz::KK] > 0) so.energy = c->h_scal[lz::KH] / c->h_scal[lz::KK];
   if (split) {
@@ -495,6 +498,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   std::memset(&out, 0, sizeof(out));
   const int svn = P.svnbond > 0 ? P.svnbond : (L + 1) / 2;
   const int svn_site = std::min(std::max(2, svn + 1), L) - 1;   // 0-based i of SvNcheck!
+  const auto h0 = std::chrono::steady_clock::now();
   Timing tm(c, P.profile != 0);
   const int t0 = tm.record();
   int j = st->dir;
@@ -512,6 +516,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     out.max_truncerr = std::max(out.max_truncerr, so.truncerr);
     out.biggest_m = std::max(out.biggest_m, so.m);
     out.n_matvec += so.nmv;
+    out.wait_seconds += so.wait;
     out.heff_flops += so.heff_flops;
     out.env_flops += ef;
     out.eig_max_n = std::max(out.eig_max_n, so.eig_max_n);
@@ -541,6 +546,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   out.gemm_flops = tm.gemm.flops;
   out.gemm_seconds = tm.gemm.seconds;
   out.gemm_launches = tm.gemm.launches;
+  out.host_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
 }
 
 }  // namespace dmrg

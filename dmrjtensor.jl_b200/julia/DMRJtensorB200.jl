@@ -51,8 +51,10 @@ mutable struct SweepStats
   gemm_seconds::Cdouble
   gemm_launches::Cint
   eig_max_n::Cint
+  host_seconds::Cdouble
+  wait_seconds::Cdouble
 end
-SweepStats() = SweepStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0.0, 8), 0, 0, 0, 0)
+SweepStats() = SweepStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0.0, 8), 0, 0, 0, 0, 0, 0)
 
 lasterror(ctx) = unsafe_string(ccall((:dmrg_last_error, libdmrg), Cstring, (Ptr{Cvoid},), ctx))
 

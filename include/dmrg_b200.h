@@ -103,6 +103,8 @@ typedef struct dmrg_sweep_stats {
   double gemm_seconds;  /* profile = 1: their summed device time                     */
   int gemm_launches;    /* profile = 1: their number                                  */
   int eig_max_n;        /* largest density-matrix block of the sweep                  */
+  double host_seconds;  /* host wall time of the sweep call                           */
+  double wait_seconds;  /* of which blocked in the per-step eigenvalue synchronisation */
 } dmrg_sweep_stats;
 
 /* ---------------------------------------------------------------- context */
