@@ -172,6 +172,7 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaFree(c->d_partial);
   cudaFree(c->d_status);
   cudaFreeHost(c->h_scal);
+  if (c->h_lam) cudaFreeHost(c->h_lam);
   cudaFree(c->d_flags);
   cudaFreeHost(c->h_flags);
   cudaFree(c->d_floors);

@@ -153,6 +153,8 @@ struct dmrg_ctx {
   double* d_partial = nullptr;   // reduction partials (16 * 296 doubles)
   int* d_status = nullptr;
   double* h_scal = nullptr;      // pinned mirror of d_scal
+  double* h_lam = nullptr;       // pinned eigenvalue download buffer (grow-only)
+  size_t h_lam_cap = 0;
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> tev;  // phase-timing events, reused across sweeps
   int max_groups = 4096;

@@ -361,8 +361,18 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
                       int(ttasks.size()), tmax);
   cuda_check(cudaGetLastError(), "density matrix and eigenvalue launch");
   run_eigs(c, c->R.p, c->R.n, etasks, J0, nullptr);
-  std::vector<double> lam(std::max<int64_t>(wtot, 1));
-  cuda_check(cudaMemcpyAsync(lam.data(), c->R.p + W0, sizeof(double) * wtot,
+  // pinned destination: the copy stays asynchronous and the host waits only in the sync below
+  if (size_t(std::max<int64_t>(wtot, 1)) > c->h_lam_cap) {
+    if (c->h_lam) cudaFreeHost(c->h_lam);
+    c->h_lam = nullptr;
+    c->h_lam_cap = 0;
+    const size_t cap = std::max<size_t>(size_t(wtot), 4096);
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&c->h_lam), cap * sizeof(double)),
+               "pinned eigenvalue buffer");
+    c->h_lam_cap = cap;
+  }
+  const double* lam = c->h_lam;
+  cuda_check(cudaMemcpyAsync(c->h_lam, c->R.p + W0, sizeof(double) * wtot,
                              cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
   const auto w0 = std::chrono::steady_clock::now();
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
@@ -381,7 +391,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   std::vector<std::vector<double>> vals(G.size());
   for (int g = 0; g < int(G.size()); ++g) {
     const int side = j > 0 ? G[g].n : G[g].np;
-    vals[g].assign(lam.begin() + G[g].woff, lam.begin() + G[g].woff + side);
+    vals[g].assign(lam + G[g].woff, lam + G[g].woff + side);
   }
   const Sel sel = select_kept(vals, P.maxm, P.minm, P.cutoff, 1.0, P.degen_rtol);
   Bond C;
