@@ -290,6 +290,59 @@ def run_serving(pkg, device, nreq, rate=20.0, slots=8, seed=5):
             "p99_latency_s": pct(0.99), "mean_latency_s": statistics.mean(lat)}
 
 
+def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
+    """``expect(psi, H)`` and ``correlationmatrix`` on the device: on the resident maxm-1024 state
+    of the sweep workload, and on the same chain after a short maxm-64 run where the CPU oracle
+    (dense, centre-moving) finishes in seconds and is timed beside the device on identical
+    tensors."""
+    Sp, Sm, Sz = pkg.spinOps()[:3]
+    psi = pkg.MPS()
+    psi._dev = dev
+    n0 = pkg.kernel_launches()
+    t = time.perf_counter()
+    E = pkg.expect(psi, mpo, ctx=ctx)
+    t_exp = time.perf_counter() - t
+    n1 = pkg.kernel_launches()
+    t = time.perf_counter()
+    rho = pkg.correlationmatrix(psi, Sz, Sz, ctx=ctx)
+    t_zz = time.perf_counter() - t
+    n2 = pkg.kernel_launches()
+    t = time.perf_counter()
+    pkg.correlationmatrix(psi, Sp, Sm, ctx=ctx)
+    t_pm = time.perf_counter() - t
+    out = {"state": f"heisenberg L={L_CHAIN} U(1), maxm {RAMP[-1]} (resident)",
+           "expect_seconds": t_exp, "expect_launches": n1 - n0,
+           "expect_rel_diff_vs_sweep_energy": abs(E - energy) / abs(energy),
+           "correlationmatrix_zz_seconds": t_zz, "correlationmatrix_pm_seconds": t_pm,
+           "correlationmatrix_launches": n2 - n1,
+           "zz_max_abs_row_sum": float(np.max(np.abs(rho.sum(axis=1))))}
+    small = pkg.neelMPS(L_CHAIN)
+    pkg.dmrg(small, mpo, m=m_small, sweeps=2, cutoff=CUTOFF, ctx=ctx)
+    t = time.perf_counter()
+    E_s = pkg.expect(small, mpo, ctx=ctx)
+    t_exp_s = time.perf_counter() - t
+    t = time.perf_counter()
+    rho_s = pkg.correlationmatrix(small, Sz, Sz, ctx=ctx)
+    t_zz_s = time.perf_counter() - t
+    cmp = {"state": f"heisenberg L={L_CHAIN} U(1) after 2 sweeps at maxm {m_small}",
+           "device_expect_seconds": t_exp_s, "device_correlationmatrix_zz_seconds": t_zz_s}
+    if cpu:
+        from oracle import measure as omeas, models as omod
+        dense = [np.array(small[i]) for i in range(L_CHAIN)]
+        ompo = omod.make_mpo([omod.heisenberg_bulk()] * L_CHAIN, 2)
+        t = time.perf_counter()
+        E_o = omeas.expect_value(dense, ompo)
+        t_exp_o = time.perf_counter() - t
+        t = time.perf_counter()
+        rho_o = omeas.correlationmatrix(dense, small.oc, Sz, Sz)
+        t_zz_o = time.perf_counter() - t
+        cmp.update({"oracle_expect_seconds": t_exp_o, "oracle_correlationmatrix_zz_seconds": t_zz_o,
+                    "oracle_cores": cpu_threads(), "abs_dE": abs(E_s - E_o),
+                    "max_abs_drho": float(np.max(np.abs(rho_s - rho_o)))})
+    out["vs_oracle"] = cmp
+    return out
+
+
 def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
     """Heff at the dense-equivalent size of the headline workload at maxm 1024 (dense random MPS,
     bond dimension 1024 either side of the centre bond): device time per application in the plain
@@ -459,6 +512,8 @@ def run_ours(args, world, rank, local, dist):
         e2e = {"value": 1.0 / statistics.mean(e2e_times), "unit": "sweeps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "seconds_per_step": statistics.mean(e2e_times)}
+    meas = (run_measurements(pkg, ctx, dev, mpo, energy, cpu=not args.no_cpu)
+            if args.measure else None)
     serving = run_serving(pkg, local, args.serve_requests) if args.serve_requests > 0 else None
     heff_large = heff_forms(pkg, ctx) if args.chosen else None
     if rank != 0:
@@ -508,6 +563,7 @@ def run_ours(args, world, rank, local, dist):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "serving": serving,
+        "measurements": meas,
         "chosen": chosen,
         "heff_forms_m1024": heff_large,
     }
@@ -529,6 +585,8 @@ def main():
     ap.add_argument("--warmup-ref", type=int, default=1)
     ap.add_argument("--no-chosen", dest="chosen", action="store_false",
                     help="skip the split-precision (3xTF32) sweeps")
+    ap.add_argument("--no-measure", dest="measure", action="store_false",
+                    help="skip the expect / correlationmatrix measurement")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests of the serving measurement (0: skip it)")
     ap.add_argument("--ramp-sweeps", type=int, default=None,

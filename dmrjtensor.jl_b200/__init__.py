@@ -9,7 +9,8 @@ from ._lib import DmrgError, PREC, lib
 from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heisenbergCylinderMPO,
                      heisenbergMPO, hubbardMPO, makeMPO, spinOps, tfiMPO)
 from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
-                    default_context, dmrg, make_params, makeEnv, neelMPS, product_MPS, randMPS)
+                    correlationmatrix, default_context, dmrg, expect, make_params, makeEnv, neelMPS,
+                    product_MPS, randMPS)
 from .serving import Server, ServerError
 
 
@@ -25,5 +26,6 @@ __all__ = [
     "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
     "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",
     "default_context", "dmrg", "make_params", "makeEnv", "neelMPS", "product_MPS", "randMPS",
+    "expect", "correlationmatrix",
     "Server", "ServerError",
 ]

@@ -141,9 +141,12 @@ int dmrg_ctx_create(int device, size_t hbm_budget_bytes, dmrg_ctx** out) {
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
       c->nsm = device_sm_count();
       cuda_check(cudaMalloc(&c->d_scal, 256 * sizeof(double)), "scalars");
-      cuda_check(cudaMalloc(&c->d_partial, 16 * 296 * sizeof(double)), "partials");
+      // 16 rows of 296 reduction partials, then the last-block reduction counter (zeroed)
+      cuda_check(cudaMalloc(&c->d_partial, (16 * 296 + 1) * sizeof(double)), "partials");
+      cuda_check(cudaMemsetAsync(c->d_partial, 0, (16 * 296 + 1) * sizeof(double), c->stream),
+                 "partials clear");
       cuda_check(cudaMalloc(&c->d_status, 16 * sizeof(int)), "status");
-      cuda_check(cudaMemset(c->d_status, 0, 16 * sizeof(int)), "status clear");
+      cuda_check(cudaMemsetAsync(c->d_status, 0, 16 * sizeof(int), c->stream), "status clear");
       cuda_check(cudaMallocHost(&c->h_scal, 256 * sizeof(double)), "pinned scalars");
       cuda_check(cudaMalloc(&c->d_flags, c->max_groups * sizeof(int)), "flags");
       cuda_check(cudaMallocHost(&c->h_flags, c->max_groups * sizeof(int)), "pinned flags");
@@ -513,6 +516,26 @@ int dmrg_rupdate(dmrg_state* st, const dmrg_mpo* mpo, int site) {
     set_device(c);
     rupdate(st, site, nullptr);
     cuda_check(cudaStreamSynchronize(c->stream), "rupdate sync");
+  });
+}
+
+int dmrg_expect(dmrg_state* st, const dmrg_mpo* H, double* value) {
+  if (!st || !H || !value) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    if (H->ctx != c) fail(DMRG_ERR_ARG, "MPO belongs to a different context");
+    set_device(c);
+    *value = measure_expect(st, H, nullptr);
+  });
+}
+
+int dmrg_correlationmatrix(dmrg_state* st, int d, const double* Cc, const double* Ca,
+                           const double* trail, double* rho) {
+  if (!st || !Cc || !Ca || !rho || d <= 0) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    set_device(c);
+    measure_correlation(st, d, Cc, Ca, trail, rho, nullptr);
   });
 }
 

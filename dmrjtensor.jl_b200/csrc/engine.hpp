@@ -278,9 +278,35 @@ void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, dou
 // Heff with every intermediate in the library's fixed device array (noalloc.cu).
 void heff_apply_noalloc(dmrg_state* st, int iL, const double* in_dev, double* out_dev);
 
+// One environment step through one site (lib/MPO_MPS/Lupdate.jl:17-26, Rupdate.jl:17-26):
+// g1 (env_in, A) -> T1, mix T1 -> T2 (the MPO site), g3 (A, T2) -> env_out in layout `out`.
+struct StepPlan {
+  GemmList g1, g3;
+  MixList mx;
+  EnvLayout out;
+  int64_t t1 = 0, t2 = 0;   // scratch sizes in doubles
+  double flops() const { return g1.flops + g3.flops + mx.flops; }
+};
+void plan_left_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const SiteLayout& lay,
+                    const EnvLayout& LL, StepPlan& sp);
+void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const SiteLayout& lay,
+                     const EnvLayout& RL, StepPlan& sp);
+void put_step(Upload& u, StepPlan& sp);
+// Launches an uploaded step; c->T1 / c->T2 must hold sp.t1 / sp.t2 doubles.
+void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, int64_t n_in,
+              const DBuf& A, double* env_out, int64_t n_out);
+
 void env_boundaries(dmrg_state* st);
 void lupdate(dmrg_state* st, int i, double* flops);
 void rupdate(dmrg_state* st, int i, double* flops);
+
+// ---- measurements (engine_meas.cpp)
+// <psi|H|psi> for an MPO over the same sites and physical charges (not normalised).
+double measure_expect(dmrg_state* st, const dmrg_mpo* H, double* flops);
+// rho (L x L, column-major): two-point correlations of Cc and Ca with an optional trail F
+// (d x d column-major operators [bra, ket]; F may be null), normalised by <psi|psi>.
+void measure_correlation(dmrg_state* st, int d, const double* Cc, const double* Ca,
+                         const double* F, double* rho, double* flops);
 
 // ---- eigensolves (engine_eig.cpp)
 int64_t eig_workspace(const std::vector<EigTask>& tasks);

@@ -207,23 +207,22 @@ void env_boundaries(dmrg_state* st) {
   st->Rvalid[L - 1] = 1;
 }
 
-void lupdate(dmrg_state* st, int i, double* flops) {
-  dmrg_ctx* c = st->ctx;
-  if (i < 0 || i + 1 >= st->L) fail(DMRG_ERR_ARG, "lupdate: site out of range");
-  if (!st->Lvalid[i]) fail(DMRG_ERR_STATE, "lupdate: Lenv[site] has not been built");
-  const Bond& Bl = st->bond[i];
-  const Bond& Br = st->bond[i + 1];
-  const MPOSite& ms = st->mpo->site[i];
-  const SiteLayout& lay = st->lay[i];
-  const EnvLayout& LL = st->Llay[i];
-  EnvLayout LN = make_left_env_layout(Br, ms.rr);
+void plan_left_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const SiteLayout& lay,
+                    const EnvLayout& LL, StepPlan& sp) {
+  sp.out = make_left_env_layout(Br, ms.rr);
+  const EnvLayout& LN = sp.out;
   const int d = ms.d, wl = ms.wl, wr = ms.wr;
 
-  GemmList g1, g3;
-  MixList mx;
+  GemmList& g1 = sp.g1;
+  GemmList& g3 = sp.g3;
+  MixList& mx = sp.mx;
+  g1.clear();
+  g3.clear();
+  mx.clear();
   g3.tA = true;
   std::vector<int64_t> t1off(Bl.nsec(), 0);
-  int64_t t1 = 0;
+  int64_t& t1 = sp.t1;
+  t1 = 0;
   for (int kb = 0; kb < Bl.nsec(); ++kb) {
     t1off[kb] = t1;
     t1 += int64_t(LL.rows[kb]) * lay.gcols[kb];
@@ -239,7 +238,8 @@ void lupdate(dmrg_state* st, int i, double* flops) {
 
   struct Out { int kbp, w2, rows; int64_t off; std::vector<int> ka, roff; };
   std::vector<Out> outs;
-  int64_t t2 = 0;
+  int64_t& t2 = sp.t2;
+  t2 = 0;
   for (int kbp = 0; kbp < Br.nsec(); ++kbp)
     for (int w2 = 0; w2 < wr; ++w2) {
       const int kap = LN.other[kbp * wr + w2];
@@ -279,40 +279,24 @@ void lupdate(dmrg_state* st, int i, double* flops) {
       g3.seg(lay.off[ka * d + t], Bl.dim[ka], o.off + o.roff[t], o.rows, Bl.dim[ka]);
     }
   }
-  Upload u;
-  u.put(g1);
-  u.put(mx);
-  u.put(g3);
-  char* db = u.send(c, 2);
-  ensure(c, c->T1, std::max<int64_t>(t1, 1));
-  ensure(c, c->T2, std::max<int64_t>(t2, 1));
-  st->Llay[i + 1] = LN;
-  dalloc(c, st->Lenv[i + 1], std::max<int64_t>(LN.size, 1));
-  run_gemm(c, g1, db, st->Lenv[i].p, st->Lenv[i].n, st->A[i].p, st->A[i].n, c->T1.p, c->T1.n);
-  run_mix(c, mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
-  run_gemm(c, g3, db, st->A[i].p, st->A[i].n, c->T2.p, c->T2.n, st->Lenv[i + 1].p,
-           st->Lenv[i + 1].n);
-  st->Lvalid[i + 1] = 1;
-  if (flops) *flops += g1.flops + g3.flops + mx.flops;
 }
 
-void rupdate(dmrg_state* st, int i, double* flops) {
-  dmrg_ctx* c = st->ctx;
-  if (i <= 0 || i >= st->L) fail(DMRG_ERR_ARG, "rupdate: site out of range");
-  if (!st->Rvalid[i]) fail(DMRG_ERR_STATE, "rupdate: Renv[site] has not been built");
-  const Bond& Bl = st->bond[i];
-  const Bond& Br = st->bond[i + 1];
-  const MPOSite& ms = st->mpo->site[i];
-  const SiteLayout& lay = st->lay[i];
-  const EnvLayout& RL = st->Rlay[i];
-  EnvLayout RN = make_right_env_layout(Bl, ms.rl);
+void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const SiteLayout& lay,
+                     const EnvLayout& RL, StepPlan& sp) {
+  sp.out = make_right_env_layout(Bl, ms.rl);
+  const EnvLayout& RN = sp.out;
   const int d = ms.d, wl = ms.wl, wr = ms.wr;
 
-  GemmList g1, g3;
-  MixList mx;
+  GemmList& g1 = sp.g1;
+  GemmList& g3 = sp.g3;
+  MixList& mx = sp.mx;
+  g1.clear();
+  g3.clear();
+  mx.clear();
   g1.tB = true;
   std::vector<int64_t> t1off(size_t(Bl.nsec()) * d, -1);
-  int64_t t1 = 0;
+  int64_t& t1 = sp.t1;
+  t1 = 0;
   for (int ka = 0; ka < Bl.nsec(); ++ka)
     for (int t = 0; t < d; ++t) {
       const int kap = lay.kb[ka * d + t];
@@ -331,7 +315,8 @@ void rupdate(dmrg_state* st, int i, double* flops) {
   for (const auto& e : ms.nz) byWS[size_t(e.w) * d + e.s].push_back(&e);
 
   std::vector<int64_t> t2off(size_t(Bl.nsec()) * wl, -1);
-  int64_t t2 = 0;
+  int64_t& t2 = sp.t2;
+  t2 = 0;
   for (int ka = 0; ka < Bl.nsec(); ++ka)
     for (int w = 0; w < wl; ++w) {
       const int kb = RN.other[ka * wl + w];
@@ -364,21 +349,59 @@ void rupdate(dmrg_state* st, int i, double* flops) {
       if (lay.gcols[kb] > 0)
         g3.seg(lay.goff[kb], Bl.dim[kb], t2off[ka * wl + w], lay.gcols[kb], lay.gcols[kb]);
     }
+}
+
+void put_step(Upload& u, StepPlan& sp) {
+  u.put(sp.g1);
+  u.put(sp.mx);
+  u.put(sp.g3);
+}
+
+void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, int64_t n_in,
+              const DBuf& A, double* env_out, int64_t n_out) {
+  if (c->T1.n < sp.t1 || c->T2.n < sp.t2 || n_out < sp.out.size)
+    fail(DMRG_ERR_ARG, "internal plan check failed: environment step scratch too small");
+  run_gemm(c, sp.g1, db, env_in, n_in, A.p, A.n, c->T1.p, c->T1.n);
+  run_mix(c, sp.mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
+  run_gemm(c, sp.g3, db, A.p, A.n, c->T2.p, c->T2.n, env_out, n_out);
+}
+
+void lupdate(dmrg_state* st, int i, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  if (i < 0 || i + 1 >= st->L) fail(DMRG_ERR_ARG, "lupdate: site out of range");
+  if (!st->Lvalid[i]) fail(DMRG_ERR_STATE, "lupdate: Lenv[site] has not been built");
+  StepPlan sp;
+  plan_left_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Llay[i], sp);
   Upload u;
-  u.put(g1);
-  u.put(mx);
-  u.put(g3);
+  put_step(u, sp);
   char* db = u.send(c, 2);
-  ensure(c, c->T1, std::max<int64_t>(t1, 1));
-  ensure(c, c->T2, std::max<int64_t>(t2, 1));
-  st->Rlay[i - 1] = RN;
-  dalloc(c, st->Renv[i - 1], std::max<int64_t>(RN.size, 1));
-  run_gemm(c, g1, db, st->Renv[i].p, st->Renv[i].n, st->A[i].p, st->A[i].n, c->T1.p, c->T1.n);
-  run_mix(c, mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
-  run_gemm(c, g3, db, st->A[i].p, st->A[i].n, c->T2.p, c->T2.n, st->Renv[i - 1].p,
+  ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
+  ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));
+  st->Llay[i + 1] = sp.out;
+  dalloc(c, st->Lenv[i + 1], std::max<int64_t>(sp.out.size, 1));
+  run_step(c, sp, db, st->Lenv[i].p, st->Lenv[i].n, st->A[i], st->Lenv[i + 1].p,
+           st->Lenv[i + 1].n);
+  st->Lvalid[i + 1] = 1;
+  if (flops) *flops += sp.flops();
+}
+
+void rupdate(dmrg_state* st, int i, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  if (i <= 0 || i >= st->L) fail(DMRG_ERR_ARG, "rupdate: site out of range");
+  if (!st->Rvalid[i]) fail(DMRG_ERR_STATE, "rupdate: Renv[site] has not been built");
+  StepPlan sp;
+  plan_right_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Rlay[i], sp);
+  Upload u;
+  put_step(u, sp);
+  char* db = u.send(c, 2);
+  ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
+  ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));
+  st->Rlay[i - 1] = sp.out;
+  dalloc(c, st->Renv[i - 1], std::max<int64_t>(sp.out.size, 1));
+  run_step(c, sp, db, st->Renv[i].p, st->Renv[i].n, st->A[i], st->Renv[i - 1].p,
            st->Renv[i - 1].n);
   st->Rvalid[i - 1] = 1;
-  if (flops) *flops += g1.flops + g3.flops + mx.flops;
+  if (flops) *flops += sp.flops();
 }
 
 }  // namespace dmrg

@@ -1,0 +1,367 @@
+// engine_meas.cpp -- measurements of a device MPS.
+//
+// expect (lib/MPO_MPS/expect.jl:19-56): <psi|H|psi> for an MPO H over the same sites, as a chain
+// of left environment steps from the boundary to the last bond. Not normalised, as in the
+// reference.
+//
+// correlationmatrix (lib/MPO_MPS/correlationmatrix.jl:21-56): for single-site operators Cc, Ca
+// and an optional trail F (a Jordan-Wigner string),
+//   rho[i,j] = <psi|(Cc F)_i F_{i+1} ... F_{j-1} Ca_j|psi> / <psi|psi>   (i < j),
+//   rho[j,i] = rho[i,j],   rho[i,i] = <psi|(Cc Ca)_i|psi> / <psi|psi>.
+// The reference moves the orthogonality centre to each i and contracts locally, relying on the
+// canonical form. The values are gauge-invariant, so the device leaves the centre where it is and
+// contracts with identity transfers from both ends instead:
+//   EL[b]  left identity environment at bond b,  ER[b]  right identity environment at bond b,
+//   RC[j]  right step of ER[j+1] through Ca at site j,
+//   row i: X = left step of EL[i] through (Cc F) at site i; for j > i, rho[i,j] = <X | RC[j]> at
+//          bond j, then X = left step of X through F at site j.
+// Operators are d x d column-major with the reference's orientation O[bra, ket] and act on the
+// ket (contract(O, 2, psi[i], 2)). As an MPO site W[0, s(ket), t(bra), 0] = O[t, s]; under
+// charge conservation an operator must change the charge by one fixed amount, which becomes the
+// label of the w = 1 environment bond (r(w') = r(w) + p(ket) - p(bra)).
+//
+// Every step of a measurement is planned on the host and uploaded in one descriptor copy; the
+// launches then run back to back on the context stream and the results are read back once.
+#include <algorithm>
+#include <cmath>
+
+#include "engine.hpp"
+
+namespace dmrg {
+namespace {
+
+constexpr int MEAS_SLOT = 7;   // descriptor slot of the measurement plans (unused by the sweep)
+
+// O[bra, ket] as a one-state MPO site. `label` is the left label (left_known) or the right one.
+MPOSite op_site(const std::vector<double>& O, int d, const std::vector<QN>& p, QN label,
+                bool left_known) {
+  MPOSite ms;
+  ms.wl = ms.wr = 1;
+  ms.d = d;
+  ms.p = p;
+  ms.dense.assign(size_t(d) * d, 0.0);
+  bool have = false;
+  QN delta;
+  for (int s = 0; s < d; ++s)
+    for (int t = 0; t < d; ++t) {
+      const double v = O[size_t(t) + size_t(s) * d];
+      if (v == 0.0) continue;
+      const QN dq = p[t] - p[s];   // charge added by the operator: p(bra) - p(ket)
+      if (have && dq != delta)
+        fail(DMRG_ERR_QN, "operator does not change the charge by one fixed amount");
+      delta = dq;
+      have = true;
+      ms.nz.push_back({0, s, t, 0, v});
+      ms.dense[size_t(s) + size_t(t) * d] = v;
+    }
+  if (left_known) {
+    ms.rl = {label};
+    ms.rr = {label - delta};
+  } else {
+    ms.rr = {label};
+    ms.rl = {label + delta};
+  }
+  return ms;
+}
+
+std::vector<double> matmul(const std::vector<double>& A, const std::vector<double>& B, int d) {
+  std::vector<double> C(size_t(d) * d, 0.0);
+  for (int j = 0; j < d; ++j)
+    for (int k = 0; k < d; ++k) {
+      const double b = B[size_t(k) + size_t(j) * d];
+      if (b == 0.0) continue;
+      for (int i = 0; i < d; ++i) C[size_t(i) + size_t(j) * d] += A[size_t(i) + size_t(k) * d] * b;
+    }
+  return C;
+}
+
+// Pair contraction at bond B of an L-type environment X and an R-type environment Y, both w = 1.
+struct PairPlan {
+  std::vector<PairTask> t;
+  int64_t total = 0;
+  size_t off = 0;
+};
+
+PairPlan plan_pair(const Bond& B, const EnvLayout& X, const EnvLayout& Y) {
+  PairPlan pp;
+  if (X.w != 1 || Y.w != 1) fail(DMRG_ERR_ARG, "pair contraction needs one-state environments");
+  for (int k = 0; k < B.nsec(); ++k) {   // ket sector
+    const int kx = X.other[k];           // bra sector of X's block
+    if (kx < 0 || Y.other[kx] != k) continue;
+    PairTask t;
+    t.x_off = X.goff[k] + X.rowoff[k];
+    t.y_off = Y.goff[kx] + Y.rowoff[kx];
+    t.rows = B.dim[kx];
+    t.cols = B.dim[k];
+    t.e0 = pp.total;
+    if (int64_t(t.rows) * t.cols == 0) continue;
+    pp.total += int64_t(t.rows) * t.cols;
+    pp.t.push_back(t);
+  }
+  return pp;
+}
+
+void check_pair(const PairPlan& pp, int64_t nX, int64_t nY) {
+  for (const PairTask& t : pp.t) {
+    const int64_t last = int64_t(t.rows) * t.cols - 1;
+    if (t.x_off < 0 || t.y_off < 0 || t.x_off + last >= nX || t.y_off + last >= nY)
+      fail(DMRG_ERR_ARG, "internal plan check failed: pair contraction out of bounds");
+  }
+}
+
+void run_pair(dmrg_ctx* c, const PairPlan& pp, char* db, const DBuf& X, const DBuf& Y,
+              double* out) {
+  check_pair(pp, X.n, Y.n);
+  launch_pair_dot(c->stream, X.p, Y.p, reinterpret_cast<const PairTask*>(db + pp.off),
+                  int(pp.t.size()), pp.total, c->d_partial, out);
+}
+
+void set_one(dmrg_ctx* c, DBuf& b) {
+  static const double one = 1.0;
+  cuda_check(cudaMemcpyAsync(b.p, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream),
+             "measurement boundary");
+}
+
+int64_t plan_scratch(const StepPlan& sp, int64_t& t1, int64_t& t2) {
+  t1 = std::max(t1, sp.t1);
+  t2 = std::max(t2, sp.t2);
+  return sp.out.size;
+}
+
+void check_edges(const dmrg_state* st) {
+  const Bond& b0 = st->bond[0];
+  const Bond& bL = st->bond[st->L];
+  if (b0.nsec() != 1 || b0.dim[0] != 1 || bL.nsec() != 1 || bL.dim[0] != 1)
+    fail(DMRG_ERR_SHAPE, "edge bonds of the MPS must be one-dimensional");
+}
+
+}  // namespace
+
+double measure_expect(dmrg_state* st, const dmrg_mpo* H, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  const int L = st->L;
+  if (!H || H->L != L) fail(DMRG_ERR_SHAPE, "expect: MPO length differs from the state's");
+  if (H->nsym != st->nsym) fail(DMRG_ERR_QN, "expect: MPO and state carry different charges");
+  for (int i = 0; i < L; ++i) {
+    const MPOSite& a = H->site[i];
+    const MPOSite& b = st->mpo->site[i];
+    if (a.d != b.d) fail(DMRG_ERR_SHAPE, "expect: physical dimension differs at a site");
+    for (int s = 0; s < a.d; ++s)
+      if (a.p[s] != b.p[s]) fail(DMRG_ERR_QN, "expect: physical charges differ at a site");
+  }
+  if (H->site[0].wl != 1 || H->site[L - 1].wr != 1)
+    fail(DMRG_ERR_SHAPE, "edge bonds of the MPO must be one-dimensional");
+  check_edges(st);
+
+  std::vector<StepPlan> sp(L);
+  EnvLayout E0 = make_left_env_layout(st->bond[0], H->site[0].rl);
+  if (E0.other[0] != 0) fail(DMRG_ERR_QN, "MPO edge labels do not connect the MPS edge sectors");
+  int64_t t1 = 1, t2 = 1, emax = 1;
+  Upload u;
+  for (int i = 0; i < L; ++i) {
+    plan_left_step(st->bond[i], st->bond[i + 1], H->site[i], st->lay[i], i ? sp[i - 1].out : E0,
+                   sp[i]);
+    emax = std::max(emax, plan_scratch(sp[i], t1, t2));
+    put_step(u, sp[i]);
+  }
+  char* db = u.send(c, MEAS_SLOT);
+  ensure(c, c->T1, t1);
+  ensure(c, c->T2, t2);
+  DBuf P[2];
+  double value = 0.0;
+  try {
+    dalloc(c, P[0], emax);
+    dalloc(c, P[1], emax);
+    set_one(c, P[1]);
+    double fl = 0.0;
+    for (int i = 0; i < L; ++i) {
+      const DBuf& in = P[(i + 1) & 1];
+      DBuf& out = P[i & 1];
+      run_step(c, sp[i], db, in.p, in.n, st->A[i], out.p, out.n);
+      fl += sp[i].flops();
+    }
+    cuda_check(cudaGetLastError(), "expect launches");
+    const EnvLayout& EL = sp[L - 1].out;
+    if (EL.size >= 1)
+      cuda_check(cudaMemcpyAsync(c->h_scal, P[(L - 1) & 1].p, sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream), "expect download");
+    cuda_check(cudaStreamSynchronize(c->stream), "expect sync");
+    value = EL.size >= 1 ? c->h_scal[0] : 0.0;
+    if (flops) *flops = fl;
+  } catch (...) {
+    dfree(c, P[0]);
+    dfree(c, P[1]);
+    throw;
+  }
+  dfree(c, P[0]);
+  dfree(c, P[1]);
+  return value;
+}
+
+void measure_correlation(dmrg_state* st, int d, const double* Cc_, const double* Ca_,
+                         const double* F_, double* rho, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  const int L = st->L;
+  for (int i = 0; i < L; ++i)
+    if (st->mpo->site[i].d != d)
+      fail(DMRG_ERR_SHAPE, "correlationmatrix: operator dimension differs from a site's");
+  check_edges(st);
+  const size_t dd = size_t(d) * d;
+  std::vector<double> Cc(Cc_, Cc_ + dd), Ca(Ca_, Ca_ + dd), Id(dd, 0.0);
+  for (int a = 0; a < d; ++a) Id[size_t(a) * (d + 1)] = 1.0;
+  std::vector<double> F = F_ ? std::vector<double>(F_, F_ + dd) : Id;
+  const std::vector<double> FCc = matmul(Cc, F, d);      // contract(Cc, 2, trail, 1)
+  const std::vector<double> onsite = matmul(Cc, Ca, d);  // contract(Cc, 2, Ca, 1)
+  const QN zero;
+
+  // ---- plans
+  std::vector<EnvLayout> ELl(L + 1), ERl(L + 1);
+  std::vector<StepPlan> spL(L), spR(L), spC(L);
+  ELl[0] = make_left_env_layout(st->bond[0], {zero});
+  ERl[L] = make_right_env_layout(st->bond[L], {zero});
+  if (ELl[0].other[0] != 0 || ERl[L].other[0] != 0)
+    fail(DMRG_ERR_QN, "edge sectors of the MPS do not connect");
+  int64_t t1 = 1, t2 = 1;
+  Upload u;
+  for (int i = 0; i < L; ++i) {
+    const MPOSite id = op_site(Id, d, st->mpo->site[i].p, zero, true);
+    plan_left_step(st->bond[i], st->bond[i + 1], id, st->lay[i], ELl[i], spL[i]);
+    ELl[i + 1] = spL[i].out;
+    plan_scratch(spL[i], t1, t2);
+    put_step(u, spL[i]);
+  }
+  for (int i = L - 1; i >= 0; --i) {
+    const MPOSite id = op_site(Id, d, st->mpo->site[i].p, zero, true);
+    plan_right_step(st->bond[i], st->bond[i + 1], id, st->lay[i], ERl[i + 1], spR[i]);
+    ERl[i] = spR[i].out;
+    plan_scratch(spR[i], t1, t2);
+    put_step(u, spR[i]);
+  }
+  for (int j = 1; j < L; ++j) {
+    const MPOSite ca = op_site(Ca, d, st->mpo->site[j].p, zero, false);
+    plan_right_step(st->bond[j], st->bond[j + 1], ca, st->lay[j], ERl[j + 1], spC[j]);
+    plan_scratch(spC[j], t1, t2);
+    put_step(u, spC[j]);
+  }
+  struct Row {
+    StepPlan diag;
+    PairPlan diag_pair;
+    std::vector<StepPlan> steps;     // steps[0]: (Cc F) at site i; steps[k]: F at site i + k
+    std::vector<PairPlan> pairs;     // pairs[k]: X at bond i + 1 + k with RC[i + 1 + k]
+  };
+  std::vector<Row> rows(L);
+  int64_t dmax = 1, xmax = 1;
+  for (int i = 0; i < L; ++i) {
+    Row& r = rows[i];
+    const MPOSite on = op_site(onsite, d, st->mpo->site[i].p, zero, true);
+    plan_left_step(st->bond[i], st->bond[i + 1], on, st->lay[i], ELl[i], r.diag);
+    dmax = std::max(dmax, plan_scratch(r.diag, t1, t2));
+    put_step(u, r.diag);
+    r.diag_pair = plan_pair(st->bond[i + 1], r.diag.out, ERl[i + 1]);
+    r.diag_pair.off = u.put(r.diag_pair.t);
+    if (i + 1 >= L) continue;
+    r.steps.resize(L - 1 - i);
+    const MPOSite fc = op_site(FCc, d, st->mpo->site[i].p, zero, true);
+    plan_left_step(st->bond[i], st->bond[i + 1], fc, st->lay[i], ELl[i], r.steps[0]);
+    const QN label = fc.rr[0];
+    for (int j = i + 1; j < L; ++j) {
+      const StepPlan& cur = r.steps[j - i - 1];
+      xmax = std::max(xmax, plan_scratch(cur, t1, t2));
+      put_step(u, r.steps[j - i - 1]);
+      r.pairs.push_back(plan_pair(st->bond[j], cur.out, spC[j].out));
+      r.pairs.back().off = u.put(r.pairs.back().t);
+      if (j + 1 < L) {
+        const MPOSite f = op_site(F, d, st->mpo->site[j].p, label, true);
+        plan_left_step(st->bond[j], st->bond[j + 1], f, st->lay[j], cur.out, r.steps[j - i]);
+      }
+    }
+  }
+  PairPlan norm = plan_pair(st->bond[L], ELl[L], ERl[L]);
+  norm.off = u.put(norm.t);
+
+  // ---- device buffers and launches
+  std::vector<DBuf> EL(L + 1), ER(L + 1), RC(L);
+  DBuf D, X[2], out;
+  auto release = [&] {
+    for (auto& b : EL) dfree(c, b);
+    for (auto& b : ER) dfree(c, b);
+    for (auto& b : RC) dfree(c, b);
+    dfree(c, D);
+    dfree(c, X[0]);
+    dfree(c, X[1]);
+    dfree(c, out);
+  };
+  try {
+    char* db = u.send(c, MEAS_SLOT);
+    ensure(c, c->T1, t1);
+    ensure(c, c->T2, t2);
+    for (int b = 0; b <= L; ++b) {
+      dalloc(c, EL[b], std::max<int64_t>(ELl[b].size, 1));
+      dalloc(c, ER[b], std::max<int64_t>(ERl[b].size, 1));
+    }
+    for (int j = 1; j < L; ++j) dalloc(c, RC[j], std::max<int64_t>(spC[j].out.size, 1));
+    dalloc(c, D, dmax);
+    dalloc(c, X[0], xmax);
+    dalloc(c, X[1], xmax);
+    dalloc(c, out, int64_t(L) * L + 1);
+    cuda_check(cudaMemsetAsync(out.p, 0, sizeof(double) * (size_t(L) * L + 1), c->stream),
+               "correlation clear");
+    set_one(c, EL[0]);
+    set_one(c, ER[L]);
+    double fl = 0.0;
+    for (int i = 0; i < L; ++i) {
+      run_step(c, spL[i], db, EL[i].p, EL[i].n, st->A[i], EL[i + 1].p, EL[i + 1].n);
+      fl += spL[i].flops();
+    }
+    for (int i = L - 1; i >= 0; --i) {
+      run_step(c, spR[i], db, ER[i + 1].p, ER[i + 1].n, st->A[i], ER[i].p, ER[i].n);
+      fl += spR[i].flops();
+    }
+    for (int j = 1; j < L; ++j) {
+      run_step(c, spC[j], db, ER[j + 1].p, ER[j + 1].n, st->A[j], RC[j].p, RC[j].n);
+      fl += spC[j].flops();
+    }
+    for (int i = 0; i < L; ++i) {
+      Row& r = rows[i];
+      run_step(c, r.diag, db, EL[i].p, EL[i].n, st->A[i], D.p, D.n);
+      run_pair(c, r.diag_pair, db, D, ER[i + 1], out.p + i + int64_t(i) * L);
+      fl += r.diag.flops() + 2.0 * r.diag_pair.total;
+      if (i + 1 >= L) continue;
+      const DBuf* in = &EL[i];
+      for (int j = i + 1; j < L; ++j) {
+        const StepPlan& sp = r.steps[j - i - 1];
+        DBuf& xo = X[(j - i - 1) & 1];
+        run_step(c, sp, db, in->p, in->n, st->A[j - 1], xo.p, xo.n);
+        fl += sp.flops();
+        const PairPlan& pp = r.pairs[j - i - 1];
+        run_pair(c, pp, db, xo, RC[j], out.p + i + int64_t(j) * L);
+        fl += 2.0 * pp.total;
+        in = &xo;
+      }
+    }
+    run_pair(c, norm, db, EL[L], ER[L], out.p + int64_t(L) * L);
+    cuda_check(cudaGetLastError(), "correlation launches");
+    std::vector<double> h(size_t(L) * L + 1);
+    cuda_check(cudaMemcpyAsync(h.data(), out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                               c->stream), "correlation download");
+    cuda_check(cudaStreamSynchronize(c->stream), "correlation sync");
+    const double nrm = h[size_t(L) * L];
+    if (!(nrm > 0.0) || !std::isfinite(nrm))
+      fail(DMRG_ERR_STATE, "correlationmatrix: <psi|psi> is not positive");
+    for (int i = 0; i < L; ++i) {
+      rho[i + size_t(i) * L] = h[i + size_t(i) * L] / nrm;
+      for (int j = i + 1; j < L; ++j) {
+        const double v = h[i + size_t(j) * L] / nrm;
+        rho[i + size_t(j) * L] = v;
+        rho[j + size_t(i) * L] = v;
+      }
+    }
+    if (flops) *flops = fl;
+  } catch (...) {
+    release();
+    throw;
+  }
+  release();
+}
+
+}  // namespace dmrg

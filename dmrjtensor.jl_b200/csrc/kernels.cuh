@@ -51,6 +51,14 @@ struct CopyTask {
   double scale;
 };
 
+// One block pair of an environment contraction across a bond: sum_{r,c} X[x_off + r + c*rows] *
+// Y[y_off + c + r*cols] (an L-type block [bra x ket] against the R-type block [ket x bra]).
+// Tasks are sorted by e0, the first element of the task in the flattened element range.
+struct PairTask {
+  int64_t x_off, y_off, e0;
+  int rows, cols;
+};
+
 // Symmetric eigenproblem of an n x n column-major matrix at a_off (leading dim n); eigenvalues
 // go to w_off (n doubles, descending) and eigenvectors (columns, same order) to v_off (n x n).
 struct EigTask {
@@ -146,6 +154,9 @@ void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, 
                         int j, double betatest);
 // lowest Ritz pair of the Krylov tridiagonal: s[EN], s[COEF + j]
 void launch_ritz(cudaStream_t s, double* scal, int kdim);
+// out[0] = sum over the pair tasks (total elements `total`; deterministic order)
+void launch_pair_dot(cudaStream_t s, const double* X, const double* Y, const PairTask* tasks,
+                     int ntasks, int64_t total, double* partial, double* out);
 // y = sum_j c[j] X_j, j < k
 void launch_lincomb(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c,
                     double* y, int64_t n);

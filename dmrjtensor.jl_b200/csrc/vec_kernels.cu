@@ -1,6 +1,8 @@
 // vec_kernels.cu -- memory-bound kernels of the sweep: sparse MPO mixing of block lists,
 // strided block copies (gathers/scatters), and the Lanczos vector operations with deterministic
 // two-stage warp-shuffle reductions (fixed grid, fixed order: bit-identical from run to run).
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace dmrg {
@@ -15,6 +17,38 @@ __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Last-block reduction: every block has written its row partials; the block that arrives last
+// (atomic counter, after a fence) sums them in the fixed order of a separate reduction kernel,
+// writes out[0..k), and resets the counter for the next kernel on the stream.
+__device__ __forceinline__ bool arrive_last(unsigned* counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  return last;
+}
+
+__device__ void finish_rows(const double* partial, int nb, int k, double* out, unsigned* counter) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) / 32;
+  __threadfence();
+  for (int j = 0; j < k; ++j) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += __ldcg(partial + j * nb + b);
+    s = warp_sum(s);
+    if (lane == 0) red[wid] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += red[w];
+      out[j] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
 __global__ void k_mix(const double* __restrict__ in, double* __restrict__ out,
@@ -63,9 +97,11 @@ __global__ void k_copy(const double* __restrict__ src, double* __restrict__ dst,
   }
 }
 
-// partial[j*gridDim + b] = sum over this block's share of X_j . y
+// partial[j*gridDim + b] = sum over this block's share of X_j . y; the last block to finish
+// writes out[j] = sum_b partial[j*gridDim + b].
 __global__ void k_mdot_partial(const double* __restrict__ X, int64_t ldx, int k,
-                               const double* __restrict__ y, int64_t n, double* partial) {
+                               const double* __restrict__ y, int64_t n, double* partial,
+                               double* out, unsigned* counter) {
   double acc[MAXK];
 #pragma unroll
   for (int j = 0; j < MAXK; ++j) acc[j] = 0.0;
@@ -91,21 +127,36 @@ __global__ void k_mdot_partial(const double* __restrict__ X, int64_t ldx, int k,
     for (int w = 0; w < RED_THREADS / 32; ++w) s += red[threadIdx.x][w];
     partial[threadIdx.x * gridDim.x + blockIdx.x] = s;
   }
+  if (arrive_last(counter)) finish_rows(partial, gridDim.x, k, out, counter);
 }
 
-__global__ void k_reduce_rows(const double* __restrict__ partial, int nb, double* out) {
-  const int j = blockIdx.x;
-  double s = 0.0;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[j * nb + b];
-  s = warp_sum(s);
-  __shared__ double red[32];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+__global__ void k_pair_dot(const double* __restrict__ X, const double* __restrict__ Y,
+                           const PairTask* __restrict__ tasks, int ntasks, int64_t total,
+                           double* partial, double* out, unsigned* counter) {
+  double acc = 0.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += stride) {
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tasks[mid].e0 <= e) lo = mid; else hi = mid - 1;
+    }
+    const PairTask tk = tasks[lo];
+    const int64_t q = e - tk.e0;
+    const int64_t r = q % tk.rows, c = q / tk.rows;
+    acc += X[tk.x_off + q] * Y[tk.y_off + c + r * tk.cols];
+  }
+  __shared__ double red[RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  acc = warp_sum(acc);
+  if (lane == 0) red[wid] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int w = 0; w < (blockDim.x + 31) / 32; ++w) t += red[w];
-    out[j] = t;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += red[w];
+    partial[blockIdx.x] = t;
   }
+  if (arrive_last(counter)) finish_rows(partial, gridDim.x, 1, out, counter);
 }
 
 __global__ void k_axpby(int64_t n, double a, const double* ap, double asign,
@@ -151,7 +202,7 @@ __global__ void k_scale_rsqrt(double* x, int64_t n, const double* nrm2) {
 
 // partial rows 0/1: this block's share of <x,x> and <x,y>
 __global__ void k_dot2_partial(const double* __restrict__ x, const double* __restrict__ y,
-                               int64_t n, double* partial) {
+                               int64_t n, double* partial, double* out, unsigned* counter) {
   double sxx = 0.0, sxy = 0.0;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -170,12 +221,14 @@ __global__ void k_dot2_partial(const double* __restrict__ x, const double* __res
     for (int w = 0; w < RED_THREADS / 32; ++w) s += red[threadIdx.x][w];
     partial[threadIdx.x * gridDim.x + blockIdx.x] = s;
   }
+  if (arrive_last(counter)) finish_rows(partial, gridDim.x, 2, out, counter);
 }
 
 // First half of the reference 2-vector Krylov step, from s[KK] = <K,K> and s[KH] = <K,HK>:
 // K <- K / |K|, a1 = <K,HK> / |K| (stored at s[ALPHA]), H <- H - a1 K, and this block's share
 // of <H,H> in partial row 0.
-__global__ void k_lanczos2_orth(double* K, double* H, int64_t n, double* s, double* partial) {
+__global__ void k_lanczos2_orth(double* K, double* H, int64_t n, double* s, double* partial,
+                                unsigned* counter) {
   const double nn = sqrt(s[lz::KK]);
   const double inv = 1.0 / nn;
   const double a1 = s[lz::KH] / nn;
@@ -199,6 +252,7 @@ __global__ void k_lanczos2_orth(double* K, double* H, int64_t n, double* s, doub
     partial[blockIdx.x] = t;
     if (blockIdx.x == 0) s[lz::ALPHA] = a1;
   }
+  if (arrive_last(counter)) finish_rows(partial, gridDim.x, 1, s + lz::B2, counter);
 }
 
 // Next Krylov vector K_{j+1} = H / beta_j with beta_j = sqrt(s[B2+j]), or 0 once the recursion
@@ -295,6 +349,12 @@ __global__ void k_lincomb(const double* __restrict__ X, int64_t ldx, int k,
   }
 }
 
+// The context's partial array holds MAXK rows of RED_BLOCKS partials followed by one unsigned
+// counter for the last-block reductions.
+unsigned* reduction_counter(double* partial) {
+  return reinterpret_cast<unsigned*>(partial + MAXK * RED_BLOCKS);
+}
+
 int grid_for(int64_t n) {
   int64_t b = (n + RED_THREADS - 1) / RED_THREADS;
   if (b > 4 * RED_BLOCKS) b = 4 * RED_BLOCKS;
@@ -322,9 +382,9 @@ void launch_copy(cudaStream_t s, const double* src, double* dst, const CopyTask*
 
 void launch_mdot(cudaStream_t s, const double* X, int64_t ldx, int k, const double* y, int64_t n,
                  double* partial, double* out) {
-  k_mdot_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(X, ldx, k, y, n, partial);
-  k_reduce_rows<<<k, 256, 0, s>>>(partial, RED_BLOCKS, out);
-  count_launch(2);
+  k_mdot_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(X, ldx, k, y, n, partial, out,
+                                                    reduction_counter(partial));
+  count_launch();
 }
 
 void launch_axpby(cudaStream_t s, int64_t n, double a, const double* ap, double asign,
@@ -356,16 +416,28 @@ void launch_scale_rsqrt(cudaStream_t s, double* x, int64_t n, const double* nrm2
 
 void launch_dot2(cudaStream_t s, const double* x, const double* y, int64_t n, double* partial,
                  double* out) {
-  k_dot2_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, y, n, partial);
-  k_reduce_rows<<<2, 256, 0, s>>>(partial, RED_BLOCKS, out);
-  count_launch(2);
+  k_dot2_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, y, n, partial, out,
+                                                    reduction_counter(partial));
+  count_launch();
 }
 
 void launch_lanczos2_orth(cudaStream_t s, double* K, double* H, int64_t n, double* scal,
                           double* partial) {
-  k_lanczos2_orth<<<RED_BLOCKS, RED_THREADS, 0, s>>>(K, H, n, scal, partial);
-  k_reduce_rows<<<1, 256, 0, s>>>(partial, RED_BLOCKS, scal + lz::B2);
-  count_launch(2);
+  k_lanczos2_orth<<<RED_BLOCKS, RED_THREADS, 0, s>>>(K, H, n, scal, partial,
+                                                     reduction_counter(partial));
+  count_launch();
+}
+
+void launch_pair_dot(cudaStream_t s, const double* X, const double* Y, const PairTask* tasks,
+                     int ntasks, int64_t total, double* partial, double* out) {
+  if (ntasks <= 0 || total <= 0) {
+    cudaMemsetAsync(out, 0, sizeof(double), s);
+    return;
+  }
+  const int grid = int(std::min<int64_t>(RED_BLOCKS, (total + RED_THREADS - 1) / RED_THREADS));
+  k_pair_dot<<<grid, RED_THREADS, 0, s>>>(X, Y, tasks, ntasks, total, partial, out,
+                                          reduction_counter(partial));
+  count_launch();
 }
 
 void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, double* scal,

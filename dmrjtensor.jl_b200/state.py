@@ -433,6 +433,67 @@ def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, si
     return energy
 
 
+# ------------------------------------------------------------------ measurements
+
+def _measure_state(psi: MPS, ctx=None):
+    """The device state of ``psi``: its resident handle, or an upload against an identity MPO
+    that carries the state's physical charges (block form) or none (dense tensors)."""
+    if psi._dev is not None and (ctx is None or psi._dev.ctx is ctx):
+        return psi._dev
+    L = len(psi)
+    if psi.tensors is None:
+        d = [len(p) for p in psi.phys]
+        ql = [list(map(tuple, p)) for p in psi.phys] if psi.phys and len(psi.phys[0][0]) else None
+    else:
+        d = [a.shape[1] for a in psi.tensors]
+        ql = None
+    ident = MPO([np.eye(di).reshape(1, di, di, 1) for di in d], ql)
+    dev = DeviceState(psi, ident.device(ctx))
+    psi._dev = dev
+    return dev
+
+
+def expect(psi: MPS, H: MPO, ctx=None):
+    """``expect(psi, H)`` (``lib/MPO_MPS/expect.jl:47-56``): <psi|H|psi> on the device, not
+    normalised (as in the reference). ``H`` may differ from the MPO the state was solved with but
+    must share its sites and physical charges. The state's centre is not moved."""
+    dev = psi._dev if psi._dev is not None and (ctx is None or psi._dev.ctx is ctx) else None
+    dh = H.device(dev.ctx if dev is not None else ctx)
+    if dev is None:
+        dev = DeviceState(psi, dh)
+        psi._dev = dev
+    v = C.c_double()
+    check(lib().dmrg_expect(dev.h, dh.h, C.byref(v)), dev.ctx.h)
+    return v.value
+
+
+def correlationmatrix(psi: MPS, Cc, Ca, trail=None, ctx=None):
+    """``correlationmatrix(psi, Cc, Ca; trail)`` (``lib/MPO_MPS/correlationmatrix.jl:21-83``):
+    ``rho[i,j] = <psi|(Cc F)_i F_{i+1}..F_{j-1} Ca_j|psi> / <psi|psi>`` for i < j, mirrored below
+    the diagonal, ``rho[i,i] = <psi|(Cc Ca)_i|psi> / <psi|psi>``; operators are d x d arrays
+    O[bra, ket]. Runs on the device and leaves the centre where it is (the reference moves it to
+    each site; the values agree for a normalised state)."""
+    dev = _measure_state(psi, ctx)
+    ops = [np.asfortranarray(np.asarray(o, dtype=float)) for o in (Cc, Ca)]
+    d = ops[0].shape[0]
+    for o in ops:
+        if o.shape != (d, d):
+            raise ValueError("operators must be square and of one size")
+    F = None
+    if trail is not None and np.size(trail):
+        F = np.asfortranarray(np.asarray(trail, dtype=float))
+        if F.shape != (d, d):
+            raise ValueError("trail must have the operators' size")
+    L = dev.L
+    rho = np.zeros((L, L), order="F")
+    dp = C.POINTER(C.c_double)
+    check(lib().dmrg_correlationmatrix(dev.h, d, ops[0].ctypes.data_as(dp),
+                                       ops[1].ctypes.data_as(dp),
+                                       F.ctypes.data_as(dp) if F is not None else None,
+                                       rho.ctypes.data_as(dp)), dev.ctx.h)
+    return rho
+
+
 class Env:
     """Device-backed environment list (``environment{W}``, ``lib/types.jl:113-115``):
     ``Lenv[i]`` downloads the dense-equivalent [m, w, m] tensor of site i."""

@@ -186,6 +186,22 @@ DMRG_API int dmrg_heff_apply_noalloc(dmrg_state* st, const dmrg_mpo* mpo, int iL
 /* Dense-equivalent dims of the two-site space at (iL, iL+1): dims[4] = {ml, d1, d2, mr}. */
 DMRG_API int dmrg_twosite_dims(const dmrg_state* st, const dmrg_mpo* mpo, int iL, int* dims);
 
+/* ---------------------------------------------------------------- measurements
+ * expect(psi, H) (lib/MPO_MPS/expect.jl:19-56): *value = <psi|H|psi> for an MPO H over the same
+ * sites and physical charges as the state's own MPO (H may differ from it), not normalised, as in
+ * the reference. The state's environments and centre are left as they are. */
+DMRG_API int dmrg_expect(dmrg_state* st, const dmrg_mpo* H, double* value);
+/* correlationmatrix(psi, Cc, Ca; trail) (lib/MPO_MPS/correlationmatrix.jl:21-83): rho [L, L]
+ * column-major with rho[i,j] = <psi|(Cc F)_i F_{i+1}..F_{j-1} Ca_j|psi> / <psi|psi> for i < j,
+ * rho[j,i] = rho[i,j] and rho[i,i] = <psi|(Cc Ca)_i|psi> / <psi|psi>. Cc, Ca and the trail F are
+ * d x d column-major operators O[bra, ket] applied on every site (every site must have physical
+ * dimension d); trail may be NULL (no string). Under charge conservation each operator must change
+ * the charge by one fixed amount (DMRG_ERR_QN otherwise). The reference moves the orthogonality
+ * centre to each site as a side effect; this call leaves the centre where it is (the values are
+ * gauge-invariant and agree with the reference's for a normalised state). */
+DMRG_API int dmrg_correlationmatrix(dmrg_state* st, int d, const double* Cc, const double* Ca,
+                                    const double* trail, double* rho);
+
 /* ---------------------------------------------------------------- the sweep
  * One optmps sweep (algs/optimizeMPS.jl:790-835): 2(L-1) twostep calls, each followed by an
  * environment update; the centre reverses at the edges. Requires dmrg_env_build first. */

@@ -1,0 +1,108 @@
+"""Device measurements against the oracle: ``expect`` and ``correlationmatrix``.
+
+``expect`` (``lib/MPO_MPS/expect.jl:19-56``): raw <psi|H|psi> on a dense random MPS, and on the
+block-form (U(1)) state a DMRG run leaves, compared with the oracle on the same tensors (relative
+1e-12); linearity in the MPO (H with J = 1/2 gives half). ``correlationmatrix``
+(``lib/MPO_MPS/correlationmatrix.jl:21-56``) against the oracle's centre-moving restatement
+(absolute 1e-12 on random states, 1e-10 after DMRG): dense spin operators, U(1) spin operators
+with charge (S+ S-), the Hubbard U(1)xU(1) creation / annihilation pairs with the Jordan-Wigner
+trail, an unnormalised non-canonical input (gauge and norm invariance), and the charge check.
+"""
+import numpy as np
+import pytest
+
+from oracle import measure as om, models as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense(psi):
+    return [np.array(psi[i]) for i in range(len(psi))]
+
+
+def test_expect_dense_random(dmrgb, ctx):
+    L = 12
+    psi = dmrgb.randMPS(2, L, 8, seed=4, oc=3)
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    ref = om.expect_value(_dense(psi), mo.make_mpo([mo.heisenberg_bulk()] * L, 2))
+    val = dmrgb.expect(psi, mpo, ctx=ctx)
+    assert abs(val - ref) <= 1e-12 * abs(ref)
+
+
+def test_expect_u1_after_dmrg_and_linearity(dmrgb, ctx):
+    L = 16
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    E = dmrgb.dmrg(psi, mpo, m=64, sweeps=4, cutoff=1e-12, ctx=ctx)
+    val = dmrgb.expect(psi, mpo, ctx=ctx)
+    ref = om.expect_value(_dense(psi), mo.make_mpo([mo.heisenberg_bulk()] * L, 2))
+    assert abs(val - ref) <= 1e-12 * abs(ref)
+    assert abs(val - E) <= 1e-8 * abs(E)
+    half = dmrgb.makeMPO(lambda i=None: dmrgb.heisenbergMPO(i, J=0.5), 2, L).with_qn(dmrgb.SPIN_QN)
+    assert abs(dmrgb.expect(psi, half, ctx=ctx) - 0.5 * val) <= 1e-12 * abs(val)
+
+
+@pytest.mark.parametrize("pair", ["zz", "pm", "xz"])
+def test_correlation_dense_random(dmrgb, ctx, pair):
+    L = 10
+    psi = dmrgb.randMPS(2, L, 6, seed=7, oc=0)
+    Sp, Sm, Sz, _, Sx, _, _ = mo.spin_ops()
+    Cc, Ca = {"zz": (Sz, Sz), "pm": (Sp, Sm), "xz": (Sx, Sz)}[pair]
+    rho = dmrgb.correlationmatrix(psi, Cc, Ca, ctx=ctx)
+    ref = om.correlationmatrix(_dense(psi), psi.oc, Cc, Ca)
+    assert np.max(np.abs(rho - ref)) <= 1e-12
+    assert psi.oc == 0
+
+
+def test_correlation_unnormalised_non_canonical(dmrgb, ctx):
+    L = 9
+    rng = np.random.default_rng(21)
+    T = mo.random_mps(L, 2, 5, rng)
+    T[4] = 3.0 * T[4]
+    psi = dmrgb.MPS(T, oc=0)
+    Sp, Sm, Sz, _, _, _, _ = mo.spin_ops()
+    rho = dmrgb.correlationmatrix(psi, Sp, Sm, ctx=ctx)
+    ref = om.correlationmatrix(mo.right_canonicalize(T), 0, Sp, Sm)
+    assert np.max(np.abs(rho - ref)) <= 1e-12
+
+
+def test_correlation_u1_after_dmrg(dmrgb, ctx):
+    L = 16
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    dmrgb.dmrg(psi, mpo, m=64, sweeps=4, cutoff=1e-12, ctx=ctx)
+    Sp, Sm, Sz, _, _, _, _ = mo.spin_ops()
+    dense = _dense(psi)
+    for Cc, Ca in [(Sz, Sz), (Sp, Sm), (Sm, Sp)]:
+        rho = dmrgb.correlationmatrix(psi, Cc, Ca, ctx=ctx)
+        ref = om.correlationmatrix(dense, psi.oc, Cc, Ca)
+        assert np.max(np.abs(rho - ref)) <= 1e-10
+    # total Sz = 0: every row of <Sz_i Sz_j> sums to zero
+    rho = dmrgb.correlationmatrix(psi, Sz, Sz, ctx=ctx)
+    assert np.max(np.abs(rho.sum(axis=1))) <= 1e-9
+
+
+def test_correlation_hubbard_trail(dmrgb, ctx):
+    L = 8
+    start = mo.hubbard_half_filling_mps(L)
+    mpo = dmrgb.makeMPO(dmrgb.hubbardMPO, 4, L).with_qn(dmrgb.HUBBARD_QN)
+    psi = dmrgb.MPS([np.array(a) for a in start], oc=0)
+    dmrgb.dmrg(psi, mpo, m=64, sweeps=4, cutoff=1e-10, ctx=ctx)
+    Cup, Cdn, F, Nup, _, _, _, _ = mo.fermion_ops()
+    dense = _dense(psi)
+    for Cc, Ca in [(Cup.T, Cup), (Cdn.T, Cdn)]:
+        rho = dmrgb.correlationmatrix(psi, Cc, Ca, trail=F, ctx=ctx)
+        ref = om.correlationmatrix(dense, psi.oc, Cc, Ca, trail=F)
+        assert np.max(np.abs(rho - ref)) <= 1e-10
+    rho = dmrgb.correlationmatrix(psi, Cup.T, Cup, trail=F, ctx=ctx)
+    assert abs(np.trace(rho) - L / 2) <= 1e-9       # N_up = L/2 at half filling, Sz = 0
+
+
+def test_correlation_rejects_operator_without_fixed_charge(dmrgb, ctx):
+    L = 8
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    dmrgb.dmrg(psi, mpo, m=16, sweeps=1, ctx=ctx)
+    _, _, Sz, _, Sx, _, _ = mo.spin_ops()
+    with pytest.raises(dmrgb.DmrgError):
+        dmrgb.correlationmatrix(psi, Sx, Sz, ctx=ctx)
