@@ -116,6 +116,55 @@ void run_pair(dmrg_ctx* c, const PairPlan& pp, char* db, const DBuf& X, const DB
                   int(pp.t.size()), pp.total, c->d_partial, out);
 }
 
+// `sp` repeated for `nrows` environments stored back to back: copy r reads env_in + r*in_stride,
+// writes env_out + r*out_stride and uses the scratch T1 + r*sp.t1, T2 + r*sp.t2; the site tensor
+// is shared by every copy.
+StepPlan replicate_step(const StepPlan& sp, int nrows, int64_t in_stride, int64_t out_stride) {
+  StepPlan b;
+  b.g1.tA = sp.g1.tA;
+  b.g1.tB = sp.g1.tB;
+  b.g3.tA = sp.g3.tA;
+  b.g3.tB = sp.g3.tB;
+  for (int r = 0; r < nrows; ++r) {
+    for (const GemmTask& t : sp.g1.tasks) {       // env_in x site -> T1
+      b.g1.add(t.c_off + r * sp.t1, t.ldc, t.M, t.N, t.alpha, t.beta);
+      for (int k = t.seg0; k < t.seg0 + t.nseg; ++k) {
+        const GemmSeg& g = sp.g1.segs[k];
+        b.g1.seg(g.a_off + r * in_stride, g.lda, g.b_off, g.ldb, g.K);
+      }
+    }
+    for (const MixTask& t : sp.mx.tasks) {        // T1 -> T2
+      b.mx.add(t.out_off + r * sp.t2, t.ld, t.rows, t.cols);
+      for (int k = t.term0; k < t.term0 + t.nterm; ++k) {
+        const MixTerm& m = sp.mx.terms[k];
+        b.mx.term(m.in_off + r * sp.t1, m.ld, m.coef);
+      }
+    }
+    for (const GemmTask& t : sp.g3.tasks) {       // site x T2 -> env_out
+      b.g3.add(t.c_off + r * out_stride, t.ldc, t.M, t.N, t.alpha, t.beta);
+      for (int k = t.seg0; k < t.seg0 + t.nseg; ++k) {
+        const GemmSeg& g = sp.g3.segs[k];
+        b.g3.seg(g.a_off, g.lda, g.b_off + r * sp.t2, g.ldb, g.K);
+      }
+    }
+  }
+  b.out = sp.out;
+  b.t1 = sp.t1 * nrows;
+  b.t2 = sp.t2 * nrows;
+  return b;
+}
+
+// out[r * out_stride] = pair contraction of row r of X (rows of x_stride doubles) with Y.
+void run_pair_rows(dmrg_ctx* c, const PairPlan& pp, char* db, const DBuf& X, int nrows,
+                   int64_t x_stride, const DBuf& Y, double* out, int64_t out_stride) {
+  check_pair(pp, x_stride, Y.n);
+  if (int64_t(nrows) * x_stride > X.n)
+    fail(DMRG_ERR_ARG, "internal plan check failed: pair rows out of bounds");
+  launch_pair_dot_rows(c->stream, X.p, x_stride, Y.p,
+                       reinterpret_cast<const PairTask*>(db + pp.off), int(pp.t.size()), nrows,
+                       out, out_stride);
+}
+
 void set_one(dmrg_ctx* c, DBuf& b) {
   static const double one = 1.0;
   cuda_check(cudaMemcpyAsync(b.p, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream),
@@ -243,38 +292,46 @@ void measure_correlation(dmrg_state* st, int d, const double* Cc_, const double*
     plan_scratch(spC[j], t1, t2);
     put_step(u, spC[j]);
   }
-  struct Row {
-    StepPlan diag;
-    PairPlan diag_pair;
-    std::vector<StepPlan> steps;     // steps[0]: (Cc F) at site i; steps[k]: F at site i + k
-    std::vector<PairPlan> pairs;     // pairs[k]: X at bond i + 1 + k with RC[i + 1 + k]
-  };
-  std::vector<Row> rows(L);
-  int64_t dmax = 1, xmax = 1;
+  // diagonal: (Cc Ca) at site i between EL[i] and ER[i+1]
+  std::vector<StepPlan> spD(L);
+  std::vector<PairPlan> ppD(L);
+  int64_t dmax = 1;
   for (int i = 0; i < L; ++i) {
-    Row& r = rows[i];
     const MPOSite on = op_site(onsite, d, st->mpo->site[i].p, zero, true);
-    plan_left_step(st->bond[i], st->bond[i + 1], on, st->lay[i], ELl[i], r.diag);
-    dmax = std::max(dmax, plan_scratch(r.diag, t1, t2));
-    put_step(u, r.diag);
-    r.diag_pair = plan_pair(st->bond[i + 1], r.diag.out, ERl[i + 1]);
-    r.diag_pair.off = u.put(r.diag_pair.t);
-    if (i + 1 >= L) continue;
-    r.steps.resize(L - 1 - i);
-    const MPOSite fc = op_site(FCc, d, st->mpo->site[i].p, zero, true);
-    plan_left_step(st->bond[i], st->bond[i + 1], fc, st->lay[i], ELl[i], r.steps[0]);
-    const QN label = fc.rr[0];
-    for (int j = i + 1; j < L; ++j) {
-      const StepPlan& cur = r.steps[j - i - 1];
-      xmax = std::max(xmax, plan_scratch(cur, t1, t2));
-      put_step(u, r.steps[j - i - 1]);
-      r.pairs.push_back(plan_pair(st->bond[j], cur.out, spC[j].out));
-      r.pairs.back().off = u.put(r.pairs.back().t);
-      if (j + 1 < L) {
-        const MPOSite f = op_site(F, d, st->mpo->site[j].p, label, true);
-        plan_left_step(st->bond[j], st->bond[j + 1], f, st->lay[j], cur.out, r.steps[j - i]);
-      }
+    plan_left_step(st->bond[i], st->bond[i + 1], on, st->lay[i], ELl[i], spD[i]);
+    dmax = std::max(dmax, plan_scratch(spD[i], t1, t2));
+    put_step(u, spD[i]);
+    ppD[i] = plan_pair(st->bond[i + 1], spD[i].out, ERl[i + 1]);
+    ppD[i].off = u.put(ppD[i].t);
+  }
+  // off-diagonal, one bond (column) j at a time: the rows i < j hold X_i at bond j back to back
+  // (one layout per bond, since every row carries the same charge label); X_{j-1} starts from
+  // EL[j-1] through (Cc F) at site j-1, the older rows move through F at site j-1 in one
+  // replicated step, and one launch contracts every row with RC[j].
+  std::vector<StepPlan> spS(L), spF(L);     // [j]: start of row j-1 / batched F step into bond j
+  std::vector<PairPlan> ppC(L);
+  std::vector<int64_t> xs(L, 0);            // X layout size at bond j
+  int64_t xmax = 1;
+  QN label;
+  for (int j = 1; j < L; ++j) {
+    const MPOSite fc = op_site(FCc, d, st->mpo->site[j - 1].p, zero, true);
+    label = fc.rr[0];
+    plan_left_step(st->bond[j - 1], st->bond[j], fc, st->lay[j - 1], ELl[j - 1], spS[j]);
+    plan_scratch(spS[j], t1, t2);
+    put_step(u, spS[j]);
+    xs[j] = spS[j].out.size;
+    if (j >= 2) {
+      const MPOSite f = op_site(F, d, st->mpo->site[j - 1].p, label, true);
+      StepPlan one;
+      plan_left_step(st->bond[j - 1], st->bond[j], f, st->lay[j - 1], spS[j - 1].out, one);
+      if (one.out.size != xs[j]) fail(DMRG_ERR_ARG, "internal plan check failed: row layouts differ");
+      spF[j] = replicate_step(one, j - 1, xs[j - 1], xs[j]);
+      plan_scratch(spF[j], t1, t2);
+      put_step(u, spF[j]);
     }
+    xmax = std::max(xmax, int64_t(j) * std::max<int64_t>(xs[j], 1));
+    ppC[j] = plan_pair(st->bond[j], spS[j].out, spC[j].out);
+    ppC[j].off = u.put(ppC[j].t);
   }
   PairPlan norm = plan_pair(st->bond[L], ELl[L], ERl[L]);
   norm.off = u.put(norm.t);
@@ -322,22 +379,22 @@ void measure_correlation(dmrg_state* st, int d, const double* Cc_, const double*
       fl += spC[j].flops();
     }
     for (int i = 0; i < L; ++i) {
-      Row& r = rows[i];
-      run_step(c, r.diag, db, EL[i].p, EL[i].n, st->A[i], D.p, D.n);
-      run_pair(c, r.diag_pair, db, D, ER[i + 1], out.p + i + int64_t(i) * L);
-      fl += r.diag.flops() + 2.0 * r.diag_pair.total;
-      if (i + 1 >= L) continue;
-      const DBuf* in = &EL[i];
-      for (int j = i + 1; j < L; ++j) {
-        const StepPlan& sp = r.steps[j - i - 1];
-        DBuf& xo = X[(j - i - 1) & 1];
-        run_step(c, sp, db, in->p, in->n, st->A[j - 1], xo.p, xo.n);
-        fl += sp.flops();
-        const PairPlan& pp = r.pairs[j - i - 1];
-        run_pair(c, pp, db, xo, RC[j], out.p + i + int64_t(j) * L);
-        fl += 2.0 * pp.total;
-        in = &xo;
+      run_step(c, spD[i], db, EL[i].p, EL[i].n, st->A[i], D.p, D.n);
+      run_pair(c, ppD[i], db, D, ER[i + 1], out.p + i + int64_t(i) * L);
+      fl += spD[i].flops() + 2.0 * ppD[i].total;
+    }
+    for (int j = 1; j < L; ++j) {
+      DBuf& xo = X[j & 1];
+      const DBuf& xi = X[(j - 1) & 1];
+      if (j >= 2) {
+        run_step(c, spF[j], db, xi.p, xi.n, st->A[j - 1], xo.p, xo.n);
+        fl += spF[j].flops();
       }
+      const int64_t at = int64_t(j - 1) * xs[j];
+      run_step(c, spS[j], db, EL[j - 1].p, EL[j - 1].n, st->A[j - 1], xo.p + at, xo.n - at);
+      fl += spS[j].flops();
+      run_pair_rows(c, ppC[j], db, xo, j, xs[j], RC[j], out.p + int64_t(j) * L, 1);
+      fl += 2.0 * ppC[j].total * j;
     }
     run_pair(c, norm, db, EL[L], ER[L], out.p + int64_t(L) * L);
     cuda_check(cudaGetLastError(), "correlation launches");

@@ -157,6 +157,11 @@ void launch_ritz(cudaStream_t s, double* scal, int kdim);
 // out[0] = sum over the pair tasks (total elements `total`; deterministic order)
 void launch_pair_dot(cudaStream_t s, const double* X, const double* Y, const PairTask* tasks,
                      int ntasks, int64_t total, double* partial, double* out);
+// out[r * out_stride] = sum over the pair tasks with X shifted by r * x_stride, r < nrows (one
+// block per row; fixed order)
+void launch_pair_dot_rows(cudaStream_t s, const double* X, int64_t x_stride, const double* Y,
+                          const PairTask* tasks, int ntasks, int nrows, double* out,
+                          int64_t out_stride);
 // y = sum_j c[j] X_j, j < k
 void launch_lincomb(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c,
                     double* y, int64_t n);

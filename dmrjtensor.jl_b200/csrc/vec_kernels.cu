@@ -159,6 +159,31 @@ __global__ void k_pair_dot(const double* __restrict__ X, const double* __restric
   if (arrive_last(counter)) finish_rows(partial, gridDim.x, 1, out, counter);
 }
 
+__global__ void k_pair_dot_rows(const double* __restrict__ X, int64_t x_stride,
+                                const double* __restrict__ Y, const PairTask* __restrict__ tasks,
+                                int ntasks, double* out, int64_t out_stride) {
+  const double* Xr = X + int64_t(blockIdx.x) * x_stride;
+  double acc = 0.0;
+  for (int k = 0; k < ntasks; ++k) {
+    const PairTask tk = tasks[k];
+    const int64_t n = int64_t(tk.rows) * tk.cols;
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+      const int64_t r = q % tk.rows, c = q / tk.rows;
+      acc += Xr[tk.x_off + q] * Y[tk.y_off + c + r * tk.cols];
+    }
+  }
+  __shared__ double red[RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  acc = warp_sum(acc);
+  if (lane == 0) red[wid] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += red[w];
+    out[int64_t(blockIdx.x) * out_stride] = t;
+  }
+}
+
 __global__ void k_axpby(int64_t n, double a, const double* ap, double asign,
                         const double* __restrict__ x, double b, const double* bp, double bsign,
                         double* y, int b_recip) {
@@ -437,6 +462,14 @@ void launch_pair_dot(cudaStream_t s, const double* X, const double* Y, const Pai
   const int grid = int(std::min<int64_t>(RED_BLOCKS, (total + RED_THREADS - 1) / RED_THREADS));
   k_pair_dot<<<grid, RED_THREADS, 0, s>>>(X, Y, tasks, ntasks, total, partial, out,
                                           reduction_counter(partial));
+  count_launch();
+}
+
+void launch_pair_dot_rows(cudaStream_t s, const double* X, int64_t x_stride, const double* Y,
+                          const PairTask* tasks, int ntasks, int nrows, double* out,
+                          int64_t out_stride) {
+  if (nrows <= 0) return;
+  k_pair_dot_rows<<<nrows, RED_THREADS, 0, s>>>(X, x_stride, Y, tasks, ntasks, out, out_stride);
   count_launch();
 }
 
