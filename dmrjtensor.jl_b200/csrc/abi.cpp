@@ -2,6 +2,8 @@
 // Exceptions (dmrg::Error) never cross this boundary: each entry point returns a status code
 // and records the message in the context (dmrg_last_error).
 #include <algorithm>
+#include <cstdio>
+#include <cstring>
 #include <cmath>
 #include <map>
 #include <numeric>
@@ -401,6 +403,181 @@ int dmrg_mps_upload_blocks(dmrg_ctx* c, const dmrg_mpo* mpo, const int* nsec,
     }
     *out = st;
   });
+}
+
+// ---- checkpoints: one little-endian binary file per state
+//   "DMRGCKP1", int32 version, L, nsym, oc, dir
+//   per bond b = 0..L: int32 nsec, then per sector int32 charge[nsym], int32 dim
+//   per site: int32 d, int64 n, n doubles (the site's blocks in canonical order)
+//   uint64 FNV-1a of every preceding byte
+namespace {
+
+constexpr char CKP_MAGIC[8] = {'D', 'M', 'R', 'G', 'C', 'K', 'P', '1'};
+constexpr int32_t CKP_VERSION = 1;
+
+struct CkpWriter {
+  std::FILE* f = nullptr;
+  uint64_t h = 1469598103934665603ull;
+  void put(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t k = 0; k < n; ++k) h = (h ^ b[k]) * 1099511628211ull;
+    if (std::fwrite(p, 1, n, f) != n) fail(DMRG_ERR_ARG, "checkpoint: write failed");
+  }
+  void i32(int32_t v) { put(&v, 4); }
+};
+
+struct CkpReader {
+  const std::vector<unsigned char>& buf;
+  size_t pos = 0;
+  explicit CkpReader(const std::vector<unsigned char>& b) : buf(b) {}
+  const unsigned char* take(size_t n) {
+    if (n > buf.size() - pos) fail(DMRG_ERR_ARG, "checkpoint: file is truncated");
+    const unsigned char* p = buf.data() + pos;
+    pos += n;
+    return p;
+  }
+  int32_t i32() { int32_t v; std::memcpy(&v, take(4), 4); return v; }
+  int64_t i64() { int64_t v; std::memcpy(&v, take(8), 8); return v; }
+};
+
+}  // namespace
+
+int dmrg_state_save(dmrg_state* st, const char* path) {
+  if (!st || !path) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    set_device(c);
+    CkpWriter w;
+    w.f = std::fopen(path, "wb");
+    if (!w.f) fail(DMRG_ERR_ARG, std::string("checkpoint: cannot open ") + path);
+    try {
+      w.put(CKP_MAGIC, 8);
+      w.i32(CKP_VERSION);
+      w.i32(st->L);
+      w.i32(st->nsym);
+      w.i32(st->oc);
+      w.i32(st->dir);
+      for (int b = 0; b <= st->L; ++b) {
+        const Bond& B = st->bond[b];
+        w.i32(B.nsec());
+        for (int k = 0; k < B.nsec(); ++k) {
+          for (int a = 0; a < st->nsym; ++a) w.i32(B.q[k].v[a]);
+          w.i32(B.dim[k]);
+        }
+      }
+      std::vector<double> h;
+      for (int i = 0; i < st->L; ++i) {
+        const int64_t n = st->lay[i].size;
+        h.resize(size_t(n));
+        if (n > 0) {
+          cuda_check(cudaMemcpyAsync(h.data(), st->A[i].p, sizeof(double) * size_t(n),
+                                     cudaMemcpyDeviceToHost, c->stream), "checkpoint download");
+          cuda_check(cudaStreamSynchronize(c->stream), "checkpoint download sync");
+        }
+        w.i32(st->mpo->site[i].d);
+        w.put(&n, 8);
+        w.put(h.data(), sizeof(double) * size_t(n));
+      }
+      const uint64_t sum = w.h;
+      if (std::fwrite(&sum, 1, 8, w.f) != 8) fail(DMRG_ERR_ARG, "checkpoint: write failed");
+      if (std::fclose(w.f) != 0) {
+        w.f = nullptr;
+        fail(DMRG_ERR_ARG, "checkpoint: close failed");
+      }
+      w.f = nullptr;
+    } catch (...) {
+      if (w.f) std::fclose(w.f);
+      throw;
+    }
+  });
+}
+
+int dmrg_state_load(dmrg_ctx* c, const dmrg_mpo* mpo, const char* path, dmrg_state** out) {
+  if (!c) return DMRG_ERR_ARG;
+  std::vector<int> nsec;
+  std::vector<std::vector<int>> qn, dims;
+  std::vector<const double*> data;
+  std::vector<std::vector<double>> sites;   // aligned copies of the site data
+  std::vector<unsigned char> buf;
+  int oc = 0, dir = 1;
+  const int rc = guarded(c, [&] {
+    if (!mpo || !path || !out) fail(DMRG_ERR_ARG, "null argument");
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) fail(DMRG_ERR_ARG, std::string("checkpoint: cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const long len = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (len < 8 + 8) {
+      std::fclose(f);
+      fail(DMRG_ERR_ARG, "checkpoint: file is truncated");
+    }
+    buf.resize(size_t(len));
+    const size_t got = std::fread(buf.data(), 1, buf.size(), f);
+    std::fclose(f);
+    if (got != buf.size()) fail(DMRG_ERR_ARG, "checkpoint: read failed");
+    uint64_t h = 1469598103934665603ull, sum;
+    for (size_t k = 0; k < buf.size() - 8; ++k) h = (h ^ buf[k]) * 1099511628211ull;
+    std::memcpy(&sum, buf.data() + buf.size() - 8, 8);
+    if (h != sum) fail(DMRG_ERR_ARG, "checkpoint: checksum mismatch (corrupt file)");
+    buf.resize(buf.size() - 8);
+    CkpReader r(buf);
+    if (std::memcmp(r.take(8), CKP_MAGIC, 8) != 0) fail(DMRG_ERR_ARG, "checkpoint: not a checkpoint");
+    if (r.i32() != CKP_VERSION) fail(DMRG_ERR_ARG, "checkpoint: unsupported version");
+    const int L = r.i32(), nsym = r.i32();
+    oc = r.i32();
+    dir = r.i32();
+    if (L != mpo->L) fail(DMRG_ERR_SHAPE, "checkpoint: chain length differs from the MPO's");
+    if (nsym != mpo->nsym) fail(DMRG_ERR_QN, "checkpoint: charges differ from the MPO's");
+    if (oc < 0 || oc >= L || (dir != 1 && dir != -1)) fail(DMRG_ERR_ARG, "checkpoint: bad centre");
+    nsec.resize(L + 1);
+    qn.resize(L + 1);
+    dims.resize(L + 1);
+    std::vector<Bond> bonds(L + 1);
+    for (int b = 0; b <= L; ++b) {
+      nsec[b] = r.i32();
+      if (nsec[b] < 0 || nsec[b] > (1 << 24)) fail(DMRG_ERR_ARG, "checkpoint: bad sector count");
+      for (int k = 0; k < nsec[b]; ++k) {
+        int q[2] = {0, 0};
+        for (int a = 0; a < nsym; ++a) {
+          q[a] = r.i32();
+          qn[b].push_back(q[a]);
+        }
+        dims[b].push_back(r.i32());
+        bonds[b].q.push_back(QN(q[0], q[1]));
+        bonds[b].dim.push_back(dims[b].back());
+        if (dims[b].back() <= 0) fail(DMRG_ERR_SHAPE, "checkpoint: sector dims must be positive");
+      }
+    }
+    data.resize(L);
+    sites.resize(L);
+    for (int i = 0; i < L; ++i) {
+      const int d = r.i32();
+      const int64_t n = r.i64();
+      if (d != mpo->site[i].d) fail(DMRG_ERR_SHAPE, "checkpoint: physical dimension differs");
+      for (int k = 1; k < bonds[i].nsec(); ++k)
+        if (!(bonds[i].q[k - 1] < bonds[i].q[k]))
+          fail(DMRG_ERR_ARG, "checkpoint: sector charges must be strictly increasing");
+      const SiteLayout lay = make_site_layout(bonds[i], mpo->site[i].p, bonds[i + 1]);
+      if (n != lay.size) fail(DMRG_ERR_SHAPE, "checkpoint: site data does not match its sectors");
+      sites[i].resize(size_t(n));
+      if (n > 0) std::memcpy(sites[i].data(), r.take(sizeof(double) * size_t(n)),
+                             sizeof(double) * size_t(n));
+      data[i] = sites[i].data();
+    }
+    if (r.pos != buf.size()) fail(DMRG_ERR_ARG, "checkpoint: trailing bytes");
+  });
+  if (rc != DMRG_OK) return rc;
+  buf.clear();
+  buf.shrink_to_fit();
+  std::vector<const int*> qp(nsec.size()), dp(nsec.size());
+  for (size_t b = 0; b < nsec.size(); ++b) {
+    qp[b] = qn[b].data();
+    dp[b] = dims[b].data();
+  }
+  const int rc2 = dmrg_mps_upload_blocks(c, mpo, nsec.data(), mpo->nsym ? qp.data() : nullptr,
+                                         dp.data(), data.data(), oc, out);
+  if (rc2 == DMRG_OK) (*out)->dir = dir;
+  return rc2;
 }
 
 int dmrg_state_destroy(dmrg_state* st) {

@@ -11,6 +11,7 @@ All arithmetic happens in libdmrgb200.so on the GPU; nothing here computes a con
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -341,6 +342,23 @@ class DeviceState:
         psi.oc = self.oc
         psi._dev = self
 
+    # -- checkpoints
+    def save(self, path):
+        """Checkpoint of the device state in one file (``dmrg_state_save``)."""
+        check(lib().dmrg_state_save(self.h, os.fsencode(str(path))), self.ctx.h)
+
+    @classmethod
+    def load(cls, path, dmpo: DeviceMPO):
+        """The device state of a checkpoint (``dmrg_state_load``); environments are not built."""
+        self = cls.__new__(cls)
+        self.ctx, self.dmpo, self._keep = dmpo.ctx, dmpo, ()
+        h = C.c_void_p()
+        check(lib().dmrg_state_load(self.ctx.h, dmpo.h, os.fsencode(str(path)), C.byref(h)),
+              self.ctx.h)
+        self.h = h
+        self.L = len(dmpo.mpo)
+        return self
+
     # -- environments and contractions
     def env_build(self):
         check(lib().dmrg_env_build(self.h, self.dmpo.h), self.ctx.h)
@@ -492,6 +510,35 @@ def correlationmatrix(psi: MPS, Cc, Ca, trail=None, ctx=None):
                                        F.ctypes.data_as(dp) if F is not None else None,
                                        rho.ctypes.data_as(dp)), dev.ctx.h)
     return rho
+
+
+# ------------------------------------------------------------------ checkpoints
+
+def largeMPS(psi: MPS, path, mpo: MPO = None, ctx=None):
+    """Writes ``psi`` to the checkpoint file ``path`` and returns the path: the persistence of
+    ``largeMPS(psi)`` (``lib/MPS/largeMPS.jl:19-33``) in one file rather than one per tensor. The
+    device state ``psi`` holds is written directly; otherwise ``psi`` is uploaded for ``mpo`` (or,
+    without one, for an identity MPO carrying its physical charges)."""
+    if psi._dev is not None:
+        dev = psi._dev
+    elif mpo is not None:
+        dev = DeviceState(psi, mpo.device(ctx))
+        psi._dev = dev
+    else:
+        dev = _measure_state(psi, ctx)
+    dev.save(path)
+    return path
+
+
+def loadMPS(path, mpo: MPO, ctx=None):
+    """``loadMPS`` (``lib/MPS/largeMPS.jl:60-79``): the MPS of a checkpoint, resident on the device
+    for ``mpo`` (same sites and charges as when it was written) and downloaded into the returned
+    object. A following ``dmrg(psi, mpo, ...)`` rebuilds the environments and continues exactly
+    as an uninterrupted run would."""
+    dev = DeviceState.load(path, mpo.device(ctx))
+    psi = MPS()
+    dev.download_into(psi)
+    return psi
 
 
 class Env:

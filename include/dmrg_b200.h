@@ -142,6 +142,17 @@ DMRG_API int dmrg_mps_upload(dmrg_ctx* ctx, const dmrg_mpo* mpo, const int* ml, 
 DMRG_API int dmrg_mps_upload_blocks(dmrg_ctx* ctx, const dmrg_mpo* mpo, const int* nsec,
                            const int* const* sec_qn, const int* const* sec_dim,
                            const double* const* data, int oc, dmrg_state** out);
+/* Checkpoint of a device state (the persistence of largeMPS / loadMPS, lib/MPS/largeMPS.jl:19-81,
+ * in one file instead of one file per tensor): the bond sectors, the centre, the sweep direction
+ * and every site's blocks, with a checksum. Environments are not stored: after dmrg_state_load
+ * call dmrg_env_build (the rebuilt environments equal the ones a sweep leaves, bit for bit, so a
+ * resumed run continues exactly as an uninterrupted one). */
+DMRG_API int dmrg_state_save(dmrg_state* st, const char* path);
+/* Reads a checkpoint into a new state for `mpo` (same length, charges and physical dimensions as
+ * the state that was saved; DMRG_ERR_SHAPE / DMRG_ERR_QN otherwise, DMRG_ERR_ARG for a corrupt or
+ * truncated file). */
+DMRG_API int dmrg_state_load(dmrg_ctx* ctx, const dmrg_mpo* mpo, const char* path,
+                             dmrg_state** out);
 DMRG_API int dmrg_state_destroy(dmrg_state* st);
 DMRG_API int dmrg_state_oc(const dmrg_state* st, int* oc);
 /* Sector structure of bond b: *nsec; if qn/dims are non-NULL they receive nsec*nsym / nsec ints. */
