@@ -12,7 +12,8 @@
 # given to makeqMPS / makeqMPO, e.g. 2Sz for U1 spin). All sizes are checked by the library.
 module DMRJtensorB200
 
-export dmrg_b200, B200Env, makeEnv_b200, Lupdate_b200!, Rupdate_b200!
+export dmrg_b200, B200Env, makeEnv_b200, Lupdate_b200!, Rupdate_b200!, expect_b200,
+       correlationmatrix_b200, save_b200, load_b200
 
 const libdmrg = get(ENV, "DMRG_B200_LIB", joinpath(@__DIR__, "..", "libdmrgb200.so"))
 
@@ -232,6 +233,43 @@ function Base.getindex(e::B200Env, i::Integer, side::Symbol)
   check(ccall((:dmrg_env_get, libdmrg), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}, Ptr{Cint}),
               e.st, i - 1, left, out, dims), e.ctx.h, "dmrg_env_get")
   out
+end
+
+# expect(psi, H) (lib/MPO_MPS/expect.jl:47-56) on the state of a B200Env: <psi|H|psi>, not
+# normalised; `H` is another uploaded MPO over the same sites (default: the Env's own).
+function expect_b200(e::B200Env, hmpo::Ptr{Cvoid}=e.mpo)
+  v = Ref{Cdouble}(0.0)
+  check(ccall((:dmrg_expect, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Cdouble}), e.st, hmpo, v),
+        e.ctx.h, "dmrg_expect")
+  v[]
+end
+
+# correlationmatrix(psi, Cc, Ca; trail) (lib/MPO_MPS/correlationmatrix.jl:21-83), operators
+# O[bra, ket] as d x d Float64 matrices; the centre of the state is not moved.
+function correlationmatrix_b200(e::B200Env, Cc::Matrix{Float64}, Ca::Matrix{Float64};
+                                trail=nothing, L::Integer)
+  d = size(Cc, 1)
+  rho = Matrix{Float64}(undef, L, L)
+  F = trail === nothing ? C_NULL : Matrix{Float64}(trail)
+  check(ccall((:dmrg_correlationmatrix, libdmrg), Cint,
+              (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+              e.st, d, Cc, Ca, F, rho), e.ctx.h, "dmrg_correlationmatrix")
+  rho
+end
+
+# Checkpoint of the Env's device state (the persistence of largeMPS / loadMPS,
+# lib/MPS/largeMPS.jl:19-81); load_b200 returns a new B200Env with rebuilt environments.
+save_b200(e::B200Env, path::AbstractString) =
+  check(ccall((:dmrg_state_save, libdmrg), Cint, (Ptr{Cvoid}, Cstring), e.st, path),
+        e.ctx.h, "dmrg_state_save")
+
+function load_b200(e::B200Env, path::AbstractString)
+  out = Ref{Ptr{Cvoid}}(C_NULL)
+  check(ccall((:dmrg_state_load, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cstring, Ref{Ptr{Cvoid}}),
+              e.ctx.h, e.mpo, path, out), e.ctx.h, "dmrg_state_load")
+  check(ccall((:dmrg_env_build, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), out[], e.mpo), e.ctx.h,
+        "dmrg_env_build")
+  B200Env(e.ctx, e.mpo, out[])   # shares the MPO handle: no finalizer of its own
 end
 
 end # module
