@@ -585,6 +585,8 @@ def main():
     ap.add_argument("--warmup-ref", type=int, default=1)
     ap.add_argument("--no-chosen", dest="chosen", action="store_false",
                     help="skip the split-precision (3xTF32) sweeps")
+    ap.add_argument("--heff-only", action="store_true",
+                    help="only time the plain and split Heff at the m=1024 dense-equivalent size")
     ap.add_argument("--no-measure", dest="measure", action="store_false",
                     help="skip the expect / correlationmatrix measurement")
     ap.add_argument("--serve-requests", type=int, default=200,
@@ -597,6 +599,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.heff_only:
+            # the plain and split Heff forms alone (the kernel-profiling case)
+            pkg = load_pkg()
+            print(json.dumps({"heff_forms_m1024": heff_forms(pkg, pkg.Context(local))}))
         else:
             run_ours(args, world, rank, local, dist)
     finally:

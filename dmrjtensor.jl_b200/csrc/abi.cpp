@@ -165,7 +165,9 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   if (!c) return DMRG_ERR_ARG;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  for (DBuf* b : {&c->X, &c->Y, &c->K, &c->H, &c->M, &c->R, &c->W, &c->T1, &c->T2}) dfree(c, *b);
+  for (DBuf* b : {&c->X, &c->Y, &c->K, &c->H, &c->M, &c->R, &c->W, &c->T1, &c->T2, &c->SA,
+                  &c->SB})
+    dfree(c, *b);
   for (auto& s : c->slot) {
     if (s.h) cudaFreeHost(s.h);
     if (s.d) cudaFreeAsync(s.d, c->stream);

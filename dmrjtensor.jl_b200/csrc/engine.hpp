@@ -163,6 +163,7 @@ struct dmrg_ctx {
   double* d_floors = nullptr;    // block-Jacobi per-group thresholds
   // growable scratch buffers
   dmrg::DBuf X, Y, K, H, M, R, W, T1, T2;
+  dmrg::DBuf SA, SB;             // pre-split (hi, lo) operand pairs of the split GEMM (8 B each)
   std::map<void*, size_t> sizes;
 };
 
@@ -231,6 +232,8 @@ struct Upload {
 void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
               const double* B, int64_t nB, double* C, int64_t nC);
 // The same list on the split-precision (3xTF32, tcgen05) kernel; the list must be retiled.
+// Lists of at least SPLIT_PRESPLIT_FLOPS convert their operands once into (hi, lo) pairs first.
+constexpr double SPLIT_PRESPLIT_FLOPS = 1e9;
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
                     const double* B, int64_t nB, double* C, int64_t nC);
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,

@@ -350,6 +350,7 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
                     const double* B, int64_t nB, double* C, int64_t nC) {
   if (g.tiles == 0) return;
   if (g.bm != TF32_TILE_M) bad_plan("split gemm tiling");
+  int64_t extA = 0, extB = 0;   // elements of A and B the tasks touch: [0, ext)
   for (const GemmTask& t : g.tasks) {
     if (t.M <= 0 || t.N <= 0) continue;
     if (t.ldc < t.M || !in_range(t.c_off, (t.M - 1) + int64_t(t.N - 1) * t.ldc, nC)) bad_plan("gemm C");
@@ -359,12 +360,26 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
       const int64_t eb = g.tB ? (t.N - 1) + int64_t(s.K - 1) * s.ldb : (s.K - 1) + int64_t(t.N - 1) * s.ldb;
       if (s.lda < (g.tA ? s.K : t.M) || !in_range(s.a_off, ea, nA)) bad_plan("gemm A");
       if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
+      extA = std::max(extA, s.a_off + ea + 1);
+      extB = std::max(extB, s.b_off + eb + 1);
     }
   }
-  launch_gemm_tf32x3(c->stream, g.tA, g.tB, A, B, C,
-                     reinterpret_cast<const GemmTask*>(dbase + g.t_off), int(g.tasks.size()),
-                     reinterpret_cast<const GemmSeg*>(dbase + g.s_off), g.tiles, c->nsm * 3,
-                     c->d_status + STATUS_MMA);
+  const GemmTask* tasks = reinterpret_cast<const GemmTask*>(dbase + g.t_off);
+  const GemmSeg* segs = reinterpret_cast<const GemmSeg*>(dbase + g.s_off);
+  if (g.flops >= SPLIT_PRESPLIT_FLOPS) {
+    // convert each operand element once instead of once per tile that reads it
+    ensure(c, c->SA, std::max<int64_t>(extA, 1));
+    ensure(c, c->SB, std::max<int64_t>(extB, 1));
+    float2* pa = reinterpret_cast<float2*>(c->SA.p);
+    float2* pb = reinterpret_cast<float2*>(c->SB.p);
+    launch_presplit(c->stream, A, pa, extA);
+    launch_presplit(c->stream, B, pb, extB);
+    launch_gemm_tf32x3_presplit(c->stream, g.tA, g.tB, pa, pb, C, tasks, int(g.tasks.size()), segs,
+                                g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
+    return;
+  }
+  launch_gemm_tf32x3(c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs, g.tiles,
+                     c->nsm * 3, c->d_status + STATUS_MMA);
 }
 
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,

@@ -14,6 +14,15 @@
 // commits to an mbarrier, and all threads wait (bounded) before the next chunk overwrites the
 // tiles. The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 =
 // rows of the tile) and writes alpha acc + beta C in FP64.
+//
+// Large lists use the pre-split form (PRE): one memory-bound pass writes every operand element as
+// an interleaved (hi, lo) FP32 pair, and the GEMM stages the pairs without converting. In the
+// direct form each tile re-splits its operands (five conversions per element on the XU pipe,
+// repeated for every tile that reads the element), which bounds the kernel at large sizes; the
+// pre-split pass converts each element once. Both forms round identically, so their results are
+// bit-identical.
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace dmrg {
@@ -64,6 +73,21 @@ __device__ __forceinline__ void split(double x, float& hi, float& lo) {
   lo = tf32r(float(x - double(hi)));
 }
 
+__device__ __forceinline__ void to_pair(double x, float& hi, float& lo) { split(x, hi, lo); }
+__device__ __forceinline__ void to_pair(float2 x, float& hi, float& lo) {
+  hi = x.x;
+  lo = x.y;
+}
+
+__global__ void k_presplit(const double* __restrict__ x, float2* __restrict__ y, int64_t n) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    float h, l;
+    split(x[i], h, l);
+    y[i] = make_float2(h, l);
+  }
+}
+
 __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -106,11 +130,15 @@ __device__ __forceinline__ void tmem_ld16_wait(uint32_t addr, float* v) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-template <bool TA, bool TB>
+template <bool TA, bool TB, bool PRE>
 __global__ void __launch_bounds__(TT)
-k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
+k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* __restrict__ C,
               const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
               int total_tiles, int* err) {
+  // operand elements: FP64 values (direct form) or pre-split (hi, lo) pairs
+  using T = typename std::conditional<PRE, float2, double>::type;
+  const T* __restrict__ A = static_cast<const T*>(Av);
+  const T* __restrict__ B = static_cast<const T*>(Bv);
   extern __shared__ unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_slot;
@@ -153,17 +181,21 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
     bool issued = false;
     int q = 0, k0 = 0;
     while (q < tk.nseg && segs[tk.seg0 + q].K <= 0) ++q;
-    // quads: 4 consecutive K elements of one row (one 16-byte unit of the staged layout);
-    // the thread-to-quad map keeps the global loads coalesced along the contiguous dimension
-    double ra[A_QUADS][4], rb[B_QUADS][4];
+    // quads: 4 consecutive K elements of one row (one 16-byte unit of the staged layout).
+    // Operand stored with rows contiguous: consecutive threads take consecutive rows. Stored
+    // with K contiguous: 8 consecutive threads take the same quad of 8 consecutive rows (their
+    // 16-byte stores land in 8 different bank groups of one 128-byte line), the next 8 the next
+    // quad, so a warp still reads 8 rows x 16 contiguous K elements.
+    T ra[A_QUADS][4], rb[B_QUADS][4];
     auto a_quad = [&](int i, int& r, int& kq) {
       const int e = tid + TT * i;
-      if (TA) { r = e >> 3; kq = e & 7; } else { r = e % TBM; kq = e / TBM; }
+      if (TA) { r = (e & 7) + 8 * (e >> 6); kq = (e >> 3) & 7; } else { r = e % TBM; kq = e / TBM; }
     };
     auto b_quad = [&](int i, int& c, int& kq) {
       const int e = tid + TT * i;
-      if (TB) { c = e % TBN; kq = e / TBN; } else { c = e >> 3; kq = e & 7; }
+      if (TB) { c = e % TBN; kq = e / TBN; } else { c = (e & 7) + 8 * (e >> 6); kq = (e >> 3) & 7; }
     };
+    const T zero = T{};
     auto load_chunk = [&](int qq, int kk0) {
       const GemmSeg sg = segs[tk.seg0 + qq];
 #pragma unroll
@@ -176,7 +208,7 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
           const int gk = kk0 + 4 * kq + j;
           ra[i][j] = (gr < tk.M && gk < sg.K)
                          ? (TA ? A[sg.a_off + gk + int64_t(gr) * sg.lda] : A[sg.a_off + gr + int64_t(gk) * sg.lda])
-                         : 0.0;
+                         : zero;
         }
       }
 #pragma unroll
@@ -189,7 +221,7 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
           const int gk = kk0 + 4 * kq + j;
           rb[i][j] = (gc < tk.N && gk < sg.K)
                          ? (TB ? B[sg.b_off + gc + int64_t(gk) * sg.ldb] : B[sg.b_off + gk + int64_t(gc) * sg.ldb])
-                         : 0.0;
+                         : zero;
         }
       }
     };
@@ -201,10 +233,10 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
         int r, kq;
         a_quad(i, r, kq);
         float4 h, l;
-        split(ra[i][0], h.x, l.x);
-        split(ra[i][1], h.y, l.y);
-        split(ra[i][2], h.z, l.z);
-        split(ra[i][3], h.w, l.w);
+        to_pair(ra[i][0], h.x, l.x);
+        to_pair(ra[i][1], h.y, l.y);
+        to_pair(ra[i][2], h.z, l.z);
+        to_pair(ra[i][3], h.w, l.w);
         const int o = soff(TBM, r, 4 * kq);
         *reinterpret_cast<float4*>(sp + o) = h;
         *reinterpret_cast<float4*>(sp + A_BYTES + o) = l;
@@ -214,10 +246,10 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
         int c, kq;
         b_quad(i, c, kq);
         float4 h, l;
-        split(rb[i][0], h.x, l.x);
-        split(rb[i][1], h.y, l.y);
-        split(rb[i][2], h.z, l.z);
-        split(rb[i][3], h.w, l.w);
+        to_pair(rb[i][0], h.x, l.x);
+        to_pair(rb[i][1], h.y, l.y);
+        to_pair(rb[i][2], h.z, l.z);
+        to_pair(rb[i][3], h.w, l.w);
         const int o = soff(TBN, c, 4 * kq);
         *reinterpret_cast<float4*>(sp + 2 * A_BYTES + o) = h;
         *reinterpret_cast<float4*>(sp + 2 * A_BYTES + B_BYTES + o) = l;
@@ -294,14 +326,29 @@ k_gemm_tf32x3(const double* __restrict__ A, const double* __restrict__ B, double
                  :: "r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
-template <bool TA, bool TB>
-void launch_tf32_variant(cudaStream_t s, const double* A, const double* B, double* C,
+template <bool TA, bool TB, bool PRE>
+void launch_tf32_variant(cudaStream_t s, const void* A, const void* B, double* C,
                          const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
                          int grid_cap, int* err) {
-  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tf32x3<TA, TB>), TF32_SMEM);
+  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tf32x3<TA, TB, PRE>), TF32_SMEM);
   const int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_tf32x3<TA, TB><<<grid, TT, TF32_SMEM, s>>>(A, B, C, tasks, ntasks, segs, total_tiles, err);
+  k_gemm_tf32x3<TA, TB, PRE><<<grid, TT, TF32_SMEM, s>>>(A, B, C, tasks, ntasks, segs,
+                                                          total_tiles, err);
   count_launch();
+}
+
+template <bool PRE>
+void dispatch(cudaStream_t s, bool transA, bool transB, const void* A, const void* B, double* C,
+              const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
+              int grid_cap, int* err) {
+  if (!transA && !transB)
+    launch_tf32_variant<false, false, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  else if (!transA && transB)
+    launch_tf32_variant<false, true, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  else if (transA && !transB)
+    launch_tf32_variant<true, false, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  else
+    launch_tf32_variant<true, true, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
 }
 
 }  // namespace
@@ -310,14 +357,21 @@ void launch_gemm_tf32x3(cudaStream_t s, bool transA, bool transB, const double* 
                         double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
                         int total_tiles, int grid_cap, int* err) {
   if (total_tiles <= 0) return;
-  if (!transA && !transB)
-    launch_tf32_variant<false, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
-  else if (!transA && transB)
-    launch_tf32_variant<false, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
-  else if (transA && !transB)
-    launch_tf32_variant<true, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
-  else
-    launch_tf32_variant<true, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  dispatch<false>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+}
+
+void launch_presplit(cudaStream_t s, const double* x, float2* pairs, int64_t n) {
+  if (n <= 0) return;
+  const int64_t blocks = (n + 255) / 256;
+  k_presplit<<<int(blocks < 1184 ? blocks : 1184), 256, 0, s>>>(x, pairs, n);
+  count_launch();
+}
+
+void launch_gemm_tf32x3_presplit(cudaStream_t s, bool transA, bool transB, const float2* A,
+                                 const float2* B, double* C, const GemmTask* tasks, int ntasks,
+                                 const GemmSeg* segs, int total_tiles, int grid_cap, int* err) {
+  if (total_tiles <= 0) return;
+  dispatch<true>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
 }
 
 }  // namespace dmrg

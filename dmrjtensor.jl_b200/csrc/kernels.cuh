@@ -105,6 +105,12 @@ constexpr int TF32_TILE_M = 128;
 void launch_gemm_tf32x3(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
                         double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
                         int total_tiles, int grid_cap, int* err);
+// The same GEMM on pre-split operands: A and B hold (hi, lo) TF32 pairs at the element offsets
+// the tasks address (launch_presplit writes them from FP64; bit-identical results).
+void launch_presplit(cudaStream_t s, const double* x, float2* pairs, int64_t n);
+void launch_gemm_tf32x3_presplit(cudaStream_t s, bool transA, bool transB, const float2* A,
+                                 const float2* B, double* C, const GemmTask* tasks, int ntasks,
+                                 const GemmSeg* segs, int total_tiles, int grid_cap, int* err);
 // slot of the context's status words that the split-precision GEMM sets on a timeout
 constexpr int STATUS_MMA = 8;
 

@@ -1,7 +1,7 @@
 """Split-precision form (3 x TF32 Heff GEMMs on tcgen05) against the plain FP64 form.
 
 One Heff application agrees with FP64 to FP32 accuracy (the split products accumulate in FP32,
-relative 1e-5 here); whole DMRG runs from the same start agree in energy within 1e-8, the
+relative 1e-5 here), in the direct form (small lists) and the pre-split form; whole DMRG runs from the same start agree in energy within 1e-8, the
 reported energy of a sweep being the FP64 Rayleigh quotient of the final Ritz vector.
 """
 import ctypes as C
@@ -43,6 +43,25 @@ def test_split_heff_matches_fp64(dmrgb, ctx, qn):
     y32 = _heff(dmrgb, dev, iL, x, 1)
     scale = np.max(np.abs(y64))
     assert np.max(np.abs(y32 - y64)) <= 1e-5 * scale
+
+
+def test_split_heff_presplit_form_matches_fp64(dmrgb, ctx):
+    """Bond dimension 384 either side: every Heff GEMM list is above 1 GFLOP and takes the
+    pre-split form (operands converted once into (hi, lo) pairs). The second GEMM accumulates
+    K = d w m = 3840 products in FP32 (ten times the first test's), so the bound is relative 5e-5
+    here (measured 1.3e-5)."""
+    L, iL = 20, 9
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    psi = dmrgb.randMPS(2, L, 384, seed=8, oc=iL)
+    Lenv, _ = dmrgb.makeEnv(psi, mpo, ctx=ctx)
+    dev = Lenv.dev
+    d = (C.c_int * 4)()
+    assert dmrgb.lib().dmrg_twosite_dims(dev.h, dev.dmpo.h, iL, d) == 0
+    assert tuple(d) == (384, 2, 2, 384)
+    x = np.random.default_rng(9).standard_normal(tuple(d))
+    y64 = _heff(dmrgb, dev, iL, x, 0)
+    y32 = _heff(dmrgb, dev, iL, x, 1)
+    assert np.max(np.abs(y32 - y64)) <= 5e-5 * np.max(np.abs(y64))
 
 
 def test_split_dmrg_energy_within_1e8_of_fp64(dmrgb, ctx):
