@@ -7,6 +7,8 @@ block-form (U(1)) state a DMRG run leaves, compared with the oracle on the same 
 (absolute 1e-12 on random states, 1e-10 after DMRG): dense spin operators, U(1) spin operators
 with charge (S+ S-), the Hubbard U(1)xU(1) creation / annihilation pairs with the Jordan-Wigner
 trail, an unnormalised non-canonical input (gauge and norm invariance), and the charge check.
+Edge cases: a charge-violating pair (S+ S+ under U(1)) gives exact zeros, a two-site chain, and an
+MPO with other physical charges is refused by ``expect``.
 """
 import numpy as np
 import pytest
@@ -106,3 +108,26 @@ def test_correlation_rejects_operator_without_fixed_charge(dmrgb, ctx):
     _, _, Sz, _, Sx, _, _ = mo.spin_ops()
     with pytest.raises(dmrgb.DmrgError):
         dmrgb.correlationmatrix(psi, Sx, Sz, ctx=ctx)
+
+
+def test_correlation_charge_violating_pair_is_zero_and_two_site_chain(dmrgb, ctx):
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    dmrgb.dmrg(psi, mpo, m=16, sweeps=2, cutoff=1e-12, ctx=ctx)
+    Sp, Sm, Sz, _, _, _, _ = mo.spin_ops()
+    assert np.array_equal(dmrgb.correlationmatrix(psi, Sp, Sp, ctx=ctx), np.zeros((L, L)))
+    two = dmrgb.randMPS(2, 2, 2, seed=3, oc=0)
+    rho = dmrgb.correlationmatrix(two, Sp, Sm, ctx=ctx)
+    ref = om.correlationmatrix(_dense(two), two.oc, Sp, Sm)
+    assert np.max(np.abs(rho - ref)) <= 1e-13
+
+
+def test_expect_rejects_mpo_with_other_physical_charges(dmrgb, ctx):
+    L = 8
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    dmrgb.dmrg(psi, mpo, m=16, sweeps=1, ctx=ctx)
+    flipped = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn([[(-1,), (1,)]] * L)
+    with pytest.raises(dmrgb.DmrgError):
+        dmrgb.expect(psi, flipped, ctx=ctx)
