@@ -113,12 +113,13 @@ struct GemmList {
   double flops = 0;
   size_t t_off = 0, s_off = 0;  // byte offsets inside the uploaded slot
   int bm = GEMM_BM;              // tile rows the tile counts refer to
+  int bn = GEMM_BN;              // tile columns the tile counts refer to
   void clear() { tasks.clear(); segs.clear(); tiles = 0; flops = 0; }
   void add(int64_t c_off, int ldc, int M, int N, double alpha, double beta);
   void seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K);
 };
-// The same products tiled for the split-precision kernel (TF32_TILE_M x GEMM_BN tiles).
-GemmList retile(const GemmList& g, int bm);
+// The same products tiled for the split-precision kernel (TF32_TILE_M x bn tiles).
+GemmList retile(const GemmList& g, int bm, int bn);
 
 struct MixList {
   std::vector<MixTask> tasks;

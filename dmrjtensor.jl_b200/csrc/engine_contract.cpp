@@ -105,8 +105,12 @@ void check_mma_status(dmrg_ctx* c) {
 }
 
 void prepare_split(HeffPlan& hp) {
-  hp.g1t = retile(hp.g1, TF32_TILE_M);
-  hp.g3t = retile(hp.g3, TF32_TILE_M);
+  // large lists take the pre-split form with 128-column tiles, small ones the direct form
+  auto bn = [](const GemmList& g) {
+    return g.flops >= SPLIT_PRESPLIT_FLOPS ? TF32_TILE_N_PRESPLIT : TF32_TILE_N_DIRECT;
+  };
+  hp.g1t = retile(hp.g1, TF32_TILE_M, bn(hp.g1));
+  hp.g3t = retile(hp.g3, TF32_TILE_M, bn(hp.g3));
   hp.split = true;
 }
 

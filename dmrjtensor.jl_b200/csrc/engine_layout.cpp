@@ -223,11 +223,12 @@ void GemmList::add(int64_t c_off, int ldc, int M, int N, double alpha, double be
   tasks.push_back(t);
 }
 
-GemmList retile(const GemmList& g, int bm) {
+GemmList retile(const GemmList& g, int bm, int bn) {
   GemmList r;
   r.tA = g.tA;
   r.tB = g.tB;
   r.bm = bm;
+  r.bn = bn;
   r.segs = g.segs;
   r.flops = g.flops;
   r.tasks = g.tasks;
@@ -235,7 +236,7 @@ GemmList retile(const GemmList& g, int bm) {
   for (GemmTask& t : r.tasks) {
     t.tiles_m = (t.M <= 0 || t.N <= 0) ? 0 : (t.M + bm - 1) / bm;
     t.tile0 = r.tiles;
-    r.tiles += t.tiles_m * ((t.N + GEMM_BN - 1) / GEMM_BN);
+    r.tiles += t.tiles_m * ((t.N + bn - 1) / bn);
   }
   return r;
 }
@@ -349,7 +350,8 @@ void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int6
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
                     const double* B, int64_t nB, double* C, int64_t nC) {
   if (g.tiles == 0) return;
-  if (g.bm != TF32_TILE_M) bad_plan("split gemm tiling");
+  if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_PRESPLIT))
+    bad_plan("split gemm tiling");
   int64_t extA = 0, extB = 0;   // elements of A and B the tasks touch: [0, ext)
   for (const GemmTask& t : g.tasks) {
     if (t.M <= 0 || t.N <= 0) continue;
@@ -366,7 +368,7 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
   }
   const GemmTask* tasks = reinterpret_cast<const GemmTask*>(dbase + g.t_off);
   const GemmSeg* segs = reinterpret_cast<const GemmSeg*>(dbase + g.s_off);
-  if (g.flops >= SPLIT_PRESPLIT_FLOPS) {
+  if (g.bn == TF32_TILE_N_PRESPLIT) {   // retiled for the pre-split form (large lists)
     // convert each operand element once instead of once per tile that reads it
     ensure(c, c->SA, std::max<int64_t>(extA, 1));
     ensure(c, c->SB, std::max<int64_t>(extB, 1));
@@ -374,8 +376,9 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
     float2* pb = reinterpret_cast<float2*>(c->SB.p);
     launch_presplit(c->stream, A, pa, extA);
     launch_presplit(c->stream, B, pb, extB);
+    // 128 x 128 tiles: 184 registers per thread leave room for 2 CTAs per SM
     launch_gemm_tf32x3_presplit(c->stream, g.tA, g.tB, pa, pb, C, tasks, int(g.tasks.size()), segs,
-                                g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
+                                g.tiles, c->nsm * 2, c->d_status + STATUS_MMA);
     return;
   }
   launch_gemm_tf32x3(c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs, g.tiles,

@@ -7,7 +7,7 @@
 // Krylov recursion, normalisation and the final Ritz energy stay FP64 in the caller.
 //
 // Same task lists as the FP64 kernel (GemmTask / GemmSeg, element offsets from base pointers),
-// tiled 128 x 64 (tiles_m and tile0 counted at 128 rows). One CTA of 4 warps per tile at a time
+// tiled 128 x 64 (direct form) or 128 x 128 (pre-split form); the lists are retiled to match. One CTA of 4 warps per tile at a time
 // (persistent over tiles): the threads stage a K chunk of 32 of op(A) and op(B) into shared
 // memory in the canonical K-major layout (8-row x 16-byte core matrices, no swizzle), one thread
 // issues 4 k-steps x 3 tcgen05.mma (M=128, N=64, K=8) into a 64-column TMEM accumulator and
@@ -28,18 +28,27 @@
 namespace dmrg {
 namespace {
 
-constexpr int TBM = 128, TBN = 64, TBK = 32;
+constexpr int TBM = 128, TBK = 32;
 constexpr int TT = 128;                          // 4 warps
 constexpr int A_BYTES = TBM * TBK * 4;           // 16 KB per split part
-constexpr int B_BYTES = TBN * TBK * 4;           // 8 KB per split part
-constexpr int TF32_SMEM = 2 * A_BYTES + 2 * B_BYTES + 1024;   // + alignment slack
-constexpr uint32_t TMEM_COLS = 64;               // FP32 accumulator 128 lanes x 64 columns
-// instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), both
-// K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(TBN >> 3) << 17) |
-                           (uint32_t(TBM >> 4) << 24);
 constexpr long long WAIT_LIMIT = 1ll << 22;      // try_wait rounds before giving up
-constexpr int A_QUADS = TBM * TBK / 4 / TT, B_QUADS = TBN * TBK / 4 / TT;   // per thread
+constexpr int A_QUADS = TBM * TBK / 4 / TT;      // per thread
+static_assert(TF32_TILE_N_DIRECT == 64 && TF32_TILE_N_PRESPLIT == 128, "tile widths");
+
+// Tile width by form: 128 x 64 for the direct form (small lists: narrow blocks), 128 x 128 for
+// the pre-split form (each staged A tile feeds twice the products).
+template <bool PRE>
+struct Tile {
+  static constexpr int BN = PRE ? TF32_TILE_N_PRESPLIT : TF32_TILE_N_DIRECT;
+  static constexpr int B_BYTES = BN * TBK * 4;                      // per split part
+  static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 1024;     // + alignment slack
+  static constexpr uint32_t TMEM_COLS = BN;                         // FP32 128 lanes x BN
+  static constexpr int B_QUADS = BN * TBK / 4 / TT;
+  // instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), both
+  // K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24
+  static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) |
+                                    (uint32_t(BN >> 3) << 17) | (uint32_t(TBM >> 4) << 24);
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -88,13 +97,14 @@ __global__ void k_presplit(const double* __restrict__ x, float2* __restrict__ y,
   }
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc,
+                                         uint32_t idesc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       :
-      : "r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
@@ -139,6 +149,8 @@ k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* 
   using T = typename std::conditional<PRE, float2, double>::type;
   const T* __restrict__ A = static_cast<const T*>(Av);
   const T* __restrict__ B = static_cast<const T*>(Bv);
+  constexpr int TBN = Tile<PRE>::BN, B_BYTES = Tile<PRE>::B_BYTES, B_QUADS = Tile<PRE>::B_QUADS;
+  constexpr uint32_t TMEM_COLS = Tile<PRE>::TMEM_COLS, IDESC = Tile<PRE>::IDESC;
   extern __shared__ unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_slot;
@@ -261,10 +273,10 @@ k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* 
         for (int st = 0; st * 8 < ks; ++st) {
           const uint64_t dah = sdesc(aH + st * (TBM * 32)), dal = sdesc(aL + st * (TBM * 32));
           const uint64_t dbh = sdesc(bH + st * (TBN * 32)), dbl = sdesc(bL + st * (TBN * 32));
-          mma_tf32(tmem, dah, dbh, issued ? 1u : 0u);
+          mma_tf32(tmem, dah, dbh, issued ? 1u : 0u, IDESC);
           issued = true;
-          mma_tf32(tmem, dah, dbl, 1u);
-          mma_tf32(tmem, dal, dbh, 1u);
+          mma_tf32(tmem, dah, dbl, 1u, IDESC);
+          mma_tf32(tmem, dal, dbh, 1u, IDESC);
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                      :: "r"(mb) : "memory");
@@ -330,10 +342,10 @@ template <bool TA, bool TB, bool PRE>
 void launch_tf32_variant(cudaStream_t s, const void* A, const void* B, double* C,
                          const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
                          int grid_cap, int* err) {
-  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tf32x3<TA, TB, PRE>), TF32_SMEM);
+  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tf32x3<TA, TB, PRE>), Tile<PRE>::SMEM);
   const int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_tf32x3<TA, TB, PRE><<<grid, TT, TF32_SMEM, s>>>(A, B, C, tasks, ntasks, segs,
-                                                          total_tiles, err);
+  k_gemm_tf32x3<TA, TB, PRE><<<grid, TT, Tile<PRE>::SMEM, s>>>(A, B, C, tasks, ntasks, segs,
+                                                                total_tiles, err);
   count_launch();
 }
 

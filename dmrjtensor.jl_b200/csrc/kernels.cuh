@@ -102,6 +102,7 @@ void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, 
 // Split-precision grouped GEMM (3 x TF32 on tcgen05, FP32 accumulation in TMEM, FP64 in/out),
 // tiles of TF32_TILE_M x GEMM_BN; err[0] is set when an MMA completion wait gave up.
 constexpr int TF32_TILE_M = 128;
+constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_PRESPLIT = 128;
 void launch_gemm_tf32x3(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
                         double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
                         int total_tiles, int grid_cap, int* err);
