@@ -376,9 +376,8 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
     float2* pb = reinterpret_cast<float2*>(c->SB.p);
     launch_presplit(c->stream, A, pa, extA);
     launch_presplit(c->stream, B, pb, extB);
-    // 128 x 128 tiles: 184 registers per thread leave room for 2 CTAs per SM
     launch_gemm_tf32x3_presplit(c->stream, g.tA, g.tB, pa, pb, C, tasks, int(g.tasks.size()), segs,
-                                g.tiles, c->nsm * 2, c->d_status + STATUS_MMA);
+                                g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
     return;
   }
   launch_gemm_tf32x3(c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs, g.tiles,

@@ -141,7 +141,7 @@ __device__ __forceinline__ void tmem_ld16_wait(uint32_t addr, float* v) {
 }
 
 template <bool TA, bool TB, bool PRE>
-__global__ void __launch_bounds__(TT)
+__global__ void __launch_bounds__(TT, 3)
 k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* __restrict__ C,
               const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
               int total_tiles, int* err) {
