@@ -408,26 +408,37 @@ def aggregate_value(world, steps, tmax):
     return world * steps / tmax
 
 
+def workload_config(args, world):
+    """The `config` of both arms' JSON lines."""
+    return {"workload": "heisenberg L=100 U(1) Sz=0, maxm 1024 sweep (two-site), after the "
+                        "64->1024 ramp", "krylov": args.krylov, "cutoff": CUTOFF,
+            "precision": args.precision, "l2": "state larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
     sectors = json.load(open(ROOT / "tests" / "golden" / "c2_sectors_m1024.json"))["sectors"]
     sectors = [[(tuple(q), d) for q, d in b] for b in sectors]
+    # the driver's --steps K --warmup W, each step a bounded sample (two bond steps at the
+    # chain centre, scaled to a sweep); --steps-ref / --warmup-ref override them
+    n_steps = args.steps_ref if args.steps_ref is not None else args.steps
+    n_warm = args.warmup_ref if args.warmup_ref is not None else args.warmup
     steps = []
-    for _ in range(args.warmup_ref):
+    for _ in range(n_warm):
         oracle_sample(sectors, args.krylov, nsteps=1)
-    for _ in range(args.steps_ref):
+    for _ in range(n_steps):
         t_step, est, desc = oracle_sample(sectors, args.krylov, nsteps=2)
         steps.append(est)
     sweep_s = statistics.mean(steps)
     cores = cpu_threads()
     value = 1.0 / sweep_s
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
-           "n_gpus": args.gpus, "steps": args.steps_ref, "warmup": args.warmup_ref,
+           "n_gpus": args.gpus, "steps": n_steps, "warmup": n_warm,
            "ms_per_step": sweep_s * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "heisenberg L=100 U(1) Sz=0, maxm 1024 sweep (two-site)",
-                      "krylov": args.krylov, "cutoff": CUTOFF},
+           "config": workload_config(args, world),
            "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": cores, "kind": "port",
                             "sample": desc},
            "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
@@ -538,10 +549,7 @@ def run_ours(args, world, rank, local, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sweep_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "heisenberg L=100 U(1) Sz=0, maxm 1024 sweep (two-site), after "
-                               "the 64->1024 ramp", "krylov": args.krylov, "cutoff": CUTOFF,
-                   "precision": args.precision, "l2": "state larger than L2 (no flush)",
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(args, world),
         "energy": energy,
         "sweep_seconds": sweep_s,
         "heff_tflops": heff_flops / heff_sec / 1e12 if heff_sec > 0 else None,
@@ -584,8 +592,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--dump-sectors", default=None)
-    ap.add_argument("--steps-ref", type=int, default=2)
-    ap.add_argument("--warmup-ref", type=int, default=1)
+    ap.add_argument("--steps-ref", type=int, default=None,
+                    help="reference arm: timed samples (default: --steps)")
+    ap.add_argument("--warmup-ref", type=int, default=None,
+                    help="reference arm: warm-up samples (default: --warmup)")
     ap.add_argument("--no-chosen", dest="chosen", action="store_false",
                     help="skip the split-precision (3xTF32) sweeps")
     ap.add_argument("--heff-only", action="store_true",
