@@ -10,7 +10,7 @@ from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heise
                      heisenbergMPO, hubbardMPO, makeMPO, spinOps, tfiMPO)
 from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
                     correlationmatrix, default_context, dmrg, expect, largeMPS, loadMPS,
-                    make_params, makeEnv, neelMPS, product_MPS, randMPS)
+                    make_params, makeEnv, mpo_product, neelMPS, product_MPS, randMPS)
 from .serving import Server, ServerError
 
 
@@ -26,6 +26,6 @@ __all__ = [
     "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
     "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",
     "default_context", "dmrg", "make_params", "makeEnv", "neelMPS", "product_MPS", "randMPS",
-    "expect", "correlationmatrix", "largeMPS", "loadMPS",
+    "expect", "mpo_product", "correlationmatrix", "largeMPS", "loadMPS",
     "Server", "ServerError",
 ]

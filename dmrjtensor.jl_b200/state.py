@@ -471,10 +471,50 @@ def _measure_state(psi: MPS, ctx=None):
     return dev
 
 
-def expect(psi: MPS, H: MPO, ctx=None):
-    """``expect(psi, H)`` (``lib/MPO_MPS/expect.jl:47-56``): <psi|H|psi> on the device, not
-    normalised (as in the reference). ``H`` may differ from the MPO the state was solved with but
-    must share its sites and physical charges. The state's centre is not moved."""
+def mpo_product(*Hs: MPO) -> MPO:
+    """The MPO of the operator product H1 H2 ... Hn, Hn acting on the ket first (the order of
+    ``expect(psi, H1, ..., Hn)``, ``lib/MPO_MPS/expect.jl:19-45``): per site
+    W[(w1,w2), s, t, (w1',w2')] = sum_u W1[w1, u, t, w1'] W2[w2, s, u, w2'] (s ket, t bra)."""
+    out = Hs[0]
+    for H in Hs[1:]:
+        if len(H) != len(out):
+            raise ValueError("MPOs of different lengths")
+        Ws = []
+        for A, B in zip(out.W, H.W):
+            W = np.einsum("auth,bsuk->absthk", A, B)
+            a, b, d1, d2, h, k = W.shape
+            Ws.append(W.reshape(a * b, d1, d2, h * k))
+        out = MPO(_prune_bonds(Ws), out.qlabels)
+    return out
+
+
+def _prune_bonds(Ws):
+    """Drops MPO bond states with no weight on one side (an all-zero column of the left site or
+    row of the right site): they contribute nothing, and the charge labels of the makeqMPO rule
+    are defined only for states that carry weight."""
+    Ws = [w.copy() for w in Ws]
+    changed = True
+    while changed:
+        changed = False
+        for i in range(len(Ws) - 1):
+            keep = np.any(Ws[i] != 0, axis=(0, 1, 2)) & np.any(Ws[i + 1] != 0, axis=(1, 2, 3))
+            if not keep.any():
+                keep[0] = True          # the zero operator: keep one state
+            if not keep.all():
+                Ws[i] = Ws[i][..., keep]
+                Ws[i + 1] = Ws[i + 1][keep]
+                changed = True
+    return Ws
+
+
+def expect(psi: MPS, *H: MPO, ctx=None):
+    """``expect(psi, H...)`` (``lib/MPO_MPS/expect.jl:47-56``): <psi|H1 H2 ... Hn|psi> on the
+    device, not normalised (as in the reference); several MPOs are multiplied on the host first
+    (:func:`mpo_product`). The MPOs may differ from the one the state was solved with but must
+    share its sites and physical charges. The state's centre is not moved."""
+    if not H:
+        raise ValueError("expect needs at least one MPO")
+    H = H[0] if len(H) == 1 else mpo_product(*H)
     dev = psi._dev if psi._dev is not None and (ctx is None or psi._dev.ctx is ctx) else None
     dh = H.device(dev.ctx if dev is not None else ctx)
     if dev is None:

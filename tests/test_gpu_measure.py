@@ -131,3 +131,21 @@ def test_expect_rejects_mpo_with_other_physical_charges(dmrgb, ctx):
     flipped = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn([[(-1,), (1,)]] * L)
     with pytest.raises(dmrgb.DmrgError):
         dmrgb.expect(psi, flipped, ctx=ctx)
+
+
+def test_expect_of_an_operator_product(dmrgb, ctx):
+    """expect(psi, H, H) = <psi|H^2|psi> against the full state vector; after DMRG the energy
+    variance <H^2> - <H>^2 is small and not negative."""
+    from oracle import ed
+    L = 8
+    psi = dmrgb.randMPS(2, L, 8, seed=12, oc=0)
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    v = om.mps_vector([np.array(psi[i]) for i in range(L)])
+    Hm = ed.full_h(mpo.W).T
+    ref = float(v @ (Hm @ (Hm @ v)))
+    assert abs(dmrgb.expect(psi, mpo, mpo, ctx=ctx) - ref) <= 1e-12 * abs(ref)
+    qmpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, 16).with_qn(dmrgb.SPIN_QN)
+    gs = dmrgb.neelMPS(16)
+    E = dmrgb.dmrg(gs, qmpo, m=64, sweeps=4, cutoff=1e-12, ctx=ctx)
+    var = dmrgb.expect(gs, qmpo, qmpo, ctx=ctx) - dmrgb.expect(gs, qmpo, ctx=ctx) ** 2
+    assert -1e-9 <= var <= 1e-6, (E, var)
