@@ -16,7 +16,11 @@
 namespace dmrg {
 namespace {
 
-// Same rule as oracle/qtensor.py select_kept (global over all groups).
+// Truncation, global over all charge groups (fsvd!, algs/DMRG.jl:387): the weights of every group
+// sorted descending together (ties by group, then index); k_c = the smallest k whose discarded
+// weight is at most cutoff x total (total = mag, or the sum of the weights when mag = 0); keep
+// k = min(maxm, max(minm, k_c)) (maxm > 0), at least 1; with degen_rtol > 0 the cut moves back out
+// of a degenerate multiplet. truncerr = the discarded weight.
 struct Sel {
   std::vector<int> keep;
   double truncerr = 0.0;
