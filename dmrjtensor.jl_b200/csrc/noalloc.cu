@@ -96,8 +96,10 @@ void heff_apply_noalloc(dmrg_state* st, int iL, const double* in, double* out) {
   cuda_check(cudaMemcpyAsync(desc, u.bytes.data(), u.bytes.size(), cudaMemcpyHostToDevice,
                              c->stream), "no-allocation descriptor copy");
   hp.dbase = desc;
-  cuda_check(cudaMemsetAsync(out, 0, size_t(ndense) * sizeof(double), c->stream), "output clear");
+  // the whole input is gathered into the block layout before the output is touched, so psi_in
+  // and psi_out may be the same (or overlapping) device buffers
   run_copy(c, gin, desc, in, ndense, bin, tl.size);
+  cuda_check(cudaMemsetAsync(out, 0, size_t(ndense) * sizeof(double), c->stream), "output clear");
   run_gemm(c, hp.g1, desc, st->Lenv[iL].p, st->Lenv[iL].n, bin, tl.size, X, hp.x_size);
   run_mix(c, hp.mix, desc, X, hp.x_size, Y, hp.y_size);
   run_gemm(c, hp.g3, desc, Y, hp.y_size, st->Renv[iL + 1].p, st->Renv[iL + 1].n, bout, tl.size);

@@ -55,6 +55,23 @@ def test_noalloc_matches_regular_heff_twice(dmrgb, ctx, qn):
         assert np.max(np.abs(y - y_ref)) <= 1e-13 * scale, f"call {call}"
 
 
+def test_noalloc_in_place(dmrgb, ctx):
+    """psi_in and psi_out may be one buffer: the input is read completely before the output is
+    written, so the result equals the regular entry point's."""
+    import torch
+    L, iL = 10, 4
+    dev = _state(dmrgb, ctx, L, 16, True, seed=4, oc=iL)
+    x = np.random.default_rng(3).standard_normal(_dims(dmrgb, dev, iL))
+    y_ref = dev.heff(iL, np.asfortranarray(x))
+    buf = torch.from_numpy(np.asfortranarray(x).ravel(order="F").copy()).cuda()
+    torch.cuda.synchronize()
+    code = dmrgb.lib().dmrg_heff_apply_noalloc(dev.h, dev.dmpo.h, iL, buf.data_ptr(),
+                                               buf.data_ptr(), 0)
+    assert code == 0, dmrgb.lib().dmrg_last_error(ctx.h)
+    y = buf.cpu().numpy().reshape(x.shape, order="F")
+    assert np.max(np.abs(y - y_ref)) <= 1e-13 * max(np.max(np.abs(y_ref)), 1e-300)
+
+
 def _dims(dmrgb, dev, iL):
     import ctypes as C
     d = (C.c_int * 4)()
