@@ -66,17 +66,6 @@ struct EigTask {
   int n, pad;
 };
 
-// One-sided Jacobi of X (r x c, column-major at x_off, overwritten by X V sorted): V (c x c) at
-// v_off, eigenvalues |x_i|^2 of X^T X (descending) at w_off.
-struct SvdTask {
-  int64_t x_off, v_off, w_off;
-  int r, c;
-};
-size_t hestenes_smem(int r, int c);
-void launch_hestenes(cudaStream_t s, double* base, const SvdTask* tasks, int ntasks, size_t smem,
-                     int* status);
-constexpr size_t HESTENES_SMEM_MAX = 200 * 1024;
-
 // Tridiagonal eigensolver for density-matrix blocks with n <= SYEVT_NMAX (syevt.cu).
 constexpr int SYEVT_NMAX = 112;
 struct TridTask {

@@ -78,43 +78,6 @@ def test_jacobi_batched(dmrgb, ctx, sizes):
         woff += n
 
 
-@pytest.mark.parametrize("shapes", [[(66, 66), (40, 66), (66, 40), (1, 3), (5, 1)], [(100, 100)],
-                                    [(130, 90)]])
-def test_one_sided_jacobi(dmrgb, ctx, shapes):
-    """X V has orthogonal columns with norms^2 = eigenvalues of X^T X (descending); V orthogonal."""
-    rng = np.random.default_rng(len(shapes))
-    mats = []
-    for (r, c) in shapes:
-        k = max(1, min(r, c) // 2)          # rank-deficient, like a truncated two-site state
-        mats.append(rng.standard_normal((r, k)) @ rng.standard_normal((k, c)))
-    X = np.concatenate([np.asfortranarray(M).ravel(order="F") for M in mats])
-    V = np.zeros(sum(c * c for _, c in shapes))
-    w = np.zeros(sum(c for _, c in shapes))
-    rr = (C.c_int * len(shapes))(*[r for r, _ in shapes])
-    cc = (C.c_int * len(shapes))(*[c for _, c in shapes])
-    sw = (C.c_int * 1)()
-    code = dmrgb.lib().dmrg_test_svd(ctx.h, len(shapes), rr, cc, X.ctypes.data_as(DP),
-                                     V.ctypes.data_as(DP), w.ctypes.data_as(DP), sw)
-    assert code == 0, dmrgb.lib().dmrg_last_error(ctx.h)
-    ox = ov = ow = 0
-    for (r, c), M in zip(shapes, mats):
-        XV = X[ox:ox + r * c].reshape((r, c), order="F")
-        Vm = V[ov:ov + c * c].reshape((c, c), order="F")
-        lam = w[ow:ow + c]
-        ref = np.sort(np.linalg.eigvalsh(M.T @ M))[::-1]
-        nrm = np.linalg.norm(M, 2) ** 2
-        tol = 2e-13 * np.sqrt(max(r, c))
-        assert np.all(np.diff(lam) <= 0)
-        assert np.max(np.abs(lam - ref)) < tol * nrm
-        assert np.max(np.abs(Vm.T @ Vm - np.eye(c))) < tol
-        assert np.max(np.abs(M @ Vm - XV)) < tol * np.sqrt(nrm)
-        G = XV.T @ XV
-        assert np.max(np.abs(G - np.diag(np.diag(G)))) < tol * nrm
-        ox += r * c
-        ov += c * c
-        ow += c
-
-
 def _rho_like(rng, n, kind):
     if kind == "rank":
         X = rng.standard_normal((n, max(1, n // 2)))
