@@ -23,7 +23,8 @@ class Params(C.Structure):
     _fields_ = [("maxm", C.c_int), ("minm", C.c_int), ("cutoff", C.c_double),
                 ("krylov", C.c_int), ("precision", C.c_int), ("svnbond", C.c_int),
                 ("degen_rtol", C.c_double), ("betatest", C.c_double), ("fp64_final", C.c_int),
-                ("profile", C.c_int), ("reserved", C.c_int * 6)]
+                ("profile", C.c_int), ("cvgE", C.c_int), ("reserved0", C.c_int),
+                ("goal", C.c_double), ("reserved", C.c_int * 2)]
 
 
 class SweepStats(C.Structure):
@@ -34,7 +35,8 @@ class SweepStats(C.Structure):
                 ("eig_seconds", C.c_double), ("vec_seconds", C.c_double),
                 ("d_top", C.c_double * 8), ("gemm_flops", C.c_double),
                 ("gemm_seconds", C.c_double), ("gemm_launches", C.c_int), ("eig_max_n", C.c_int),
-                ("host_seconds", C.c_double), ("wait_seconds", C.c_double)]
+                ("host_seconds", C.c_double), ("wait_seconds", C.c_double),
+                ("converged", C.c_int), ("reserved_s", C.c_int), ("cvg_check", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "d_top"}
@@ -117,7 +119,6 @@ SIGNATURES = {
     "dmrg_test_gemm": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int,
                                  _DP, C.c_int, _DP, C.c_int]),
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),
-    "dmrg_test_svd": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP, _IP]),
     "dmrg_test_syevt": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP]),
     "dmrg_test_heff_time": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _DP, _DP]),
     "dmrg_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_P)]),

@@ -115,6 +115,8 @@ void dmrg_params_default(dmrg_params* p) {
   p->degen_rtol = 0.0;
   p->betatest = 1e-10;
   p->fp64_final = 1;
+  p->cvgE = 1;
+  p->goal = 0.0;
 }
 
 const char* dmrg_last_error(const dmrg_ctx* ctx) {
@@ -673,6 +675,7 @@ int dmrg_env_build(dmrg_state* st, const dmrg_mpo* mpo) {
     for (int i = st->L - 1; i > st->oc; --i) rupdate(st, i, nullptr);
     cuda_check(cudaStreamSynchronize(c->stream), "env build sync");
     st->env_built = true;
+    st->have_last = false;
   });
 }
 
@@ -868,7 +871,25 @@ int dmrg_sweep(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_s
     if (mpo != st->mpo) fail(DMRG_ERR_ARG, "state was uploaded with a different MPO");
     if (!p || !out) fail(DMRG_ERR_ARG, "null params/stats");
     set_device(c);
+    // dmrgcvg (algs/DMRG.jl:610-652): the first comparison is against the starting energy
+    // (startval, algs/optimizeMPS.jl:365-371; <psi|H|psi> of the canonical input) or entropy 0
+    if (p->goal > 0 && !st->have_last) {
+      if (!st->env_built) fail(DMRG_ERR_STATE, "call dmrg_env_build before dmrg_sweep");
+      st->last_energy = p->cvgE ? measure_expect(st, st->mpo, nullptr) : 0.0;
+      st->last_entropy = 0.0;
+      st->have_last = true;
+    }
     do_sweep(st, *p, *out);
+    if (p->goal > 0) {
+      const double chk = p->cvgE ? std::fabs(out->energy - st->last_energy)
+                                 : std::fabs(st->last_entropy - out->entropy);
+      out->cvg_check = chk;
+      out->converged = chk < p->goal ? 1 : 0;
+      if (!out->converged) {
+        st->last_energy = out->energy;
+        st->last_entropy = out->entropy;
+      }
+    }
   });
 }
 
@@ -911,52 +932,6 @@ int dmrg_test_syevt(dmrg_ctx* c, int nmat, const int* n, const int* k, double* A
     cuda_check(cudaMemcpyAsync(U, buf.p + ta + 4 * tw, tu * 8, cudaMemcpyDeviceToHost, c->stream), "U");
     cuda_check(cudaStreamSynchronize(c->stream), "syevt sync");
     dfree(c, buf);
-  });
-}
-
-int dmrg_test_svd(dmrg_ctx* c, int nmat, const int* r, const int* cc, double* X, double* V,
-                  double* w, int* sweeps) {
-  if (!c) return DMRG_ERR_ARG;
-  return guarded(c, [&] {
-    if (nmat <= 0 || !r || !cc || !X || !V || !w) fail(DMRG_ERR_ARG, "bad svd arguments");
-    set_device(c);
-    int64_t tx = 0, tv = 0, tw = 0;
-    for (int i = 0; i < nmat; ++i) {
-      tx += int64_t(r[i]) * cc[i];
-      tv += int64_t(cc[i]) * cc[i];
-      tw += cc[i];
-    }
-    std::vector<SvdTask> tasks;
-    size_t smem = 0;
-    int64_t ox = 0, ov = tx, ow = tx + tv;
-    for (int i = 0; i < nmat; ++i) {
-      SvdTask t{ox, ov, ow, r[i], cc[i]};
-      tasks.push_back(t);
-      smem = std::max(smem, hestenes_smem(r[i], cc[i]));
-      ox += int64_t(r[i]) * cc[i];
-      ov += int64_t(cc[i]) * cc[i];
-      ow += cc[i];
-    }
-    if (smem > HESTENES_SMEM_MAX) fail(DMRG_ERR_SHAPE, "matrix too large for the shared-memory kernel");
-    DBuf buf;
-    dalloc(c, buf, tx + tv + tw);
-    cuda_check(cudaMemcpyAsync(buf.p, X, tx * 8, cudaMemcpyHostToDevice, c->stream), "X");
-    Upload u;
-    const size_t off = u.put(tasks);
-    char* db = u.send(c, 0);
-    cuda_check(cudaMemsetAsync(c->d_status, 0, 2 * sizeof(int), c->stream), "status");
-    launch_hestenes(c->stream, buf.p, reinterpret_cast<const SvdTask*>(db + off), nmat, smem,
-                    c->d_status);
-    int st[2] = {0, 0};
-    cuda_check(cudaMemcpyAsync(X, buf.p, tx * 8, cudaMemcpyDeviceToHost, c->stream), "X D2H");
-    cuda_check(cudaMemcpyAsync(V, buf.p + tx, tv * 8, cudaMemcpyDeviceToHost, c->stream), "V D2H");
-    cuda_check(cudaMemcpyAsync(w, buf.p + tx + tv, tw * 8, cudaMemcpyDeviceToHost, c->stream), "w");
-    cuda_check(cudaMemcpyAsync(st, c->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
-               "st");
-    cuda_check(cudaStreamSynchronize(c->stream), "svd sync");
-    dfree(c, buf);
-    if (sweeps) *sweeps = st[1];
-    if (st[0]) fail(DMRG_ERR_CUDA, "one-sided Jacobi did not converge");
   });
 }
 

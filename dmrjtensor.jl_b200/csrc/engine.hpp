@@ -186,6 +186,10 @@ struct dmrg_state {
   std::vector<dmrg::DBuf> Lenv, Renv;           // L
   std::vector<char> Lvalid, Rvalid;
   bool env_built = false;
+  // dmrgcvg bookkeeping (algs/DMRG.jl:610-652): set at the first sweep with goal > 0 after an
+  // environment build (the start of a dmrg call), then updated after every sweep
+  bool have_last = false;
+  double last_energy = 0.0, last_entropy = 0.0;
 };
 
 namespace dmrg {

@@ -140,6 +140,7 @@ bool run_job(dmrg_ctx* c, Job& j) {
     j.entropy = ss.entropy;
     j.biggest_m = ss.biggest_m;
     j.sweeps_done = s + 1;
+    if (ss.converged) break;     // dmrgcvg's goal test (algs/DMRG.jl:610-652)
   }
   if (!bad) {
     j.site.resize(j.L);

@@ -403,7 +403,7 @@ class DeviceState:
 
 
 def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
-                degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0):
+                degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0, goal=0.0, cvgE=True):
     p = Params()
     lib().dmrg_params_default(C.byref(p))
     p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)
@@ -412,18 +412,22 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
     p.svnbond, p.degen_rtol, p.betatest, p.fp64_final = int(svnbond), float(degen_rtol), \
         float(betatest), int(fp64_final)
     p.profile = int(profile)
+    p.goal, p.cvgE = float(goal), 1 if cvgE else 0
     return p
 
 
 # ------------------------------------------------------------------ the drop-in
 
 def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, silent=True,
-         method="twosite", krylov=2, precision="fp64", SvNbond=0, degen_rtol=0.0, ctx=None,
-         download=True):
+         method="twosite", krylov=2, precision="fp64", SvNbond=0, degen_rtol=0.0, goal=0.0,
+         cvgE=True, ctx=None, download=True):
     """Two-site DMRG on the GPU: ``dmrg(psi, mpo; m, minm, sweeps, cutoff)`` of
     ``algs/DMRG.jl:549-588``. ``maxm`` is accepted as an alias of ``m``; ``m`` may also be a
     per-sweep list (a bond-dimension ramp). Returns the energy of the last bond step and updates
     ``psi`` (tensors, ``oc``) in place; per-sweep records go to ``psi.sweep_stats``.
+    ``goal > 0`` stops after the first sweep whose energy (``cvgE``) or centre entropy changed by
+    less than ``goal`` (``dmrgcvg``, ``algs/DMRG.jl:610-652``; the first sweep is compared with
+    the starting energy <psi|H|psi>).
     ``download=False`` leaves the result on the device (``psi`` keeps a handle to it)."""
     if method != "twosite":
         raise ValueError(f"DMRG method ({method}) not defined")
@@ -435,13 +439,20 @@ def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, si
     energy = 0.0
     stats = []
     for n, mcur in enumerate(sched):
-        st = dev.sweep(make_params(mcur, minm, cutoff, krylov, precision, SvNbond, degen_rtol))
+        st = dev.sweep(make_params(mcur, minm, cutoff, krylov, precision, SvNbond, degen_rtol,
+                                   goal=goal, cvgE=cvgE))
         energy = st["energy"]
         stats.append(st)
         if not silent:
             print(f"Sweep {n + 1} (back and forth): {st['seconds']:.5f} sec")
             print(f"Largest truncation = {st['max_truncerr']}, m = {st['biggest_m']}")
             print(f"Energy at sweep {n + 1} is {energy:.12f}\n")
+        if st["converged"]:
+            if not silent:
+                what = "energy" if cvgE else "entropy"
+                print(f"The {what} for DMRG converged to a difference of {st['cvg_check']} "
+                      f"after {n + 1} sweeps!\n")
+            break
     psi.sweep_stats = stats
     if download:
         dev.download_into(psi)

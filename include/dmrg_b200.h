@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG_ABI_VERSION 1
+#define DMRG_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define DMRG_API __attribute__((visibility("default")))
@@ -81,7 +81,13 @@ typedef struct dmrg_params {
   double betatest;   /* Krylov breakdown threshold, 1e-10 (algs/DMRG.jl:57)     */
   int fp64_final;    /* chosen forms: 1 = re-evaluate the Ritz energy with one FP64 matvec */
   int profile;       /* 1 = time every Heff GEMM launch with CUDA events (gemm_* stats)  */
-  int reserved[6];
+  int cvgE;          /* convergence test of dmrgcvg (algs/DMRG.jl:610-652): 1 = energy, 0 = entropy */
+  int reserved0;
+  double goal;       /* > 0: the sweep reports `converged` when |E - E_last| < goal (cvgE = 1) or
+                        |S - S_last| < goal (cvgE = 0); E_last starts at <psi|H|psi> of the state
+                        the environments were built for (startval, algs/optimizeMPS.jl:255-258,
+                        365-371), S_last at 0. 0 (the default) never converges: all sweeps run */
+  int reserved[2];
 } dmrg_params;
 
 /* Per-sweep record (what dmrgcvg prints, algs/DMRG.jl:610-652, plus timings). */
@@ -105,6 +111,9 @@ typedef struct dmrg_sweep_stats {
   int eig_max_n;        /* largest density-matrix block of the sweep                  */
   double host_seconds;  /* host wall time of the sweep call                           */
   double wait_seconds;  /* of which blocked in the per-step eigenvalue synchronisation */
+  int converged;        /* goal > 0 and the dmrgcvg test passed: the caller stops sweeping */
+  int reserved_s;
+  double cvg_check;     /* the tested difference (energy or entropy) when goal > 0        */
 } dmrg_sweep_stats;
 
 /* ---------------------------------------------------------------- context */
@@ -191,6 +200,9 @@ DMRG_API int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const 
  * vector/intermediate data and 1 MiB of task descriptors: larger two-site spaces are rejected with
  * DMRG_ERR_BUDGET. Nothing is allocated, no cudaMalloc/cudaFree is called. The first call on a
  * device looks up the array's device address, so make that first call before any stream capture.
+ * The call runs on the context's own stream, which is not ordered after the caller's streams:
+ * finish writing psi_in first (for example synchronise the stream that produced it). psi_in and
+ * psi_out may be the same buffer (the input is read completely before the output is written).
  * Calls share the array: calls that overlap on the GPU race. Returns after the result is written. */
 DMRG_API int dmrg_heff_apply_noalloc(dmrg_state* st, const dmrg_mpo* mpo, int iL,
                                      const double* psi_in, double* psi_out, int precision);
@@ -227,12 +239,6 @@ DMRG_API int dmrg_test_gemm(dmrg_ctx* ctx, int transA, int transB, int M, int N,
  * sizes n[i] packed back to back in A; eigenvalues (descending) packed into w and eigenvectors
  * (columns) overwrite A. */
 DMRG_API int dmrg_test_eigh(dmrg_ctx* ctx, int nmat, const int* n, double* A, double* w);
-
-/* One-sided Jacobi of nmat column-major matrices X_i (r[i] x c[i], packed in X): on return X
- * holds X_i V_i with columns sorted by descending norm, V the c[i] x c[i] rotations (packed),
- * w the squared column norms (descending) and sweeps[0] the largest sweep count. */
-DMRG_API int dmrg_test_svd(dmrg_ctx* ctx, int nmat, const int* r, const int* c, double* X,
-                           double* V, double* w, int* sweeps);
 
 /* Tridiagonal-path eigensolver (n[i] <= 112): all eigenvalues (descending, packed in w) and the
  * eigenvectors of the k[i] largest (packed n[i] x k[i] column-major in U). A is overwritten. */

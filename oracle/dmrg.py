@@ -246,7 +246,7 @@ def startval(Lenv, Renv, A, W):
 
 
 def dmrg(psi, mpo, m=0, minm=2, sweeps=1, cutoff=0.0, oc=0, krylov=2, trunc="svd",
-         svnbond=None, degen_rtol=0.0, maxm_schedule=None, record=None):
+         svnbond=None, degen_rtol=0.0, maxm_schedule=None, record=None, goal=0.0, cvgE=True):
     """``dmrg(psi, mpo; m, minm, sweeps, cutoff)`` with ``method="twosite"`` (``algs/DMRG.jl:549-588``
     -> ``dmrg_twosite`` ``:675-691`` -> ``optmps``). ``psi`` (list of tensors) is modified in place.
 
@@ -254,6 +254,11 @@ def dmrg(psi, mpo, m=0, minm=2, sweeps=1, cutoff=0.0, oc=0, krylov=2, trunc="svd
     (``algs/optimizeMPS.jl:848``). ``info`` holds per-sweep records (energy, maxtrunc, biggestm,
     entropy at bond ``svnbond``, seconds) and the final centre ``oc`` (0-based).
     ``maxm_schedule`` (optional list) overrides ``m`` per sweep.
+    ``goal``/``cvgE``: the convergence test of ``dmrgcvg`` (``algs/DMRG.jl:610-652``): after each
+    sweep, stop when |E - E_last| < goal (energy, ``cvgE``) or |S_last - S| < goal (entropy);
+    E_last starts at ``startval`` (``algs/optimizeMPS.jl:365-371``), S_last at 0, and both are
+    updated only when the test fails. ``goal = 0`` (the default, ``algs/optimizeMPS.jl:527``)
+    never stops early.
     """
     L = len(psi)
     P = Params(L, m, minm, cutoff, krylov, trunc, svnbond, degen_rtol)
@@ -267,6 +272,7 @@ def dmrg(psi, mpo, m=0, minm=2, sweeps=1, cutoff=0.0, oc=0, krylov=2, trunc="svd
     else:
         j = 1
     recs = []
+    last_e, last_s = e0, 0.0
     for n in range(sweeps):
         if maxm_schedule is not None:
             P.maxm = int(maxm_schedule[n])
@@ -277,6 +283,10 @@ def dmrg(psi, mpo, m=0, minm=2, sweeps=1, cutoff=0.0, oc=0, krylov=2, trunc="svd
                          entropy=P.entropy, seconds=dt, maxm=P.maxm))
         if record is not None:
             record(recs[-1])
+        check = abs(P.energy - last_e) if cvgE else abs(last_s - P.entropy)
+        if check < goal:
+            break
+        last_e, last_s = P.energy, P.entropy
     return P.energy, dict(sweeps=recs, oc=oc, e0=e0, nmatvec=P.nmatvec, storeD=P.storeD)
 
 

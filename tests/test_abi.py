@@ -26,11 +26,15 @@ def test_library_exports_every_declared_symbol(dmrgb):
 
 def test_abi_version_and_defaults(dmrgb):
     lib = dmrgb.lib()
-    assert lib.dmrg_abi_version() == 1
+    assert lib.dmrg_abi_version() == 2
     p = dmrgb._lib.Params()
     lib.dmrg_params_default(C.byref(p))
     assert (p.minm, p.krylov, p.maxm, p.precision) == (2, 2, 0, 0)
     assert p.betatest == 1e-10
+    # algvars defaults (algs/optimizeMPS.jl:527-528): energy convergence test, goal 0 (never stops)
+    assert (p.cvgE, p.goal) == (1, 0.0)
+    # the ctypes mirrors have the C layout: 80-byte params, stats end with the convergence fields
+    assert C.sizeof(dmrgb._lib.Params) == 80
 
 
 def test_null_handles_are_rejected(dmrgb):

@@ -139,3 +139,21 @@ def test_qn_heisenberg_dmrg_matches_oracle_and_ed(dmrgb, ctx):
     assert abs(E - E0) <= 1e-10 * abs(E0)
     assert abs(psi.sweep_stats[-1]["entropy"] - info["sweeps"][-1]["entropy"]) <= 1e-8
     assert abs(E - (-4.258035207282883)) < 1e-8
+
+
+@pytest.mark.parametrize("cvgE", [True, False])
+def test_goal_stops_after_the_same_sweep_as_the_oracle(dmrgb, ctx, cvgE):
+    """dmrgcvg's convergence test (algs/DMRG.jl:610-652): with goal > 0 the run stops after the
+    first sweep whose energy (cvgE) or centre entropy moved by less than goal, the first sweep
+    compared with the starting energy (startval) or entropy 0."""
+    L = 10
+    mpo, ompo = _heis(dmrgb, L, False)
+    psi = dmrgb.randMPS(2, L, 8, seed=1)
+    ref = [a.copy() for a in psi.tensors]
+    E = dmrgb.dmrg(psi, mpo, m=32, sweeps=20, cutoff=1e-12, goal=1e-7, cvgE=cvgE, ctx=ctx)
+    E0, info = od.dmrg(ref, ompo, m=32, sweeps=20, cutoff=1e-12, trunc="rho", goal=1e-7,
+                       cvgE=cvgE)
+    assert len(psi.sweep_stats) == len(info["sweeps"]) < 20
+    assert psi.sweep_stats[-1]["converged"] == 1
+    assert all(s["converged"] == 0 for s in psi.sweep_stats[:-1])
+    assert abs(E - E0) <= 1e-10 * abs(E0)

@@ -101,3 +101,18 @@ def test_truncation_rule():
     # a cut inside a degenerate pair drops the pair when degen_rtol > 0
     kept, _ = oq.select_kept([np.array([0.6, 0.2, 0.2])], maxm=2, minm=1, cutoff=0, degen_rtol=1e-6)
     assert kept == [1]
+
+
+def test_oracle_goal_semantics():
+    """goal = 0 runs every sweep; a large goal stops after the first; the energy test compares the
+    first sweep with startval (algs/optimizeMPS.jl:365-371, algs/DMRG.jl:627-637)."""
+    L = 6
+    mpo = om.make_mpo([om.heisenberg_bulk()] * L, 2)
+    rng = np.random.default_rng(2)
+    start = om.right_canonicalize(om.random_mps(L, 2, 4, rng))
+    _, info = od.dmrg([a.copy() for a in start], mpo, m=16, sweeps=4, trunc="rho")
+    assert len(info["sweeps"]) == 4
+    _, info = od.dmrg([a.copy() for a in start], mpo, m=16, sweeps=4, trunc="rho", goal=1e3)
+    assert len(info["sweeps"]) == 1
+    e0 = info["e0"]
+    assert e0 == pytest.approx(od.expect([a.copy() for a in start], mpo), rel=1e-12)
