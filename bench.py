@@ -6,13 +6,14 @@ U(1) block-sparse (Sz_total = 0), MPO bond dimension 5, Neel product start, cuto
 maxm ramped 64 -> 1024 over 12 sweeps (64, 82, 105, 135, 173, 222, 284, 364, 467, 598, 766, 1024).
 The first 11 ramp sweeps prepare the state (untimed); a "step" is one full sweep (2(L-1) two-site
 bond steps with their environment updates) at maxm = 1024. W warm-up steps, then K timed steps.
-The resident MPS + environments (several hundred MB) exceed the 126 MB L2, so no flush is needed.
+The resident MPS + environments are smaller than the 126 MB L2, so L2 is flushed (a 256 MB
+device write, outside the device-timed region) before every timed sweep.
 
 Reported: value = sweeps/s over all ranks (device-timed, state resident in HBM); e2e = the same
 through the public ``dmrg(psi, mpo; m, sweeps=1)`` call with the MPS in host memory (upload,
 environment build, sweep, download inside the timed region); roofline of the dominant kernel
 (the grouped FP64 GEMM) against the FP64 GEMM peak measured here with cuBLAS; and the CPU oracle
-timed on a bounded sample of the same workload.
+timed on the device's own state (the oracle's sweep() on the host cores).
 """
 from __future__ import annotations
 
@@ -158,95 +159,80 @@ def fp64_gemm_peak(device):
     return 2.0 * n ** 3 / best / 1e12
 
 
+class L2Flush:
+    """Writes a 256 MB device buffer (twice the 126 MB L2) and waits for it: called between timed
+    sweeps, outside their device-timed region, so that no sweep starts with a warm L2 (the
+    resident state of the headline workload is smaller than L2)."""
+
+    def __init__(self, device):
+        import torch
+        self.torch = torch
+        self.buf = torch.empty(256 << 20, dtype=torch.uint8, device=torch.device("cuda", device))
+
+    def __call__(self):
+        self.buf.fill_(1)
+        self.torch.cuda.synchronize(self.buf.device)
+
+
 def host_block_bytes(psi):
     return int(sum(b.size for b in psi.blocks) * 8)
 
 
 # ------------------------------------------------------------------ CPU oracle sample
 
-def bond_profile_from_sectors(sectors):
-    """Relative per-bond cost proxy for scaling a sampled bond step to a sweep: the dense-equivalent
-    two-site contraction volume m_l * m_r * (m_l + m_r) of every bond step."""
-    tot = [sum(d for _, d in s) for s in sectors]
-    L = len(sectors) - 1
-    cost = [tot[i] * tot[i + 2] * (tot[i] + tot[i + 2]) for i in range(L - 1)]
-    return cost
-
-
-def oracle_sample(sectors, krylov, nsteps=2, seed=0):
-    """Time the oracle's twostep + environment update at the centre bond(s) of a chain with the
-    given bond sector structure (random block values: the cost does not depend on them).
-    Returns (seconds per sampled step, sweep-seconds estimate, description)."""
+def oracle_qmps(sectors, blocks, phys):
+    """The oracle's block tensors A[a(+1), s(+1), b(-1)] of an MPS given in the library's block
+    form (bond sectors, per-site flat block data in canonical order, physical charges)."""
     sys.path.insert(0, str(ROOT))
-    from oracle import dmrg as od, models as om, qtensor as oq
-    rng = np.random.default_rng(seed)
-    L = len(sectors) - 1
-    pq = [(1,), (-1,)]
-    mpo = om.to_qmpo(om.make_mpo([om.heisenberg_bulk()] * L, 2), [pq] * L)
-    c = L // 2 - 1
-    idx = {b: oq.Index([q for q, _ in sectors[b]], [d for _, d in sectors[b]], +1)
-           for b in range(c, c + 2 + nsteps + 1)}
+    from oracle import qtensor as oq
+    out = []
+    for i, data in enumerate(blocks):
+        Bl, Br = sectors[i], sectors[i + 1]
+        ia = oq.Index([q for q, _ in Bl], [d for _, d in Bl], +1)
+        isx = oq.Index(phys[i], [1] * len(phys[i]), +1)
+        ib = oq.Index([q for q, _ in Br], [d for _, d in Br], -1)
+        rq = {q: k for k, (q, _) in enumerate(Br)}
+        T = oq.QTensor([ia, isx, ib], {}, tuple(0 for _ in phys[i][0]))
+        off = 0
+        for ka, (qa, da) in enumerate(Bl):
+            for si, ps in enumerate(phys[i]):
+                kb = rq.get(tuple(x + y for x, y in zip(qa, ps)))
+                if kb is None:
+                    continue
+                db = Br[kb][1]
+                T.blocks[(ka, si, kb)] = np.asarray(data[off:off + da * db]).reshape(
+                    (da, db), order="F").reshape(da, 1, db).copy()
+                off += da * db
+        out.append(T)
+    return out
 
-    def rand_site(b):
-        ia, ib = idx[b], idx[b + 1].dual()
-        T = oq.QTensor([ia, oq.Index(pq, [1, 1], +1), ib], {}, (0,))
-        for ka, qa in enumerate(ia.qns):
-            for s, ps in enumerate(pq):
-                q = (qa[0] + ps[0],)
-                if q in ib.qns:
-                    kb = ib.qns.index(q)
-                    T.blocks[(ka, s, kb)] = rng.standard_normal((ia.dims[ka], 1, ib.dims[kb]))
-        return T
 
-    def rand_env(b, site_mpo_index, left):
-        ia = idx[b]
-        iw = site_mpo_index
-        if left:
-            ind = [ia, iw.dual(), ia.dual()]
-        else:
-            ind = [ia, iw.dual(), ia.dual()]
-        T = oq.QTensor(ind, {}, (0,))
-        for k1 in range(len(ia.dims)):
-            for w in range(len(iw.dims)):
-                for k3 in range(len(ia.dims)):
-                    if T.allowed((k1, w, k3)):
-                        T.blocks[(k1, w, k3)] = rng.standard_normal((ia.dims[k1], 1, ia.dims[k3]))
-        return T
+def oracle_workload():
+    """The oracle's copy of the headline workload: Heisenberg L=100, U(1), Neel start."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import models as om
+    q = [[(1,), (-1,)]] * L_CHAIN
+    return (om.to_qmps(om.neel_mps(L_CHAIN), q),
+            om.to_qmpo(om.make_mpo([om.heisenberg_bulk()] * L_CHAIN, 2), q))
 
-    psi = {b: rand_site(b) for b in range(c, c + 1 + nsteps)}
-    Lenv = {c: rand_env(c, mpo[c].indices[0], True)}
-    P = od.Params(L, RAMP[-1], 2, CUTOFF, krylov, "svd")
-    times = []
-    for k in range(nsteps):
-        iL, iR = c + k, c + k + 1
-        # a right environment of the correct structure for site iR
-        ib = idx[iR + 1]
-        R = oq.QTensor([ib, mpo[iR].indices[3].dual(), ib.dual()], {}, (0,))
-        for k1 in range(len(ib.dims)):
-            for w in range(len(mpo[iR].indices[3].dims)):
-                for k3 in range(len(ib.dims)):
-                    if R.allowed((k1, w, k3)):
-                        R.blocks[(k1, w, k3)] = rng.standard_normal((ib.dims[k1], 1, ib.dims[k3]))
-        Renv_list = [None] * L
-        Lenv_list = [None] * L
-        Renv_list[iR] = R
-        Lenv_list[iL] = Lenv[iL]
-        plist = [None] * L
-        plist[iL], plist[iR] = psi[iL], psi[iR]
+
+class OracleSweeps:
+    """The oracle's own sweep loop (algs/optimizeMPS.jl:790-835 restated in numpy) on a state:
+    environments built once, then one ``sweep()`` call per timed step at maxm 1024."""
+
+    def __init__(self, psi, mpo, krylov, oc=0, j=1):
+        from oracle import dmrg as od
+        self.od = od
+        self.psi, self.mpo, self.oc, self.j = psi, mpo, oc, j
+        self.Lenv, self.Renv = od.make_env(psi, mpo, oc)
+        self.P = od.Params(L_CHAIN, RAMP[-1], 2, CUTOFF, krylov, "rho")
+
+    def sweep(self, maxm=RAMP[-1]):
+        self.P.maxm = maxm
         t0 = time.perf_counter()
-        od.twostep(1, iL, iL, iR, plist, mpo, Lenv_list, Renv_list, P)
-        Lenv[iL + 1] = od.Lupdate(Lenv[iL], plist[iL], plist[iL], mpo[iL])
-        times.append(time.perf_counter() - t0)
-        psi[iR] = plist[iR]
-        # keep the next step's left tensor on the original sector structure
-        idx[iR] = plist[iR].indices[0]
-    t_step = statistics.mean(times)
-    cost = bond_profile_from_sectors(sectors)
-    est = t_step * 2 * sum(cost) / (statistics.mean(cost[c:c + nsteps]))
-    desc = (f"oracle twostep+Lupdate at bonds {c}..{c + nsteps} of the m={RAMP[-1]} sector "
-            f"structure (random block values, krylov {krylov}); sweep = 2(L-1) steps scaled by "
-            f"the dense-equivalent m_l*m_r*(m_l+m_r) cost of every bond")
-    return t_step, est, desc
+        self.oc, self.j = self.od.sweep(self.psi, self.mpo, self.Lenv, self.Renv, self.oc, self.j,
+                                        self.P)
+        return time.perf_counter() - t0
 
 
 def run_serving(pkg, device, nreq, rate=20.0, slots=8, seed=5):
@@ -412,38 +398,62 @@ def workload_config(args, world):
     """The `config` of both arms' JSON lines."""
     return {"workload": "heisenberg L=100 U(1) Sz=0, maxm 1024 sweep (two-site), after the "
                         "64->1024 ramp", "krylov": args.krylov, "cutoff": CUTOFF,
-            "precision": args.precision, "l2": "state larger than L2 (no flush)",
+            "precision": args.precision, "l2": "flushed before every timed sweep (256 MB write)",
             "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args, world, rank):
+    """The CPU arm: the oracle (numpy/scipy restatement of the reference's two-site path; the
+    reference itself is Julia and cannot run here) on the host cores. It ramps the same Neel start
+    through the same 64 -> 766 maxm schedule (untimed), then times W warm-up and K measured full
+    sweeps at maxm 1024, one oracle ``sweep()`` call per step -- the unit the device arm times."""
     if rank != 0:
         return
-    sectors = json.load(open(ROOT / "tests" / "golden" / "c2_sectors_m1024.json"))["sectors"]
-    sectors = [[(tuple(q), d) for q, d in b] for b in sectors]
-    # the driver's --steps K --warmup W, each step a bounded sample (two bond steps at the
-    # chain centre, scaled to a sweep); --steps-ref / --warmup-ref override them
     n_steps = args.steps_ref if args.steps_ref is not None else args.steps
     n_warm = args.warmup_ref if args.warmup_ref is not None else args.warmup
-    steps = []
+    psi, mpo = oracle_workload()
+    run = OracleSweeps(psi, mpo, args.krylov)
+    t_ramp = time.perf_counter()
+    for m in ramp_schedule(args.ramp_sweeps):
+        run.sweep(m)
+    t_ramp = time.perf_counter() - t_ramp
     for _ in range(n_warm):
-        oracle_sample(sectors, args.krylov, nsteps=1)
-    for _ in range(n_steps):
-        t_step, est, desc = oracle_sample(sectors, args.krylov, nsteps=2)
-        steps.append(est)
-    sweep_s = statistics.mean(steps)
+        run.sweep()
+    times = [run.sweep() for _ in range(n_steps)]
+    sweep_s = statistics.mean(times)
     cores = cpu_threads()
     value = 1.0 / sweep_s
+    desc = (f"oracle sweep() (numpy/scipy, OpenBLAS threads {cores}) on its own ramped state: "
+            f"{n_steps} full sweeps at maxm {RAMP[-1]} after the untimed 64->766 ramp")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
            "n_gpus": args.gpus, "steps": n_steps, "warmup": n_warm,
            "ms_per_step": sweep_s * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": workload_config(args, world),
+           "energy": run.P.energy, "ramp_seconds": t_ramp,
            "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": cores, "kind": "port",
                             "sample": desc},
            "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+
+
+def cpu_baseline_on_state(dev, krylov, nsweeps=2):
+    """The oracle timed on the device arm's own resident state (downloaded block by block): the
+    same sweep at maxm 1024 on the host cores. Returns the cpu_baseline record and the oracle's
+    energy after those sweeps."""
+    sectors = [dev.bond(b) for b in range(L_CHAIN + 1)]
+    blocks = [dev.site_blocks(i) for i in range(L_CHAIN)]
+    phys = [[(1,), (-1,)]] * L_CHAIN
+    psi = oracle_qmps(sectors, blocks, phys)
+    _, mpo = oracle_workload()
+    run = OracleSweeps(psi, mpo, krylov, oc=dev.oc, j=1 if dev.oc == 0 else -1)
+    times = [run.sweep() for _ in range(nsweeps)]
+    t = statistics.mean(times)
+    return ({"value": 1.0 / t, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
+             "sample": f"oracle sweep() at maxm {RAMP[-1]} on the device's resident state, "
+                       f"{nsweeps} full sweeps timed (mean)", "seconds_per_sweep": t},
+            run.P.energy)
 
 
 def run_ours(args, world, rank, local, dist):
@@ -468,7 +478,11 @@ def run_ours(args, world, rank, local, dist):
     n0 = pkg.kernel_launches()
     nvtx("push", "timed_sweeps")     # lets a profiler select exactly the timed launches
     t0 = time.perf_counter()
-    stats = [dev.sweep(params(pkg, mfin, args)) for _ in range(args.steps)]
+    flush = L2Flush(local)
+    stats = []
+    for _ in range(args.steps):
+        flush()
+        stats.append(dev.sweep(params(pkg, mfin, args)))
     wall = time.perf_counter() - t0
     nvtx("pop")
     launches = pkg.kernel_launches() - n0
@@ -491,7 +505,10 @@ def run_ours(args, world, rank, local, dist):
             dev.sweep(params(pkg, mfin, args, precision="3xtf32"))
         if dist:
             dist.barrier()
-        st_c = [dev.sweep(params(pkg, mfin, args, precision="3xtf32")) for _ in range(args.steps)]
+        st_c = []
+        for _ in range(args.steps):
+            flush()
+            st_c.append(dev.sweep(params(pkg, mfin, args, precision="3xtf32")))
         tc = reduce_max(dist, sum(x["seconds"] for x in st_c))
         prof_c = dev.sweep(params(pkg, mfin, args, profile=1, precision="3xtf32"))
         chosen = {"form": "3xtf32: Heff GEMMs as three TF32 products on tcgen05 (FP32 accumulate "
@@ -503,6 +520,13 @@ def run_ours(args, world, rank, local, dist):
                   "abs_dE_vs_plain": abs(st_c[-1]["energy"] - energy),
                   "heff_tflops": (prof_c["heff_flops"] / prof_c["heff_seconds"] / 1e12
                                   if prof_c["heff_seconds"] > 0 else None)}
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        # the oracle on this very state: the same sweeps on the host cores, energies side by side
+        cpu, e_oracle = cpu_baseline_on_state(dev, args.krylov, nsweeps=args.cpu_sweeps)
+        e_dev = [dev.sweep(params(pkg, mfin, args))["energy"] for _ in range(args.cpu_sweeps)][-1]
+        cpu.update({"oracle_energy": e_oracle, "device_energy_same_sweeps": e_dev,
+                    "abs_dE_device_vs_oracle": abs(e_dev - e_oracle)})
     sectors = [dev.bond(b) for b in range(L_CHAIN + 1)]
     if args.dump_sectors:
         Path(args.dump_sectors).write_text(json.dumps(
@@ -539,11 +563,6 @@ def run_ours(args, world, rank, local, dist):
     if tfile.exists():
         # DRAM bytes per Heff GEMM launch of this workload, from the committed ncu capture
         traffic = json.loads(tfile.read_text()).get("dram_bytes_per_heff_launch")
-    cpu = None
-    if not args.no_cpu:
-        t_step, est, desc = oracle_sample(sectors, args.krylov, nsteps=2)
-        cpu = {"value": 1.0 / est, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
-               "sample": desc, "seconds_per_sampled_step": t_step}
     out = {
         "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sweep_s * 1e3,
@@ -552,6 +571,7 @@ def run_ours(args, world, rank, local, dist):
         "config": workload_config(args, world),
         "energy": energy,
         "sweep_seconds": sweep_s,
+        "device_bytes_in_use": ctx.memory()[0],
         "heff_tflops": heff_flops / heff_sec / 1e12 if heff_sec > 0 else None,
         "phase_seconds_profiled_sweep": {k: prof[k] for k in
                                          ("seconds", "heff_seconds", "env_seconds",
@@ -592,6 +612,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--dump-sectors", default=None)
+    ap.add_argument("--cpu-sweeps", type=int, default=2,
+                    help="oracle sweeps timed on the device state for cpu_baseline")
     ap.add_argument("--steps-ref", type=int, default=None,
                     help="reference arm: timed samples (default: --steps)")
     ap.add_argument("--warmup-ref", type=int, default=None,
