@@ -110,6 +110,8 @@ SIGNATURES = {
     "dmrg_state_save": (C.c_int, [_P, C.c_char_p]),
     "dmrg_state_load": (C.c_int, [_P, _P, C.c_char_p, C.POINTER(_P)]),
     "dmrg_expect": (C.c_int, [_P, _P, _DP]),
+    "dmrg_env_step": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP,
+                                _DP, _DP, _DP, _DP]),
     "dmrg_correlationmatrix": (C.c_int, [_P, C.c_int, _DP, _DP, _DP, _DP]),
     "dmrg_heff_apply": (C.c_int, [_P, _P, C.c_int, _DP, _DP, C.c_int]),
     "dmrg_heff_apply_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),

@@ -701,6 +701,17 @@ int dmrg_rupdate(dmrg_state* st, const dmrg_mpo* mpo, int site) {
   });
 }
 
+int dmrg_env_step(dmrg_ctx* c, int left, int ml, int d, int mr, int wl, int wr,
+                  const double* env_in, const double* dual, const double* psi, const double* W,
+                  double* env_out) {
+  if (!c) return DMRG_ERR_ARG;
+  return guarded(c, [&] {
+    if (!env_in || !psi || !W || !env_out) fail(DMRG_ERR_ARG, "env step: null array");
+    set_device(c);
+    env_step_dense(c, left != 0, ml, d, mr, wl, wr, env_in, dual ? dual : psi, psi, W, env_out);
+  });
+}
+
 int dmrg_expect(dmrg_state* st, const dmrg_mpo* H, double* value) {
   if (!st || !H || !value) return DMRG_ERR_ARG;
   dmrg_ctx* c = st->ctx;

@@ -300,9 +300,15 @@ void plan_left_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const Sit
 void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const SiteLayout& lay,
                      const EnvLayout& RL, StepPlan& sp);
 void put_step(Upload& u, StepPlan& sp);
-// Launches an uploaded step; c->T1 / c->T2 must hold sp.t1 / sp.t2 doubles.
+// Launches an uploaded step; c->T1 / c->T2 must hold sp.t1 / sp.t2 doubles. `bra` (optional)
+// is the conjugated tensor when it differs from the ket tensor A (the dualpsi argument of
+// Lupdate/Rupdate); both share A's layout.
 void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, int64_t n_in,
-              const DBuf& A, double* env_out, int64_t n_out);
+              const DBuf& A, double* env_out, int64_t n_out, const DBuf* bra = nullptr);
+// Lupdate(Lenv, dualpsi, psi, mpo) / Rupdate(...) as a pure function of dense host tensors.
+void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int wr,
+                    const double* env_in, const double* dual, const double* psi, const double* W,
+                    double* env_out);
 
 void env_boundaries(dmrg_state* st);
 void lupdate(dmrg_state* st, int i, double* flops);

@@ -362,12 +362,89 @@ void put_step(Upload& u, StepPlan& sp) {
 }
 
 void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, int64_t n_in,
-              const DBuf& A, double* env_out, int64_t n_out) {
+              const DBuf& A, double* env_out, int64_t n_out, const DBuf* bra) {
   if (c->T1.n < sp.t1 || c->T2.n < sp.t2 || n_out < sp.out.size)
     fail(DMRG_ERR_ARG, "internal plan check failed: environment step scratch too small");
-  run_gemm(c, sp.g1, db, env_in, n_in, A.p, A.n, c->T1.p, c->T1.n);
+  // the left step reads the ket tensor first (L psi) and the bra tensor last (conj(dual)^T T2);
+  // the right step the other way round (R dual^T, then psi T2)
+  const DBuf& B = bra ? *bra : A;
+  const bool left = sp.g3.tA;
+  const DBuf& first = left ? A : B;
+  const DBuf& last = left ? B : A;
+  run_gemm(c, sp.g1, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n);
   run_mix(c, sp.mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
-  run_gemm(c, sp.g3, db, A.p, A.n, c->T2.p, c->T2.n, env_out, n_out);
+  run_gemm(c, sp.g3, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out);
+}
+
+void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int wr,
+                    const double* env_in, const double* dual, const double* psi, const double* W,
+                    double* env_out) {
+  if (ml <= 0 || d <= 0 || mr <= 0 || wl <= 0 || wr <= 0)
+    fail(DMRG_ERR_SHAPE, "env step: every dimension must be positive");
+  // dense tensors: every bond and physical state carries charge 0 (one sector per bond)
+  Bond Bl, Br;
+  Bl.q = {QN()}; Bl.dim = {ml};
+  Br.q = {QN()}; Br.dim = {mr};
+  MPOSite ms;
+  ms.wl = wl; ms.d = d; ms.wr = wr;
+  ms.rl.assign(wl, QN());
+  ms.rr.assign(wr, QN());
+  ms.p.assign(d, QN());
+  ms.dense.assign(W, W + size_t(wl) * d * d * wr);
+  for (int w2 = 0; w2 < wr; ++w2)
+    for (int t = 0; t < d; ++t)
+      for (int s = 0; s < d; ++s)
+        for (int w = 0; w < wl; ++w) {
+          const double v = W[w + size_t(wl) * (s + size_t(d) * (t + size_t(d) * w2))];
+          if (v != 0.0) ms.nz.push_back({w, s, t, w2, v});
+        }
+  const SiteLayout lay = make_site_layout(Bl, ms.p, Br);
+  // site [ml, d, mr] column-major -> blocks (s) of [ml x mr], s-major
+  std::vector<double> hA(size_t(ml) * d * mr), hB(hA.size());
+  for (int s = 0; s < d; ++s)
+    for (int b = 0; b < mr; ++b)
+      for (int a = 0; a < ml; ++a) {
+        const size_t src = a + size_t(ml) * (s + size_t(d) * b);
+        const size_t dst = size_t(lay.off[s]) + a + size_t(ml) * b;
+        hA[dst] = psi[src];
+        hB[dst] = dual[src];
+      }
+  StepPlan sp;
+  EnvLayout in_lay;
+  if (left) {
+    in_lay = make_left_env_layout(Bl, ms.rl);
+    plan_left_step(Bl, Br, ms, lay, in_lay, sp);
+  } else {
+    in_lay = make_right_env_layout(Br, ms.rr);
+    plan_right_step(Bl, Br, ms, lay, in_lay, sp);
+  }
+  // a dense environment [m, w, m] column-major is exactly the one-sector block layout
+  Upload u;
+  put_step(u, sp);
+  char* db = u.send(c, 2);
+  DBuf dA, dB, din, dout;
+  try {
+    dalloc(c, dA, int64_t(hA.size()));
+    dalloc(c, dB, int64_t(hB.size()));
+    dalloc(c, din, std::max<int64_t>(in_lay.size, 1));
+    dalloc(c, dout, std::max<int64_t>(sp.out.size, 1));
+    ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
+    ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));
+    cuda_check(cudaMemcpyAsync(dA.p, hA.data(), hA.size() * 8, cudaMemcpyHostToDevice, c->stream),
+               "env step psi");
+    cuda_check(cudaMemcpyAsync(dB.p, hB.data(), hB.size() * 8, cudaMemcpyHostToDevice, c->stream),
+               "env step dual");
+    cuda_check(cudaMemcpyAsync(din.p, env_in, size_t(in_lay.size) * 8, cudaMemcpyHostToDevice,
+                               c->stream), "env step input");
+    run_step(c, sp, db, din.p, din.n, dA, dout.p, dout.n, &dB);
+    cuda_check(cudaMemcpyAsync(env_out, dout.p, size_t(sp.out.size) * 8, cudaMemcpyDeviceToHost,
+                               c->stream), "env step output");
+    cuda_check(cudaStreamSynchronize(c->stream), "env step sync");
+  } catch (...) {
+    dfree(c, dA); dfree(c, dB); dfree(c, din); dfree(c, dout);
+    throw;
+  }
+  dfree(c, dA); dfree(c, dB); dfree(c, din); dfree(c, dout);
 }
 
 void lupdate(dmrg_state* st, int i, double* flops) {

@@ -1,19 +1,30 @@
 # DMRJtensorB200.jl -- Julia host binding of libdmrgb200.so (C ABI in include/dmrg_b200.h).
 #
-# A drop-in for DMRJtensor's two-site ground-state path:
-#   dmrg(psi::MPS, mpo::MPO; m, minm, sweeps, cutoff, silent, SvNbond)   algs/DMRG.jl:549-588
-#   makeEnv(psi, mpo) / Lupdate / Rupdate                               lib/Env/makeEnv.jl:196-246
-# `dmrg_b200(psi, mpo; ...)` takes the reference's own MPS/MPO objects (fields `psi.A`, `psi.oc`,
-# `mpo.H`, lib/types.jl:84-101), runs every sweep on the GPU and writes the optimised tensors back
-# into `psi` (dense `tens` or, for quantum-number MPS, rebuilt with `makeqMPS`), returning the
-# energy exactly as `dmrg` does. Tensors cross the boundary in their dense-equivalent column-major
-# form ([ml,d,mr] sites, [wl,d,d,wr] MPO sites); quantum numbers cross as integer charges
-# (`charges[i]` = d x nsym Int32 matrix of site i's physical charges, the same labels that were
-# given to makeqMPS / makeqMPO, e.g. 2Sz for U1 spin). All sizes are checked by the library.
+# A drop-in for DMRJtensor's two-site ground-state path. Loading this module after DMRJtensor adds
+#   * a method of DMRJtensor.dmrg for the concrete MPS/MPO types (algs/DMRG.jl:549-588): the same
+#     call, dmrg(psi, mpo; m (or maxm), minm, sweeps, cutoff, silent, goal, cvgE, SvNbond, method),
+#     runs every sweep of method "twosite" on the GPU, writes the optimised tensors back into psi
+#     and sets psi.oc as optmps leaves it; other methods go to the reference's own implementation
+#     (`invoke` on the abstract signature), so no call site changes;
+#   * the Env API on device-resident environments (lib/Env/makeEnv.jl:196-246,
+#     lib/MPO_MPS/Lupdate.jl:17-37, Rupdate.jl:17-37): makeEnv_b200(psi, mpo) returns (Lenv, Renv)
+#     whose Lenv[i] / Renv[i] download the dense-equivalent tensor, and Lupdate!(i, Lenv, psi, mpo)
+#     / Rupdate!(i, Renv, psi, mpo) methods for them; Lupdate(L, dualpsi, psi, W) /
+#     Rupdate(R, dualpsi, psi, W) on dense Float64 arrays computed on the device.
+# Quantum-number MPS cross the boundary in block form: the Qtens blocks (.T, .ind, .currblock,
+# the fields the reference itself reads in lib/MPS/makeqMPS.jl:62-99 and lib/MPO/MPO.jl:85-92)
+# are scattered straight into the library's block layout (dmrg_mps_upload_blocks), so no
+# dense-equivalent site array is built on the way in. Bond charges are propagated from the left
+# edge with the integer physical charges (q(right) = q(left) + p(s)), which come from the
+# `charges` keyword (d x nsym integer matrix per site, or one for all sites) or, when it is not
+# given, from `qnum_ints(getQnum(2, s, psi[i]))`, a hook a program overrides for its own @makeQNs
+# type. The MPO (w x d x d x w per site) crosses in dense form.
 module DMRJtensorB200
 
-export dmrg_b200, B200Env, makeEnv_b200, Lupdate_b200!, Rupdate_b200!, expect_b200,
-       correlationmatrix_b200, save_b200, load_b200
+import DMRJtensor
+
+export dmrg_b200, makeEnv_b200, B200Env, B200Side, expect_b200, correlationmatrix_b200,
+       save_b200, load_b200
 
 const libdmrg = get(ENV, "DMRG_B200_LIB", joinpath(@__DIR__, "..", "libdmrgb200.so"))
 
@@ -29,9 +40,12 @@ mutable struct Params
   betatest::Cdouble
   fp64_final::Cint
   profile::Cint
-  reserved::NTuple{6,Cint}
+  cvgE::Cint
+  reserved0::Cint
+  goal::Cdouble
+  reserved::NTuple{2,Cint}
 end
-Params() = Params(0, 0, 0.0, 0, 0, 0, 0.0, 0.0, 0, 0, ntuple(_ -> Cint(0), 6))
+Params() = Params(0, 0, 0.0, 0, 0, 0, 0.0, 0.0, 0, 0, 0, 0, 0.0, ntuple(_ -> Cint(0), 2))
 
 # mirrors struct dmrg_sweep_stats
 mutable struct SweepStats
@@ -54,8 +68,12 @@ mutable struct SweepStats
   eig_max_n::Cint
   host_seconds::Cdouble
   wait_seconds::Cdouble
+  converged::Cint
+  reserved_s::Cint
+  cvg_check::Cdouble
 end
-SweepStats() = SweepStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0.0, 8), 0, 0, 0, 0, 0, 0)
+SweepStats() = SweepStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0.0, 8), 0, 0, 0, 0, 0, 0,
+                          0, 0, 0)
 
 lasterror(ctx) = unsafe_string(ccall((:dmrg_last_error, libdmrg), Cstring, (Ptr{Cvoid},), ctx))
 
@@ -77,9 +95,39 @@ function Context(device::Integer=0; hbm_budget_bytes::Integer=0)
   c
 end
 
-# The reference stores tensors as `tens` (dense) or `Qtens`; `makeArray` (TensorPACK) gives the
-# dense-equivalent Array of either. `densify` is a hook so that other containers can be passed.
-densify(T) = Array{Float64}(Main.makeArray(T))
+const default_ctx = Ref{Union{Nothing,Context}}(nothing)
+context(device::Integer) = (default_ctx[] === nothing && (default_ctx[] = Context(device));
+                            default_ctx[])
+
+# ------------------------------------------------------------------------ tensors and charges
+
+isqtens(T) = T isa DMRJtensor.Qtens
+# dense-equivalent Array of a dense tensor (tens or Array) or an MPO site
+densify(T) = T isa Array ? Array{Float64}(T) : Array{Float64}(DMRJtensor.makeArray(T))
+
+"""
+    qnum_ints(q) -> Vector{Int}
+
+Integer charges of a quantum-number label (one entry per U(1) factor). Override this for the
+label type your program's `@makeQNs` defines when `charges` is not passed to `dmrg`.
+"""
+qnum_ints(q) = error("qnum_ints is not defined for $(typeof(q)); pass charges= to dmrg, or " *
+                     "define DMRJtensorB200.qnum_ints for this label type")
+
+# per-site d x nsym integer charges, from `charges` or from the MPS's own physical labels
+function site_charges(psi, charges)
+  L = length(psi.A)
+  if charges !== nothing
+    return charges isa AbstractMatrix ? [Matrix{Int}(charges) for _ = 1:L] :
+           [Matrix{Int}(charges[(i - 1) % length(charges) + 1]) for i = 1:L]
+  end
+  isqtens(psi.A[1]) || return nothing
+  return [begin
+            d = size(psi.A[i], 2)
+            rows = [qnum_ints(DMRJtensor.getQnum(2, s, psi.A[i])) for s = 1:d]
+            Matrix{Int}(permutedims(hcat(rows...), (2, 1)))
+          end for i = 1:L]
+end
 
 function upload_mpo(ctx::Context, mpo, charges)
   L = length(mpo.H)
@@ -104,7 +152,7 @@ function upload_mpo(ctx::Context, mpo, charges)
   out[]
 end
 
-function upload_mps(ctx::Context, hmpo, psi)
+function upload_dense_mps(ctx::Context, hmpo, psi)
   L = length(psi.A)
   As = [densify(psi.A[i]) for i = 1:L]
   ml = Cint[size(A, 1) for A in As]
@@ -120,36 +168,179 @@ function upload_mps(ctx::Context, hmpo, psi)
   out[]
 end
 
-"""
-    dmrg_b200(psi, mpo; m, minm=2, sweeps=1, cutoff=0.0, silent=false, SvNbond=0, krylov=2,
-              charges=nothing, Qlabels=nothing, precision=0, device=0)
+# Every stored entry of a Qtens site tensor A[a, s, b] as (a, s, b, value), 1-based: block q of
+# A.T has rows indexed by the tensor indices A.currblock[1] and columns by A.currblock[2]; the
+# 0-based positions of entry r of a group are the column A.ind[q][g][:, r].
+function foreach_entry(f, A)
+  cb = A.currblock
+  full = zeros(Int, 3)
+  for q = 1:length(A.T)
+    B = A.T[q]
+    rows, cols = A.ind[q][1], A.ind[q][2]
+    for c = 1:size(B, 2), r = 1:size(B, 1)
+      for (k, x) in enumerate(cb[1]); full[x] = rows[k, r] + 1; end
+      for (k, x) in enumerate(cb[2]); full[x] = cols[k, c] + 1; end
+      f(full[1], full[2], full[3], B[r, c])
+    end
+  end
+end
 
-Two-site DMRG of the reference's `dmrg(psi, mpo; method="twosite")` on the GPU. `charges`:
-per-site d x nsym integer charges (required for quantum-number MPS; `Qlabels` are forwarded to
-`makeqMPS` when the result is written back). Returns the energy of the last bond step, like `dmrg`.
+struct BondSectors
+  q::Vector{Vector{Int}}      # sector charges, strictly increasing (lexicographic)
+  dim::Vector{Int}
+  sector::Vector{Int}         # state -> sector (1-based)
+  pos::Vector{Int}            # state -> position inside its sector (0-based)
+end
+
+function group_bond(labels::Vector{Vector{Int}})
+  qs = sort(unique(labels))
+  idx = Dict(q => k for (k, q) in enumerate(qs))
+  dim = zeros(Int, length(qs))
+  sector = zeros(Int, length(labels))
+  pos = zeros(Int, length(labels))
+  for (x, l) in enumerate(labels)            # states keep their order inside a sector
+    k = idx[l]
+    sector[x] = k
+    pos[x] = dim[k]
+    dim[k] += 1
+  end
+  BondSectors(qs, dim, sector, pos)
+end
+
+# Block-form upload of a Qtens MPS (dmrg_mps_upload_blocks): bond charges propagated from the
+# left edge, then every stored entry scattered into the canonical block order (for each left
+# sector, for each physical state s, the [dim ka x dim kb] column-major block of the right sector
+# q(ka) + p(s)).
+function upload_qn_mps(ctx::Context, hmpo, psi, ch)
+  L = length(psi.A)
+  nsym = size(ch[1], 2)
+  labels = Vector{Vector{Vector{Int}}}(undef, L + 1)
+  labels[1] = [zeros(Int, nsym)]
+  for i = 1:L
+    A = psi.A[i]
+    lab = [zeros(Int, nsym) for _ = 1:size(A, 3)]   # states no block touches keep charge 0
+    foreach_entry(A) do a, s, b, v
+      lab[b] = labels[i][a] .+ ch[i][s, :]
+    end
+    labels[i + 1] = lab
+  end
+  bonds = [group_bond(labels[b]) for b = 1:L + 1]
+  data = Vector{Vector{Float64}}(undef, L)
+  for i = 1:L
+    Bl, Br = bonds[i], bonds[i + 1]
+    d = size(ch[i], 1)
+    rq = Dict(q => k for (k, q) in enumerate(Br.q))
+    off = Dict{Tuple{Int,Int},Int}()
+    n = 0
+    for ka = 1:length(Bl.q), s = 1:d
+      kb = get(rq, Bl.q[ka] .+ ch[i][s, :], 0)
+      kb == 0 && continue
+      off[(ka, s)] = n
+      n += Bl.dim[ka] * Br.dim[kb]
+    end
+    buf = zeros(Float64, n)
+    foreach_entry(psi.A[i]) do a, s, b, v
+      ka = Bl.sector[a]
+      o = get(off, (ka, s), -1)
+      o < 0 && (v == 0 || error("site $i: entry ($a,$s,$b) violates the charges"); return)
+      buf[o + Bl.pos[a] + Br.pos[b] * Bl.dim[ka] + 1] = v
+    end
+    data[i] = buf
+  end
+  nsec = Cint[length(b.q) for b in bonds]
+  qn = [Cint[x for q in b.q for x in q] for b in bonds]
+  dims = [Cint.(b.dim) for b in bonds]
+  out = Ref{Ptr{Cvoid}}(C_NULL)
+  GC.@preserve qn dims data begin
+    code = ccall((:dmrg_mps_upload_blocks, libdmrg), Cint,
+                 (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cint}, Ptr{Ptr{Cint}}, Ptr{Ptr{Cint}},
+                  Ptr{Ptr{Cdouble}}, Cint, Ref{Ptr{Cvoid}}),
+                 ctx.h, hmpo, nsec, [pointer(x) for x in qn], [pointer(x) for x in dims],
+                 [pointer(x) for x in data], psi.oc - 1, out)
+  end
+  check(code, ctx.h, "dmrg_mps_upload_blocks")
+  out[]
+end
+
+upload_mps(ctx, hmpo, psi, ch) =
+  (ch !== nothing && isqtens(psi.A[1])) ? upload_qn_mps(ctx, hmpo, psi, ch) :
+                                          upload_dense_mps(ctx, hmpo, psi)
+
+# ------------------------------------------------------------------------ dmrg
+
+function run_sweeps!(ctx, st, hmpo, p::Params, sweeps, silent)
+  energy = 0.0
+  for s = 1:sweeps
+    stats = SweepStats()
+    check(ccall((:dmrg_sweep, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Params}, Ref{SweepStats}),
+                st, hmpo, p, stats), ctx.h, "dmrg_sweep")
+    energy = stats.energy
+    if !silent    # dmrgcvg's report (algs/DMRG.jl:614-620)
+      println("Sweep $s (back and forth): $(round(stats.seconds, digits=5)) sec")
+      println("Largest truncation = $(stats.max_truncerr), m = $(stats.biggest_m)")
+      println("Energy at sweep $s is $(round(stats.energy, digits=12))")
+      println()
+    end
+    if stats.converged != 0
+      silent || println("DMRG converged to a difference of $(stats.cvg_check) after $s sweeps!\n")
+      break
+    end
+  end
+  energy
+end
+
 """
-function dmrg_b200(psi, mpo; m::Integer=0, minm::Integer=2, sweeps::Integer=1, cutoff::Float64=0.0,
-                   silent::Bool=false, SvNbond::Integer=0, krylov::Integer=2, charges=nothing,
-                   Qlabels=nothing, precision::Integer=0, device::Integer=0)
-  ctx = Context(device)
-  hmpo = upload_mpo(ctx, mpo, charges)
-  st = upload_mps(ctx, hmpo, psi)
+    dmrg(psi, mpo; m, maxm, minm=2, sweeps, cutoff, silent, goal, cvgE, SvNbond, method="twosite",
+         krylov=2, precision=0, charges=nothing, device=0, kwargs...)
+
+The reference's `dmrg` (algs/DMRG.jl:549-588) for `method = "twosite"` on the GPU; defaults come
+from `algvars(psi)` as in the reference. `m` and `maxm` are the same keyword. `krylov > 2` runs
+Lanczos with full re-orthogonalisation instead of the reference's 2-vector step; `precision = 1`
+selects the split-precision (3xTF32) contractions. Other methods run the reference's own code.
+"""
+function DMRJtensor.dmrg(psi::DMRJtensor.matrixproductstate, mpo::DMRJtensor.matrixproductoperator;
+                         params=DMRJtensor.algvars(psi), method::String="twosite",
+                         m::Integer=params.maxm, maxm::Integer=m, minm::Integer=2,
+                         sweeps::Integer=params.sweeps, cutoff::Float64=params.cutoff,
+                         silent::Bool=params.silent, goal::Float64=params.goal,
+                         cvgE::Bool=params.cvgE, SvNbond::Integer=params.SvNbond,
+                         krylov::Integer=2, precision::Integer=0, charges=nothing,
+                         device::Integer=0, kwargs...)
+  if method != "twosite"
+    return invoke(DMRJtensor.dmrg, Tuple{DMRJtensor.MPS,DMRJtensor.MPO}, psi, mpo;
+                  params=params, method=method, m=maxm, minm=minm, sweeps=sweeps, cutoff=cutoff,
+                  silent=silent, goal=goal, cvgE=cvgE, SvNbond=SvNbond, kwargs...)
+  end
+  dmrg_b200(psi, mpo; maxm=maxm, minm=minm, sweeps=sweeps, cutoff=cutoff, silent=silent,
+            goal=goal, cvgE=cvgE, SvNbond=SvNbond, krylov=krylov, precision=precision,
+            charges=charges, device=device)
+end
+
+"""
+    dmrg_b200(psi, mpo; maxm, minm=2, sweeps=1, cutoff=0.0, silent=false, goal=0.0, cvgE=true,
+              SvNbond=0, krylov=2, precision=0, charges=nothing, device=0)
+
+The GPU two-site DMRG behind the `dmrg` method. Returns the energy of the last bond step and
+updates `psi` (tensors and `oc`) in place.
+"""
+function dmrg_b200(psi, mpo; maxm::Integer=0, minm::Integer=2, sweeps::Integer=1,
+                   cutoff::Float64=0.0, silent::Bool=false, goal::Float64=0.0, cvgE::Bool=true,
+                   SvNbond::Integer=0, krylov::Integer=2, precision::Integer=0, charges=nothing,
+                   device::Integer=0)
+  ctx = context(device)
+  ch = site_charges(psi, charges)
+  hmpo = upload_mpo(ctx, mpo, ch)
+  st = upload_mps(ctx, hmpo, psi, ch)
   try
     check(ccall((:dmrg_env_build, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), st, hmpo), ctx.h,
           "dmrg_env_build")
     p = Params()
     ccall((:dmrg_params_default, libdmrg), Cvoid, (Ref{Params},), p)
-    p.maxm, p.minm, p.cutoff, p.krylov, p.precision, p.svnbond = m, minm, cutoff, krylov, precision, SvNbond
-    energy = 0.0
-    for s = 1:sweeps
-      stats = SweepStats()
-      check(ccall((:dmrg_sweep, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Params}, Ref{SweepStats}),
-                  st, hmpo, p, stats), ctx.h, "dmrg_sweep")
-      energy = stats.energy
-      silent || println("sweep $s, energy $(stats.energy), largest truncation $(stats.max_truncerr), ",
-                        "m $(stats.biggest_m), entropy $(stats.entropy), $(stats.seconds) s")
-    end
-    write_back!(ctx, st, psi, Qlabels)
+    p.maxm, p.minm, p.cutoff, p.krylov, p.precision, p.svnbond = maxm, minm, cutoff, krylov,
+                                                                 precision, SvNbond
+    p.goal, p.cvgE = goal, cvgE ? 1 : 0
+    energy = run_sweeps!(ctx, st, hmpo, p, sweeps, silent)
+    write_back!(ctx, st, psi, ch)
     return energy
   finally
     ccall((:dmrg_state_destroy, libdmrg), Cint, (Ptr{Cvoid},), st)
@@ -157,11 +348,31 @@ function dmrg_b200(psi, mpo; m::Integer=0, minm::Integer=2, sweeps::Integer=1, c
   end
 end
 
-# Downloads every site in its dense-equivalent form (bond bases grouped by charge: a gauge change
-# of the same state) and stores it in psi; quantum-number states are rebuilt with makeqMPS.
-function write_back!(ctx::Context, st, psi, Qlabels)
+function bond_info(ctx, st, b, nsym)
+  n = Ref{Cint}(0)
+  check(ccall((:dmrg_bond_info, libdmrg), Cint, (Ptr{Cvoid}, Cint, Ref{Cint}, Ptr{Cint}, Ptr{Cint}),
+              st, b, n, C_NULL, C_NULL), ctx.h, "dmrg_bond_info")
+  q = zeros(Cint, max(n[] * max(nsym, 1), 1))
+  dims = zeros(Cint, max(n[], 1))
+  check(ccall((:dmrg_bond_info, libdmrg), Cint, (Ptr{Cvoid}, Cint, Ref{Cint}, Ptr{Cint}, Ptr{Cint}),
+              st, b, n, q, dims), ctx.h, "dmrg_bond_info")
+  ([Int.(q[(k - 1) * nsym + 1:k * nsym]) for k = 1:n[]], Int.(dims[1:n[]]))
+end
+
+# Writes the device MPS back into psi, one site at a time. Dense states receive the
+# dense-equivalent array; quantum-number states a Qtens built from it with the bond labels the
+# library reports (the bond bases grouped by charge: a gauge change of the same state), as
+# makeqMPS does (lib/MPS/makeqMPS.jl:40-64).
+function write_back!(ctx::Context, st, psi, ch)
   L = length(psi.A)
-  arrays = Vector{Array{Float64,3}}(undef, L)
+  qn = ch !== nothing && isqtens(psi.A[1])
+  nsym = qn ? size(ch[1], 2) : 0
+  Q = qn ? typeof(DMRJtensor.getQnum(2, 1, psi.A[1])) : Nothing
+  qlab(b) = begin
+    qs, dims = bond_info(ctx, st, b, nsym)
+    [Q(q...) for (q, dd) in zip(qs, dims) for _ = 1:dd]
+  end
+  left = qn ? qlab(0) : nothing
   for i = 1:L
     ml, mr = Ref{Cint}(0), Ref{Cint}(0)
     check(ccall((:dmrg_mps_download, libdmrg), Cint,
@@ -172,104 +383,144 @@ function write_back!(ctx::Context, st, psi, Qlabels)
     check(ccall((:dmrg_mps_download, libdmrg), Cint,
                 (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ref{Cint}, Ref{Cint}), st, i - 1, A, ml, mr),
           ctx.h, "dmrg_mps_download")
-    arrays[i] = A
+    if qn
+      right = qlab(i)
+      phys = [DMRJtensor.getQnum(2, s, psi.A[i]) for s = 1:d]
+      psi.A[i] = DMRJtensor.Qtens(A, [left, phys, inv.(right)])
+      left = right
+    else
+      psi.A[i] = DMRJtensor.convertTens(eltype(psi.A), A)
+    end
   end
   oc = Ref{Cint}(0)
   check(ccall((:dmrg_state_oc, libdmrg), Cint, (Ptr{Cvoid}, Ref{Cint}), st, oc), ctx.h, "dmrg_state_oc")
-  if Qlabels === nothing
-    for i = 1:L
-      psi.A[i] = Main.tens(arrays[i])
-    end
-  else
-    qpsi = Main.makeqMPS(Qlabels, Main.MPS(arrays; oc=oc[] + 1); newnorm=false)
-    for i = 1:L
-      psi.A[i] = qpsi.A[i]
-    end
-  end
   psi.oc = oc[] + 1
   psi
 end
 
-"""
-    B200Env
+# ------------------------------------------------------------------------ the Env API
 
-Resident environments of one (psi, mpo) pair on the GPU: `makeEnv_b200` builds them
-(makeEnv, lib/Env/makeEnv.jl:196-221), `Lupdate_b200!(i, env)` / `Rupdate_b200!(i, env)` are
-Lupdate!/Rupdate! (lib/MPO_MPS/Lupdate.jl:17-37, Rupdate.jl:17-37) and `env[i, :left]` /
-`env[i, :right]` download Lenv[i] / Renv[i] as dense [m, w, m] arrays.
+"""
+    B200Env, B200Side
+
+Resident environments of one (psi, mpo) pair on the GPU. `Lenv, Renv = makeEnv_b200(psi, mpo)`
+builds them (makeEnv, lib/Env/makeEnv.jl:196-221); `Lenv[i]` / `Renv[i]` download the
+dense-equivalent [m, w, m] tensors (L[bra, w, ket], R[ket, w, bra]); `Lupdate!(i, Lenv, psi, mpo)`
+and `Rupdate!(i, Renv, psi, mpo)` are the reference's in-place updates (lib/MPO_MPS/Lupdate.jl:34,
+Rupdate.jl:34) on the device, with the state's own site tensors.
 """
 mutable struct B200Env
   ctx::Context
   mpo::Ptr{Cvoid}
   st::Ptr{Cvoid}
+  L::Int
+end
+
+struct B200Side
+  env::B200Env
+  left::Bool
 end
 
 function makeEnv_b200(psi, mpo; charges=nothing, device::Integer=0)
-  ctx = Context(device)
-  hmpo = upload_mpo(ctx, mpo, charges)
-  st = upload_mps(ctx, hmpo, psi)
+  ctx = context(device)
+  ch = site_charges(psi, charges)
+  hmpo = upload_mpo(ctx, mpo, ch)
+  st = upload_mps(ctx, hmpo, psi, ch)
   check(ccall((:dmrg_env_build, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), st, hmpo), ctx.h, "dmrg_env_build")
-  e = B200Env(ctx, hmpo, st)
+  e = B200Env(ctx, hmpo, st, length(psi.A))
   finalizer(e) do x
     ccall((:dmrg_state_destroy, libdmrg), Cint, (Ptr{Cvoid},), x.st)
     ccall((:dmrg_mpo_destroy, libdmrg), Cint, (Ptr{Cvoid},), x.mpo)
   end
-  e
+  (B200Side(e, true), B200Side(e, false))
 end
 
-Lupdate_b200!(i::Integer, e::B200Env) =
-  check(ccall((:dmrg_lupdate, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint), e.st, e.mpo, i - 1),
-        e.ctx.h, "dmrg_lupdate")
-Rupdate_b200!(i::Integer, e::B200Env) =
-  check(ccall((:dmrg_rupdate, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint), e.st, e.mpo, i - 1),
-        e.ctx.h, "dmrg_rupdate")
+Base.length(s::B200Side) = s.env.L
 
-function Base.getindex(e::B200Env, i::Integer, side::Symbol)
-  left = side === :left ? 1 : 0
+function Base.getindex(s::B200Side, i::Integer)
+  e = s.env
   dims = zeros(Cint, 3)
   check(ccall((:dmrg_env_get, libdmrg), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}, Ptr{Cint}),
-              e.st, i - 1, left, C_NULL, dims), e.ctx.h, "dmrg_env_get (sizes)")
+              e.st, i - 1, s.left ? 1 : 0, C_NULL, dims), e.ctx.h, "dmrg_env_get (sizes)")
   out = Array{Float64}(undef, dims...)
   check(ccall((:dmrg_env_get, libdmrg), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}, Ptr{Cint}),
-              e.st, i - 1, left, out, dims), e.ctx.h, "dmrg_env_get")
+              e.st, i - 1, s.left ? 1 : 0, out, dims), e.ctx.h, "dmrg_env_get")
   out
 end
 
-# expect(psi, H) (lib/MPO_MPS/expect.jl:47-56) on the state of a B200Env: <psi|H|psi>, not
-# normalised; `H` is another uploaded MPO over the same sites (default: the Env's own).
-function expect_b200(e::B200Env, hmpo::Ptr{Cvoid}=e.mpo)
+function DMRJtensor.Lupdate!(i::Integer, Lenv::B200Side, psi::DMRJtensor.MPS, mpo::DMRJtensor.MPO...)
+  Lenv.left || error("Lupdate! needs the left environment list")
+  check(ccall((:dmrg_lupdate, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint), Lenv.env.st,
+              Lenv.env.mpo, i - 1), Lenv.env.ctx.h, "dmrg_lupdate")
+  nothing
+end
+
+function DMRJtensor.Rupdate!(i::Integer, Renv::B200Side, psi::DMRJtensor.MPS, mpo::DMRJtensor.MPO...)
+  Renv.left && error("Rupdate! needs the right environment list")
+  check(ccall((:dmrg_rupdate, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint), Renv.env.st,
+              Renv.env.mpo, i - 1), Renv.env.ctx.h, "dmrg_rupdate")
+  nothing
+end
+
+# Lupdate(Lenv, dualpsi, psi, mpo) / Rupdate(Renv, dualpsi, psi, mpo) (lib/MPO_MPS/Lupdate.jl:17,
+# Rupdate.jl:17) on dense Float64 arrays, computed on the device (dmrg_env_step).
+function env_step(left::Bool, E::Array{Float64,3}, dual::Array{Float64,3}, psi::Array{Float64,3},
+                  W::Array{Float64,4}; device::Integer=0)
+  ctx = context(device)
+  ml, d, mr = size(psi)
+  wl, wr = size(W, 1), size(W, 4)
+  out = Array{Float64}(undef, left ? (mr, wr, mr) : (ml, wl, ml))
+  check(ccall((:dmrg_env_step, libdmrg), Cint,
+              (Ptr{Cvoid}, Cint, Cint, Cint, Cint, Cint, Cint, Ptr{Cdouble}, Ptr{Cdouble},
+               Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+              ctx.h, left ? 1 : 0, ml, d, mr, wl, wr, E, dual, psi, W, out), ctx.h, "dmrg_env_step")
+  out
+end
+
+DMRJtensor.Lupdate(L::Array{Float64,3}, dual::Array{Float64,3}, psi::Array{Float64,3},
+                   W::Array{Float64,4}) = env_step(true, L, dual, psi, W)
+DMRJtensor.Rupdate(R::Array{Float64,3}, dual::Array{Float64,3}, psi::Array{Float64,3},
+                   W::Array{Float64,4}) = env_step(false, R, dual, psi, W)
+
+# expect(psi, H) (lib/MPO_MPS/expect.jl:47-56) on the state of a device environment pair:
+# <psi|H|psi>, not normalised; `H` is another uploaded MPO over the same sites (default: its own).
+function expect_b200(s::B200Side, hmpo::Ptr{Cvoid}=s.env.mpo)
   v = Ref{Cdouble}(0.0)
-  check(ccall((:dmrg_expect, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Cdouble}), e.st, hmpo, v),
-        e.ctx.h, "dmrg_expect")
+  check(ccall((:dmrg_expect, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Cdouble}), s.env.st,
+              hmpo, v), s.env.ctx.h, "dmrg_expect")
   v[]
 end
 
 # correlationmatrix(psi, Cc, Ca; trail) (lib/MPO_MPS/correlationmatrix.jl:21-83), operators
 # O[bra, ket] as d x d Float64 matrices; the centre of the state is not moved.
-function correlationmatrix_b200(e::B200Env, Cc::Matrix{Float64}, Ca::Matrix{Float64};
-                                trail=nothing, L::Integer)
+function correlationmatrix_b200(s::B200Side, Cc::Matrix{Float64}, Ca::Matrix{Float64};
+                                trail=nothing)
   d = size(Cc, 1)
+  L = s.env.L
   rho = Matrix{Float64}(undef, L, L)
   F = trail === nothing ? C_NULL : Matrix{Float64}(trail)
   check(ccall((:dmrg_correlationmatrix, libdmrg), Cint,
               (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
-              e.st, d, Cc, Ca, F, rho), e.ctx.h, "dmrg_correlationmatrix")
+              s.env.st, d, Cc, Ca, F, rho), s.env.ctx.h, "dmrg_correlationmatrix")
   rho
 end
 
-# Checkpoint of the Env's device state (the persistence of largeMPS / loadMPS,
-# lib/MPS/largeMPS.jl:19-81); load_b200 returns a new B200Env with rebuilt environments.
-save_b200(e::B200Env, path::AbstractString) =
-  check(ccall((:dmrg_state_save, libdmrg), Cint, (Ptr{Cvoid}, Cstring), e.st, path),
-        e.ctx.h, "dmrg_state_save")
+# Checkpoint of the device state (the persistence of largeMPS / loadMPS,
+# lib/MPS/largeMPS.jl:19-81); load_b200 returns a new environment pair, rebuilt.
+save_b200(s::B200Side, path::AbstractString) =
+  check(ccall((:dmrg_state_save, libdmrg), Cint, (Ptr{Cvoid}, Cstring), s.env.st, path),
+        s.env.ctx.h, "dmrg_state_save")
 
-function load_b200(e::B200Env, path::AbstractString)
+function load_b200(s::B200Side, path::AbstractString)
+  e = s.env
   out = Ref{Ptr{Cvoid}}(C_NULL)
   check(ccall((:dmrg_state_load, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cstring, Ref{Ptr{Cvoid}}),
               e.ctx.h, e.mpo, path, out), e.ctx.h, "dmrg_state_load")
   check(ccall((:dmrg_env_build, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), out[], e.mpo), e.ctx.h,
         "dmrg_env_build")
-  B200Env(e.ctx, e.mpo, out[])   # shares the MPO handle: no finalizer of its own
+  ne = B200Env(e.ctx, e.mpo, out[], e.L)   # shares the MPO handle: frees only its state
+  finalizer(x -> ccall((:dmrg_state_destroy, libdmrg), Cint, (Ptr{Cvoid},), x.st), ne)
+  (B200Side(ne, true), B200Side(ne, false))
 end
 
 end # module

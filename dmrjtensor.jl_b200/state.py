@@ -616,11 +616,53 @@ def makeEnv(psi: MPS, mpo: MPO, ctx=None):
     return Env(dev, True), Env(dev, False)
 
 
-def Lupdate(i, Lenv: Env, psi: MPS = None, mpo: MPO = None):
-    """``Lupdate!(i, Lenv, psi, mpo)``: ``Lenv[i+1] = Lupdate(Lenv[i], psi[i], psi[i], mpo[i])``."""
-    Lenv.dev.lupdate(i)
+def _env_step(left, env, dual, psi, W, ctx=None):
+    """One dense environment step on the device (``dmrg_env_step``)."""
+    ctx = ctx or default_context()
+    A = np.asfortranarray(np.asarray(psi, dtype=float))
+    B = np.asfortranarray(np.asarray(dual, dtype=float)) if dual is not None else A
+    Wf = np.asfortranarray(np.asarray(W, dtype=float))
+    E = np.asfortranarray(np.asarray(env, dtype=float))
+    if A.ndim != 3 or B.shape != A.shape or Wf.ndim != 4 or E.ndim != 3:
+        raise ValueError("env step: environment [m,w,m], sites [ml,d,mr], MPO [wl,d,d,wr]")
+    ml, d, mr = A.shape
+    wl, wr = Wf.shape[0], Wf.shape[3]
+    if Wf.shape[1:3] != (d, d):
+        raise ValueError("MPO physical dimensions differ from the site's")
+    want = (ml, wl, ml) if left else (mr, wr, mr)
+    if E.shape != want:
+        raise ValueError(f"environment has shape {E.shape}, expected {want}")
+    out = np.zeros((mr, wr, mr) if left else (ml, wl, ml), order="F")
+    dp = C.POINTER(C.c_double)
+    check(lib().dmrg_env_step(ctx.h, 1 if left else 0, ml, d, mr, wl, wr, E.ctypes.data_as(dp),
+                              B.ctypes.data_as(dp), A.ctypes.data_as(dp), Wf.ctypes.data_as(dp),
+                              out.ctypes.data_as(dp)), ctx.h)
+    return out
 
 
-def Rupdate(i, Renv: Env, psi: MPS = None, mpo: MPO = None):
-    """``Rupdate!(i, Renv, psi, mpo)``: ``Renv[i-1] = Rupdate(Renv[i], psi[i], psi[i], mpo[i])``."""
-    Renv.dev.rupdate(i)
+def Lupdate(*args, ctx=None):
+    """Both forms of the reference's left update (``lib/MPO_MPS/Lupdate.jl:17-37``):
+
+    * ``Lupdate(Lenv, dualpsi, psi, mpo)`` with dense tensors returns the next left environment
+      ``L'[a',w',b'] = conj(dualpsi[a,t,a']) L[a,w,b] W[w,s,t,w'] psi[b,s,b']``, computed on the
+      device;
+    * ``Lupdate(i, Lenv, psi, mpo)`` (the reference's ``Lupdate!``) updates the device-resident
+      environment list of :func:`makeEnv`: ``Lenv[i+1]`` from ``Lenv[i]`` and the state's site i.
+    """
+    if isinstance(args[0], (int, np.integer)):
+        args[1].dev.lupdate(int(args[0]))
+        return None
+    L, dual, psi, W = args
+    return _env_step(True, L, dual, psi, W, ctx)
+
+
+def Rupdate(*args, ctx=None):
+    """Both forms of the reference's right update (``lib/MPO_MPS/Rupdate.jl:17-37``):
+    ``Rupdate(Renv, dualpsi, psi, mpo)`` returns ``R[b,w,a] = psi[b,s,b'] W[w,s,t,w']
+    conj(dualpsi[a,t,a']) R'[b',w',a']``; ``Rupdate(i, Renv, psi, mpo)`` (``Rupdate!``) updates
+    ``Renv[i-1]`` of a device-resident list."""
+    if isinstance(args[0], (int, np.integer)):
+        args[1].dev.rupdate(int(args[0]))
+        return None
+    R, dual, psi, W = args
+    return _env_step(False, R, dual, psi, W, ctx)

@@ -181,6 +181,15 @@ DMRG_API int dmrg_env_build(dmrg_state* st, const dmrg_mpo* mpo);
 DMRG_API int dmrg_lupdate(dmrg_state* st, const dmrg_mpo* mpo, int site);
 /* Rupdate!(i, Renv, psi, mpo): Renv[i-1] = Rupdate(Renv[i], ...) (lib/MPO_MPS/Rupdate.jl:17-37). */
 DMRG_API int dmrg_rupdate(dmrg_state* st, const dmrg_mpo* mpo, int site);
+/* Lupdate(Lenv, dualpsi, psi, mpo) / Rupdate(Renv, dualpsi, psi, mpo) as pure functions of dense
+ * host tensors (lib/MPO_MPS/Lupdate.jl:17-26, lib/MPO_MPS/Rupdate.jl:17-26), computed on the device:
+ *   left = 1: env_in = L[ml(bra), wl, ml(ket)], env_out = L'[mr(bra), wr, mr(ket)]
+ *   left = 0: env_in = R[mr(ket), wr, mr(bra)], env_out = R'[ml(ket), wl, ml(bra)]
+ * psi and dual are [ml, d, mr] sites (dual = NULL: the same tensor as psi), W is [wl, d, d, wr];
+ * all column-major. */
+DMRG_API int dmrg_env_step(dmrg_ctx* ctx, int left, int ml, int d, int mr, int wl, int wr,
+                           const double* env_in, const double* dual, const double* psi,
+                           const double* W, double* env_out);
 /* Lenv[i] (left=1) or Renv[i] (left=0) as a dense-equivalent column-major [m, w, m] array
  * (L[bra,w,ket] / R[ket,w,bra]). dims receives the 3 sizes; out may be NULL to query them. */
 DMRG_API int dmrg_env_get(dmrg_state* st, int site, int left, double* out, int* dims);

@@ -157,3 +157,56 @@ def test_goal_stops_after_the_same_sweep_as_the_oracle(dmrgb, ctx, cvgE):
     assert psi.sweep_stats[-1]["converged"] == 1
     assert all(s["converged"] == 0 for s in psi.sweep_stats[:-1])
     assert abs(E - E0) <= 1e-10 * abs(E0)
+
+
+def test_functional_env_updates_match_oracle(dmrgb, ctx):
+    """Lupdate(Lenv, dualpsi, psi, mpo) / Rupdate(Renv, dualpsi, psi, mpo) on dense tensors
+    (lib/MPO_MPS/Lupdate.jl:17-26, Rupdate.jl:17-26) with a dual tensor different from psi."""
+    rng = np.random.default_rng(21)
+    ml, d, mr, wl, wr = 7, 3, 5, 4, 6
+    psi = rng.standard_normal((ml, d, mr))
+    dual = rng.standard_normal((ml, d, mr))
+    W = rng.standard_normal((wl, d, d, wr))
+    W[np.abs(W) < 0.5] = 0.0                   # sparse like a real MPO
+    L = rng.standard_normal((ml, wl, ml))
+    R = rng.standard_normal((mr, wr, mr))
+    Lo = od.Lupdate(L, dual, psi, W)
+    Ro = od.Rupdate(R, dual, psi, W)
+    assert _rel(dmrgb.Lupdate(L, dual, psi, W, ctx=ctx), Lo) < RTOL_CONTRACT
+    assert _rel(dmrgb.Rupdate(R, dual, psi, W, ctx=ctx), Ro) < RTOL_CONTRACT
+    # dual = psi (the form every sweep uses)
+    assert _rel(dmrgb.Lupdate(L, psi, psi, W, ctx=ctx), od.Lupdate(L, psi, psi, W)) < RTOL_CONTRACT
+
+
+def test_block_upload_round_trip_at_a_4096_bond(dmrgb, ctx):
+    """The block-form upload (dmrg_mps_upload_blocks, what the Julia binding sends for a Qtens
+    MPS) at a bond of dimension 4096 in three U(1) sectors, the size of the 4x16 cylinder's largest
+    bond: the blocks come back bit for bit, and the environments built from them agree with the
+    dense-equivalent contraction of the same state."""
+    rng = np.random.default_rng(4)
+    sectors = [[((0,), 1)], [((-1,), 1), ((1,), 1)], [((-2,), 1000), ((0,), 2096), ((2,), 1000)],
+               [((-1,), 1), ((1,), 1)], [((0,), 1)]]
+    phys = [[(1,), (-1,)]] * 4
+    blocks = []
+    for i in range(4):
+        n = 0
+        rq = {q: dd for q, dd in sectors[i + 1]}
+        for qa, da in sectors[i]:
+            for ps in phys[i]:
+                qb = (qa[0] + ps[0],)
+                if qb in rq:
+                    n += da * rq[qb]
+        blocks.append(rng.standard_normal(n))
+    psi = dmrgb.MPS(oc=1)
+    psi.sectors, psi.blocks, psi.phys = sectors, blocks, phys
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, 4).with_qn(dmrgb.SPIN_QN)
+    dev = dmrgb.DeviceState(psi, mpo.device(ctx))
+    assert dev.bond(2) == sectors[2]
+    for i in range(4):
+        assert np.array_equal(dev.site_blocks(i), blocks[i])
+    dev.env_build()
+    dense = [dev.site_dense(i) for i in range(4)]
+    W = [np.asarray(w) for w in mpo.W]
+    L2 = od.Lupdate(od.Lupdate(np.ones((1, 1, 1)), dense[0], dense[0], W[0]), dense[1], dense[1], W[1])
+    dev.lupdate(1)
+    assert _rel(dev.env(2, True), L2) < RTOL_CONTRACT
