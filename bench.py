@@ -332,6 +332,123 @@ def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
     return out
 
 
+def geometric_ramp(m0, m1, n):
+    """n maxm values from m0 to m1, geometric, rounded."""
+    return [int(round(m0 * (m1 / m0) ** (i / (n - 1)))) for i in range(n)]
+
+
+# The two large benchmark configurations, full size: the Hubbard chain (N, 2Sz) at half filling
+# with maxm up to 2048 over 10 sweeps, and the Heisenberg 4x16 cylinder with maxm up to 4096 over
+# 8 sweeps; both from their product starts.
+CONFIGS = {
+    "c3": {"workload": "hubbard L=32 t=1 U=4 mu=0 U(1)xU(1) (N=32, Sz=0), half-filling product "
+                       "start, maxm 64->2048 over 10 sweeps, cutoff 1e-10",
+           "schedule": geometric_ramp(64, 2048, 10), "cutoff": 1e-10},
+    "c4": {"workload": "heisenberg 4x16 open cylinder (periodic W=4, snake order) U(1) Sz=0, Neel "
+                       "start, maxm 64->4096 over 8 sweeps, cutoff 1e-9",
+           "schedule": geometric_ramp(64, 4096, 8), "cutoff": 1e-9},
+}
+
+
+def config_inputs(pkg, which):
+    sys.path.insert(0, str(ROOT))
+    from oracle import models as om
+    if which == "c3":
+        L = 32
+        mpo = pkg.makeMPO(lambda i: pkg.hubbardMPO(mu=0.0, HubU=4.0, t=1.0), 4, L)
+        return (pkg.MPS([np.array(a) for a in om.hubbard_half_filling_mps(L)], oc=0),
+                mpo.with_qn(pkg.HUBBARD_QN))
+    return pkg.neelMPS(64), pkg.heisenbergCylinderMPO(4, 16).with_qn(pkg.SPIN_QN)
+
+
+def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, tmpdir):
+    """One large configuration at full size, plain FP64 and split 3xTF32: (1) the whole sweep
+    schedule from the product start in each form (device time, final energies); (2) the same state
+    (the plain run's final MPS, checkpointed) swept once more in each form, the second of two
+    sweeps timed, with the phase breakdown and Heff/environment TFLOP/s of a profiled sweep."""
+    cfg = CONFIGS[which]
+    sched, cutoff = cfg["schedule"], cfg["cutoff"]
+    psi0, mpo = config_inputs(pkg, which)
+    dmpo = mpo.device(ctx)
+    ckpt = str(Path(tmpdir) / f"{which}.ckp")
+    out = {"workload": cfg["workload"], "schedule": sched}
+    for form in ("fp64", "3xtf32"):
+        dev = pkg.DeviceState(psi0, dmpo)
+        dev.env_build()
+        st = [dev.sweep(pkg.make_params(maxm=m, minm=2, cutoff=cutoff, precision=form))
+              for m in sched]
+        out[form] = {"run_seconds": sum(s["seconds"] for s in st),
+                     "last_sweep_seconds": st[-1]["seconds"], "energy": st[-1]["energy"],
+                     "biggest_m": max(s["biggest_m"] for s in st),
+                     "eig_max_n": max(s["eig_max_n"] for s in st),
+                     "max_truncerr_last": st[-1]["max_truncerr"]}
+        if form == "fp64":
+            dev.save(ckpt)
+        del dev
+    out["run_speedup_3xtf32"] = out["fp64"]["run_seconds"] / out["3xtf32"]["run_seconds"]
+    out["run_abs_dE"] = abs(out["fp64"]["energy"] - out["3xtf32"]["energy"])
+    same = {}
+    for form in ("fp64", "3xtf32"):
+        rec = {}
+        for rep in range(2):
+            dev = pkg.DeviceState.load(ckpt, dmpo)
+            dev.env_build()
+            s = dev.sweep(pkg.make_params(maxm=sched[-1], minm=2, cutoff=cutoff, precision=form))
+            rec = {"sweep_seconds": s["seconds"], "energy": s["energy"],
+                   "host_seconds": s["host_seconds"], "wait_seconds": s["wait_seconds"]}
+            del dev
+        dev = pkg.DeviceState.load(ckpt, dmpo)
+        dev.env_build()
+        p = dev.sweep(pkg.make_params(maxm=sched[-1], minm=2, cutoff=cutoff, precision=form,
+                                      profile=1))
+        del dev
+        rec["phases_profiled"] = {k: p[k] for k in ("heff_seconds", "env_seconds", "eig_seconds",
+                                                     "vec_seconds")}
+        rec["heff_tflops"] = p["heff_flops"] / p["heff_seconds"] / 1e12 if p["heff_seconds"] else None
+        rec["env_tflops"] = p["env_flops"] / p["env_seconds"] / 1e12 if p["env_seconds"] else None
+        rec["heff_gemm_tflops"] = (p["gemm_flops"] / p["gemm_seconds"] / 1e12
+                                   if p["gemm_seconds"] else None)
+        rec["eig_max_n"] = p["eig_max_n"]
+        same[form] = rec
+    same["speedup_3xtf32"] = same["fp64"]["sweep_seconds"] / same["3xtf32"]["sweep_seconds"]
+    same["abs_dE"] = abs(same["fp64"]["energy"] - same["3xtf32"]["energy"])
+    g64, g32 = same["fp64"]["heff_gemm_tflops"], same["3xtf32"]["heff_gemm_tflops"]
+    same["roofline"] = {
+        "fp64_heff_gemm": {"achieved": g64, "peak": fp64_peak, "unit": "TFLOP/s",
+                           "frac": g64 / fp64_peak if (g64 and fp64_peak) else None},
+        "3xtf32_heff_gemm": {"achieved": g32, "peak": tf32_peak / 3 if tf32_peak else None,
+                             "unit": "TFLOP/s (algorithmic; ceiling = TF32 peak / 3)",
+                             "frac": 3 * g32 / tf32_peak if (g32 and tf32_peak) else None}}
+    out["same_state_sweep"] = same
+    return out
+
+
+def tf32_gemm_peak(device):
+    """cuBLAS TF32 GEMM (FP32 operands, TF32 tensor cores) 8192^3 on this GPU, best of 5."""
+    import torch
+    dev = torch.device("cuda", device)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float32, device=dev)
+    b = torch.randn(n, n, dtype=torch.float32, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
 def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
     """Heff at the dense-equivalent size of the headline workload at maxm 1024 (dense random MPS,
     bond dimension 1024 either side of the centre bond): device time per application in the plain
@@ -557,6 +674,12 @@ def run_ours(args, world, rank, local, dist):
     if rank != 0:
         return
     peak = fp64_gemm_peak(local)
+    tf32_peak = tf32_gemm_peak(local)
+    configs = {}
+    if args.configs:
+        with tempfile.TemporaryDirectory() as td:
+            for which in args.configs.split(","):
+                configs[which] = config_leg(pkg, ctx, which, peak, tf32_peak, td)
     g_ach = prof["gemm_flops"] / prof["gemm_seconds"] / 1e12 if prof["gemm_seconds"] > 0 else None
     traffic = None
     tfile = ROOT / "profiles" / "gemm_f64_traffic.json"
@@ -597,6 +720,8 @@ def run_ours(args, world, rank, local, dist):
         "measurements": meas,
         "chosen": chosen,
         "heff_forms_m1024": heff_large,
+        "tf32_gemm_peak_tflops": tf32_peak,
+        "configs": configs,
     }
     print(json.dumps(out))
 
@@ -612,6 +737,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--dump-sectors", default=None)
+    ap.add_argument("--configs", default="c3,c4",
+                    help="large configurations to run at full size, plain and split ('' = none)")
     ap.add_argument("--cpu-sweeps", type=int, default=2,
                     help="oracle sweeps timed on the device state for cpu_baseline")
     ap.add_argument("--steps-ref", type=int, default=None,

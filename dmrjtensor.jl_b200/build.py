@@ -18,7 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xcompiler", "-fvisibility=hidden"]
 
-SOURCES = ["gemm_f64.cu", "gemm_tf32.cu", "vec_kernels.cu", "jacobi.cu", "jacobi_block.cu", "syevt.cu", "noalloc.cu", "engine_layout.cpp", "engine_eig.cpp",
+SOURCES = ["gemm_f64.cu", "gemm_tf32.cu", "vec_kernels.cu", "jacobi.cu", "jacobi_block.cu", "syevt.cu", "syevt_mid.cu", "noalloc.cu", "engine_layout.cpp", "engine_eig.cpp",
            "engine_contract.cpp", "engine_sweep.cpp", "engine_meas.cpp", "abi.cpp", "server.cpp"]
 
 

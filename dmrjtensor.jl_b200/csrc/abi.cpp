@@ -913,7 +913,8 @@ int dmrg_test_syevt(dmrg_ctx* c, int nmat, const int* n, const int* k, double* A
     int64_t ta = 0, tw = 0, tu = 0;
     int mn = 0, mk = 0;
     for (int i = 0; i < nmat; ++i) {
-      if (n[i] <= 0 || n[i] > SYEVT_NMAX || k[i] < 0 || k[i] > n[i]) fail(DMRG_ERR_SHAPE, "bad size");
+      if (n[i] <= 0 || n[i] > SYEVT_MID_NMAX || k[i] < 0 || k[i] > n[i])
+        fail(DMRG_ERR_SHAPE, "bad size");
       ta += int64_t(n[i]) * n[i];
       tw += n[i];
       tu += int64_t(n[i]) * k[i];
@@ -923,7 +924,7 @@ int dmrg_test_syevt(dmrg_ctx* c, int nmat, const int* n, const int* k, double* A
     std::vector<TridTask> tasks;
     int64_t oa = 0, ow = ta, ows = ta + tw, ou = ta + 4 * tw;
     for (int i = 0; i < nmat; ++i) {
-      TridTask t{oa, ow, ows, ou, n[i], k[i]};
+      TridTask t{oa, ow, ows, ou, n[i], k[i], 0};
       tasks.push_back(t);
       oa += int64_t(n[i]) * n[i];
       ow += n[i];
@@ -933,12 +934,8 @@ int dmrg_test_syevt(dmrg_ctx* c, int nmat, const int* n, const int* k, double* A
     DBuf buf;
     dalloc(c, buf, ta + 4 * tw + tu);
     cuda_check(cudaMemcpyAsync(buf.p, A, ta * 8, cudaMemcpyHostToDevice, c->stream), "A");
-    Upload u;
-    const size_t off = u.put(tasks);
-    char* db = u.send(c, 0);
-    launch_trid_eigvals(c->stream, buf.p, reinterpret_cast<const TridTask*>(db + off), nmat, mn);
-    if (mk > 0)
-      launch_trid_vectors(c->stream, buf.p, reinterpret_cast<const TridTask*>(db + off), nmat, mn, mk);
+    run_trid_eigvals(c, buf.p, buf.n, tasks, 8);
+    if (mk > 0) run_trid_vectors(c, buf.p, buf.n, tasks, 6);
     cuda_check(cudaMemcpyAsync(w, buf.p + ta, tw * 8, cudaMemcpyDeviceToHost, c->stream), "w");
     cuda_check(cudaMemcpyAsync(U, buf.p + ta + 4 * tw, tu * 8, cudaMemcpyDeviceToHost, c->stream), "U");
     cuda_check(cudaStreamSynchronize(c->stream), "syevt sync");

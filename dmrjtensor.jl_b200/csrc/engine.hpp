@@ -149,7 +149,7 @@ struct dmrg_ctx {
   size_t budget = 0, in_use = 0, peak = 0;
   std::string err;
   int nsm = 148;
-  dmrg::DescSlot slot[8];
+  dmrg::DescSlot slot[10];     // descriptor upload slots, one per family (see Upload::send)
   double* d_scal = nullptr;      // small scalar workspace (256 doubles)
   double* d_partial = nullptr;   // reduction partials (16 * 296 doubles)
   int* d_status = nullptr;
@@ -290,6 +290,8 @@ void heff_apply_noalloc(dmrg_state* st, int iL, const double* in_dev, double* ou
 // g1 (env_in, A) -> T1, mix T1 -> T2 (the MPO site), g3 (A, T2) -> env_out in layout `out`.
 struct StepPlan {
   GemmList g1, g3;
+  GemmList g1t, g3t;        // retiled copies for the split-precision kernel (split = true)
+  bool split = false;
   MixList mx;
   EnvLayout out;
   int64_t t1 = 0, t2 = 0;   // scratch sizes in doubles
@@ -299,7 +301,9 @@ void plan_left_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const Sit
                     const EnvLayout& LL, StepPlan& sp);
 void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const SiteLayout& lay,
                      const EnvLayout& RL, StepPlan& sp);
-void put_step(Upload& u, StepPlan& sp);
+// Uploads the step's lists; with split = true also their split-precision retilings (the step then
+// runs its two GEMMs on the 3xTF32 tensor-core kernel; the MPO mixing stays FP64).
+void put_step(Upload& u, StepPlan& sp, bool split = false);
 // Launches an uploaded step; c->T1 / c->T2 must hold sp.t1 / sp.t2 doubles. `bra` (optional)
 // is the conjugated tensor when it differs from the ket tensor A (the dualpsi argument of
 // Lupdate/Rupdate); both share A's layout.
@@ -311,8 +315,8 @@ void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int w
                     double* env_out);
 
 void env_boundaries(dmrg_state* st);
-void lupdate(dmrg_state* st, int i, double* flops);
-void rupdate(dmrg_state* st, int i, double* flops);
+void lupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP64);
+void rupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP64);
 
 // ---- measurements (engine_meas.cpp)
 // <psi|H|psi> for an MPO over the same sites and physical charges (not normalised).
@@ -323,6 +327,13 @@ void measure_correlation(dmrg_state* st, int d, const double* Cc, const double* 
                          const double* F, double* rho, double* flops);
 
 // ---- eigensolves (engine_eig.cpp)
+// Tridiagonal-path eigenvalues of every task (n <= SYEVT_MID_NMAX; small and mid-size blocks in
+// one launch each), then the kept eigenvectors (tasks with keep > 0; mid-size blocks use c->W
+// as workspace). Offsets are checked against nbase before any launch.
+void run_trid_eigvals(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<TridTask>& t,
+                      int slot);
+void run_trid_vectors(dmrg_ctx* c, double* base, int64_t nbase, std::vector<TridTask> t,
+                      int slot);
 int64_t eig_workspace(const std::vector<EigTask>& tasks);
 void run_eigs(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<EigTask>& tasks,
               int64_t ws_off, int* sweeps);

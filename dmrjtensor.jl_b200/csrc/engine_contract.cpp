@@ -355,10 +355,23 @@ void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const Si
     }
 }
 
-void put_step(Upload& u, StepPlan& sp) {
+namespace {
+int split_tile_n(const GemmList& g) {
+  return g.flops >= SPLIT_PRESPLIT_FLOPS ? TF32_TILE_N_PRESPLIT : TF32_TILE_N_DIRECT;
+}
+}  // namespace
+
+void put_step(Upload& u, StepPlan& sp, bool split) {
   u.put(sp.g1);
   u.put(sp.mx);
   u.put(sp.g3);
+  sp.split = split;
+  if (split) {
+    sp.g1t = retile(sp.g1, TF32_TILE_M, split_tile_n(sp.g1));
+    sp.g3t = retile(sp.g3, TF32_TILE_M, split_tile_n(sp.g3));
+    u.put(sp.g1t);
+    u.put(sp.g3t);
+  }
 }
 
 void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, int64_t n_in,
@@ -371,9 +384,15 @@ void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, i
   const bool left = sp.g3.tA;
   const DBuf& first = left ? A : B;
   const DBuf& last = left ? B : A;
-  run_gemm(c, sp.g1, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n);
+  if (sp.split)
+    run_gemm_split(c, sp.g1t, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n);
+  else
+    run_gemm(c, sp.g1, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n);
   run_mix(c, sp.mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
-  run_gemm(c, sp.g3, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out);
+  if (sp.split)
+    run_gemm_split(c, sp.g3t, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out);
+  else
+    run_gemm(c, sp.g3, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out);
 }
 
 void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int wr,
@@ -447,14 +466,14 @@ void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int w
   dfree(c, dA); dfree(c, dB); dfree(c, din); dfree(c, dout);
 }
 
-void lupdate(dmrg_state* st, int i, double* flops) {
+void lupdate(dmrg_state* st, int i, double* flops, int precision) {
   dmrg_ctx* c = st->ctx;
   if (i < 0 || i + 1 >= st->L) fail(DMRG_ERR_ARG, "lupdate: site out of range");
   if (!st->Lvalid[i]) fail(DMRG_ERR_STATE, "lupdate: Lenv[site] has not been built");
   StepPlan sp;
   plan_left_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Llay[i], sp);
   Upload u;
-  put_step(u, sp);
+  put_step(u, sp, precision == DMRG_PREC_3XTF32);
   char* db = u.send(c, 2);
   ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
   ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));
@@ -466,14 +485,14 @@ void lupdate(dmrg_state* st, int i, double* flops) {
   if (flops) *flops += sp.flops();
 }
 
-void rupdate(dmrg_state* st, int i, double* flops) {
+void rupdate(dmrg_state* st, int i, double* flops, int precision) {
   dmrg_ctx* c = st->ctx;
   if (i <= 0 || i >= st->L) fail(DMRG_ERR_ARG, "rupdate: site out of range");
   if (!st->Rvalid[i]) fail(DMRG_ERR_STATE, "rupdate: Renv[site] has not been built");
   StepPlan sp;
   plan_right_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Rlay[i], sp);
   Upload u;
-  put_step(u, sp);
+  put_step(u, sp, precision == DMRG_PREC_3XTF32);
   char* db = u.send(c, 2);
   ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
   ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));

@@ -6,6 +6,76 @@
 
 namespace dmrg {
 
+namespace {
+void check_trid(const std::vector<TridTask>& ts, int64_t nbase, bool vectors) {
+  for (const TridTask& t : ts) {
+    const int64_t nn = int64_t(t.n) * t.n;
+    if (t.n <= 0 || t.n > SYEVT_MID_NMAX || t.a_off < 0 || t.a_off + nn > nbase ||
+        t.w_off < 0 || t.w_off + t.n > nbase || t.ws_off < 0 || t.ws_off + 3 * t.n > nbase)
+      fail(DMRG_ERR_ARG, "internal plan check failed: tridiagonal eigensolver task");
+    if (vectors && (t.keep < 0 || t.keep > t.n || t.u_off < 0 ||
+                    t.u_off + int64_t(t.n) * t.keep > nbase))
+      fail(DMRG_ERR_ARG, "internal plan check failed: tridiagonal eigenvector task");
+  }
+}
+}  // namespace
+
+void run_trid_eigvals(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<TridTask>& t,
+                      int slot) {
+  check_trid(t, nbase, false);
+  std::vector<TridTask> small, mid;
+  int ns = 0, nm = 0;
+  for (const TridTask& x : t) {
+    if (x.n <= SYEVT_NMAX) { small.push_back(x); ns = std::max(ns, x.n); }
+    else { mid.push_back(x); nm = std::max(nm, x.n); }
+  }
+  if (small.empty() && mid.empty()) return;
+  Upload u;
+  const size_t o1 = u.put(small), o2 = u.put(mid);
+  char* db = u.send(c, slot);
+  if (!small.empty())
+    launch_trid_eigvals(c->stream, base, reinterpret_cast<const TridTask*>(db + o1),
+                        int(small.size()), ns);
+  if (!mid.empty())
+    launch_trid_mid_eigvals(c->stream, base, reinterpret_cast<const TridTask*>(db + o2),
+                            int(mid.size()), nm);
+  cuda_check(cudaGetLastError(), "tridiagonal eigenvalues");
+}
+
+void run_trid_vectors(dmrg_ctx* c, double* base, int64_t nbase, std::vector<TridTask> t,
+                      int slot) {
+  check_trid(t, nbase, true);
+  std::vector<TridTask> small, mid;
+  int ns = 0, ks = 0, nm = 0, km = 0;
+  int64_t xw = 0;
+  for (TridTask x : t) {
+    if (x.keep <= 0) continue;
+    if (x.n <= SYEVT_NMAX) {
+      small.push_back(x);
+      ns = std::max(ns, x.n);
+      ks = std::max(ks, x.keep);
+    } else {
+      x.x_off = xw;
+      xw += syevt_mid_workspace(x.n, x.keep);
+      mid.push_back(x);
+      nm = std::max(nm, x.n);
+      km = std::max(km, x.keep);
+    }
+  }
+  if (small.empty() && mid.empty()) return;
+  if (!mid.empty()) ensure(c, c->W, xw);
+  Upload u;
+  const size_t o1 = u.put(small), o2 = u.put(mid);
+  char* db = u.send(c, slot);
+  if (!small.empty())
+    launch_trid_vectors(c->stream, base, reinterpret_cast<const TridTask*>(db + o1),
+                        int(small.size()), ns, ks);
+  if (!mid.empty())
+    launch_trid_mid_vectors(c->stream, base, reinterpret_cast<const TridTask*>(db + o2),
+                            int(mid.size()), nm, km, c->W.p);
+  cuda_check(cudaGetLastError(), "tridiagonal eigenvectors");
+}
+
 int64_t eig_workspace(const std::vector<EigTask>& tasks) {
   int64_t ws = 0;
   for (const EigTask& t : tasks) {

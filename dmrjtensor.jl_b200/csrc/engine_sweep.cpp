@@ -296,13 +296,12 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   std::vector<TridTask> ttasks;
   std::vector<int> tgroup;
   std::vector<int64_t> uoff(G.size(), 0);
-  int tmax = 0;
   for (int gi = 0; gi < int(G.size()); ++gi) {
     const Group& g = G[gi];
     const int side = j > 0 ? g.n : g.np;
     if (side == 0) continue;
     so.eig_max_n = std::max(so.eig_max_n, side);
-    if (side <= SYEVT_NMAX) {
+    if (side <= SYEVT_MID_NMAX) {
       TridTask t{};
       t.a_off = g.roff;
       t.w_off = W0 + g.woff;
@@ -312,7 +311,6 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
       ttasks.push_back(t);
       tgroup.push_back(gi);
       uoff[gi] = t.u_off;
-      tmax = std::max(tmax, side);
     } else {
       EigTask et{};
       et.a_off = g.roff;
@@ -326,12 +324,6 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   const int64_t ews = eig_workspace(etasks);
   ensure(c, c->M, std::max<int64_t>(mtot, 1));
   ensure(c, c->R, std::max<int64_t>(J0 + ews, 1));
-  for (const TridTask& t : ttasks) {
-    const int64_t nn = int64_t(t.n) * t.n;
-    if (t.a_off + nn > c->R.n || t.w_off + t.n > c->R.n || t.ws_off + 3 * t.n > c->R.n ||
-        t.u_off + nn > c->R.n)
-      fail(DMRG_ERR_ARG, "internal plan check failed: tridiagonal eigensolver task");
-  }
   CopyList gather;
   for (int ka = 0; ka < tl.nl; ++ka)
     for (int s1 = 0; s1 < d1; ++s1)
@@ -357,12 +349,10 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   Upload u2;
   u2.put(gather);
   u2.put(grho);
-  const size_t tt_off = u2.put(ttasks);
   char* db2 = u2.send(c, 1);
   run_copy(c, gather, db2, psi, n, c->M.p, c->M.n);
   run_gemm(c, grho, db2, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
-  launch_trid_eigvals(s, c->R.p, reinterpret_cast<const TridTask*>(db2 + tt_off),
-                      int(ttasks.size()), tmax);
+  run_trid_eigvals(c, c->R.p, c->R.n, ttasks, 8);
   cuda_check(cudaGetLastError(), "density matrix and eigenvalue launch");
   run_eigs(c, c->R.p, c->R.n, etasks, J0, nullptr);
   // pinned destination: the copy stays asynchronous and the host waits only in the sync below
@@ -415,23 +405,13 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   so.m = int(kept.size());
   // eigenvectors of the kept states of the tridiagonal-path blocks
   std::vector<TridTask> vt;
-  int vmax_n = 0, vmax_k = 0;
   for (size_t a = 0; a < ttasks.size(); ++a) {
     TridTask t = ttasks[a];
     t.keep = G[tgroup[a]].keep;
-    if (t.keep == 0) continue;
-    vt.push_back(t);
-    vmax_n = std::max(vmax_n, t.n);
-    vmax_k = std::max(vmax_k, t.keep);
+    if (t.keep > 0) vt.push_back(t);
   }
   cuda_check(cudaGetLastError(), "eigenvalue download");
-  if (!vt.empty()) {
-    Upload uv;
-    const size_t vo = uv.put(vt);
-    char* dbv = uv.send(c, 6);
-    launch_trid_vectors(s, c->R.p, reinterpret_cast<const TridTask*>(dbv + vo), int(vt.size()),
-                        vmax_n, vmax_k);
-  }
+  run_trid_vectors(c, c->R.p, c->R.n, vt, 6);
 
   // ---------------- split back into the two site tensors (algs/DMRG.jl:389-395, 483-490)
   cuda_check(cudaGetLastError(), "eigenvectors");
@@ -516,6 +496,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   Timing tm(c, P.profile != 0);
   const int t0 = tm.record();
   int j = st->dir;
+  const int j0 = j;
   for (int ns = 0; ns < 2 * (L - 1); ++ns) {
     const int i = st->oc;
     const int iL = j > 0 ? i : i - 1, iR = j > 0 ? i + 1 : i;
@@ -523,7 +504,13 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     twostep(st, P, j, iL, iR, ns == 2 * (L - 1) - 1, tm, so);
     const int tenv = tm.begin();
     double ef = 0.0;
-    if (j > 0) lupdate(st, i, &ef); else rupdate(st, i, &ef);
+    // split form: the environment updates run on the tensor cores too, except those of the
+    // second half-sweep when the sweep's energy is the FP64 Rayleigh quotient (fp64_final): that
+    // half-sweep builds, from the final site tensors, every environment the last bond step reads,
+    // so the quotient is exact FP64 arithmetic on the final Ritz vector
+    const int eprec = (P.precision == DMRG_PREC_3XTF32 && !(P.fp64_final && j != j0))
+                          ? DMRG_PREC_3XTF32 : DMRG_PREC_FP64;
+    if (j > 0) lupdate(st, i, &ef, eprec); else rupdate(st, i, &ef, eprec);
     cuda_check(cudaGetLastError(), "environment update");
     tm.end(tenv, 1);
     out.energy = so.energy;
@@ -549,6 +536,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   st->dir = j;
   const int t1 = tm.record();
   cuda_check(cudaEventSynchronize(tm.event(t1)), "sweep sync");
+  if (P.precision == DMRG_PREC_3XTF32) check_mma_status(c);   // the last environment update
   float ms = 0;
   cudaEventElapsedTime(&ms, tm.event(t0), tm.event(t1));
   out.seconds = ms * 1e-3;

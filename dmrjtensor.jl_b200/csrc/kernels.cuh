@@ -66,20 +66,29 @@ struct EigTask {
   int n, pad;
 };
 
-// Tridiagonal eigensolver for density-matrix blocks with n <= SYEVT_NMAX (syevt.cu).
+// Tridiagonal eigensolver for density-matrix blocks with n <= SYEVT_NMAX (syevt.cu, shared
+// memory) and SYEVT_NMAX < n <= SYEVT_MID_NMAX (syevt_mid.cu, global memory + shared memory).
 constexpr int SYEVT_NMAX = 112;
+constexpr int SYEVT_MID_NMAX = 512;
 struct TridTask {
   int64_t a_off;   // n x n matrix (column-major, ld n); reflectors are stored in its lower part
   int64_t w_off;   // n eigenvalues, descending
   int64_t ws_off;  // 3n workspace: d, e, tau
   int64_t u_off;   // n x keep eigenvectors (launch 2)
   int n, keep;
+  int64_t x_off;   // mid-size launch 2: workspace offset (syevt_mid_workspace(n, keep) doubles)
 };
 size_t syevt_smem_vals(int n);
 size_t syevt_smem_vecs(int n, int k);
 void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks, int max_n);
 void launch_trid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
                          int max_n, int max_k);
+int64_t syevt_mid_workspace(int n, int k);
+void launch_trid_mid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
+                             int max_n);
+// xws: workspace base of the tasks' x_off
+void launch_trid_mid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
+                             int max_n, int max_k, double* xws);
 
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
 

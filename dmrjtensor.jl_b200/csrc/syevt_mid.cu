@@ -1,0 +1,583 @@
+// syevt_mid.cu -- density-matrix eigensolver for mid-size blocks, SYEVT_NMAX < n <= SYEVT_MID_NMAX:
+// the method of syevt.cu (Householder tridiagonalisation, multisection, inverse iteration,
+// Cholesky QR, blocked back-transformation), one CTA of 512 threads per block, for matrices that
+// do not fit in shared memory.
+//
+// Launch 1 (k_trid_mid_vals): the Householder steps run on the matrix in place in global memory
+// (L2-resident: a 512 x 512 block is 2 MB) until the trailing block is small enough for shared
+// memory (m <= ms); it is then copied there and the remaining steps run on the copy, which is
+// written back at the end (its strictly lower part holds the last reflectors). Per step: the
+// product p = tau B v by columns (B is symmetric: p_j = tau B(:,j).v, one warp per column, a
+// warp sum per column), one block barrier, then the rank-2 update B -= v w^T + w v^T by the other
+// warps while warp 0 updates the next pivot column first and builds the next reflector from it.
+// Eigenvalues by trisection as in syevt.cu, in rounds of 256 eigenvalues.
+// Launch 2 (k_trid_mid_vectors): inverse iteration (one thread per kept vector, LU factors in a
+// global workspace interleaved by thread so that every factor access of a warp is one line),
+// Cholesky QR (a second pass unless the Gram matrix is within 1e-3/k of the identity; classical
+// Gram-Schmidt with restarts if a pivot shows nearly dependent vectors), back-transformation
+// U = H_0 ... H_{n-3} Z in blocks of 8 reflectors (compact WY) reading the reflectors from the
+// matrix in global memory.
+#include "kernels.cuh"
+#include "syevt_common.cuh"
+
+namespace dmrg {
+namespace {
+
+constexpr int MT = 512;             // threads per CTA
+constexpr int NW = MT / 32;         // warps
+constexpr int MID_BT_NB = 8;        // reflectors per back-transformation block
+constexpr size_t MID_SMEM_LIMIT = 227 * 1024 - 2048;
+
+// Householder reflector of x = col[0..m) (one warp): H x = beta e_1 with v[0] = 1,
+// H = I - tau v v^T. Writes v to vout and v[1..m) into col[1..m); returns beta and tau.
+__device__ void house_warp(double* __restrict__ col, int m, double* __restrict__ vout,
+                           double& beta_o, double& tau_o, int lane) {
+  double part = 0.0;
+  for (int i = 1 + lane; i < m; i += 32) part += col[i] * col[i];
+  const double xn2 = wsum(part);
+  const double alpha = col[0];
+  double t, sc, beta;
+  if (xn2 == 0.0) {
+    t = 0.0; sc = 0.0; beta = alpha;
+  } else {
+    beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    t = (beta - alpha) / beta;
+    sc = 1.0 / (alpha - beta);
+  }
+  for (int i = lane; i < m; i += 32) {
+    const double vi = (i == 0) ? 1.0 : col[i] * sc;
+    vout[i] = vi;
+    if (i > 0) col[i] = vi;
+  }
+  beta_o = beta;
+  tau_o = t;
+}
+
+// RM = register rows per lane: n <= 32 RM.
+template <int RM>
+__global__ void __launch_bounds__(MT, 1)
+k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, int ms) {
+  const TridTask tk = tasks[blockIdx.x];
+  const int n = tk.n;
+  if (n < 3 || n > 32 * RM) return;
+  extern __shared__ double sm[];
+  double* S = sm;                          // ms x ms: the trailing block once it fits
+  double* vb = S + size_t(ms) * ms;        // 2 x n: reflector of this step / of the next
+  double* p = vb + 2 * n;                  // n
+  double* d = p + n;                       // n
+  double* e = d + n;                       // n
+  double* e2 = e + n;                      // n
+  double* tau = e2 + n;                    // n
+  __shared__ double kw[NW];
+  __shared__ double s_lo, s_hi;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* Ag = base + tk.a_off;
+  double* B = Ag + n + 1;                  // trailing block of step 0, A[1:, 1:]
+  int ld = n;
+  int k_sw = -1;                           // step at which the trailing block moved to S
+  if (warp == 0) {
+    double be, ta;
+    house_warp(Ag + 1, n - 1, vb, be, ta, lane);
+    if (lane == 0) { d[0] = Ag[0]; e[0] = be; tau[0] = ta; }
+  }
+  __syncthreads();
+  for (int k = 0; k + 2 < n; ++k) {
+    const int m = n - k - 1;
+    if (k_sw < 0 && m <= ms) {
+      for (int x = tid; x < m * m; x += MT) {
+        const int i = x % m, j = x / m;
+        S[i + j * ms] = B[i + int64_t(j) * ld];
+      }
+      B = S;
+      ld = ms;
+      k_sw = k;
+      __syncthreads();
+    }
+    const double* v = vb + (k & 1) * n;
+    double* vn = vb + ((k + 1) & 1) * n;
+    const double t = tau[k];
+    {   // p = t B v by columns, and this warp's share of K = p.v
+      double vr[RM];
+#pragma unroll
+      for (int r = 0; r < RM; ++r) {
+        const int i = lane + 32 * r;
+        vr[r] = (i < m) ? v[i] : 0.0;
+      }
+      double kpart = 0.0;
+      for (int j = warp; j < m; j += NW) {
+        const double* col = B + int64_t(j) * ld;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int r = 0; r < RM; r += 2) {
+          const int i0 = lane + 32 * r, i1 = i0 + 32;
+          if (i0 < m) s0 += col[i0] * vr[r];
+          if (r + 1 < RM && i1 < m) s1 += col[i1] * vr[r + 1];
+        }
+        const double sj = wsum(s0 + s1);
+        if (lane == 0) {
+          const double pj = t * sj;
+          p[j] = pj;
+          kpart += pj * v[j];
+        }
+      }
+      if (lane == 0) kw[warp] = kpart;
+    }
+    __syncthreads();
+    double K = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) K += kw[w];
+    const double hk = 0.5 * t * K;
+    if (warp == 0) {
+      // pivot column (column 0 of B) with the update applied, then the next reflector from it
+      const double v0 = v[0];
+      const double w0 = p[0] - hk * v0;
+      double c[RM];
+#pragma unroll
+      for (int r = 0; r < RM; ++r) {
+        const int i = lane + 32 * r;
+        double vi = 0.0, pi = 0.0, bi = 0.0;
+        if (i < m) { vi = v[i]; pi = p[i]; bi = B[i]; }
+        const double wi = pi - hk * vi;
+        c[r] = bi - (vi * w0 + wi * v0);
+      }
+      if (k + 3 < n) {
+        double part = 0.0;
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = lane + 32 * r;
+          if (i >= 2 && i < m) part += c[r] * c[r];
+        }
+        const double xn2 = wsum(part);
+        const double alpha = __shfl_sync(FULL, c[0], 1);
+        double tn, sc, beta;
+        if (xn2 == 0.0) {
+          tn = 0.0; sc = 0.0; beta = alpha;
+        } else {
+          beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+          tn = (beta - alpha) / beta;
+          sc = 1.0 / (alpha - beta);
+        }
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = lane + 32 * r;
+          if (i >= 1 && i < m) {
+            const double vi = (i == 1) ? 1.0 : c[r] * sc;
+            vn[i - 1] = vi;
+            if (i >= 2) B[i] = vi;         // reflector tail, below the subdiagonal
+          }
+        }
+        if (lane == 0) {
+          d[k + 1] = c[0];
+          e[k + 1] = beta;
+          tau[k + 1] = tn;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = lane + 32 * r;
+          if (i < m) B[i] = c[r];
+        }
+      }
+    } else {
+      // columns 1..m-1, rows 1..m-1 (row 0 of B is never read again)
+      for (int j = warp; j < m; j += NW - 1) {
+        const double vj = v[j], wj = p[j] - hk * vj;
+        double* col = B + int64_t(j) * ld;
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = 1 + lane + 32 * r;
+          if (i < m) {
+            const double vi = v[i], wi = p[i] - hk * vi;
+            col[i] = col[i] - (vi * wj + wi * vj);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    B += ld + 1;
+  }
+  // B now addresses A[n-1, n-1] (the storage of the last steps)
+  if (tid == 0) {
+    d[n - 2] = B[-(ld + 1)];
+    e[n - 2] = B[-ld];
+    tau[n - 2] = 0.0;
+    d[n - 1] = B[0];
+    e[n - 1] = 0.0;
+    tau[n - 1] = 0.0;
+  }
+  if (k_sw >= 0) {   // the shared copy back into the caller's matrix (its reflector tails)
+    const int m0 = n - k_sw - 1;
+    double* G = Ag + int64_t(k_sw + 1) * n + (k_sw + 1);
+    for (int x = tid; x < m0 * m0; x += MT) {
+      const int i = x % m0, j = x / m0;
+      G[i + int64_t(j) * n] = S[i + j * ms];
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += MT) e2[i] = e[i] * e[i];
+  double* ws = base + tk.ws_off;          // d | e | tau
+  for (int i = tid; i < n; i += MT) {
+    ws[i] = d[i];
+    ws[n + i] = e[i];
+    ws[2 * n + i] = tau[i];
+  }
+  if (warp == 0) {   // Gershgorin interval
+    double lo = 1e300, hi = -1e300;
+    for (int i = lane; i < n; i += 32) {
+      const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+      lo = fmin(lo, d[i] - r);
+      hi = fmax(hi, d[i] + r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(FULL, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(FULL, hi, o));
+    }
+    if (lane == 0) {
+      const double pad = 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300;
+      s_lo = lo - pad;
+      s_hi = hi + pad;
+    }
+  }
+  __syncthreads();
+  // trisection, MT/2 eigenvalues per round: threads 2i, 2i+1 count at the interval's two
+  // interior points
+  const double tnm = fmax(fabs(s_lo), fabs(s_hi));
+  const double tol = 8.9e-16 * tnm;
+  for (int e0 = 0; e0 < n; e0 += MT / 2) {
+    const int ei = e0 + (tid >> 1), h = tid & 1;
+    const int target = n - 1 - ei;         // i-th largest = (n-1-i)-th smallest
+    bool done = ei >= n;
+    double a = s_lo, b = s_hi;
+    for (int it = 0; it < 200; ++it) {
+      if (__all_sync(FULL, done)) break;
+      double x0 = 0.0, x1 = 0.0;
+      bool below = false;
+      if (!done) {
+        const double w = b - a;
+        x0 = a + w * (1.0 / 3.0);
+        x1 = a + w * (2.0 / 3.0);
+        if (w <= tol || !(a < x0 && x0 < x1 && x1 < b)) done = true;
+        else below = sturm_below(d, e2, n, h ? x1 : x0) > target;
+      }
+      const bool other = __shfl_xor_sync(FULL, below, 1);
+      if (!done) {
+        const bool r0 = h ? other : below, r1 = h ? below : other;
+        if (r0) b = x0;
+        else if (r1) { a = x0; b = x1; }
+        else a = x1;
+      }
+    }
+    if (h == 0 && ei < n) base[tk.w_off + ei] = 0.5 * (a + b);
+  }
+}
+
+// Workspace of one task of k_trid_mid_vectors, in doubles from x_off: LU factors (4 n k),
+// pivots (n k ints), Z (n x (k|1), row-major), Gram matrix (k x k).
+__host__ __device__ inline int64_t mid_vec_workspace(int n, int k) {
+  const int64_t ldz = k | 1;
+  return 4 * int64_t(n) * k + (int64_t(n) * k + 1) / 2 + int64_t(n) * ldz + int64_t(k) * k + 8;
+}
+
+__host__ __device__ inline size_t mid_vec_smem(int n, int k) {
+  const int nblk = n >= 3 ? (n - 2 + MID_BT_NB - 1) / MID_BT_NB : 0;
+  return sizeof(double) * (2 * size_t(n) + size_t(MID_BT_NB) * k + size_t(nblk) * 64 +
+                           size_t(NW) * 64 + 2 * size_t(k)) + 64;
+}
+
+__global__ void __launch_bounds__(MT, 1)
+k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks,
+                   double* __restrict__ xws) {
+  const TridTask tk = tasks[blockIdx.x];
+  const int n = tk.n, kk = tk.keep;
+  if (n < 3 || kk <= 0) return;
+  const int ldz = kk | 1;
+  const int nblk = (n - 2 + MID_BT_NB - 1) / MID_BT_NB;
+  extern __shared__ double sm[];
+  double* d = sm;                          // n
+  double* e = d + n;                       // n
+  double* Y = e + n;                       // MID_BT_NB x kk
+  double* Tb = Y + MID_BT_NB * kk;         // nblk x 64: T factor of each reflector block
+  double* Sw = Tb + nblk * 64;             // NW x 64: reflector Gram entries
+  double* rinv = Sw + NW * 64;             // kk
+  double* sq = rinv + kk;                  // kk
+  __shared__ double red[32];
+  __shared__ double s_tn;
+  __shared__ int s_flag, s_need2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* X = xws + tk.x_off;
+  double* Un = X;                                          // 4 n kk factors
+  int* piv = reinterpret_cast<int*>(X + 4 * int64_t(n) * kk);
+  double* Z = X + 4 * int64_t(n) * kk + (int64_t(n) * kk + 1) / 2;   // n x ldz
+  double* G = Z + int64_t(n) * ldz;                        // kk x kk row-major, upper triangle
+  const double* ws = base + tk.ws_off;
+  const double* W = base + tk.w_off;
+  const double* V = base + tk.a_off;       // reflector k: V[k n + r], r > k + 1 (unit at k + 1)
+  const double* tau = ws + 2 * n;
+  for (int i = tid; i < n; i += MT) { d[i] = ws[i]; e[i] = ws[n + i]; }
+  if (warp == 0) {
+    double tn = 0.0;
+    for (int i = lane; i < n; i += 32) tn = fmax(tn, fabs(W[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tn = fmax(tn, __shfl_xor_sync(FULL, tn, o));
+    if (lane == 0) {
+      s_tn = fmax(tn, 1e-300);
+      s_flag = 0;
+      s_need2 = 0;
+    }
+  }
+  __syncthreads();
+  const double tn = s_tn;
+  // ---- inverse iteration: one thread per kept vector; factor element q of thread j at
+  // [q * kk + j], so that a warp's accesses to one factor element form one line
+  for (int b0 = 0; b0 < kk; b0 += MT) {
+    const int j = b0 + tid;
+    if (j < kk) {
+      LUSlot f{Un + j, Un + int64_t(n) * kk + j, Un + 2 * int64_t(n) * kk + j,
+               Un + 3 * int64_t(n) * kk + j, piv + j, kk};
+      for (int r = 0; r < n; ++r) Z[int64_t(r) * ldz + j] = prand(r, j);
+      if (W[j] > 1e-13 * tn) inverse_iteration(d, e, n, W[j], Z, ldz, j, tn, f);
+    }
+  }
+  __syncthreads();
+  // ---- Cholesky QR
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int x = tid; x < kk * kk; x += MT) {
+      const int pp = x / kk, q = x - pp * kk;
+      if (pp > q) continue;
+      double s0 = 0.0, s1 = 0.0;
+      int r = 0;
+      for (; r + 2 <= n; r += 2) {
+        s0 += Z[int64_t(r) * ldz + pp] * Z[int64_t(r) * ldz + q];
+        s1 += Z[int64_t(r + 1) * ldz + pp] * Z[int64_t(r + 1) * ldz + q];
+      }
+      if (r < n) s0 += Z[int64_t(r) * ldz + pp] * Z[int64_t(r) * ldz + q];
+      const double g = s0 + s1;
+      G[int64_t(pp) * kk + q] = g;
+      if (pass == 0 && fabs(g - (pp == q ? 1.0 : 0.0)) > 1e-3 / kk) s_need2 = 1;
+    }
+    __syncthreads();
+    for (int j = 0; j < kk; ++j) {
+      const double gjj = G[int64_t(j) * kk + j];
+      if (!(gjj > 1e-8) && tid == 0) s_flag = 1;
+      const double inv = 1.0 / fmax(gjj, 1e-300);
+      const int t = kk - j - 1;
+      for (int x = tid; x < t * t; x += MT) {
+        const int pp = j + 1 + x / t, q = j + 1 + x % t;
+        if (pp <= q)
+          G[int64_t(pp) * kk + q] -= G[int64_t(j) * kk + pp] * G[int64_t(j) * kk + q] * inv;
+      }
+      __syncthreads();
+    }
+    for (int q = tid; q < kk; q += MT) {
+      const double g = fmax(G[int64_t(q) * kk + q], 1e-300);
+      rinv[q] = 1.0 / g;
+      sq[q] = sqrt(g);
+    }
+    __syncthreads();
+    if (s_flag) break;
+    for (int r = tid; r < n; r += MT) {
+      double* zr = Z + int64_t(r) * ldz;
+      for (int q = 0; q < kk; ++q) {
+        double s0 = zr[q], s1 = 0.0;
+        int pp = 0;
+        for (; pp + 2 <= q; pp += 2) {
+          s0 -= zr[pp] * G[int64_t(pp) * kk + q];
+          s1 -= zr[pp + 1] * G[int64_t(pp + 1) * kk + q];
+        }
+        if (pp < q) s0 -= zr[pp] * G[int64_t(pp) * kk + q];
+        zr[q] = (s0 + s1) * rinv[q];
+      }
+      for (int q = 0; q < kk; ++q) zr[q] *= sq[q];
+    }
+    __syncthreads();
+    if (!s_need2) break;
+  }
+  if (s_flag) {
+    // two passes of classical Gram-Schmidt, largest eigenvalue first, with fresh starts for
+    // vectors that lie (numerically) in the span of the previous ones
+    int attempt = 0;
+    for (int c = 0; c < kk; ++c) {
+      for (int pass = 0; pass < 2; ++pass) {
+        {
+          const int g8 = tid >> 3, l8 = tid & 7, ng8 = MT >> 3;
+          for (int qb = 0; qb < c; qb += ng8) {
+            const int q = qb + g8;
+            double s = 0.0;
+            if (q < c)
+              for (int r = l8; r < n; r += 8) s += Z[int64_t(r) * ldz + q] * Z[int64_t(r) * ldz + c];
+            s += __shfl_xor_sync(FULL, s, 4, 8);
+            s += __shfl_xor_sync(FULL, s, 2, 8);
+            s += __shfl_xor_sync(FULL, s, 1, 8);
+            if (q < c && l8 == 0) G[q] = s;      // G reused as the coefficient row
+          }
+        }
+        __syncthreads();
+        for (int r = tid; r < n; r += MT) {
+          double s = Z[int64_t(r) * ldz + c];
+          for (int q = 0; q < c; ++q) s -= G[q] * Z[int64_t(r) * ldz + q];
+          Z[int64_t(r) * ldz + c] = s;
+        }
+        __syncthreads();
+      }
+      double part = 0.0;
+      for (int r = tid; r < n; r += MT) part += Z[int64_t(r) * ldz + c] * Z[int64_t(r) * ldz + c];
+      const double nr = sqrt(bsum(part, red));
+      if (nr < 1e-8 && attempt < 8) {
+        ++attempt;
+        for (int r = tid; r < n; r += MT) Z[int64_t(r) * ldz + c] = prand(r, c + 1000 * attempt);
+        __syncthreads();
+        --c;
+        continue;
+      }
+      attempt = 0;
+      for (int r = tid; r < n; r += MT) Z[int64_t(r) * ldz + c] /= fmax(nr, 1e-300);
+      __syncthreads();
+    }
+  }
+  // ---- back-transformation U = H_0 H_1 ... H_{n-3} Z in blocks of MID_BT_NB reflectors
+  for (int bb = warp; bb < nblk; bb += NW) {
+    const int k0 = bb * MID_BT_NB, nb = min(MID_BT_NB, n - 2 - k0);
+    double* Sg = Sw + warp * 64;
+    if (lane < 28) {                      // Sg[c][i] = v_c . v_i, c < i
+      int c = 0, i = 0, x = lane;
+      for (int cc = 0; cc < MID_BT_NB; ++cc) {
+        const int cnt = MID_BT_NB - 1 - cc;
+        if (x < cnt) { c = cc; i = cc + 1 + x; break; }
+        x -= cnt;
+      }
+      if (i < nb) {
+        const int kc = k0 + c, ki = k0 + i;
+        const double* vc = V + int64_t(kc) * n;
+        const double* vi = V + int64_t(ki) * n;
+        double s0 = vc[ki + 1], s1 = 0.0;      // v_i[ki+1] = 1
+        int r = ki + 2;
+        for (; r + 2 <= n; r += 2) { s0 += vc[r] * vi[r]; s1 += vc[r + 1] * vi[r + 1]; }
+        if (r < n) s0 += vc[r] * vi[r];
+        Sg[c * 8 + i] = s0 + s1;
+      }
+    }
+    __syncwarp();
+    if (lane < nb) {                      // row a of T: T[a][i] = -tau_i sum_{c=a}^{i-1} T[a][c] S[c][i]
+      const int a = lane;
+      double Tr[MID_BT_NB];
+#pragma unroll
+      for (int i = 0; i < MID_BT_NB; ++i) {
+        double v = 0.0;
+        if (i == a) {
+          v = tau[k0 + a];
+        } else if (i > a && i < nb) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < MID_BT_NB; ++c)
+            if (c >= a && c < i) s += Tr[c] * Sg[c * 8 + i];
+          v = -tau[k0 + i] * s;
+        }
+        Tr[i] = v;
+      }
+#pragma unroll
+      for (int i = 0; i < MID_BT_NB; ++i) Tb[bb * 64 + a * 8 + i] = Tr[i];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int bb = nblk - 1; bb >= 0; --bb) {
+    const int k0 = bb * MID_BT_NB, nb = min(MID_BT_NB, n - 2 - k0);
+    const double* T = Tb + bb * 64;
+    {   // Y = T (V^T Z): 8-lane groups, lane a = reflector, group = vector q
+      const int g8 = tid >> 3, a = tid & 7, ng8 = MT >> 3;
+      for (int qb = 0; qb < kk; qb += ng8) {
+        const int q = qb + g8;
+        double y = 0.0;
+        if (q < kk && a < nb) {
+          const int k = k0 + a;
+          const double* vk = V + int64_t(k) * n;
+          double s0 = Z[int64_t(k + 1) * ldz + q], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+          int r = k + 2;
+          for (; r + 4 <= n; r += 4) {
+            double vv[4], zz[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) { vv[u] = vk[r + u]; zz[u] = Z[int64_t(r + u) * ldz + q]; }
+            s0 += vv[0] * zz[0]; s1 += vv[1] * zz[1]; s2 += vv[2] * zz[2]; s3 += vv[3] * zz[3];
+          }
+          for (; r < n; ++r) s0 += vk[r] * Z[int64_t(r) * ldz + q];
+          y = (s0 + s1) + (s2 + s3);
+        }
+        double y2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < MID_BT_NB; ++c) {
+          const double yc = __shfl_sync(FULL, y, c, 8);
+          if (c >= a && c < nb) y2 += T[a * 8 + c] * yc;
+        }
+        if (q < kk && a < nb) Y[a * kk + q] = y2;
+      }
+    }
+    __syncthreads();
+    // Z -= V Y on rows r0..n-1: a thread owns row r (its reflector entries in registers) and
+    // the vectors q = g, g + Gc, ... of its group g
+    const int r0 = k0 + 1, nr = n - r0;
+    const int Gc = max(1, MT / nr);
+    for (int rt = tid; rt < Gc * nr; rt += MT) {
+      const int g = rt / nr, r = r0 + (rt - g * nr);
+      double va[MID_BT_NB];
+#pragma unroll
+      for (int a = 0; a < MID_BT_NB; ++a) {
+        const int k = k0 + a;
+        va[a] = (a >= nb) ? 0.0 : (r == k + 1) ? 1.0 : (r > k + 1 ? V[int64_t(k) * n + r] : 0.0);
+      }
+      double* zr = Z + int64_t(r) * ldz;
+      for (int q = g; q < kk; q += Gc) {
+        double s0 = 0.0;
+#pragma unroll
+        for (int a = 0; a < MID_BT_NB; ++a)
+          if (a < nb) s0 += va[a] * Y[a * kk + q];
+        zr[q] -= s0;
+      }
+    }
+    __syncthreads();
+  }
+  double* U = base + tk.u_off;
+  for (int64_t x = tid; x < int64_t(n) * kk; x += MT) {
+    const int q = int(x / n), r = int(x - int64_t(q) * n);
+    U[x] = Z[int64_t(r) * ldz + q];
+  }
+}
+
+int mid_ms(int max_n) {
+  // largest trailing block that fits in shared memory beside the 7 n vectors
+  const size_t avail = MID_SMEM_LIMIT - sizeof(double) * 7 * size_t(max_n) - 64;
+  int ms = 8;
+  while (size_t(ms + 8) * (ms + 8) * sizeof(double) <= avail) ms += 8;
+  return ms;
+}
+
+template <int RM>
+void launch_vals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks, int max_n) {
+  const int ms = mid_ms(max_n);
+  const size_t sm = sizeof(double) * (size_t(ms) * ms + 7 * size_t(max_n)) + 64;
+  raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vals<RM>), sm);
+  k_trid_mid_vals<RM><<<ntasks, MT, sm, s>>>(base, tasks, ms);
+  count_launch();
+}
+
+}  // namespace
+
+int64_t syevt_mid_workspace(int n, int k) { return mid_vec_workspace(n, k); }
+
+void launch_trid_mid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
+                             int max_n) {
+  if (ntasks <= 0) return;
+  if (max_n <= 256) launch_vals<8>(s, base, tasks, ntasks, max_n);
+  else launch_vals<16>(s, base, tasks, ntasks, max_n);
+}
+
+void launch_trid_mid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
+                             int max_n, int max_k, double* xws) {
+  if (ntasks <= 0) return;
+  const size_t sm = mid_vec_smem(max_n, max_k);
+  raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vectors), sm);
+  k_trid_mid_vectors<<<ntasks, MT, sm, s>>>(base, tasks, xws);
+  count_launch();
+}
+
+}  // namespace dmrg

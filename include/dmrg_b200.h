@@ -60,7 +60,10 @@ enum dmrg_status {
 
 enum dmrg_precision {
   DMRG_PREC_FP64 = 0,    /* plain form: every contraction in FP64 (DMMA) */
-  DMRG_PREC_3XTF32 = 1,  /* chosen form: Heff contractions as 3 TF32 tensor-core products */
+  DMRG_PREC_3XTF32 = 1,  /* chosen form: the Heff and environment-update GEMMs as 3 TF32
+                            tensor-core products (FP32-accurate); with fp64_final the environments
+                            of the sweep's second half are FP64 so that the reported energy is the
+                            exact FP64 Rayleigh quotient of the final Ritz vector */
   DMRG_PREC_BF16X9 = 2   /* reserved (9 BF16 products): not built, rejected with DMRG_ERR_ARG */
 };
 
@@ -249,7 +252,8 @@ DMRG_API int dmrg_test_gemm(dmrg_ctx* ctx, int transA, int transB, int M, int N,
  * (columns) overwrite A. */
 DMRG_API int dmrg_test_eigh(dmrg_ctx* ctx, int nmat, const int* n, double* A, double* w);
 
-/* Tridiagonal-path eigensolver (n[i] <= 112): all eigenvalues (descending, packed in w) and the
+/* Tridiagonal-path eigensolver (n[i] <= 512; blocks above 112 take the mid-size kernels): all
+ * eigenvalues (descending, packed in w) and the
  * eigenvectors of the k[i] largest (packed n[i] x k[i] column-major in U). A is overwritten. */
 DMRG_API int dmrg_test_syevt(dmrg_ctx* ctx, int nmat, const int* n, const int* k, double* A,
                              double* w, double* U);

@@ -46,3 +46,59 @@ def test_hubbard_u1xu1_half_filling(dmrgb, ctx):
     E0, info = od.dmrg(om.to_qmps(start, [hq] * L), ompo, m=64, sweeps=6, cutoff=1e-10,
                        trunc="rho")
     _compare(psi, E, E0, info)
+
+
+# ---------------------------------------------------------------- capped benchmark configurations
+# The oracle's per-sweep invariants (tests/golden/config_parity.json, written by
+# tests/golden/make_config_fixtures.py) on the L=100 Heisenberg U(1) ramp capped at maxm 128, the
+# L=32 Hubbard U(1)xU(1) chain at maxm 256 and the 4x16 cylinder at maxm 256. The device runs the
+# same deterministic inputs; energies agree to 1e-10 relative at every sweep, the last sweep's
+# largest truncation error and centre entropy to 1e-8, and the kept bond dimensions exactly.
+
+import json
+from pathlib import Path
+
+FIXTURES = json.loads((Path(__file__).resolve().parent / "golden" / "config_parity.json").read_text())
+
+
+def _config_inputs(dmrgb, case):
+    L = case["L"]
+    if case["model"] == "heisenberg":
+        return dmrgb.neelMPS(L), dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    if case["model"] == "hubbard":
+        mpo = dmrgb.makeMPO(lambda i: dmrgb.hubbardMPO(t=case["t"], mu=case["mu"], HubU=case["U"]),
+                            4, L).with_qn(dmrgb.HUBBARD_QN)
+        return dmrgb.MPS([np.array(a) for a in om.hubbard_half_filling_mps(L)], oc=0), mpo
+    mpo = dmrgb.heisenbergCylinderMPO(case["W"], case["Lx"]).with_qn(dmrgb.SPIN_QN)
+    return dmrgb.neelMPS(L), mpo
+
+
+@pytest.mark.parametrize("name", sorted(FIXTURES))
+def test_capped_config_matches_oracle(dmrgb, ctx, name):
+    fx = FIXTURES[name]
+    case = fx["case"]
+    psi, mpo = _config_inputs(dmrgb, case)
+    E = dmrgb.dmrg(psi, mpo, m=case["schedule"], cutoff=case["cutoff"], krylov=2,
+                   degen_rtol=case["degen_rtol"], ctx=ctx)
+    assert len(psi.sweep_stats) == len(fx["sweeps"])
+    for n, (d, o) in enumerate(zip(psi.sweep_stats, fx["sweeps"])):
+        assert abs(d["energy"] - o["energy"]) <= 1e-10 * abs(o["energy"]), f"sweep {n}"
+        assert d["biggest_m"] == o["biggestm"], f"sweep {n}"
+    d, o = psi.sweep_stats[-1], fx["sweeps"][-1]
+    assert abs(d["max_truncerr"] - o["maxtrunc"]) <= 1e-8
+    assert abs(d["entropy"] - o["entropy"]) <= 1e-8
+    assert abs(E - fx["energy"]) <= 1e-10 * abs(fx["energy"])
+
+
+def test_density_matrix_blocks_above_the_tridiagonal_limit(dmrgb, ctx):
+    """Dense chain whose centre density matrix (m=64, d=2: side 128) is larger than the
+    tridiagonal kernel's limit (112), so the block-Jacobi path runs inside the sweep."""
+    L = 12
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    psi = dmrgb.randMPS(2, L, 64, seed=7)
+    ref = [a.copy() for a in psi.tensors]
+    E = dmrgb.dmrg(psi, mpo, m=100, sweeps=3, cutoff=1e-14, krylov=2, ctx=ctx)
+    E0, info = od.dmrg(ref, om.make_mpo([om.heisenberg_bulk()] * L, 2), m=100, sweeps=3,
+                       cutoff=1e-14, krylov=2, trunc="rho")
+    assert max(s["eig_max_n"] for s in psi.sweep_stats) > 112
+    _compare(psi, E, E0, info)

@@ -96,7 +96,11 @@ def _rho_like(rng, n, kind):
 
 @pytest.mark.parametrize("case", [[(66, "rank", 40), (1, "rank", 1), (2, "rank", 2), (3, "rank", 1)],
                                   [(66, "deg", 50), (90, "deg", 60)],
-                                  [(112, "decay", 100), (40, "decay", 40)]])
+                                  [(112, "decay", 100), (40, "decay", 40)],
+                                  # mid-size blocks (global-memory Householder steps, then shared)
+                                  [(113, "decay", 113), (66, "rank", 30), (240, "rank", 120)],
+                                  [(233, "deg", 150), (160, "decay", 1)],
+                                  [(512, "decay", 400), (300, "rank", 150), (129, "deg", 80)]])
 def test_tridiagonal_eigensolver(dmrgb, ctx, case):
     """All eigenvalues within 2e-14 ||A||; the k kept eigenvectors orthonormal to 1e-13 and with
     residual ||A u - lambda u|| <= 1e-12 ||A|| (the truncation's tolerance needs)."""

@@ -1,4 +1,5 @@
-"""Split-precision form (3 x TF32 Heff GEMMs on tcgen05) against the plain FP64 form.
+"""Split-precision form (3 x TF32 Heff and environment GEMMs on tcgen05) against the plain FP64
+form.
 
 One Heff application agrees with FP64 to FP32 accuracy (the split products accumulate in FP32,
 relative 1e-5 here), in the direct form (small lists) and the pre-split form; whole DMRG runs from the same start agree in energy within 1e-8, the
@@ -103,3 +104,21 @@ def test_heff_timing_hook_reports_both_forms(dmrgb, ctx):
                                                C.byref(fl)) == 0
         assert sec.value > 0 and fl.value > 0
     assert dmrgb.lib().dmrg_test_heff_time(dev.h, dev.dmpo.h, 5, 2, 1, C.byref(sec), None) == 1
+
+
+def test_split_environment_updates_match_fp64(dmrgb, ctx):
+    """The environment updates of a split-precision sweep (fp64_final = 0: every update on the
+    tensor cores) agree with an FP64 rebuild from the same site tensors to FP32 accuracy: relative
+    1e-5 after a chain of 13 updates."""
+    L = 14
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    psi = dmrgb.randMPS(2, L, 128, seed=5)
+    dev = dmrgb.DeviceState(psi, mpo.device(ctx))
+    dev.env_build()
+    dev.sweep(dmrgb.make_params(maxm=256, cutoff=1e-14, precision="3xtf32", fp64_final=0))
+    assert dev.oc == 0
+    R32 = [dev.env(i, False) for i in range(1, L)]
+    dev.env_build()                                  # FP64, from the same site tensors
+    for i, R in zip(range(1, L), R32):
+        R64 = dev.env(i, False)
+        assert np.max(np.abs(R - R64)) <= 1e-5 * np.max(np.abs(R64)), f"Renv[{i}]"
