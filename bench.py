@@ -343,10 +343,12 @@ def geometric_ramp(m0, m1, n):
 CONFIGS = {
     "c3": {"workload": "hubbard L=32 t=1 U=4 mu=0 U(1)xU(1) (N=32, Sz=0), half-filling product "
                        "start, maxm 64->2048 over 10 sweeps, cutoff 1e-10",
-           "schedule": geometric_ramp(64, 2048, 10), "cutoff": 1e-10},
+           "schedule": geometric_ramp(64, 2048, 10), "cutoff": 1e-10,
+           "forms": ("fp64", "3xtf32")},
     "c4": {"workload": "heisenberg 4x16 open cylinder (periodic W=4, snake order) U(1) Sz=0, Neel "
                        "start, maxm 64->4096 over 8 sweeps, cutoff 1e-9",
-           "schedule": geometric_ramp(64, 4096, 8), "cutoff": 1e-9},
+           "schedule": geometric_ramp(64, 4096, 8), "cutoff": 1e-9,
+           "forms": ("fp64", "3xtf32", "bf16x9")},
 }
 
 
@@ -361,7 +363,7 @@ def config_inputs(pkg, which):
     return pkg.neelMPS(64), pkg.heisenbergCylinderMPO(4, 16).with_qn(pkg.SPIN_QN)
 
 
-def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, tmpdir):
+def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, bf16_peak, tmpdir):
     """One large configuration at full size, plain FP64 and split 3xTF32: (1) the whole sweep
     schedule from the product start in each form (device time, final energies); (2) the same state
     (the plain run's final MPS, checkpointed) swept once more in each form, the second of two
@@ -372,7 +374,8 @@ def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, tmpdir):
     dmpo = mpo.device(ctx)
     ckpt = str(Path(tmpdir) / f"{which}.ckp")
     out = {"workload": cfg["workload"], "schedule": sched}
-    for form in ("fp64", "3xtf32"):
+    forms = cfg["forms"]
+    for form in forms:
         dev = pkg.DeviceState(psi0, dmpo)
         dev.env_build()
         st = [dev.sweep(pkg.make_params(maxm=m, minm=2, cutoff=cutoff, precision=form))
@@ -385,10 +388,11 @@ def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, tmpdir):
         if form == "fp64":
             dev.save(ckpt)
         del dev
-    out["run_speedup_3xtf32"] = out["fp64"]["run_seconds"] / out["3xtf32"]["run_seconds"]
-    out["run_abs_dE"] = abs(out["fp64"]["energy"] - out["3xtf32"]["energy"])
+    for form in forms[1:]:
+        out[f"run_speedup_{form}"] = out["fp64"]["run_seconds"] / out[form]["run_seconds"]
+        out[f"run_abs_dE_{form}"] = abs(out["fp64"]["energy"] - out[form]["energy"])
     same = {}
-    for form in ("fp64", "3xtf32"):
+    for form in forms:
         rec = {}
         for rep in range(2):
             dev = pkg.DeviceState.load(ckpt, dmpo)
@@ -410,17 +414,30 @@ def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, tmpdir):
                                    if p["gemm_seconds"] else None)
         rec["eig_max_n"] = p["eig_max_n"]
         same[form] = rec
-    same["speedup_3xtf32"] = same["fp64"]["sweep_seconds"] / same["3xtf32"]["sweep_seconds"]
-    same["abs_dE"] = abs(same["fp64"]["energy"] - same["3xtf32"]["energy"])
-    g64, g32 = same["fp64"]["heff_gemm_tflops"], same["3xtf32"]["heff_gemm_tflops"]
-    same["roofline"] = {
-        "fp64_heff_gemm": {"achieved": g64, "peak": fp64_peak, "unit": "TFLOP/s",
-                           "frac": g64 / fp64_peak if (g64 and fp64_peak) else None},
-        "3xtf32_heff_gemm": {"achieved": g32, "peak": tf32_peak / 3 if tf32_peak else None,
-                             "unit": "TFLOP/s (algorithmic; ceiling = TF32 peak / 3)",
-                             "frac": 3 * g32 / tf32_peak if (g32 and tf32_peak) else None}}
+    g64 = same["fp64"]["heff_gemm_tflops"]
+    same["roofline"] = {"fp64_heff_gemm": {"achieved": g64, "peak": fp64_peak, "unit": "TFLOP/s",
+                                           "frac": g64 / fp64_peak if (g64 and fp64_peak) else None}}
+    ceilings = {"3xtf32": (tf32_peak / 3 if tf32_peak else None, "TF32 peak / 3"),
+                "bf16x9": (bf16_peak / 9 if bf16_peak else None, "BF16 peak / 9")}
+    for form in forms[1:]:
+        same[f"speedup_{form}"] = same["fp64"]["sweep_seconds"] / same[form]["sweep_seconds"]
+        same[f"abs_dE_{form}"] = abs(same["fp64"]["energy"] - same[form]["energy"])
+        g = same[form]["heff_gemm_tflops"]
+        ceil, how = ceilings[form]
+        same["roofline"][f"{form}_heff_gemm"] = {
+            "achieved": g, "peak": ceil, "unit": f"TFLOP/s (algorithmic; ceiling = {how})",
+            "frac": g / ceil if (g and ceil) else None}
     out["same_state_sweep"] = same
     return out
+
+
+def measured_bf16_peak():
+    """Dense BF16 TFLOP/s of this pool's B200s (burst), from MEASURED_PEAKS.json when present."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(f.read_text())["bf16_tflops"])
+    except Exception:
+        return 1590.0   # earlier measurement on this pool (fallback)
 
 
 def tf32_gemm_peak(device):
@@ -462,13 +479,14 @@ def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
     dev.env_build()
     out = {"workload": f"dense Heisenberg L={L}, random MPS with m={m} at bond {iL + 1} "
                        f"(two-site vector {m}x2x2x{m}); Heff at sites {iL},{iL + 1}"}
-    for name, code in (("fp64", 0), ("3xtf32", 1)):
+    for name, code in (("fp64", 0), ("3xtf32", 1), ("bf16x9", 2)):
         sec, fl = C.c_double(), C.c_double()
         pkg._lib.check(lib.dmrg_test_heff_time(dev.h, dev.dmpo.h, iL, code, reps, C.byref(sec),
                                                C.byref(fl)), ctx.h)
         out["flops_per_apply"] = fl.value
         out[name] = {"seconds": sec.value, "tflops": fl.value / sec.value / 1e12}
     out["speedup_3xtf32"] = out["fp64"]["seconds"] / out["3xtf32"]["seconds"]
+    out["speedup_bf16x9"] = out["fp64"]["seconds"] / out["bf16x9"]["seconds"]
     return out
 
 
@@ -675,11 +693,12 @@ def run_ours(args, world, rank, local, dist):
         return
     peak = fp64_gemm_peak(local)
     tf32_peak = tf32_gemm_peak(local)
+    bf16_peak = measured_bf16_peak()
     configs = {}
     if args.configs:
         with tempfile.TemporaryDirectory() as td:
             for which in args.configs.split(","):
-                configs[which] = config_leg(pkg, ctx, which, peak, tf32_peak, td)
+                configs[which] = config_leg(pkg, ctx, which, peak, tf32_peak, bf16_peak, td)
     g_ach = prof["gemm_flops"] / prof["gemm_seconds"] / 1e12 if prof["gemm_seconds"] > 0 else None
     traffic = None
     tfile = ROOT / "profiles" / "gemm_f64_traffic.json"

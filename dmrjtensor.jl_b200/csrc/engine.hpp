@@ -236,11 +236,17 @@ struct Upload {
 // device fault.
 void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
               const double* B, int64_t nB, double* C, int64_t nC);
-// The same list on the split-precision (3xTF32, tcgen05) kernel; the list must be retiled.
-// Lists of at least SPLIT_PRESPLIT_FLOPS convert their operands once into (hi, lo) pairs first.
+// The same list on a split-precision tcgen05 kernel (form SPLIT_TF32X3 or SPLIT_BF16X9); the list
+// must be retiled. Lists of at least SPLIT_PRESPLIT_FLOPS convert their operands once into split
+// records first.
 constexpr double SPLIT_PRESPLIT_FLOPS = 1e9;
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
-                    const double* B, int64_t nB, double* C, int64_t nC);
+                    const double* B, int64_t nB, double* C, int64_t nC, int form);
+// The split form of a precision (0 for DMRG_PREC_FP64).
+inline int split_form(int precision) {
+  return precision == DMRG_PREC_3XTF32 ? SPLIT_TF32X3
+         : precision == DMRG_PREC_BF16X9 ? SPLIT_BF16X9 : 0;
+}
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,
              double* out, int64_t nout);
 void run_copy(dmrg_ctx* c, const CopyList& l, char* dbase, const double* src, int64_t nsrc,
@@ -290,8 +296,8 @@ void heff_apply_noalloc(dmrg_state* st, int iL, const double* in_dev, double* ou
 // g1 (env_in, A) -> T1, mix T1 -> T2 (the MPO site), g3 (A, T2) -> env_out in layout `out`.
 struct StepPlan {
   GemmList g1, g3;
-  GemmList g1t, g3t;        // retiled copies for the split-precision kernel (split = true)
-  bool split = false;
+  GemmList g1t, g3t;        // retiled copies for the split-precision kernel (split != 0)
+  int split = 0;            // split form of the two GEMMs, 0 = FP64
   MixList mx;
   EnvLayout out;
   int64_t t1 = 0, t2 = 0;   // scratch sizes in doubles
@@ -303,7 +309,7 @@ void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const Si
                      const EnvLayout& RL, StepPlan& sp);
 // Uploads the step's lists; with split = true also their split-precision retilings (the step then
 // runs its two GEMMs on the 3xTF32 tensor-core kernel; the MPO mixing stays FP64).
-void put_step(Upload& u, StepPlan& sp, bool split = false);
+void put_step(Upload& u, StepPlan& sp, int split = 0);
 // Launches an uploaded step; c->T1 / c->T2 must hold sp.t1 / sp.t2 doubles. `bra` (optional)
 // is the conjugated tensor when it differs from the ket tensor A (the dualpsi argument of
 // Lupdate/Rupdate); both share A's layout.

@@ -115,7 +115,7 @@ void prepare_split(HeffPlan& hp) {
 }
 
 void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision) {
-  if (precision == DMRG_PREC_3XTF32 && !hp.split) prepare_split(hp);
+  if (split_form(precision) && !hp.split) prepare_split(hp);
   Upload u;
   u.put(hp.g1);
   u.put(hp.mix);
@@ -159,14 +159,15 @@ void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, dou
   ensure(c, c->X, std::max<int64_t>(hp.x_size, 1));
   ensure(c, c->Y, std::max<int64_t>(hp.y_size, 1));
   const int64_t n = hp.tl.size;
-  // split form: the two GEMM steps on the tensor-core 3xTF32 kernel; the MPO mixing stays FP64
-  const bool split = precision == DMRG_PREC_3XTF32;
+  // split forms: the two GEMM steps on a tensor-core split kernel; the MPO mixing stays FP64
+  const int split = split_form(precision);
   if (split && !hp.split) fail(DMRG_ERR_STATE, "split-precision Heff lists were not uploaded");
   if (precision != DMRG_PREC_FP64 && !split)
-    fail(DMRG_ERR_ARG, "precision: only FP64 and 3xTF32 Heff forms are built");
+    fail(DMRG_ERR_ARG, "precision: FP64, 3xTF32 and BF16x9 are the built forms");
   if (prof) prof->begin(c->stream, hp.g1.flops);
   if (split)
-    run_gemm_split(c, hp.g1t, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
+    run_gemm_split(c, hp.g1t, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n,
+                   split);
   else
     run_gemm(c, hp.g1, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
   if (prof) prof->end(c->stream);
@@ -174,7 +175,7 @@ void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, dou
   if (prof) prof->begin(c->stream, hp.g3.flops);
   if (split)
     run_gemm_split(c, hp.g3t, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n,
-                   y, n);
+                   y, n, split);
   else
     run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n, y, n);
   if (prof) prof->end(c->stream);
@@ -361,7 +362,7 @@ int split_tile_n(const GemmList& g) {
 }
 }  // namespace
 
-void put_step(Upload& u, StepPlan& sp, bool split) {
+void put_step(Upload& u, StepPlan& sp, int split) {
   u.put(sp.g1);
   u.put(sp.mx);
   u.put(sp.g3);
@@ -385,12 +386,12 @@ void run_step(dmrg_ctx* c, const StepPlan& sp, char* db, const double* env_in, i
   const DBuf& first = left ? A : B;
   const DBuf& last = left ? B : A;
   if (sp.split)
-    run_gemm_split(c, sp.g1t, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n);
+    run_gemm_split(c, sp.g1t, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n, sp.split);
   else
     run_gemm(c, sp.g1, db, env_in, n_in, first.p, first.n, c->T1.p, c->T1.n);
   run_mix(c, sp.mx, db, c->T1.p, c->T1.n, c->T2.p, c->T2.n);
   if (sp.split)
-    run_gemm_split(c, sp.g3t, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out);
+    run_gemm_split(c, sp.g3t, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out, sp.split);
   else
     run_gemm(c, sp.g3, db, last.p, last.n, c->T2.p, c->T2.n, env_out, n_out);
 }
@@ -473,7 +474,7 @@ void lupdate(dmrg_state* st, int i, double* flops, int precision) {
   StepPlan sp;
   plan_left_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Llay[i], sp);
   Upload u;
-  put_step(u, sp, precision == DMRG_PREC_3XTF32);
+  put_step(u, sp, split_form(precision));
   char* db = u.send(c, 2);
   ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
   ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));
@@ -492,7 +493,7 @@ void rupdate(dmrg_state* st, int i, double* flops, int precision) {
   StepPlan sp;
   plan_right_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Rlay[i], sp);
   Upload u;
-  put_step(u, sp, precision == DMRG_PREC_3XTF32);
+  put_step(u, sp, split_form(precision));
   char* db = u.send(c, 2);
   ensure(c, c->T1, std::max<int64_t>(sp.t1, 1));
   ensure(c, c->T2, std::max<int64_t>(sp.t2, 1));

@@ -348,7 +348,8 @@ void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int6
 }
 
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
-                    const double* B, int64_t nB, double* C, int64_t nC) {
+                    const double* B, int64_t nB, double* C, int64_t nC, int form) {
+  if (form != SPLIT_TF32X3 && form != SPLIT_BF16X9) bad_plan("split gemm form");
   if (g.tiles == 0) return;
   if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_PRESPLIT))
     bad_plan("split gemm tiling");
@@ -372,16 +373,16 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
     // convert each operand element once instead of once per tile that reads it
     ensure(c, c->SA, std::max<int64_t>(extA, 1));
     ensure(c, c->SB, std::max<int64_t>(extB, 1));
-    float2* pa = reinterpret_cast<float2*>(c->SA.p);
-    float2* pb = reinterpret_cast<float2*>(c->SB.p);
-    launch_presplit(c->stream, A, pa, extA);
-    launch_presplit(c->stream, B, pb, extB);
-    launch_gemm_tf32x3_presplit(c->stream, g.tA, g.tB, pa, pb, C, tasks, int(g.tasks.size()), segs,
-                                g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
+    uint2* pa = reinterpret_cast<uint2*>(c->SA.p);
+    uint2* pb = reinterpret_cast<uint2*>(c->SB.p);
+    launch_presplit(form, c->stream, A, pa, extA);
+    launch_presplit(form, c->stream, B, pb, extB);
+    launch_gemm_split_presplit(form, c->stream, g.tA, g.tB, pa, pb, C, tasks, int(g.tasks.size()),
+                               segs, g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
     return;
   }
-  launch_gemm_tf32x3(c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs, g.tiles,
-                     c->nsm * 3, c->d_status + STATUS_MMA);
+  launch_gemm_split(form, c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs,
+                    g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
 }
 
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,

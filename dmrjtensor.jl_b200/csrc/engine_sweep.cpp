@@ -158,7 +158,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
         if (kc >= 0 && lb.kb[kc * d2 + s2] == kd)
           gaa.seg(la.off[ka * d1 + s1], Bl.dim[ka], lb.off[kc * d2 + s2], Bc.dim[kc], Bc.dim[kc]);
       }
-  const bool split = P.precision == DMRG_PREC_3XTF32;
+  const bool split = split_form(P.precision) != 0;
   if (split) prepare_split(hp);
   Upload u;
   u.put(hp.g1);
@@ -508,8 +508,8 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     // second half-sweep when the sweep's energy is the FP64 Rayleigh quotient (fp64_final): that
     // half-sweep builds, from the final site tensors, every environment the last bond step reads,
     // so the quotient is exact FP64 arithmetic on the final Ritz vector
-    const int eprec = (P.precision == DMRG_PREC_3XTF32 && !(P.fp64_final && j != j0))
-                          ? DMRG_PREC_3XTF32 : DMRG_PREC_FP64;
+    const int eprec = (split_form(P.precision) && !(P.fp64_final && j != j0))
+                          ? P.precision : DMRG_PREC_FP64;
     if (j > 0) lupdate(st, i, &ef, eprec); else rupdate(st, i, &ef, eprec);
     cuda_check(cudaGetLastError(), "environment update");
     tm.end(tenv, 1);
@@ -536,7 +536,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   st->dir = j;
   const int t1 = tm.record();
   cuda_check(cudaEventSynchronize(tm.event(t1)), "sweep sync");
-  if (P.precision == DMRG_PREC_3XTF32) check_mma_status(c);   // the last environment update
+  if (split_form(P.precision)) check_mma_status(c);   // the last environment update
   float ms = 0;
   cudaEventElapsedTime(&ms, tm.event(t0), tm.event(t1));
   out.seconds = ms * 1e-3;

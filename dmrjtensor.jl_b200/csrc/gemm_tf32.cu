@@ -1,26 +1,30 @@
 // gemm_tf32.cu -- grouped GEMM C = alpha op(A) op(B) + beta C with FP64 operands and result,
-// computed as three TF32 tensor-core products on tcgen05 (the split form of the Heff GEMMs).
+// computed as several low-precision tensor-core products on tcgen05 (the split forms of the Heff
+// and environment GEMMs). Two forms:
 //
-// Each FP64 operand element x is split into x_hi = tf32(x) and x_lo = tf32(x - x_hi), and
-// C ~ A_hi B_hi + A_hi B_lo + A_lo B_hi is accumulated in FP32 in tensor memory: about FP32
-// accuracy (relative ~1e-7 per product), with the tensor pipe doing the arithmetic. The FP64
-// Krylov recursion, normalisation and the final Ritz energy stay FP64 in the caller.
+//  * 3xTF32: each FP64 operand element x is split into x_hi = tf32(x) and x_lo = tf32(x - x_hi),
+//    and C ~ A_hi B_hi + A_hi B_lo + A_lo B_hi (tcgen05.mma kind::tf32, K = 8 per instruction);
+//  * 9xBF16: x = b0 + b1 + b2 with b0 = bf16(x), b1 = bf16(x - b0), b2 = bf16(x - b0 - b1)
+//    (each part rounded to nearest even from the exact remainder), and C ~ sum over all nine
+//    products A_i B_j (kind::f16 with BF16 operands, K = 16 per instruction).
+// Both accumulate in FP32 in tensor memory: about FP32 accuracy (relative ~1e-7 per product), with
+// the tensor pipe doing the arithmetic. The FP64 Krylov recursion, normalisation and the final
+// Ritz energy stay FP64 in the caller.
 //
 // Same task lists as the FP64 kernel (GemmTask / GemmSeg, element offsets from base pointers),
-// tiled 128 x 64 (direct form) or 128 x 128 (pre-split form); the lists are retiled to match. One CTA of 4 warps per tile at a time
-// (persistent over tiles): the threads stage a K chunk of 32 of op(A) and op(B) into shared
-// memory in the canonical K-major layout (8-row x 16-byte core matrices, no swizzle), one thread
-// issues 4 k-steps x 3 tcgen05.mma (M=128, N=64, K=8) into a 64-column TMEM accumulator and
-// commits to an mbarrier, and all threads wait (bounded) before the next chunk overwrites the
-// tiles. The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 =
-// rows of the tile) and writes alpha acc + beta C in FP64.
+// tiled 128 x 64 (direct form) or 128 x 128 (pre-split form); the lists are retiled to match. One
+// CTA of 4 warps per tile at a time (persistent over tiles): the threads stage a K chunk of 32 of
+// op(A) and op(B) into shared memory in the canonical K-major layout (8-row x 16-byte core
+// matrices, no swizzle; one plane per split part), one thread issues the chunk's MMAs into a TMEM
+// accumulator and commits to an mbarrier, and all threads wait (bounded) before the next chunk
+// overwrites the tiles. The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31 = rows of the tile) and writes alpha acc + beta C in FP64.
 //
 // Large lists use the pre-split form (PRE): one memory-bound pass writes every operand element as
-// an interleaved (hi, lo) FP32 pair, and the GEMM stages the pairs without converting. In the
-// direct form each tile re-splits its operands (five conversions per element on the XU pipe,
-// repeated for every tile that reads the element), which bounds the kernel at large sizes; the
-// pre-split pass converts each element once. Both forms round identically, so their results are
-// bit-identical.
+// its split parts (8 bytes: two FP32 TF32 values, or four BF16 values of which three are used),
+// and the GEMM stages the parts without converting. In the direct form each tile re-splits its
+// operands (repeated for every tile that reads the element). Both forms round identically, so
+// their results are bit-identical.
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -30,24 +34,34 @@ namespace {
 
 constexpr int TBM = 128, TBK = 32;
 constexpr int TT = 128;                          // 4 warps
-constexpr int A_BYTES = TBM * TBK * 4;           // 16 KB per split part
 constexpr long long WAIT_LIMIT = 1ll << 22;      // try_wait rounds before giving up
-constexpr int A_QUADS = TBM * TBK / 4 / TT;      // per thread
 static_assert(TF32_TILE_N_DIRECT == 64 && TF32_TILE_N_PRESPLIT == 128, "tile widths");
 
-// Tile width by form: 128 x 64 for the direct form (small lists: narrow blocks), 128 x 128 for
-// the pre-split form (each staged A tile feeds twice the products).
-template <bool PRE>
+// The two split forms. A 16-byte unit of a staged plane holds QE consecutive K elements of one
+// row; an MMA consumes KSTEP K elements (two core matrices along K).
+struct FormTF32 {
+  static constexpr int PLANES = 2, EB = 4, QE = 4, KSTEP = 8, PRODUCTS = 3;
+  static constexpr uint32_t KIND_BITS = (2u << 7) | (2u << 10);   // A, B = TF32
+};
+struct FormBF16 {
+  static constexpr int PLANES = 3, EB = 2, QE = 8, KSTEP = 16, PRODUCTS = 9;
+  static constexpr uint32_t KIND_BITS = (1u << 7) | (1u << 10);   // A, B = BF16
+};
+
+template <class F, bool PRE>
 struct Tile {
   static constexpr int BN = PRE ? TF32_TILE_N_PRESPLIT : TF32_TILE_N_DIRECT;
-  static constexpr int B_BYTES = BN * TBK * 4;                      // per split part
-  static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 1024;     // + alignment slack
-  static constexpr uint32_t TMEM_COLS = BN;                         // FP32 128 lanes x BN
-  static constexpr int B_QUADS = BN * TBK / 4 / TT;
-  // instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), both
-  // K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24
-  static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) |
-                                    (uint32_t(BN >> 3) << 17) | (uint32_t(TBM >> 4) << 24);
+  static constexpr int KQ = TBK / F::QE;                        // units per row and chunk
+  static constexpr int A_BYTES = TBM * TBK * F::EB;             // per plane
+  static constexpr int B_BYTES = BN * TBK * F::EB;
+  static constexpr int SMEM = F::PLANES * (A_BYTES + B_BYTES) + 1024;   // + alignment slack
+  static constexpr uint32_t TMEM_COLS = BN;                     // FP32 128 lanes x BN
+  static constexpr int A_UNITS = TBM * KQ / TT;                 // per thread
+  static constexpr int B_UNITS = BN * KQ / TT;
+  // instruction descriptor: D F32 (bits 4-5 = 1), A and B types, both K-major (bits 15, 16 = 0),
+  // N >> 3 at bit 17, M >> 4 at bit 24
+  static constexpr uint32_t IDESC = (1u << 4) | F::KIND_BITS | (uint32_t(BN >> 3) << 17) |
+                                    (uint32_t(TBM >> 4) << 24);
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -55,8 +69,8 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 }
 
 // Shared-memory matrix descriptor, K-major without swizzle: core matrices of 8 rows x 16 bytes;
-// the next 4 K elements (second core matrix of a k-step) 128 bytes on (leading byte offset), the
-// next 8 rows 256 bytes on (stride byte offset); descriptor version 1 at bit 46.
+// the second core matrix along K of a k-step 128 bytes on (leading byte offset), the next 8 rows
+// 256 bytes on (stride byte offset); descriptor version 1 at bit 46.
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
   uint64_t d = uint64_t((addr >> 4) & 0x3FFFu);
   d |= uint64_t(128 >> 4) << 16;
@@ -65,10 +79,11 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
   return d;
 }
 
-// byte offset of element (row, k) of a staged operand with R rows and a K chunk of TBK
-__device__ __forceinline__ int soff(int R, int row, int k) {
-  return (k >> 3) * (R * 32) + (row >> 3) * 256 + ((k >> 2) & 1) * 128 + (row & 7) * 16 +
-         (k & 3) * 4;
+// byte offset of the 16-byte unit (row, kq) of a staged plane with R rows: a k-step block (all
+// rows, KSTEP = 2 QE elements) is R*32 bytes; inside it 8-row groups of 256 bytes, each two core
+// matrices (K halves) of 128 bytes, each 8 rows of 16 bytes
+__device__ __forceinline__ int uoff(int R, int row, int kq) {
+  return (kq >> 1) * (R * 32) + (row >> 3) * 256 + (kq & 1) * 128 + (row & 7) * 16;
 }
 
 __device__ __forceinline__ float tf32r(float f) {
@@ -77,24 +92,59 @@ __device__ __forceinline__ float tf32r(float f) {
   return __uint_as_float(r);
 }
 
-__device__ __forceinline__ void split(double x, float& hi, float& lo) {
-  hi = tf32r(float(x));
-  lo = tf32r(float(x - double(hi)));
+// bf16 bits of f, rounded to nearest (ties to even); f finite
+__device__ __forceinline__ uint32_t bf16_bits(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
 }
+__device__ __forceinline__ double bf16_value(uint32_t b) { return double(__uint_as_float(b << 16)); }
 
-__device__ __forceinline__ void to_pair(double x, float& hi, float& lo) { split(x, hi, lo); }
-__device__ __forceinline__ void to_pair(float2 x, float& hi, float& lo) {
-  hi = x.x;
-  lo = x.y;
+// The split parts of one element, as the 8-byte pre-split record: TF32 (hi, lo) as two floats;
+// BF16 (b0, b1, b2, 0) as four 16-bit values.
+__device__ __forceinline__ uint2 split_rec(FormTF32, double x) {
+  const float hi = tf32r(float(x));
+  const float lo = tf32r(float(x - double(hi)));
+  return make_uint2(__float_as_uint(hi), __float_as_uint(lo));
 }
+__device__ __forceinline__ uint2 split_rec(FormBF16, double x) {
+  const uint32_t b0 = bf16_bits(float(x));
+  const double r1 = x - bf16_value(b0);
+  const uint32_t b1 = bf16_bits(float(r1));
+  const double r2 = r1 - bf16_value(b1);
+  const uint32_t b2 = bf16_bits(float(r2));
+  return make_uint2(b0 | (b1 << 16), b2);
+}
+__device__ __forceinline__ uint2 to_rec(FormTF32 f, double x) { return split_rec(f, x); }
+__device__ __forceinline__ uint2 to_rec(FormBF16 f, double x) { return split_rec(f, x); }
+template <class F>
+__device__ __forceinline__ uint2 to_rec(F, uint2 x) { return x; }
 
-__global__ void k_presplit(const double* __restrict__ x, float2* __restrict__ y, int64_t n) {
-  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-    float h, l;
-    split(x[i], h, l);
-    y[i] = make_float2(h, l);
+// stores one 16-byte unit per plane from QE records
+__device__ __forceinline__ void store_unit(FormTF32, unsigned char* sp, int plane_bytes, int o,
+                                           const uint2* r) {
+  *reinterpret_cast<uint4*>(sp + o) = make_uint4(r[0].x, r[1].x, r[2].x, r[3].x);
+  *reinterpret_cast<uint4*>(sp + plane_bytes + o) = make_uint4(r[0].y, r[1].y, r[2].y, r[3].y);
+}
+__device__ __forceinline__ void store_unit(FormBF16, unsigned char* sp, int plane_bytes, int o,
+                                           const uint2* r) {
+  uint32_t p0[4], p1[4], p2[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint2 a = r[2 * q], b = r[2 * q + 1];
+    p0[q] = (a.x & 0xFFFFu) | (b.x << 16);
+    p1[q] = (a.x >> 16) | (b.x & 0xFFFF0000u);
+    p2[q] = (a.y & 0xFFFFu) | (b.y << 16);
   }
+  *reinterpret_cast<uint4*>(sp + o) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
+  *reinterpret_cast<uint4*>(sp + plane_bytes + o) = make_uint4(p1[0], p1[1], p1[2], p1[3]);
+  *reinterpret_cast<uint4*>(sp + 2 * plane_bytes + o) = make_uint4(p2[0], p2[1], p2[2], p2[3]);
+}
+
+template <class F>
+__global__ void k_presplit(const double* __restrict__ x, uint2* __restrict__ y, int64_t n) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    y[i] = split_rec(F{}, x[i]);
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc,
@@ -105,6 +155,38 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       :
       : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc,
+                                        uint32_t idesc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+// The products of one k-step: plane descriptors of A and B (plane p at base + p * plane bytes).
+// TF32: hi.hi, hi.lo, lo.hi; BF16: all nine pairs, smallest parts first.
+__device__ __forceinline__ void kstep_mmas(FormTF32, uint32_t tmem, uint32_t a, uint32_t ab,
+                                           uint32_t b, uint32_t bb, bool& issued, uint32_t idesc) {
+  const uint64_t a0 = sdesc(a), a1 = sdesc(a + ab), b0 = sdesc(b), b1 = sdesc(b + bb);
+  mma_tf32(tmem, a0, b0, issued ? 1u : 0u, idesc);
+  issued = true;
+  mma_tf32(tmem, a0, b1, 1u, idesc);
+  mma_tf32(tmem, a1, b0, 1u, idesc);
+}
+__device__ __forceinline__ void kstep_mmas(FormBF16, uint32_t tmem, uint32_t a, uint32_t ab,
+                                           uint32_t b, uint32_t bb, bool& issued, uint32_t idesc) {
+#pragma unroll
+  for (int s = 4; s >= 0; --s)        // part-index sum s = i + j, small terms first
+#pragma unroll
+    for (int i = 2; i >= 0; --i) {
+      const int jj = s - i;
+      if (jj < 0 || jj > 2) continue;
+      mma_f16(tmem, sdesc(a + i * ab), sdesc(b + jj * bb), issued ? 1u : 0u, idesc);
+      issued = true;
+    }
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
@@ -140,27 +222,29 @@ __device__ __forceinline__ void tmem_ld16_wait(uint32_t addr, float* v) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-template <bool TA, bool TB, bool PRE>
+template <class F, bool TA, bool TB, bool PRE>
 __global__ void __launch_bounds__(TT, 3)
-k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* __restrict__ C,
-              const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
-              int total_tiles, int* err) {
-  // operand elements: FP64 values (direct form) or pre-split (hi, lo) pairs
-  using T = typename std::conditional<PRE, float2, double>::type;
+k_gemm_split(const void* __restrict__ Av, const void* __restrict__ Bv, double* __restrict__ C,
+             const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
+             int total_tiles, int* err) {
+  // operand elements: FP64 values (direct form) or pre-split 8-byte records
+  using T = typename std::conditional<PRE, uint2, double>::type;
+  using TL = Tile<F, PRE>;
   const T* __restrict__ A = static_cast<const T*>(Av);
   const T* __restrict__ B = static_cast<const T*>(Bv);
-  constexpr int TBN = Tile<PRE>::BN, B_BYTES = Tile<PRE>::B_BYTES, B_QUADS = Tile<PRE>::B_QUADS;
-  constexpr uint32_t TMEM_COLS = Tile<PRE>::TMEM_COLS, IDESC = Tile<PRE>::IDESC;
+  constexpr int TBN = TL::BN, KQ = TL::KQ, QE = F::QE;
+  constexpr int A_BYTES = TL::A_BYTES, B_BYTES = TL::B_BYTES;
+  constexpr int A_UNITS = TL::A_UNITS, B_UNITS = TL::B_UNITS;
+  constexpr uint32_t TMEM_COLS = TL::TMEM_COLS, IDESC = TL::IDESC;
   extern __shared__ unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // 1024-byte aligned operand area: A_hi | A_lo | B_hi | B_lo
+  // 1024-byte aligned operand area: A planes | B planes
   const uint32_t raw = smem_u32(smraw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* sp = smraw + (base - raw);
-  const uint32_t aH = base, aL = base + A_BYTES, bH = base + 2 * A_BYTES,
-                 bL = base + 2 * A_BYTES + B_BYTES;
+  const uint32_t aS = base, bS = base + F::PLANES * A_BYTES;
   const uint32_t mb = smem_u32(&mbar);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
@@ -188,49 +272,48 @@ k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* 
     const int local = tile - tk.tile0;
     const int m0 = (local % tk.tiles_m) * TBM, n0 = (local / tk.tiles_m) * TBN;
     // K chunks of this tile, over all its segments: (segment q, offset k0). Each thread owns
-    // the elements tid + TT i of a chunk: loaded into registers in one batch (the next chunk's
-    // loads are issued while the current chunk's MMAs run), then split into the staged tiles.
+    // the 16-byte units tid + TT i of a chunk (QE consecutive K elements of one row): loaded into
+    // registers in one batch (the next chunk's loads are issued while the current chunk's MMAs
+    // run), then split into the staged planes. Operand stored with rows contiguous: consecutive
+    // threads take consecutive rows. Stored with K contiguous: 8 consecutive threads take the
+    // same unit of 8 consecutive rows (their 16-byte stores land in 8 different bank groups of
+    // one 128-byte line), the next 8 the next unit.
     bool issued = false;
     int q = 0, k0 = 0;
     while (q < tk.nseg && segs[tk.seg0 + q].K <= 0) ++q;
-    // quads: 4 consecutive K elements of one row (one 16-byte unit of the staged layout).
-    // Operand stored with rows contiguous: consecutive threads take consecutive rows. Stored
-    // with K contiguous: 8 consecutive threads take the same quad of 8 consecutive rows (their
-    // 16-byte stores land in 8 different bank groups of one 128-byte line), the next 8 the next
-    // quad, so a warp still reads 8 rows x 16 contiguous K elements.
-    T ra[A_QUADS][4], rb[B_QUADS][4];
-    auto a_quad = [&](int i, int& r, int& kq) {
+    T ra[A_UNITS][QE], rb[B_UNITS][QE];
+    auto a_unit = [&](int i, int& r, int& kq) {
       const int e = tid + TT * i;
-      if (TA) { r = (e & 7) + 8 * (e >> 6); kq = (e >> 3) & 7; } else { r = e % TBM; kq = e / TBM; }
+      if (TA) { r = (e & 7) + 8 * (e / (8 * KQ)); kq = (e >> 3) % KQ; } else { r = e % TBM; kq = e / TBM; }
     };
-    auto b_quad = [&](int i, int& c, int& kq) {
+    auto b_unit = [&](int i, int& c, int& kq) {
       const int e = tid + TT * i;
-      if (TB) { c = e % TBN; kq = e / TBN; } else { c = (e & 7) + 8 * (e >> 6); kq = (e >> 3) & 7; }
+      if (TB) { c = e % TBN; kq = e / TBN; } else { c = (e & 7) + 8 * (e / (8 * KQ)); kq = (e >> 3) % KQ; }
     };
     const T zero = T{};
     auto load_chunk = [&](int qq, int kk0) {
       const GemmSeg sg = segs[tk.seg0 + qq];
 #pragma unroll
-      for (int i = 0; i < A_QUADS; ++i) {
+      for (int i = 0; i < A_UNITS; ++i) {
         int r, kq;
-        a_quad(i, r, kq);
+        a_unit(i, r, kq);
         const int gr = m0 + r;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int gk = kk0 + 4 * kq + j;
+        for (int j = 0; j < QE; ++j) {
+          const int gk = kk0 + QE * kq + j;
           ra[i][j] = (gr < tk.M && gk < sg.K)
                          ? (TA ? A[sg.a_off + gk + int64_t(gr) * sg.lda] : A[sg.a_off + gr + int64_t(gk) * sg.lda])
                          : zero;
         }
       }
 #pragma unroll
-      for (int i = 0; i < B_QUADS; ++i) {
+      for (int i = 0; i < B_UNITS; ++i) {
         int c, kq;
-        b_quad(i, c, kq);
+        b_unit(i, c, kq);
         const int gc = n0 + c;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int gk = kk0 + 4 * kq + j;
+        for (int j = 0; j < QE; ++j) {
+          const int gk = kk0 + QE * kq + j;
           rb[i][j] = (gc < tk.N && gk < sg.K)
                          ? (TB ? B[sg.b_off + gc + int64_t(gk) * sg.ldb] : B[sg.b_off + gk + int64_t(gc) * sg.ldb])
                          : zero;
@@ -241,43 +324,30 @@ k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* 
     while (q < tk.nseg) {
       const int ks = min(TBK, segs[tk.seg0 + q].K - k0);
 #pragma unroll
-      for (int i = 0; i < A_QUADS; ++i) {
+      for (int i = 0; i < A_UNITS; ++i) {
         int r, kq;
-        a_quad(i, r, kq);
-        float4 h, l;
-        to_pair(ra[i][0], h.x, l.x);
-        to_pair(ra[i][1], h.y, l.y);
-        to_pair(ra[i][2], h.z, l.z);
-        to_pair(ra[i][3], h.w, l.w);
-        const int o = soff(TBM, r, 4 * kq);
-        *reinterpret_cast<float4*>(sp + o) = h;
-        *reinterpret_cast<float4*>(sp + A_BYTES + o) = l;
+        a_unit(i, r, kq);
+        uint2 rec[QE];
+#pragma unroll
+        for (int j = 0; j < QE; ++j) rec[j] = to_rec(F{}, ra[i][j]);
+        store_unit(F{}, sp, A_BYTES, uoff(TBM, r, kq), rec);
       }
 #pragma unroll
-      for (int i = 0; i < B_QUADS; ++i) {
+      for (int i = 0; i < B_UNITS; ++i) {
         int c, kq;
-        b_quad(i, c, kq);
-        float4 h, l;
-        to_pair(rb[i][0], h.x, l.x);
-        to_pair(rb[i][1], h.y, l.y);
-        to_pair(rb[i][2], h.z, l.z);
-        to_pair(rb[i][3], h.w, l.w);
-        const int o = soff(TBN, c, 4 * kq);
-        *reinterpret_cast<float4*>(sp + 2 * A_BYTES + o) = h;
-        *reinterpret_cast<float4*>(sp + 2 * A_BYTES + B_BYTES + o) = l;
+        b_unit(i, c, kq);
+        uint2 rec[QE];
+#pragma unroll
+        for (int j = 0; j < QE; ++j) rec[j] = to_rec(F{}, rb[i][j]);
+        store_unit(F{}, sp + F::PLANES * A_BYTES, B_BYTES, uoff(TBN, c, kq), rec);
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncthreads();
       if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        for (int st = 0; st * 8 < ks; ++st) {
-          const uint64_t dah = sdesc(aH + st * (TBM * 32)), dal = sdesc(aL + st * (TBM * 32));
-          const uint64_t dbh = sdesc(bH + st * (TBN * 32)), dbl = sdesc(bL + st * (TBN * 32));
-          mma_tf32(tmem, dah, dbh, issued ? 1u : 0u, IDESC);
-          issued = true;
-          mma_tf32(tmem, dah, dbl, 1u, IDESC);
-          mma_tf32(tmem, dal, dbh, 1u, IDESC);
-        }
+        for (int st = 0; st * F::KSTEP < ks; ++st)
+          kstep_mmas(F{}, tmem, aS + st * (TBM * 32), A_BYTES, bS + st * (TBN * 32), B_BYTES,
+                     issued, IDESC);
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                      :: "r"(mb) : "memory");
       }
@@ -301,7 +371,7 @@ k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* 
       if (failed) break;
     }
     if (failed) break;
-    // epilogue: row m0 + 32 warp + lane of the tile, 64 columns
+    // epilogue: row m0 + 32 warp + lane of the tile
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const int row = m0 + 32 * warp + lane;
     const double alpha = tk.alpha, beta = tk.beta;
@@ -338,52 +408,61 @@ k_gemm_tf32x3(const void* __restrict__ Av, const void* __restrict__ Bv, double* 
                  :: "r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
-template <bool TA, bool TB, bool PRE>
-void launch_tf32_variant(cudaStream_t s, const void* A, const void* B, double* C,
-                         const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
-                         int grid_cap, int* err) {
-  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tf32x3<TA, TB, PRE>), Tile<PRE>::SMEM);
+template <class F, bool TA, bool TB, bool PRE>
+void launch_variant(cudaStream_t s, const void* A, const void* B, double* C,
+                    const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
+                    int grid_cap, int* err) {
+  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_split<F, TA, TB, PRE>), Tile<F, PRE>::SMEM);
   const int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_tf32x3<TA, TB, PRE><<<grid, TT, Tile<PRE>::SMEM, s>>>(A, B, C, tasks, ntasks, segs,
-                                                                total_tiles, err);
+  k_gemm_split<F, TA, TB, PRE><<<grid, TT, Tile<F, PRE>::SMEM, s>>>(A, B, C, tasks, ntasks, segs,
+                                                                     total_tiles, err);
   count_launch();
 }
 
-template <bool PRE>
+template <class F, bool PRE>
 void dispatch(cudaStream_t s, bool transA, bool transB, const void* A, const void* B, double* C,
               const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
               int grid_cap, int* err) {
   if (!transA && !transB)
-    launch_tf32_variant<false, false, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+    launch_variant<F, false, false, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
   else if (!transA && transB)
-    launch_tf32_variant<false, true, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+    launch_variant<F, false, true, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
   else if (transA && !transB)
-    launch_tf32_variant<true, false, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+    launch_variant<F, true, false, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
   else
-    launch_tf32_variant<true, true, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+    launch_variant<F, true, true, PRE>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
 }
 
 }  // namespace
 
-void launch_gemm_tf32x3(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
-                        double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
-                        int total_tiles, int grid_cap, int* err) {
+void launch_gemm_split(int form, cudaStream_t s, bool transA, bool transB, const double* A,
+                       const double* B, double* C, const GemmTask* tasks, int ntasks,
+                       const GemmSeg* segs, int total_tiles, int grid_cap, int* err) {
   if (total_tiles <= 0) return;
-  dispatch<false>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  if (form == SPLIT_BF16X9)
+    dispatch<FormBF16, false>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  else
+    dispatch<FormTF32, false>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
 }
 
-void launch_presplit(cudaStream_t s, const double* x, float2* pairs, int64_t n) {
+void launch_presplit(int form, cudaStream_t s, const double* x, uint2* recs, int64_t n) {
   if (n <= 0) return;
   const int64_t blocks = (n + 255) / 256;
-  k_presplit<<<int(blocks < 1184 ? blocks : 1184), 256, 0, s>>>(x, pairs, n);
+  const int grid = int(blocks < 1184 ? blocks : 1184);
+  if (form == SPLIT_BF16X9) k_presplit<FormBF16><<<grid, 256, 0, s>>>(x, recs, n);
+  else k_presplit<FormTF32><<<grid, 256, 0, s>>>(x, recs, n);
   count_launch();
 }
 
-void launch_gemm_tf32x3_presplit(cudaStream_t s, bool transA, bool transB, const float2* A,
-                                 const float2* B, double* C, const GemmTask* tasks, int ntasks,
-                                 const GemmSeg* segs, int total_tiles, int grid_cap, int* err) {
+void launch_gemm_split_presplit(int form, cudaStream_t s, bool transA, bool transB,
+                                const uint2* A, const uint2* B, double* C, const GemmTask* tasks,
+                                int ntasks, const GemmSeg* segs, int total_tiles, int grid_cap,
+                                int* err) {
   if (total_tiles <= 0) return;
-  dispatch<true>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  if (form == SPLIT_BF16X9)
+    dispatch<FormBF16, true>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
+  else
+    dispatch<FormTF32, true>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap, err);
 }
 
 }  // namespace dmrg

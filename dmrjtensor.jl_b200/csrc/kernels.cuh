@@ -97,19 +97,23 @@ void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, 
                      double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
                      int total_tiles, int grid_cap);
 
-// Split-precision grouped GEMM (3 x TF32 on tcgen05, FP32 accumulation in TMEM, FP64 in/out),
-// tiles of TF32_TILE_M x GEMM_BN; err[0] is set when an MMA completion wait gave up.
+// Split-precision grouped GEMM on tcgen05 (FP32 accumulation in TMEM, FP64 in/out), tiles of
+// TF32_TILE_M x (64 or 128): form SPLIT_TF32X3 = three TF32 products, SPLIT_BF16X9 = nine BF16
+// products; err[0] is set when an MMA completion wait gave up.
+constexpr int SPLIT_TF32X3 = 1, SPLIT_BF16X9 = 2;
 constexpr int TF32_TILE_M = 128;
 constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_PRESPLIT = 128;
-void launch_gemm_tf32x3(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
-                        double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
-                        int total_tiles, int grid_cap, int* err);
-// The same GEMM on pre-split operands: A and B hold (hi, lo) TF32 pairs at the element offsets
-// the tasks address (launch_presplit writes them from FP64; bit-identical results).
-void launch_presplit(cudaStream_t s, const double* x, float2* pairs, int64_t n);
-void launch_gemm_tf32x3_presplit(cudaStream_t s, bool transA, bool transB, const float2* A,
-                                 const float2* B, double* C, const GemmTask* tasks, int ntasks,
-                                 const GemmSeg* segs, int total_tiles, int grid_cap, int* err);
+void launch_gemm_split(int form, cudaStream_t s, bool transA, bool transB, const double* A,
+                       const double* B, double* C, const GemmTask* tasks, int ntasks,
+                       const GemmSeg* segs, int total_tiles, int grid_cap, int* err);
+// The same GEMM on pre-split operands: A and B hold 8-byte records of the split parts at the
+// element offsets the tasks address (launch_presplit writes them from FP64; bit-identical
+// results).
+void launch_presplit(int form, cudaStream_t s, const double* x, uint2* recs, int64_t n);
+void launch_gemm_split_presplit(int form, cudaStream_t s, bool transA, bool transB,
+                                const uint2* A, const uint2* B, double* C, const GemmTask* tasks,
+                                int ntasks, const GemmSeg* segs, int total_tiles, int grid_cap,
+                                int* err);
 // slot of the context's status words that the split-precision GEMM sets on a timeout
 constexpr int STATUS_MMA = 8;
 

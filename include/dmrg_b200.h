@@ -64,7 +64,9 @@ enum dmrg_precision {
                             tensor-core products (FP32-accurate); with fp64_final the environments
                             of the sweep's second half are FP64 so that the reported energy is the
                             exact FP64 Rayleigh quotient of the final Ritz vector */
-  DMRG_PREC_BF16X9 = 2   /* reserved (9 BF16 products): not built, rejected with DMRG_ERR_ARG */
+  DMRG_PREC_BF16X9 = 2   /* chosen form with BF16 parts: every FP64 operand split into three BF16
+                            values, the nine products on the BF16 tensor cores (kind::f16, FP32
+                            accumulation); same FP64 parts and fp64_final rule as 3XTF32 */
 };
 
 typedef struct dmrg_ctx dmrg_ctx;

@@ -1,5 +1,5 @@
-"""Split-precision form (3 x TF32 Heff and environment GEMMs on tcgen05) against the plain FP64
-form.
+"""Split-precision forms (Heff and environment GEMMs on tcgen05 as 3 TF32 products or as 9 BF16
+products) against the plain FP64 form.
 
 One Heff application agrees with FP64 to FP32 accuracy (the split products accumulate in FP32,
 relative 1e-5 here), in the direct form (small lists) and the pre-split form; whole DMRG runs from the same start agree in energy within 1e-8, the
@@ -22,8 +22,12 @@ def _heff(dmrgb, dev, iL, x, precision):
     return y
 
 
+FORMS = [1, 2]        # DMRG_PREC_3XTF32, DMRG_PREC_BF16X9
+
+
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("qn", [False, True])
-def test_split_heff_matches_fp64(dmrgb, ctx, qn):
+def test_split_heff_matches_fp64(dmrgb, ctx, qn, form):
     L, iL = 12, 5
     mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
     if qn:
@@ -41,12 +45,13 @@ def test_split_heff_matches_fp64(dmrgb, ctx, qn):
     assert dmrgb.lib().dmrg_twosite_dims(dev.h, dev.dmpo.h, iL, d) == 0
     x = np.random.default_rng(2).standard_normal(tuple(d))
     y64 = _heff(dmrgb, dev, iL, x, 0)
-    y32 = _heff(dmrgb, dev, iL, x, 1)
+    y32 = _heff(dmrgb, dev, iL, x, form)
     scale = np.max(np.abs(y64))
     assert np.max(np.abs(y32 - y64)) <= 1e-5 * scale
 
 
-def test_split_heff_presplit_form_matches_fp64(dmrgb, ctx):
+@pytest.mark.parametrize("form", FORMS)
+def test_split_heff_presplit_form_matches_fp64(dmrgb, ctx, form):
     """Bond dimension 384 either side: every Heff GEMM list is above 1 GFLOP and takes the
     pre-split form (operands converted once into (hi, lo) pairs). The second GEMM accumulates
     K = d w m = 3840 products in FP32 (ten times the first test's), so the bound is relative 5e-5
@@ -61,22 +66,23 @@ def test_split_heff_presplit_form_matches_fp64(dmrgb, ctx):
     assert tuple(d) == (384, 2, 2, 384)
     x = np.random.default_rng(9).standard_normal(tuple(d))
     y64 = _heff(dmrgb, dev, iL, x, 0)
-    y32 = _heff(dmrgb, dev, iL, x, 1)
+    y32 = _heff(dmrgb, dev, iL, x, form)
     assert np.max(np.abs(y32 - y64)) <= 5e-5 * np.max(np.abs(y64))
 
 
-def test_split_dmrg_energy_within_1e8_of_fp64(dmrgb, ctx):
+@pytest.mark.parametrize("form", ["3xtf32", "bf16x9"])
+def test_split_dmrg_energy_within_1e8_of_fp64(dmrgb, ctx, form):
     L = 16
     mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
     ramp = [16, 32, 64, 64, 64, 64]
     e = {}
-    for prec in ("fp64", "3xtf32"):
+    for prec in ("fp64", form):
         psi = dmrgb.neelMPS(L)
         e[prec] = dmrgb.dmrg(psi, mpo, m=ramp, cutoff=1e-12, precision=prec, ctx=ctx)
-    assert abs(e["3xtf32"] - e["fp64"]) <= 1e-8
+    assert abs(e[form] - e["fp64"]) <= 1e-8
     from oracle import ed, models as om
     ref = ed.sparse_ground_energy(om.make_mpo([om.heisenberg_bulk()] * L, 2))
-    assert abs(e["3xtf32"] - ref) <= 1e-8 * abs(ref)
+    assert abs(e[form] - ref) <= 1e-8 * abs(ref)
 
 
 def test_split_dense_lanczos_k(dmrgb, ctx):
@@ -93,20 +99,23 @@ def test_split_dense_lanczos_k(dmrgb, ctx):
     assert abs(e["3xtf32"] - ref) <= 1e-8 * abs(ref)
 
 
-def test_heff_timing_hook_reports_both_forms(dmrgb, ctx):
+def test_heff_timing_hook_reports_every_form(dmrgb, ctx):
     psi = dmrgb.randMPS(2, 12, 64, seed=5, oc=5)
     mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, 12)
     Lenv, _ = dmrgb.makeEnv(psi, mpo, ctx=ctx)
     dev = Lenv.dev
-    for prec in (0, 1):
+    for prec in (0, 1, 2):
         sec, fl = C.c_double(), C.c_double()
         assert dmrgb.lib().dmrg_test_heff_time(dev.h, dev.dmpo.h, 5, prec, 3, C.byref(sec),
                                                C.byref(fl)) == 0
         assert sec.value > 0 and fl.value > 0
-    assert dmrgb.lib().dmrg_test_heff_time(dev.h, dev.dmpo.h, 5, 2, 1, C.byref(sec), None) == 1
+    # an unknown precision code is refused
+    assert dmrgb.lib().dmrg_test_heff_time(dev.h, dev.dmpo.h, 5, 7, 1, C.byref(sec),
+                                           C.byref(fl)) == dmrgb._lib.ERR_ARG
 
 
-def test_split_environment_updates_match_fp64(dmrgb, ctx):
+@pytest.mark.parametrize("form", ["3xtf32", "bf16x9"])
+def test_split_environment_updates_match_fp64(dmrgb, ctx, form):
     """The environment updates of a split-precision sweep (fp64_final = 0: every update on the
     tensor cores) agree with an FP64 rebuild from the same site tensors to FP32 accuracy: relative
     1e-5 after a chain of 13 updates."""
@@ -115,7 +124,7 @@ def test_split_environment_updates_match_fp64(dmrgb, ctx):
     psi = dmrgb.randMPS(2, L, 128, seed=5)
     dev = dmrgb.DeviceState(psi, mpo.device(ctx))
     dev.env_build()
-    dev.sweep(dmrgb.make_params(maxm=256, cutoff=1e-14, precision="3xtf32", fp64_final=0))
+    dev.sweep(dmrgb.make_params(maxm=256, cutoff=1e-14, precision=form, fp64_final=0))
     assert dev.oc == 0
     R32 = [dev.env(i, False) for i in range(1, L)]
     dev.env_build()                                  # FP64, from the same site tensors
