@@ -131,9 +131,29 @@ def build_workload(pkg):
     return mpo, psi
 
 
-def params(pkg, m, args, profile=0, precision=None):
+def params(pkg, m, args, profile=0, precision=None, tune=True):
     return pkg.make_params(maxm=m, minm=2, cutoff=CUTOFF, krylov=args.krylov,
-                           precision=precision or args.precision, profile=profile)
+                           precision=precision or args.precision, profile=profile, tune=tune)
+
+
+def autotune_report(pkg, ctx, dev, mfin, args, flush):
+    """Tile autotuner on the resident state: profiled sweeps with the tuned tile shapes and with
+    fixed 64 x 64 tiles (the numbers are identical; the GEMM device time and the sweep time are
+    compared), plus the tuner's table size."""
+    rec = {}
+    for name, tune in (("fixed_64x64", False), ("tuned", True)):
+        ms, gs, en = [], [], []
+        for _ in range(3):
+            flush()
+            st = dev.sweep(params(pkg, mfin, args, profile=1, tune=tune))
+            ms.append(st["seconds"] * 1e3)
+            gs.append(st["gemm_seconds"] * 1e3)
+            en.append(st["energy"])
+        rec[name] = {"sweep_ms": min(ms), "heff_gemm_ms": min(gs)}
+    sig, decided, small = ctx.tuner()
+    rec.update({"signatures": sig, "decided": decided, "won_by_32x32": small,
+                "gemm_speedup": rec["fixed_64x64"]["heff_gemm_ms"] / rec["tuned"]["heff_gemm_ms"]})
+    return rec
 
 
 def fp64_gemm_peak(device):
@@ -630,6 +650,7 @@ def run_ours(args, world, rank, local, dist):
     # one extra profiled sweep (CUDA events around every phase and every Heff GEMM launch; not
     # part of the timed steps): phase breakdown and per-launch timing of the dominant kernel
     prof = dev.sweep(params(pkg, mfin, args, profile=1))
+    tuner = autotune_report(pkg, ctx, dev, mfin, args, flush)
     heff_flops = prof["heff_flops"]
     heff_sec = prof["heff_seconds"]
     # chosen form on the same resident state: Heff GEMMs as 3xTF32 on the tensor cores (FP64
@@ -740,6 +761,7 @@ def run_ours(args, world, rank, local, dist):
         "chosen": chosen,
         "heff_forms_m1024": heff_large,
         "tf32_gemm_peak_tflops": tf32_peak,
+        "autotune": tuner,
         "configs": configs,
     }
     print(json.dumps(out))

@@ -23,7 +23,7 @@ class Params(C.Structure):
     _fields_ = [("maxm", C.c_int), ("minm", C.c_int), ("cutoff", C.c_double),
                 ("krylov", C.c_int), ("precision", C.c_int), ("svnbond", C.c_int),
                 ("degen_rtol", C.c_double), ("betatest", C.c_double), ("fp64_final", C.c_int),
-                ("profile", C.c_int), ("cvgE", C.c_int), ("reserved0", C.c_int),
+                ("profile", C.c_int), ("cvgE", C.c_int), ("tune", C.c_int),
                 ("goal", C.c_double), ("reserved", C.c_int * 2)]
 
 
@@ -92,6 +92,7 @@ SIGNATURES = {
     "dmrg_ctx_destroy": (C.c_int, [_P]),
     "dmrg_last_error": (C.c_char_p, [_P]),
     "dmrg_ctx_memory": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "dmrg_ctx_tuner": (C.c_int, [_P, _IP, _IP, _IP]),
     "dmrg_mpo_upload": (C.c_int, [_P, C.c_int, C.c_int, _IP, _IP, _IP, _DPP, _IPP, _IPP,
                                   C.POINTER(_P)]),
     "dmrg_mpo_destroy": (C.c_int, [_P]),

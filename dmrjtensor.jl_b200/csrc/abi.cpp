@@ -117,6 +117,7 @@ void dmrg_params_default(dmrg_params* p) {
   p->fp64_final = 1;
   p->cvgE = 1;
   p->goal = 0.0;
+  p->tune = 1;
 }
 
 const char* dmrg_last_error(const dmrg_ctx* ctx) {
@@ -188,6 +189,23 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaStreamDestroy(c->stream);
   delete c;
   return DMRG_OK;
+}
+
+int dmrg_ctx_tuner(dmrg_ctx* c, int* signatures, int* decided, int* small) {
+  if (!c) return DMRG_ERR_ARG;
+  return guarded(c, [&] {
+    set_device(c);
+    tuner_collect(c);
+    int n = 0, d = 0, s = 0;
+    for (const auto& kv : c->tuner.table) {
+      ++n;
+      if (kv.second.choice >= 0) ++d;
+      if (kv.second.choice == 1) ++s;
+    }
+    if (signatures) *signatures = n;
+    if (decided) *decided = d;
+    if (small) *small = s;
+  });
 }
 
 int dmrg_ctx_memory(const dmrg_ctx* c, size_t* in_use, size_t* peak) {

@@ -107,6 +107,8 @@ struct DescSlot {
 
 struct GemmList {
   bool tA = false, tB = false;
+  uint64_t tune_key = 0;         // block-size histogram signature (0: not tuned)
+  int tune_trial = 0;            // 1: this launch is timed for the tuner
   std::vector<GemmTask> tasks;
   std::vector<GemmSeg> segs;
   int tiles = 0;
@@ -143,8 +145,35 @@ struct CopyList {
 
 }  // namespace dmrg
 
+namespace dmrg {
+// Tile-shape autotuner of the FP64 grouped GEMM. A list's signature quantises its block-size
+// histogram (FLOP-weighted mean M, N and K, task count, total FLOPs, transposes, in half-octave
+// buckets). The first launches of a new signature are timed once in each tile shape (64 x 64 and
+// 32 x 32) with CUDA events; from then on the faster shape is used for that signature (64 x 64
+// unless 32 x 32 is more than 3% faster). Both shapes give bit-identical results, so the choice
+// never changes a number, only the time. The table lives in the context (one device).
+struct GemmTuner {
+  struct Entry {
+    int trials[2] = {0, 0};       // [0] 64 x 64, [1] 32 x 32
+    double best[2] = {1e30, 1e30};
+    int choice = -1;
+  };
+  struct Pending {
+    uint64_t key;
+    int variant;
+    cudaEvent_t a, b;
+  };
+  std::map<uint64_t, Entry> table;
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> free_events;
+  ~GemmTuner();
+};
+}  // namespace dmrg
+
 struct dmrg_ctx {
   int device = 0;
+  bool tune = true;              // FP64 GEMM tile autotuner on (dmrg_params.tune of the sweep)
+  dmrg::GemmTuner tuner;
   cudaStream_t stream = nullptr;
   size_t budget = 0, in_use = 0, peak = 0;
   std::string err;
@@ -236,6 +265,11 @@ struct Upload {
 // device fault.
 void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
               const double* B, int64_t nB, double* C, int64_t nC);
+// Picks the FP64 tile shape of a list (before its upload): retiles it to 32 x 32 when the tuner
+// says so or while that shape is on trial, and marks trial launches for timing.
+void tune_gemm(dmrg_ctx* c, GemmList& g);
+// Folds the timings of completed trial launches into the tuner (no synchronisation).
+void tuner_collect(dmrg_ctx* c);
 // The same list on a split-precision tcgen05 kernel (form SPLIT_TF32X3 or SPLIT_BF16X9); the list
 // must be retiled. Lists of at least SPLIT_PRESPLIT_FLOPS convert their operands once into split
 // records first.

@@ -116,6 +116,8 @@ void prepare_split(HeffPlan& hp) {
 
 void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision) {
   if (split_form(precision) && !hp.split) prepare_split(hp);
+  tune_gemm(c, hp.g1);
+  tune_gemm(c, hp.g3);
   Upload u;
   u.put(hp.g1);
   u.put(hp.mix);
@@ -473,6 +475,8 @@ void lupdate(dmrg_state* st, int i, double* flops, int precision) {
   if (!st->Lvalid[i]) fail(DMRG_ERR_STATE, "lupdate: Lenv[site] has not been built");
   StepPlan sp;
   plan_left_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Llay[i], sp);
+  tune_gemm(c, sp.g1);
+  tune_gemm(c, sp.g3);
   Upload u;
   put_step(u, sp, split_form(precision));
   char* db = u.send(c, 2);
@@ -492,6 +496,8 @@ void rupdate(dmrg_state* st, int i, double* flops, int precision) {
   if (!st->Rvalid[i]) fail(DMRG_ERR_STATE, "rupdate: Renv[site] has not been built");
   StepPlan sp;
   plan_right_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i], st->Rlay[i], sp);
+  tune_gemm(c, sp.g1);
+  tune_gemm(c, sp.g3);
   Upload u;
   put_step(u, sp, split_form(precision));
   char* db = u.send(c, 2);

@@ -1,5 +1,6 @@
 // engine_layout.cpp -- block layouts, device memory, descriptor upload, launch wrappers.
 #include <algorithm>
+#include <cmath>
 #include <map>
 
 #include "engine.hpp"
@@ -341,10 +342,99 @@ void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int6
       if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
     }
   }
-  if (g.bm != GEMM_BM) bad_plan("gemm tiling");
-  launch_gemm_f64(c->stream, g.tA, g.tB, A, B, C,
+  if ((g.bm != GEMM_BM || g.bn != GEMM_BN) &&
+      (g.bm != GEMM_SMALL_TILE || g.bn != GEMM_SMALL_TILE))
+    bad_plan("gemm tiling");
+  GemmTuner::Pending tp{};
+  const bool timed = g.tune_trial && g.tune_key != 0;
+  if (timed) {
+    for (cudaEvent_t* e : {&tp.a, &tp.b}) {
+      if (!c->tuner.free_events.empty()) {
+        *e = c->tuner.free_events.back();
+        c->tuner.free_events.pop_back();
+      } else {
+        cuda_check(cudaEventCreate(e), "tuner event");
+      }
+    }
+    tp.key = g.tune_key;
+    tp.variant = g.bm == GEMM_SMALL_TILE ? 1 : 0;
+    cudaEventRecord(tp.a, c->stream);
+  }
+  launch_gemm_f64(c->stream, g.bm, g.tA, g.tB, A, B, C,
                   reinterpret_cast<const GemmTask*>(dbase + g.t_off), int(g.tasks.size()),
                   reinterpret_cast<const GemmSeg*>(dbase + g.s_off), g.tiles, c->nsm * 4);
+  if (timed) {
+    cudaEventRecord(tp.b, c->stream);
+    c->tuner.pending.push_back(tp);
+  }
+}
+
+GemmTuner::~GemmTuner() {
+  for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+  for (cudaEvent_t e : free_events) cudaEventDestroy(e);
+}
+
+namespace {
+int half_octave(double x) { return x <= 1.0 ? 0 : int(std::floor(2.0 * std::log2(x))) + 1; }
+}  // namespace
+
+void tune_gemm(dmrg_ctx* c, GemmList& g) {
+  g.tune_key = 0;
+  g.tune_trial = 0;
+  if (!c->tune || g.tasks.empty() || g.flops <= 0) return;
+  double wm = 0, wn = 0, wk = 0, w = 0;
+  for (const GemmTask& t : g.tasks) {
+    if (t.M <= 0 || t.N <= 0) continue;
+    for (int q = 0; q < t.nseg; ++q) {
+      const GemmSeg& s = g.segs[t.seg0 + q];
+      const double f = double(t.M) * t.N * s.K;
+      wm += f * t.M; wn += f * t.N; wk += f * s.K; w += f;
+    }
+  }
+  if (w <= 0) return;
+  uint64_t key = 1;
+  for (int v : {int(g.tA), int(g.tB), half_octave(wm / w), half_octave(wn / w), half_octave(wk / w),
+                half_octave(double(g.tasks.size())), half_octave(g.flops)})
+    key = key * 131 + uint64_t(v & 0xff);
+  g.tune_key = key;
+  GemmTuner::Entry& e = c->tuner.table[key];
+  int v = e.choice;
+  if (v < 0) {   // on trial: the shape with fewer finished or pending trials
+    int pend[2] = {0, 0};
+    for (const auto& p : c->tuner.pending)
+      if (p.key == key) pend[p.variant] += 1;
+    v = (e.trials[0] + pend[0] <= e.trials[1] + pend[1]) ? 0 : 1;
+    g.tune_trial = 1;
+  }
+  if (v == 1) g = [&] {
+    GemmList r = retile(g, GEMM_SMALL_TILE, GEMM_SMALL_TILE);
+    r.tune_key = g.tune_key;
+    r.tune_trial = g.tune_trial;
+    return r;
+  }();
+}
+
+void tuner_collect(dmrg_ctx* c) {
+  auto& P = c->tuner.pending;
+  size_t keep = 0;
+  for (size_t i = 0; i < P.size(); ++i) {
+    GemmTuner::Pending& p = P[i];
+    if (cudaEventQuery(p.b) != cudaSuccess) {
+      cudaGetLastError();     // not ready is not an error
+      P[keep++] = p;
+      continue;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    GemmTuner::Entry& e = c->tuner.table[p.key];
+    e.trials[p.variant] += 1;
+    e.best[p.variant] = std::min(e.best[p.variant], double(ms));
+    if (e.choice < 0 && e.trials[0] > 0 && e.trials[1] > 0)
+      e.choice = (e.best[1] < 0.97 * e.best[0]) ? 1 : 0;
+    c->tuner.free_events.push_back(p.a);
+    c->tuner.free_events.push_back(p.b);
+  }
+  P.resize(keep);
 }
 
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,

@@ -160,6 +160,9 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
       }
   const bool split = split_form(P.precision) != 0;
   if (split) prepare_split(hp);
+  tune_gemm(c, hp.g1);
+  tune_gemm(c, hp.g3);
+  tune_gemm(c, gaa);
   Upload u;
   u.put(hp.g1);
   u.put(hp.mix);
@@ -346,6 +349,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     const int K2 = j > 0 ? g.np : g.n;
     if (K2 > 0) grho.seg(g.moff, g.n, g.moff, g.n, K2);
   }
+  tune_gemm(c, grho);
   Upload u2;
   u2.put(gather);
   u2.put(grho);
@@ -371,6 +375,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   const auto w0 = std::chrono::steady_clock::now();
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
   so.wait = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+  tuner_collect(c);
   so.energy = c->h_scal[lz::EN];
   if (fp64_energy && c->h_scal[lz::KK] > 0) so.energy = c->h_scal[lz::KH] / c->h_scal[lz::KK];
   if (split) {
@@ -456,6 +461,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
       }
     }
   }
+  tune_gemm(c, gs);
   Upload u3;
   u3.put(cp);
   u3.put(gs);
@@ -490,6 +496,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   if (L < 2) fail(DMRG_ERR_SHAPE, "a two-site sweep needs at least two sites");
   if (!st->env_built) fail(DMRG_ERR_STATE, "call dmrg_env_build before dmrg_sweep");
   std::memset(&out, 0, sizeof(out));
+  c->tune = P.tune != 0;
   const int svn = P.svnbond > 0 ? P.svnbond : (L + 1) / 2;
   const int svn_site = std::min(std::max(2, svn + 1), L) - 1;   // 0-based i of SvNcheck!
   const auto h0 = std::chrono::steady_clock::now();
@@ -537,6 +544,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   const int t1 = tm.record();
   cuda_check(cudaEventSynchronize(tm.event(t1)), "sweep sync");
   if (split_form(P.precision)) check_mma_status(c);   // the last environment update
+  tuner_collect(c);
   float ms = 0;
   cudaEventElapsedTime(&ms, tm.event(t0), tm.event(t1));
   out.seconds = ms * 1e-3;

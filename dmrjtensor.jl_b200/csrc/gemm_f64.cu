@@ -16,11 +16,17 @@
 namespace dmrg {
 namespace {
 
-constexpr int BM = GEMM_BM, BN = GEMM_BN, BK = GEMM_BK;
+constexpr int BK = GEMM_BK;
 constexpr int STAGES = 3, PAD = 4, THREADS = 128;
-constexpr int LDS_A = BM + PAD;   // 68 doubles: rows of a k-slice are 8 banks apart (no conflicts)
-constexpr int LDS_B = BN + PAD;
-constexpr size_t SMEM_BYTES = size_t(STAGES) * BK * (LDS_A + LDS_B) * sizeof(double);
+
+template <int BM, int BN>
+struct F64Tile {
+  static constexpr int LDS_A = BM + PAD;   // k-slices of A / B in shared memory, padded rows
+  static constexpr int LDS_B = BN + PAD;
+  static constexpr size_t SMEM = size_t(STAGES) * BK * (LDS_A + LDS_B) * sizeof(double);
+  static constexpr int MI = BM / 16, NI = BN / 16;   // m8n8 fragments per warp (2 x 2 warps)
+  static constexpr int A_PER = BM * BK / THREADS, B_PER = BN * BK / THREADS;
+};
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -39,11 +45,14 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <bool TA, bool TB>
+template <int BM, int BN, bool TA, bool TB>
 __global__ void __launch_bounds__(THREADS)
 k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
            const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
            int total_tiles) {
+  using TL = F64Tile<BM, BN>;
+  constexpr int LDS_A = TL::LDS_A, LDS_B = TL::LDS_B, MI = TL::MI, NI = TL::NI;
+  constexpr int A_PER = TL::A_PER, B_PER = TL::B_PER;
   extern __shared__ double smem[];
   double* As = smem;
   double* Bs = smem + STAGES * BK * LDS_A;
@@ -64,11 +73,11 @@ k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* _
     int nsteps = 0;
     for (int q = 0; q < tk.nseg; ++q) nsteps += (segs[tk.seg0 + q].K + BK - 1) / BK;
 
-    double acc[4][4][2];
+    double acc[MI][NI][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+      for (int j = 0; j < NI; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     int p_seg = 0, p_k = 0;  // producer cursor
     auto issue = [&](int stage) {
@@ -78,39 +87,25 @@ k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* _
       const double* Bb = B + sg.b_off;
       double* as = As + stage * BK * LDS_A;
       double* bs = Bs + stage * BK * LDS_B;
-      if (!TA) {  // A(i,k) = Ab[i + k*lda]
-        const int i = tid & 63, kq = tid >> 6;
+      // thread e = tid + THREADS r covers element (i, k) of the A slice (rows fastest unless A is
+      // stored K-contiguous) and (k, j) of the B slice (K fastest unless B is stored N-contiguous)
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int k = kq + 2 * r, gi = m0 + i, gk = p_k + k;
-          const bool ok = gi < tk.M && gk < sg.K;
-          cp_async8(&as[k * LDS_A + i], ok ? Ab + gi + int64_t(gk) * sg.lda : Ab, ok);
-        }
-      } else {    // A(i,k) = Ab[k + i*lda]
-        const int k = tid & 15, iq = tid >> 4;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int i = iq + 8 * r, gi = m0 + i, gk = p_k + k;
-          const bool ok = gi < tk.M && gk < sg.K;
-          cp_async8(&as[k * LDS_A + i], ok ? Ab + gk + int64_t(gi) * sg.lda : Ab, ok);
-        }
+      for (int r = 0; r < A_PER; ++r) {
+        const int e = tid + THREADS * r;
+        const int i = TA ? e / BK : e % BM, k = TA ? e % BK : e / BM;
+        const int gi = m0 + i, gk = p_k + k;
+        const bool ok = gi < tk.M && gk < sg.K;
+        const double* src = TA ? Ab + gk + int64_t(gi) * sg.lda : Ab + gi + int64_t(gk) * sg.lda;
+        cp_async8(&as[k * LDS_A + i], ok ? src : Ab, ok);
       }
-      if (!TB) {  // B(k,j) = Bb[k + j*ldb]
-        const int k = tid & 15, jq = tid >> 4;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int j = jq + 8 * r, gj = n0 + j, gk = p_k + k;
-          const bool ok = gj < tk.N && gk < sg.K;
-          cp_async8(&bs[k * LDS_B + j], ok ? Bb + gk + int64_t(gj) * sg.ldb : Bb, ok);
-        }
-      } else {    // B(k,j) = Bb[j + k*ldb]
-        const int j = tid & 63, kq = tid >> 6;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int k = kq + 2 * r, gj = n0 + j, gk = p_k + k;
-          const bool ok = gj < tk.N && gk < sg.K;
-          cp_async8(&bs[k * LDS_B + j], ok ? Bb + gj + int64_t(gk) * sg.ldb : Bb, ok);
-        }
+      for (int r = 0; r < B_PER; ++r) {
+        const int e = tid + THREADS * r;
+        const int j = TB ? e % BN : e / BK, k = TB ? e / BN : e % BK;
+        const int gj = n0 + j, gk = p_k + k;
+        const bool ok = gj < tk.N && gk < sg.K;
+        const double* src = TB ? Bb + gj + int64_t(gk) * sg.ldb : Bb + gk + int64_t(gj) * sg.ldb;
+        cp_async8(&bs[k * LDS_B + j], ok ? src : Bb, ok);
       }
       p_k += BK;
     };
@@ -130,15 +125,15 @@ k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* _
       const double* bs = Bs + (step % STAGES) * BK * LDS_B;
 #pragma unroll
       for (int kk = 0; kk < BK; kk += 4) {
-        double a[4], b[4];
+        double a[MI], b[NI];
 #pragma unroll
-        for (int mi = 0; mi < 4; ++mi) a[mi] = as[(kk + t) * LDS_A + wm * 32 + mi * 8 + g];
+        for (int mi = 0; mi < MI; ++mi) a[mi] = as[(kk + t) * LDS_A + wm * (BM / 2) + mi * 8 + g];
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) b[ni] = bs[(kk + t) * LDS_B + wn * 32 + ni * 8 + g];
+        for (int ni = 0; ni < NI; ++ni) b[ni] = bs[(kk + t) * LDS_B + wn * (BN / 2) + ni * 8 + g];
 #pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
+        for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+          for (int ni = 0; ni < NI; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
       }
     }
     cp_wait<0>();
@@ -146,14 +141,14 @@ k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* _
 
     double* Cb = C + tk.c_off;
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
-      const int row = m0 + wm * 32 + mi * 8 + g;
+    for (int mi = 0; mi < MI; ++mi) {
+      const int row = m0 + wm * (BM / 2) + mi * 8 + g;
       if (row >= tk.M) continue;
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
+      for (int ni = 0; ni < NI; ++ni) {
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int col = n0 + wn * 32 + ni * 8 + 2 * t + e;
+          const int col = n0 + wn * (BN / 2) + ni * 8 + 2 * t + e;
           if (col < tk.N) {
             const int64_t idx = row + int64_t(col) * tk.ldc;
             double v = tk.alpha * acc[mi][ni][e];
@@ -166,30 +161,41 @@ k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* _
   }
 }
 
-template <bool TA, bool TB>
+template <int BM, int BN, bool TA, bool TB>
 void launch_variant(cudaStream_t s, const double* A, const double* B, double* C,
                     const GemmTask* tasks, int ntasks, const GemmSeg* segs, int total_tiles,
                     int grid_cap) {
-  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_f64<TA, TB>), SMEM_BYTES);
+  constexpr size_t SM = F64Tile<BM, BN>::SMEM;
+  raise_smem_limit(reinterpret_cast<const void*>(k_gemm_f64<BM, BN, TA, TB>), SM);
   int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_f64<TA, TB><<<grid, THREADS, SMEM_BYTES, s>>>(A, B, C, tasks, ntasks, segs, total_tiles);
+  k_gemm_f64<BM, BN, TA, TB><<<grid, THREADS, SM, s>>>(A, B, C, tasks, ntasks, segs, total_tiles);
   count_launch();
+}
+
+template <int BM, int BN>
+void dispatch_f64(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
+                  double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
+                  int total_tiles, int grid_cap) {
+  if (!transA && !transB)
+    launch_variant<BM, BN, false, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  else if (!transA && transB)
+    launch_variant<BM, BN, false, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  else if (transA && !transB)
+    launch_variant<BM, BN, true, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  else
+    launch_variant<BM, BN, true, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
 }
 
 }  // namespace
 
-void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
-                     double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
-                     int total_tiles, int grid_cap) {
+void launch_gemm_f64(cudaStream_t s, int tile, bool transA, bool transB, const double* A,
+                     const double* B, double* C, const GemmTask* tasks, int ntasks,
+                     const GemmSeg* segs, int total_tiles, int grid_cap) {
   if (total_tiles <= 0 || ntasks <= 0) return;
-  if (!transA && !transB)
-    launch_variant<false, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
-  else if (!transA && transB)
-    launch_variant<false, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
-  else if (transA && !transB)
-    launch_variant<true, false>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+  if (tile == 32)
+    dispatch_f64<32, 32>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
   else
-    launch_variant<true, true>(s, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
+    dispatch_f64<64, 64>(s, transA, transB, A, B, C, tasks, ntasks, segs, total_tiles, grid_cap);
 }
 
 // Raises (never lowers) the dynamic shared-memory limit of a kernel on the current device. The

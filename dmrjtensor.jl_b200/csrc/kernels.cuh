@@ -91,11 +91,14 @@ void launch_trid_mid_vectors(cudaStream_t s, double* base, const TridTask* tasks
                              int max_n, int max_k, double* xws);
 
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
+constexpr int GEMM_SMALL_TILE = 32;   // the second tile shape of the FP64 GEMM (32 x 32)
 
-// Persistent grouped FP64 GEMM (DMMA m8n8k4 tensor-core path).
-void launch_gemm_f64(cudaStream_t s, bool transA, bool transB, const double* A, const double* B,
-                     double* C, const GemmTask* tasks, int ntasks, const GemmSeg* segs,
-                     int total_tiles, int grid_cap);
+// Persistent grouped FP64 GEMM (DMMA m8n8k4 tensor-core path), square tiles of `tile` = 64 or
+// 32 (the task list's tile counts must match). Every output element accumulates its K products
+// in the same order for both tile shapes, so the results are bit-identical.
+void launch_gemm_f64(cudaStream_t s, int tile, bool transA, bool transB, const double* A,
+                     const double* B, double* C, const GemmTask* tasks, int ntasks,
+                     const GemmSeg* segs, int total_tiles, int grid_cap);
 
 // Split-precision grouped GEMM on tcgen05 (FP32 accumulation in TMEM, FP64 in/out), tiles of
 // TF32_TILE_M x (64 or 128): form SPLIT_TF32X3 = three TF32 products, SPLIT_BF16X9 = nine BF16

@@ -31,6 +31,12 @@ class Context:
         self.h = h
         self.device = device
 
+    def tuner(self):
+        """FP64 GEMM tile autotuner: (signatures seen, decided, won by 32 x 32 tiles)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().dmrg_ctx_tuner(self.h, C.byref(a), C.byref(b), C.byref(c)), self.h)
+        return a.value, b.value, c.value
+
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()
         check(lib().dmrg_ctx_memory(self.h, C.byref(a), C.byref(b)), self.h)
@@ -403,7 +409,8 @@ class DeviceState:
 
 
 def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
-                degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0, goal=0.0, cvgE=True):
+                degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0, goal=0.0, cvgE=True,
+                tune=True):
     p = Params()
     lib().dmrg_params_default(C.byref(p))
     p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)
@@ -413,6 +420,7 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
         float(betatest), int(fp64_final)
     p.profile = int(profile)
     p.goal, p.cvgE = float(goal), 1 if cvgE else 0
+    p.tune = 1 if tune else 0
     return p
 
 

@@ -87,7 +87,8 @@ typedef struct dmrg_params {
   int fp64_final;    /* chosen forms: 1 = re-evaluate the Ritz energy with one FP64 matvec */
   int profile;       /* 1 = time every Heff GEMM launch with CUDA events (gemm_* stats)  */
   int cvgE;          /* convergence test of dmrgcvg (algs/DMRG.jl:610-652): 1 = energy, 0 = entropy */
-  int reserved0;
+  int tune;          /* 1 (default): FP64 GEMM tile shapes picked per block-size histogram by the
+                        context's autotuner (timed trials, bit-identical results); 0: 64 x 64 */
   double goal;       /* > 0: the sweep reports `converged` when |E - E_last| < goal (cvgE = 1) or
                         |S - S_last| < goal (cvgE = 0); E_last starts at <psi|H|psi> of the state
                         the environments were built for (startval, algs/optimizeMPS.jl:255-258,
@@ -131,6 +132,10 @@ DMRG_API const char* dmrg_last_error(const dmrg_ctx* ctx);
 DMRG_API long long dmrg_kernel_launches(void);
 /* Bytes currently allocated on the device by this context, and its peak. */
 DMRG_API int dmrg_ctx_memory(const dmrg_ctx* ctx, size_t* in_use, size_t* peak);
+/* The FP64 GEMM tile autotuner of the context (no reference counterpart): *signatures = block-size
+ * histograms seen, *decided = of which both tile shapes were timed, *small = of which 32 x 32
+ * tiles won. Any pointer may be NULL. */
+DMRG_API int dmrg_ctx_tuner(dmrg_ctx* ctx, int* signatures, int* decided, int* small);
 
 /* ---------------------------------------------------------------- MPO (MPO(...), makeMPO, makeqMPO)
  * W[i]: column-major [wl[i], d[i], d[i], wr[i]] doubles (lib/MPO/makeMPO.jl:59-92 layout).

@@ -126,3 +126,24 @@ def test_tridiagonal_eigensolver(dmrgb, ctx, case):
         assert np.max(np.abs(M @ Uk - Uk * lam[:k])) < 1e-12 * nrm
         ow += n
         ou += n * k
+
+
+def test_tile_autotuner_keeps_every_number(dmrgb, ctx):
+    """The FP64 GEMM tile autotuner (64 x 64 or 32 x 32 tiles per block-size histogram) changes
+    only the time: a U(1) run with it and one with fixed 64 x 64 tiles agree bit for bit, and the
+    tuner has timed both shapes for the histograms it met."""
+    L = 40
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    out = {}
+    for tune in (False, True):
+        dev = dmrgb.DeviceState(dmrgb.neelMPS(L), mpo.device(ctx))
+        dev.env_build()
+        st = [dev.sweep(dmrgb.make_params(maxm=m, cutoff=1e-12, tune=tune))
+              for m in (16, 32, 64, 64, 64)]
+        out[tune] = ([s["energy"] for s in st], [s["max_truncerr"] for s in st],
+                     dev.site_blocks(L // 2))
+    assert out[True][0] == out[False][0]
+    assert out[True][1] == out[False][1]
+    assert np.array_equal(out[True][2], out[False][2])
+    sig, decided, small = ctx.tuner()
+    assert sig > 0 and decided > 0 and 0 <= small <= decided
