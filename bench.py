@@ -255,11 +255,10 @@ class OracleSweeps:
         return time.perf_counter() - t0
 
 
-def run_serving(pkg, device, nreq, rate=20.0, slots=8, seed=5):
-    """Serving workload (transverse-field Ising chains, Poisson arrivals): requests are submitted
-    at their arrival times to a server with `slots` concurrent solves and a 150 GB budget;
-    returns solves/s over the whole run (first arrival to last completion) and the latency
-    percentiles (submit to completion)."""
+def serving_requests(pkg, nreq, seed=5, rate=20.0):
+    """The serving workload: transverse-field Ising chains H = -sum Z Z - h sum X with h ~ U[0.5,
+    1.5], L in {16, 32, 64, 128}, maxm in {64, 128, 256, 512}, |+...+> start, Poisson arrival
+    gaps at `rate` per second (all from default_rng(seed))."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, nreq)
     hs = rng.uniform(0.5, 1.5, nreq)
@@ -270,30 +269,48 @@ def run_serving(pkg, device, nreq, rate=20.0, slots=8, seed=5):
         mpo = pkg.makeMPO(pkg.tfiMPO(h=float(h)), 2, int(L))
         psi = pkg.MPS([np.full((1, 2, 1), 1 / math.sqrt(2)) for _ in range(int(L))], oc=0)
         reqs.append((psi, mpo, int(m)))
+    return reqs, gaps
+
+
+def run_serving(pkg, device, nreq, rate=20.0, slots=16, seed=5, saturate=False, precision="fp64",
+                batched=True):
+    """Serving workload: requests submitted at their Poisson arrival times (or all at once when
+    `saturate`, which measures capacity instead of offered load) to a server with `slots`
+    concurrent solves (16: measured capacity flattens there, 35 solves/s with or without shared
+    launches, while 8 slots with shared launches lose a quarter) and a 150 GB budget; returns solves/s over the whole run (first submission
+    to last completion), the latency percentiles (submit to completion) and how many solves the
+    shared Heff launches carried on average."""
+    reqs, gaps = serving_requests(pkg, nreq, seed, rate)
     lat = []
-    with pkg.Server(device=device, slots=slots, hbm_budget=150 * 10**9) as srv:
+    with pkg.Server(device=device, slots=slots, hbm_budget=150 * 10**9, batched=batched) as srv:
         t0 = time.perf_counter()
         tick = []
         arrival = t0
         for (psi, mpo, m), g in zip(reqs, gaps):
-            arrival += g
-            now = time.perf_counter()
-            if arrival > now:
-                time.sleep(arrival - now)
-            tick.append((srv.submit(psi, mpo, m=m, sweeps=6, cutoff=CUTOFF), time.perf_counter()))
+            if not saturate:
+                arrival += g
+                now = time.perf_counter()
+                if arrival > now:
+                    time.sleep(arrival - now)
+            tick.append((srv.submit(psi, mpo, m=m, sweeps=6, cutoff=CUTOFF, precision=precision),
+                         time.perf_counter()))
         for t, ts in tick:
             st = srv.poll(t, -1)
             if st["status"] != 2:
                 raise RuntimeError(f"served solve failed: {st}")
             lat.append(st["queue_seconds"] + st["run_seconds"])
         t1 = time.perf_counter()
+        batches, carried = srv.stats()
     lat.sort()
     pct = lambda q: lat[min(len(lat) - 1, int(math.ceil(q * len(lat))) - 1)]
     return {"workload": "TFI chains, h~U[0.5,1.5], L in {16,32,64,128}, maxm in {64,128,256,512}, "
-                        "6 sweeps, cutoff 1e-10, |+...+> start, Poisson arrivals",
-            "requests": nreq, "arrival_rate_per_s": rate, "slots": slots,
+                        "6 sweeps, cutoff 1e-10, |+...+> start, " +
+                        ("all submitted at once (capacity)" if saturate else "Poisson arrivals"),
+            "requests": nreq, "arrival_rate_per_s": None if saturate else rate, "slots": slots,
+            "precision": precision, "shared_heff_launches": batched,
             "solves_per_s": nreq / (t1 - t0), "p50_latency_s": pct(0.50),
-            "p99_latency_s": pct(0.99), "mean_latency_s": statistics.mean(lat)}
+            "p99_latency_s": pct(0.99), "mean_latency_s": statistics.mean(lat),
+            "solves_per_shared_launch": (carried / batches) if batches else None}
 
 
 def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
@@ -708,7 +725,14 @@ def run_ours(args, world, rank, local, dist):
                "seconds_per_step": statistics.mean(e2e_times)}
     meas = (run_measurements(pkg, ctx, dev, mpo, energy, cpu=not args.no_cpu)
             if args.measure else None)
-    serving = run_serving(pkg, local, args.serve_requests) if args.serve_requests > 0 else None
+    serving = None
+    if args.serve_requests > 0:
+        serving = {"poisson_fp64": run_serving(pkg, local, args.serve_requests),
+                   "capacity_fp64": run_serving(pkg, local, args.serve_saturate, saturate=True),
+                   "capacity_fp64_own_launches": run_serving(pkg, local, args.serve_saturate,
+                                                             saturate=True, batched=False),
+                   "capacity_3xtf32": run_serving(pkg, local, args.serve_saturate, saturate=True,
+                                                  precision="3xtf32")}
     heff_large = heff_forms(pkg, ctx) if args.chosen else None
     if rank != 0:
         return
@@ -793,7 +817,12 @@ def main():
     ap.add_argument("--no-measure", dest="measure", action="store_false",
                     help="skip the expect / correlationmatrix measurement")
     ap.add_argument("--serve-requests", type=int, default=200,
-                    help="requests of the serving measurement (0: skip it)")
+                    help="requests of the Poisson serving measurement (0: skip serving)")
+    ap.add_argument("--serve-saturate", type=int, default=200,
+                    help="requests of the capacity runs (all submitted at once)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="only the serving measurements (--serve-requests Poisson arrivals, FP64 "
+                         "and 3xTF32, plus the capacity runs)")
     ap.add_argument("--ramp-sweeps", type=int, default=None,
                     help="untimed ramp sweeps before the timed ones (default: the full 11-sweep "
                          "ramp); fewer only for profiler runs")
@@ -802,6 +831,15 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.serve_only:
+            pkg = load_pkg()
+            out = {}
+            for prec in ("fp64", "3xtf32"):
+                out[f"poisson_{prec}"] = run_serving(pkg, local, args.serve_requests,
+                                                     precision=prec)
+                out[f"capacity_{prec}"] = run_serving(pkg, local, args.serve_saturate,
+                                                      saturate=True, precision=prec)
+            print(json.dumps({"serving": out}))
         elif args.heff_only:
             # the plain and split Heff forms alone (the kernel-profiling case)
             pkg = load_pkg()

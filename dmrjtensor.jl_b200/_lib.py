@@ -46,7 +46,7 @@ class SweepStats(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("slots", C.c_int), ("hbm_budget_bytes", C.c_size_t),
-                ("reserved", C.c_int * 8)]
+                ("unbatched", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class Request(C.Structure):
@@ -131,6 +131,7 @@ SIGNATURES = {
     "dmrg_server_release": (C.c_int, [_P, C.c_longlong]),
     "dmrg_server_destroy": (C.c_int, [_P]),
     "dmrg_server_last_error": (C.c_char_p, [_P]),
+    "dmrg_server_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
 }
 
 _lib = None

@@ -146,6 +146,7 @@ struct CopyList {
 }  // namespace dmrg
 
 namespace dmrg {
+struct HeffBatcher;   // shared Heff launches of a server's solves (batch.cpp)
 // Tile-shape autotuner of the FP64 grouped GEMM. A list's signature quantises its block-size
 // histogram (FLOP-weighted mean M, N and K, task count, total FLOPs, transposes, in half-octave
 // buckets). The first launches of a new signature are timed once in each tile shape (64 x 64 and
@@ -173,6 +174,8 @@ struct GemmTuner {
 struct dmrg_ctx {
   int device = 0;
   bool tune = true;              // FP64 GEMM tile autotuner on (dmrg_params.tune of the sweep)
+  dmrg::HeffBatcher* batch = nullptr;   // server contexts: the shared Heff batcher
+  bool batch_on = false;         // inside a served solve's sweeps: Heff goes to the batcher
   dmrg::GemmTuner tuner;
   cudaStream_t stream = nullptr;
   size_t budget = 0, in_use = 0, peak = 0;
@@ -265,6 +268,9 @@ struct Upload {
 // device fault.
 void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
               const double* B, int64_t nB, double* C, int64_t nC);
+// The launch wrappers' bounds checks alone (DMRG_ERR_ARG on a violation).
+void check_gemm_list(const GemmList& g, int64_t nA, int64_t nB, int64_t nC);
+void check_mix_list(const MixList& m, int64_t nin, int64_t nout);
 // Picks the FP64 tile shape of a list (before its upload): retiles it to 32 x 32 when the tuner
 // says so or while that shape is on trial, and marks trial launches for timing.
 void tune_gemm(dmrg_ctx* c, GemmList& g);
@@ -322,6 +328,16 @@ void prepare_split(HeffPlan& hp);
 void check_mma_status(dmrg_ctx* c);
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
                 int precision, GemmProfile* prof = nullptr);
+
+// ---- shared Heff launches across the solves of a server (batch.cpp)
+HeffBatcher* batcher_create(int device);
+void batcher_destroy(HeffBatcher* b);
+void batcher_enter(HeffBatcher* b);   // a solve starts its sweeps
+void batcher_leave(HeffBatcher* b);   // ... and ends them
+void batcher_stats(HeffBatcher* b, long long* batches, long long* contributions);
+// y = Heff x of one solve, run inside the batcher's next shared launch.
+void batched_heff(dmrg_ctx* c, dmrg_state* st, int iL, const HeffPlan& hp, const double* x,
+                  double* y, int precision);
 
 // Heff with every intermediate in the library's fixed device array (noalloc.cu).
 void heff_apply_noalloc(dmrg_state* st, int iL, const double* in_dev, double* out_dev);

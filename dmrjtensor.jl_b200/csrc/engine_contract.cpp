@@ -158,6 +158,10 @@ GemmProfile::~GemmProfile() { for (auto e : pool) cudaEventDestroy(e); }
 void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, double* y,
                 int precision, GemmProfile* prof) {
   dmrg_ctx* c = st->ctx;
+  if (c->batch && c->batch_on) {   // a served solve: the server's shared launch
+    batched_heff(c, st, iL, hp, x, y, precision);
+    return;
+  }
   ensure(c, c->X, std::max<int64_t>(hp.x_size, 1));
   ensure(c, c->Y, std::max<int64_t>(hp.y_size, 1));
   const int64_t n = hp.tl.size;

@@ -328,9 +328,7 @@ inline bool in_range(int64_t off, int64_t last, int64_t n) { return off >= 0 && 
 }
 }  // namespace
 
-void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
-              const double* B, int64_t nB, double* C, int64_t nC) {
-  if (g.tiles == 0) return;
+void check_gemm_list(const GemmList& g, int64_t nA, int64_t nB, int64_t nC) {
   for (const GemmTask& t : g.tasks) {
     if (t.M <= 0 || t.N <= 0) continue;
     if (t.ldc < t.M || !in_range(t.c_off, (t.M - 1) + int64_t(t.N - 1) * t.ldc, nC)) bad_plan("gemm C");
@@ -342,6 +340,25 @@ void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int6
       if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
     }
   }
+}
+
+void check_mix_list(const MixList& m, int64_t nin, int64_t nout) {
+  for (const MixTask& t : m.tasks) {
+    if (t.rows <= 0 || t.cols <= 0) continue;
+    const int64_t ext = (t.rows - 1) + int64_t(t.cols - 1) * t.ld;
+    if (t.ld < t.rows || !in_range(t.out_off, ext, nout)) bad_plan("mix out");
+    for (int q = 0; q < t.nterm; ++q) {
+      const MixTerm& tm = m.terms[t.term0 + q];
+      if (tm.ld < t.rows || !in_range(tm.in_off, (t.rows - 1) + int64_t(t.cols - 1) * tm.ld, nin))
+        bad_plan("mix in");
+    }
+  }
+}
+
+void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
+              const double* B, int64_t nB, double* C, int64_t nC) {
+  if (g.tiles == 0) return;
+  check_gemm_list(g, nA, nB, nC);
   if ((g.bm != GEMM_BM || g.bn != GEMM_BN) &&
       (g.bm != GEMM_SMALL_TILE || g.bn != GEMM_SMALL_TILE))
     bad_plan("gemm tiling");
@@ -478,16 +495,7 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
 void run_mix(dmrg_ctx* c, const MixList& m, char* dbase, const double* in, int64_t nin,
              double* out, int64_t nout) {
   if (m.tiles == 0) return;
-  for (const MixTask& t : m.tasks) {
-    if (t.rows <= 0 || t.cols <= 0) continue;
-    const int64_t ext = (t.rows - 1) + int64_t(t.cols - 1) * t.ld;
-    if (t.ld < t.rows || !in_range(t.out_off, ext, nout)) bad_plan("mix out");
-    for (int q = 0; q < t.nterm; ++q) {
-      const MixTerm& tm = m.terms[t.term0 + q];
-      if (tm.ld < t.rows || !in_range(tm.in_off, (t.rows - 1) + int64_t(t.cols - 1) * tm.ld, nin))
-        bad_plan("mix in");
-    }
-  }
+  check_mix_list(m, nin, nout);
   launch_mix(c->stream, in, out, reinterpret_cast<const MixTask*>(dbase + m.t_off),
              int(m.tasks.size()), reinterpret_cast<const MixTerm*>(dbase + m.m_off), m.tiles);
 }

@@ -84,6 +84,7 @@ size_t footprint(const Job& j) {
 struct dmrg_server {
   int device = 0;
   size_t budget = 0;
+  dmrg::HeffBatcher* batch = nullptr;   // shared Heff launches (null: every solve on its own)
   std::vector<dmrg_ctx*> ctx;
   std::vector<std::thread> workers;
   std::mutex mu;
@@ -131,6 +132,17 @@ bool run_job(dmrg_ctx* c, Job& j) {
     code = dmrg_env_build(st, mpo);
     bad = code != DMRG_OK && failed(code);
   }
+  // inside the sweeps the solve's Heff applications join the server's shared launches
+  struct Batched {
+    dmrg_ctx* c;
+    explicit Batched(dmrg_ctx* x) : c(x) {
+      if (c->batch) { batcher_enter(c->batch); c->batch_on = true; }
+    }
+    ~Batched() {
+      if (c->batch) { c->batch_on = false; batcher_leave(c->batch); }
+    }
+  };
+  std::unique_ptr<Batched> batched(bad ? nullptr : new Batched(c));
   for (int s = 0; !bad && s < j.sweeps; ++s) {
     dmrg_sweep_stats ss;
     code = dmrg_sweep(st, mpo, &j.params, &ss);
@@ -142,6 +154,7 @@ bool run_job(dmrg_ctx* c, Job& j) {
     j.sweeps_done = s + 1;
     if (ss.converged) break;     // dmrgcvg's goal test (algs/DMRG.jl:610-652)
   }
+  batched.reset();
   if (!bad) {
     j.site.resize(j.L);
     j.sml.resize(j.L);
@@ -223,6 +236,16 @@ int dmrg_server_create(const dmrg_server_config* cfg, dmrg_server** out) {
       return code;
     }
     s->ctx.push_back(c);
+  }
+  if (!cfg->unbatched) {
+    try {
+      s->batch = dmrg::batcher_create(cfg->device);
+    } catch (const dmrg::Error& e) {
+      for (dmrg_ctx* x : s->ctx) dmrg_ctx_destroy(x);
+      delete s;
+      return e.code;
+    }
+    for (dmrg_ctx* c : s->ctx) c->batch = s->batch;
   }
   for (int w = 0; w < cfg->slots; ++w) s->workers.emplace_back(worker, s, w);
   *out = s;
@@ -356,7 +379,16 @@ int dmrg_server_destroy(dmrg_server* s) {
   s->cv.notify_all();
   for (auto& t : s->workers) t.join();
   for (dmrg_ctx* c : s->ctx) dmrg_ctx_destroy(c);
+  dmrg::batcher_destroy(s->batch);
   delete s;
+  return DMRG_OK;
+}
+
+int dmrg_server_stats(dmrg_server* s, long long* batches, long long* contributions) {
+  if (!s) return DMRG_ERR_ARG;
+  if (batches) *batches = 0;
+  if (contributions) *contributions = 0;
+  if (s->batch) dmrg::batcher_stats(s->batch, batches, contributions);
   return DMRG_OK;
 }
 

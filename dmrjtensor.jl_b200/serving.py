@@ -4,7 +4,9 @@
 ``dmrg(psi, mpo; m, minm, sweeps, cutoff)`` (``algs/DMRG.jl:549-588``) computes and returns a
 ticket at once; ``poll``/``result`` report it. Up to ``slots`` solves run at the same time, each
 in its own context and CUDA stream, admitted first come first served while their worst-case
-device footprints fit in ``hbm_budget`` bytes. A solve's result is the same alone and in a mix.
+device footprints fit in ``hbm_budget`` bytes. Inside their sweeps the solves' Heff applications
+share grouped launches (``batched=False`` gives every solve its own). A solve's result is the
+same alone and in a mix.
 """
 from __future__ import annotations
 
@@ -22,9 +24,10 @@ class ServerError(_lib.DmrgError):
 
 
 class Server:
-    def __init__(self, device=0, slots=4, hbm_budget=0):
+    def __init__(self, device=0, slots=4, hbm_budget=0, batched=True):
         cfg = ServerConfig()
         cfg.device, cfg.slots, cfg.hbm_budget_bytes = int(device), int(slots), int(hbm_budget)
+        cfg.unbatched = 0 if batched else 1
         h = C.c_void_p()
         code = lib().dmrg_server_create(C.byref(cfg), C.byref(h))
         if code != _lib.OK:
@@ -37,8 +40,14 @@ class Server:
             msg = lib().dmrg_server_last_error(self.h)
             raise ServerError(code, msg.decode() if msg else "")
 
+    def stats(self):
+        """(shared Heff launches, Heff applications they carried) since the server started."""
+        a, b = C.c_longlong(), C.c_longlong()
+        self._check(lib().dmrg_server_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def submit(self, psi: MPS, mpo: MPO, m=0, sweeps=1, minm=2, cutoff=0.0, krylov=2,
-               SvNbond=0, degen_rtol=0.0):
+               SvNbond=0, degen_rtol=0.0, precision="fp64"):
         """Queue one solve; returns its ticket. ``psi`` is copied (dense-equivalent tensors)."""
         L = len(mpo)
         if psi.tensors is None:
@@ -59,7 +68,7 @@ class Server:
         r.ml, r.mr = _int_arr([a.shape[0] for a in As]), _int_arr([a.shape[2] for a in As])
         r.A = _ptr_array(As, C.c_double)
         r.oc, r.sweeps = int(psi.oc), int(sweeps)
-        r.params = make_params(m, minm, cutoff, krylov, "fp64", SvNbond, degen_rtol)
+        r.params = make_params(m, minm, cutoff, krylov, precision, SvNbond, degen_rtol)
         t = C.c_longlong()
         self._check(lib().dmrg_server_submit(self.h, C.byref(r), C.byref(t)))
         del keep

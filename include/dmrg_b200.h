@@ -281,14 +281,19 @@ DMRG_API void dmrg_params_default(dmrg_params* p);
  * context (CUDA stream) each, so that the latency-bound bond steps of different solves overlap on
  * the GPU; a request starts as soon as a slot is free and its worst-case device footprint fits
  * in what the running solves leave of `hbm_budget_bytes` (continuous admission, first come first
- * served). A solve's results do not depend on the other solves running beside it. */
+ * served). Inside their sweeps the solves' Heff applications are gathered into shared grouped
+ * launches (one per phase for all solves at a Lanczos step). A solve's results do not depend on
+ * the other solves running beside it: every block is computed as in a launch of its own. */
 typedef struct dmrg_server dmrg_server;
 
 typedef struct dmrg_server_config {
   int device;
   int slots;                 /* concurrent solves, >= 1 */
   size_t hbm_budget_bytes;   /* 0: no budget (slots alone limit admission) */
-  int reserved[8];
+  int unbatched;             /* 0 (default): the Heff applications of all solves inside their
+                                sweeps share grouped launches (continuous batching); 1: every
+                                solve launches its own */
+  int reserved[7];
 } dmrg_server_config;
 
 /* One solve. Same arrays and conventions as dmrg_mpo_upload / dmrg_mps_upload (dense-equivalent
@@ -340,6 +345,10 @@ DMRG_API int dmrg_server_release(dmrg_server* s, long long ticket);
 /* Finishes the queued and running solves, then stops the workers. */
 DMRG_API int dmrg_server_destroy(dmrg_server* s);
 DMRG_API const char* dmrg_server_last_error(const dmrg_server* s);
+/* Shared-launch statistics since the server started: *batches = rounds of shared Heff launches
+ * (each one launch per phase and form), *contributions = Heff applications they carried
+ * (contributions / batches = mean number of solves per shared launch). */
+DMRG_API int dmrg_server_stats(dmrg_server* s, long long* batches, long long* contributions);
 
 #ifdef __cplusplus
 }

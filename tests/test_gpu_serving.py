@@ -1,10 +1,13 @@
 """Serving loop (dmrg_server_* through the C ABI): a solve gives the same result alone and in a mix.
 
 The same five requests (transverse-field Ising chains and one U(1) Heisenberg chain) run one at
-a time on a one-slot server, all at once on a four-slot server, and through the plain ``dmrg``
-call; energies, truncation errors, entropies and final tensors must agree bit for bit (each
-solve has its own context and the kernels are deterministic). One result is also checked
-against exact diagonalisation, and a request larger than the HBM budget is refused.
+a time on a one-slot server, all at once on a four-slot server whose solves share their Heff
+launches (the batched launches must have carried more than one solve on average), all at once
+on a four-slot server without shared launches, and through the plain ``dmrg`` call; energies,
+truncation errors, entropies and final tensors must agree bit for bit (every block of a shared
+launch is computed as in a launch of its own, and the kernels are deterministic). The same holds
+for the split-precision (3xTF32) option. One result is also checked against exact
+diagonalisation, and a request larger than the HBM budget is refused.
 """
 import numpy as np
 import pytest
@@ -52,14 +55,33 @@ def test_alone_equals_mixed_equals_direct(dmrgb):
         alone = _run(s1, reqs, together=False)
     with dmrgb.Server(slots=4) as s4:
         mixed = _run(s4, reqs, together=True)
-    for a, b in zip(alone, mixed):
+        batches, carried = s4.stats()
+    assert batches > 0 and carried / batches > 1.0     # Heff launches were shared
+    with dmrgb.Server(slots=4, batched=False) as s4u:
+        own = _run(s4u, reqs, together=True)
+        assert s4u.stats() == (0, 0)
+    for a, b, c in zip(alone, mixed, own):
         assert a[0]["status"] == 2
         _same(a, b)
+        _same(a, c)
     # the plain dmrg() call computes the same numbers
     for (psi, mpo, kw), (st, _) in zip(reqs, alone):
         p = dmrgb.MPS([t.copy() for t in psi.tensors], oc=psi.oc)
         e = dmrgb.dmrg(p, mpo, m=kw["m"], sweeps=kw["sweeps"], cutoff=kw["cutoff"])
         assert e == st["energy"]
+
+
+def test_split_precision_alone_equals_mixed(dmrgb):
+    reqs = _requests(dmrgb)
+    for _, _, kw in reqs:
+        kw["precision"] = "3xtf32"
+    with dmrgb.Server(slots=1) as s1:
+        alone = _run(s1, reqs, together=False)
+    with dmrgb.Server(slots=4) as s4:
+        mixed = _run(s4, reqs, together=True)
+    for a, b in zip(alone, mixed):
+        assert a[0]["status"] == 2
+        _same(a, b)
 
 
 def test_served_energy_matches_exact_diagonalisation(dmrgb):
