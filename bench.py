@@ -136,6 +136,36 @@ def params(pkg, m, args, profile=0, precision=None, tune=True):
                            precision=precision or args.precision, profile=profile, tune=tune)
 
 
+def graph_report(pkg, ctx, dev, mfin, args, flush):
+    """The Lanczos step as one CUDA graph per bond step against plain launches: the headline state
+    (2-vector Krylov step) and the dense L=20 chain of the benchmark's small configuration (maxm
+    100, Krylov 8, after its 10 sweeps), device time per sweep (best of 3) in each mode."""
+    out = {}
+    for name, tune_graph in (("plain_launches", False), ("graph", True)):
+        ms = []
+        for _ in range(3):
+            flush()
+            st = dev.sweep(pkg.make_params(maxm=mfin, minm=2, cutoff=CUTOFF, krylov=args.krylov,
+                                           precision=args.precision, graph=tune_graph))
+            ms.append(st["seconds"] * 1e3)
+        out.setdefault("heisenberg_l100_u1", {})[name + "_ms"] = min(ms)
+    L = 20
+    mpo = pkg.makeMPO(pkg.heisenbergMPO, 2, L)
+    small = pkg.DeviceState(pkg.randMPS(2, L, 10, seed=20), mpo.device(ctx))
+    small.env_build()
+    for _ in range(10):
+        small.sweep(pkg.make_params(maxm=100, cutoff=1e-12, krylov=8))
+    for name, g in (("plain_launches", False), ("graph", True)):
+        ms = []
+        for _ in range(3):
+            st = small.sweep(pkg.make_params(maxm=100, cutoff=1e-12, krylov=8, graph=g))
+            ms.append(st["seconds"] * 1e3)
+        out.setdefault("heisenberg_l20_dense_krylov8", {})[name + "_ms"] = min(ms)
+    for v in out.values():
+        v["speedup"] = v["plain_launches_ms"] / v["graph_ms"]
+    return out
+
+
 def autotune_report(pkg, ctx, dev, mfin, args, flush):
     """Tile autotuner on the resident state: profiled sweeps with the tuned tile shapes and with
     fixed 64 x 64 tiles (the numbers are identical; the GEMM device time and the sweep time are
@@ -668,6 +698,7 @@ def run_ours(args, world, rank, local, dist):
     # part of the timed steps): phase breakdown and per-launch timing of the dominant kernel
     prof = dev.sweep(params(pkg, mfin, args, profile=1))
     tuner = autotune_report(pkg, ctx, dev, mfin, args, flush)
+    graphs = graph_report(pkg, ctx, dev, mfin, args, flush)
     heff_flops = prof["heff_flops"]
     heff_sec = prof["heff_seconds"]
     # chosen form on the same resident state: Heff GEMMs as 3xTF32 on the tensor cores (FP64
@@ -786,6 +817,7 @@ def run_ours(args, world, rank, local, dist):
         "heff_forms_m1024": heff_large,
         "tf32_gemm_peak_tflops": tf32_peak,
         "autotune": tuner,
+        "graph": graphs,
         "configs": configs,
     }
     print(json.dumps(out))

@@ -24,7 +24,7 @@ class Params(C.Structure):
                 ("krylov", C.c_int), ("precision", C.c_int), ("svnbond", C.c_int),
                 ("degen_rtol", C.c_double), ("betatest", C.c_double), ("fp64_final", C.c_int),
                 ("profile", C.c_int), ("cvgE", C.c_int), ("tune", C.c_int),
-                ("goal", C.c_double), ("reserved", C.c_int * 2)]
+                ("goal", C.c_double), ("graph", C.c_int), ("reserved1", C.c_int)]
 
 
 class SweepStats(C.Structure):
@@ -36,7 +36,7 @@ class SweepStats(C.Structure):
                 ("d_top", C.c_double * 8), ("gemm_flops", C.c_double),
                 ("gemm_seconds", C.c_double), ("gemm_launches", C.c_int), ("eig_max_n", C.c_int),
                 ("host_seconds", C.c_double), ("wait_seconds", C.c_double),
-                ("converged", C.c_int), ("reserved_s", C.c_int), ("cvg_check", C.c_double)]
+                ("converged", C.c_int), ("graph_launches", C.c_int), ("cvg_check", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "d_top"}

@@ -118,6 +118,7 @@ void dmrg_params_default(dmrg_params* p) {
   p->cvgE = 1;
   p->goal = 0.0;
   p->tune = 1;
+  p->graph = 1;
 }
 
 const char* dmrg_last_error(const dmrg_ctx* ctx) {
@@ -186,6 +187,7 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaFree(c->d_flags);
   cudaFreeHost(c->h_flags);
   cudaFree(c->d_floors);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
   cudaStreamDestroy(c->stream);
   delete c;
   return DMRG_OK;

@@ -175,6 +175,9 @@ struct dmrg_ctx {
   int device = 0;
   bool tune = true;              // FP64 GEMM tile autotuner on (dmrg_params.tune of the sweep)
   dmrg::HeffBatcher* batch = nullptr;   // server contexts: the shared Heff batcher
+  cudaGraphExec_t gexec = nullptr;       // the Krylov step's executable graph (dmrg_params.graph)
+  bool capturing = false;                // inside a stream capture: no timed tuner trials
+  long long graph_launches = 0;
   bool batch_on = false;         // inside a served solve's sweeps: Heff goes to the batcher
   dmrg::GemmTuner tuner;
   cudaStream_t stream = nullptr;

@@ -363,7 +363,7 @@ void run_gemm(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int6
       (g.bm != GEMM_SMALL_TILE || g.bn != GEMM_SMALL_TILE))
     bad_plan("gemm tiling");
   GemmTuner::Pending tp{};
-  const bool timed = g.tune_trial && g.tune_key != 0;
+  const bool timed = g.tune_trial && g.tune_key != 0 && !c->capturing;
   if (timed) {
     for (cudaEvent_t* e : {&tp.a, &tp.b}) {
       if (!c->tuner.free_events.empty()) {

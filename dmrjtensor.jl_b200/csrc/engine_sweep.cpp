@@ -183,6 +183,13 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   cuda_check(cudaGetLastError(), "two-site tensor");
   tm.end(tv, 3);
 
+  // P.graph: everything of the Krylov step after its first Heff application (which makes every
+  // scratch allocation the step needs) is captured into a CUDA graph and launched as one graph;
+  // the context keeps the executable graph and updates it in place from the next step's capture
+  // when the kernel sequence has the same shape (it does for a fixed Krylov dimension), so a step
+  // costs one graph update and one graph launch instead of one launch per kernel.
+  const bool use_graph = P.graph && !P.profile && !(c->batch && c->batch_on);
+  bool capturing = false;
   auto heff = [&](const double* x, double* y) {
     const int th = tm.begin();
     apply_heff(st, iL, hp, x, y, P.precision, P.profile ? &tm.gemm : nullptr);
@@ -190,6 +197,11 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     tm.end(th, 0);
     so.nmv += 1;
     so.heff_flops += hp.flops;
+    if (use_graph && !capturing) {
+      cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+      capturing = true;
+      c->capturing = true;
+    }
   };
 
   // Krylov solve with every scalar in device memory (slots lz::*): no host round trip; a
@@ -240,6 +252,31 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     tm.end(tv, 3);
   }
   cuda_check(cudaGetLastError(), "Krylov step");
+  if (capturing) {
+    cudaGraph_t graph = nullptr;
+    c->capturing = false;
+    cuda_check(cudaStreamEndCapture(s, &graph), "graph capture end");
+    bool updated = false;
+    if (c->gexec) {
+      cudaGraphExecUpdateResultInfo info{};
+      updated = cudaGraphExecUpdate(c->gexec, graph, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+      }
+    }
+    if (!updated) {
+      const cudaError_t e = cudaGraphInstantiate(&c->gexec, graph, 0ull);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        cuda_check(e, "graph instantiate");
+      }
+    }
+    cudaGraphDestroy(graph);
+    cuda_check(cudaGraphLaunch(c->gexec, s), "graph launch");
+    c->graph_launches += 1;
+  }
   const double* psi = H;
   // split form, last bond step of the sweep: the reported energy is the FP64 Rayleigh quotient
   // <psi|H|psi>/<psi|psi> of the Ritz vector (one FP64 matvec; the Krylov vectors are free now)
@@ -497,6 +534,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   if (!st->env_built) fail(DMRG_ERR_STATE, "call dmrg_env_build before dmrg_sweep");
   std::memset(&out, 0, sizeof(out));
   c->tune = P.tune != 0;
+  const long long g0 = c->graph_launches;
   const int svn = P.svnbond > 0 ? P.svnbond : (L + 1) / 2;
   const int svn_site = std::min(std::max(2, svn + 1), L) - 1;   // 0-based i of SvNcheck!
   const auto h0 = std::chrono::steady_clock::now();
@@ -545,6 +583,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   cuda_check(cudaEventSynchronize(tm.event(t1)), "sweep sync");
   if (split_form(P.precision)) check_mma_status(c);   // the last environment update
   tuner_collect(c);
+  out.graph_launches = int(c->graph_launches - g0);
   float ms = 0;
   cudaEventElapsedTime(&ms, tm.event(t0), tm.event(t1));
   out.seconds = ms * 1e-3;

@@ -41,11 +41,12 @@ mutable struct Params
   fp64_final::Cint
   profile::Cint
   cvgE::Cint
-  reserved0::Cint
+  tune::Cint
   goal::Cdouble
-  reserved::NTuple{2,Cint}
+  graph::Cint
+  reserved1::Cint
 end
-Params() = Params(0, 0, 0.0, 0, 0, 0, 0.0, 0.0, 0, 0, 0, 0, 0.0, ntuple(_ -> Cint(0), 2))
+Params() = Params(0, 0, 0.0, 0, 0, 0, 0.0, 0.0, 0, 0, 0, 0, 0.0, 0, 0)
 
 # mirrors struct dmrg_sweep_stats
 mutable struct SweepStats
@@ -69,7 +70,7 @@ mutable struct SweepStats
   host_seconds::Cdouble
   wait_seconds::Cdouble
   converged::Cint
-  reserved_s::Cint
+  graph_launches::Cint
   cvg_check::Cdouble
 end
 SweepStats() = SweepStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0.0, 8), 0, 0, 0, 0, 0, 0,

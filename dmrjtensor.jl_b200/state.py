@@ -410,7 +410,7 @@ class DeviceState:
 
 def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
                 degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0, goal=0.0, cvgE=True,
-                tune=True):
+                tune=True, graph=True):
     p = Params()
     lib().dmrg_params_default(C.byref(p))
     p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)
@@ -421,6 +421,7 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
     p.profile = int(profile)
     p.goal, p.cvgE = float(goal), 1 if cvgE else 0
     p.tune = 1 if tune else 0
+    p.graph = 1 if graph else 0
     return p
 
 

@@ -93,7 +93,10 @@ typedef struct dmrg_params {
                         |S - S_last| < goal (cvgE = 0); E_last starts at <psi|H|psi> of the state
                         the environments were built for (startval, algs/optimizeMPS.jl:255-258,
                         365-371), S_last at 0. 0 (the default) never converges: all sweeps run */
-  int reserved[2];
+  int graph;         /* 1 (default): the Lanczos step after its first Heff runs as one CUDA graph
+                        (captured per step, the context's executable updated in place); 0: plain
+                        launches. Same numbers either way */
+  int reserved1;
 } dmrg_params;
 
 /* Per-sweep record (what dmrgcvg prints, algs/DMRG.jl:610-652, plus timings). */
@@ -118,7 +121,7 @@ typedef struct dmrg_sweep_stats {
   double host_seconds;  /* host wall time of the sweep call                           */
   double wait_seconds;  /* of which blocked in the per-step eigenvalue synchronisation */
   int converged;        /* goal > 0 and the dmrgcvg test passed: the caller stops sweeping */
-  int reserved_s;
+  int graph_launches;   /* graph = 1: Krylov steps that ran as one CUDA graph launch       */
   double cvg_check;     /* the tested difference (energy or entropy) when goal > 0        */
 } dmrg_sweep_stats;
 

@@ -147,3 +147,23 @@ def test_tile_autotuner_keeps_every_number(dmrgb, ctx):
     assert np.array_equal(out[True][2], out[False][2])
     sig, decided, small = ctx.tuner()
     assert sig > 0 and decided > 0 and 0 <= small <= decided
+
+
+@pytest.mark.parametrize("krylov,precision", [(2, "fp64"), (8, "fp64"), (2, "3xtf32")])
+def test_graph_krylov_step_keeps_every_number(dmrgb, ctx, krylov, precision):
+    """The Lanczos step as one CUDA graph per bond step (graph = 1) gives the same bits as plain
+    launches, and every bond step of the sweep ran its graph."""
+    L = 24
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    out = {}
+    for graph in (False, True):
+        dev = dmrgb.DeviceState(dmrgb.neelMPS(L), mpo.device(ctx))
+        dev.env_build()
+        st = [dev.sweep(dmrgb.make_params(maxm=m, cutoff=1e-12, krylov=krylov,
+                                          precision=precision, graph=graph))
+              for m in (16, 32, 48)]
+        out[graph] = ([s["energy"] for s in st], dev.site_blocks(L // 2))
+        if graph:
+            assert all(s["graph_launches"] == 2 * (L - 1) for s in st)
+    assert out[True][0] == out[False][0]
+    assert np.array_equal(out[True][1], out[False][1])
