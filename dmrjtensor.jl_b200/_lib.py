@@ -44,6 +44,11 @@ class SweepStats(C.Structure):
         return d
 
 
+class Noise(C.Structure):
+    _fields_ = [("noise", C.c_double), ("noise_goal", C.c_double), ("noise_incr", C.c_double),
+                ("reserved", C.c_double)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("slots", C.c_int), ("hbm_budget_bytes", C.c_size_t),
                 ("unbatched", C.c_int), ("reserved", C.c_int * 7)]
@@ -119,6 +124,8 @@ SIGNATURES = {
     "dmrg_twosite_dims": (C.c_int, [_P, _P, C.c_int, _IP]),
     "dmrg_sweep": (C.c_int, [_P, _P, C.POINTER(Params), C.POINTER(SweepStats)]),
     "dmrg_params_default": (None, [C.POINTER(Params)]),
+    "dmrg_noise_default": (None, [C.POINTER(Noise)]),
+    "dmrg_sweep3s": (C.c_int, [_P, _P, C.POINTER(Params), C.POINTER(Noise), C.POINTER(SweepStats)]),
     "dmrg_test_gemm": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int,
                                  _DP, C.c_int, _DP, C.c_int]),
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),

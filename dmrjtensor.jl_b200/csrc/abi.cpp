@@ -295,6 +295,8 @@ int dmrg_mpo_upload(dmrg_ctx* c, int L, int nsym, const int* d, const int* wl, c
       }
       m->two.resize(std::max(L - 1, 0));
       for (int i = 0; i + 1 < L; ++i) m->two[i] = make_two_site_op(m->site[i], m->site[i + 1]);
+      m->one.resize(L);
+      for (int i = 0; i < L; ++i) m->one[i] = make_one_site_op(m->site[i]);
     } catch (...) {
       delete m;
       throw;
@@ -920,6 +922,44 @@ int dmrg_sweep(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_s
         st->last_energy = out->energy;
         st->last_entropy = out->entropy;
       }
+    }
+  });
+}
+
+void dmrg_noise_default(dmrg_noise* nz) {
+  if (!nz) return;
+  std::memset(nz, 0, sizeof(*nz));
+  nz->noise = 1.0;
+  nz->noise_goal = 0.3;
+  nz->noise_incr = 0.01;
+}
+
+int dmrg_sweep3s(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_noise* nz,
+                 dmrg_sweep_stats* out) {
+  if (!st) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    if (mpo != st->mpo) fail(DMRG_ERR_ARG, "state was uploaded with a different MPO");
+    if (!p || !out || !nz) fail(DMRG_ERR_ARG, "null params/noise/stats");
+    set_device(c);
+    // lastenergy starts at startval (algs/optimizeMPS.jl:365-371), <psi|H|psi> of the input
+    if (!st->have_last) {
+      if (!st->env_built) fail(DMRG_ERR_STATE, "call dmrg_env_build before dmrg_sweep3s");
+      st->last_energy = measure_expect(st, st->mpo, nullptr);
+      st->last_entropy = 0.0;
+      st->have_last = true;
+    }
+    double alpha = nz->noise;
+    do_sweep3s(st, *p, *nz, &alpha, st->last_energy, *out);
+    nz->noise = alpha;
+    // dmrgcvg (algs/DMRG.jl:626-652): with cvgE the last energy moves on unless converged
+    const double chk = p->cvgE ? std::fabs(out->energy - st->last_energy)
+                               : std::fabs(st->last_entropy - out->entropy);
+    out->cvg_check = p->goal > 0 ? chk : 0.0;
+    out->converged = (p->goal > 0 && chk < p->goal) ? 1 : 0;
+    if (!out->converged) {
+      if (p->cvgE) st->last_energy = out->energy;
+      else st->last_entropy = out->entropy;
     }
   });
 }

@@ -277,8 +277,9 @@ void batched_heff(dmrg_ctx* c, dmrg_state* st, int iL, const HeffPlan& hp, const
   const int form = split_form(precision);
   if (precision != DMRG_PREC_FP64 && !form)
     fail(DMRG_ERR_ARG, "precision: FP64, 3xTF32 and BF16x9 are the built forms");
-  const DBuf& Le = st->Lenv[iL];
-  const DBuf& Re = st->Renv[iL + 1];
+  (void)iL;
+  const DBuf& Le = st->Lenv[hp.le];
+  const DBuf& Re = st->Renv[hp.re];
   // the solve's own lists, tiled for the batched launch, checked against its own buffers
   const GemmList g1 = form ? retile(hp.g1, TF32_TILE_M, TF32_TILE_N_DIRECT)
                            : retile(hp.g1, GEMM_BM, GEMM_BN);

@@ -208,6 +208,7 @@ struct dmrg_mpo {
   int L = 0, nsym = 0;
   std::vector<dmrg::MPOSite> site;
   std::vector<dmrg::TwoSiteOp> two;   // per bond (iL, iL+1)
+  std::vector<dmrg::TwoSiteOp> one;   // per site, for the single-site Heff
 };
 
 struct dmrg_state {
@@ -249,6 +250,8 @@ TwoLayout make_two_layout(const Bond& Bl, const std::vector<QN>& p1, const std::
 EnvLayout make_left_env_layout(const Bond& B, const std::vector<QN>& r);
 EnvLayout make_right_env_layout(const Bond& B, const std::vector<QN>& r);
 TwoSiteOp make_two_site_op(const MPOSite& a, const MPOSite& b);
+// One MPO site in the two-site form with a trivial second site (d2 = 1): out[t * wr + w'].
+TwoSiteOp make_one_site_op(const MPOSite& a);
 
 // ---- descriptor upload
 struct Upload {
@@ -311,6 +314,7 @@ struct GemmProfile {
 
 // ---- contractions (engine_contract.cpp)
 struct HeffPlan {
+  int le = 0, re = 0;            // the environments it reads: Lenv[le], Renv[re]
   TwoLayout tl;
   GemmList g1, g3;
   GemmList g1t, g3t;             // retiled copies for the split-precision kernel (when used)
@@ -321,11 +325,15 @@ struct HeffPlan {
   char* dbase = nullptr;
 };
 void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp);
+// The single-site Heff at site i (singlesite_update, algs/optimizeMPS.jl:503-511): the same three
+// launches with a second site of dimension one (charge zero), reading Lenv[i] and Renv[i]; its
+// vector layout is the site layout of A[i].
+void plan_heff1(const dmrg_state* st, int i, HeffPlan& hp);
 // Uploads the Heff task lists; with precision DMRG_PREC_3XTF32 also the retiled copies.
 void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision = DMRG_PREC_FP64);
 // Adds the retiled split-precision lists to a plan (before its upload).
 void prepare_split(HeffPlan& hp);
-// y = Heff x for vectors in the tl layout (device pointers).
+// y = Heff x for vectors in the tl layout (device pointers); reads Lenv[hp.le] and Renv[hp.re].
 // Fails (DMRG_ERR_TIMEOUT) if a split-precision GEMM reported an MMA wait that gave up since the
 // last check, and clears the flag. Synchronous read; call after a stream synchronisation.
 void check_mma_status(dmrg_ctx* c);
@@ -399,5 +407,10 @@ void run_eigs(dmrg_ctx* c, double* base, int64_t nbase, const std::vector<EigTas
 
 // ---- sweep (engine_sweep.cpp)
 void do_sweep(dmrg_state* st, const dmrg_params& p, dmrg_sweep_stats& out);
+// ---- single-site sweep with subspace expansion (engine_3s.cpp). `noise` is alpha (in: the
+// current value, out: after the sweep's last alpha_update); last_energy is the lastEnergy of
+// alpha_update (the previous sweep's energy, or the starting energy).
+void do_sweep3s(dmrg_state* st, const dmrg_params& p, const dmrg_noise& nz, double* noise,
+                double last_energy, dmrg_sweep_stats& out);
 
 }  // namespace dmrg

@@ -12,18 +12,39 @@
 
 namespace dmrg {
 
+namespace {
+// Heff plan over the sites' combined physical index (p1, p2), between bonds Bl and Br, with the
+// MPO bond labels rl of the left MPO site, the combined operator op, and the environments' layouts
+void plan_heff_core(const Bond& Bl, const Bond& Br, const std::vector<QN>& p1,
+                    const std::vector<QN>& p2, const std::vector<QN>& rl, const TwoSiteOp& op,
+                    const EnvLayout& LL, const EnvLayout& RL, HeffPlan& hp);
+}  // namespace
+
 void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp) {
   const int iR = iL + 1;
-  const Bond& Bl = st->bond[iL];
-  const Bond& Br = st->bond[iL + 2];
-  const MPOSite& ml = st->mpo->site[iL];
-  const MPOSite& mr = st->mpo->site[iR];
-  const TwoSiteOp& op = st->mpo->two[iL];
-  const EnvLayout& LL = st->Llay[iL];
-  const EnvLayout& RL = st->Rlay[iR];
-  hp.tl = make_two_layout(Bl, ml.p, mr.p, Br);
+  hp.le = iL;
+  hp.re = iR;
+  plan_heff_core(st->bond[iL], st->bond[iL + 2], st->mpo->site[iL].p, st->mpo->site[iR].p,
+                 st->mpo->site[iL].rl, st->mpo->two[iL], st->Llay[iL], st->Rlay[iR], hp);
+}
+
+void plan_heff1(const dmrg_state* st, int i, HeffPlan& hp) {
+  static const std::vector<QN> trivial(1, QN());
+  hp.le = i;
+  hp.re = i;
+  plan_heff_core(st->bond[i], st->bond[i + 1], st->mpo->site[i].p, trivial, st->mpo->site[i].rl,
+                 st->mpo->one[i], st->Llay[i], st->Rlay[i], hp);
+  if (hp.tl.size != st->lay[i].size)
+    fail(DMRG_ERR_ARG, "internal plan check failed: single-site Heff layout");
+}
+
+namespace {
+void plan_heff_core(const Bond& Bl, const Bond& Br, const std::vector<QN>& p1,
+                    const std::vector<QN>& p2, const std::vector<QN>& rl, const TwoSiteOp& op,
+                    const EnvLayout& LL, const EnvLayout& RL, HeffPlan& hp) {
+  hp.tl = make_two_layout(Bl, p1, p2, Br);
   const TwoLayout& tl = hp.tl;
-  const int d1 = tl.d1, d2 = tl.d2, wl = ml.wl, wr = mr.wr;
+  const int d1 = tl.d1, d2 = tl.d2, wl = op.wl, wr = op.wr;
 
   hp.g1.clear();
   hp.g3.clear();
@@ -69,7 +90,7 @@ void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp) {
           if (kd < 0) continue;
           hp.mix.add(yoff[id] + int64_t(RL.rowoff[kap * wr + w2]) * dka, dka, dka, Br.dim[kd]);
           for (const auto& tm : op.out[(size_t(t1) * d2 + t2) * wr + w2]) {
-            const int kb = Bl.find(Bl.q[ka] + ml.rl[tm.w]);
+            const int kb = Bl.find(Bl.q[ka] + rl[tm.w]);
             if (kb < 0 || LL.other[kb * wl + tm.w] != ka) continue;
             const int id2 = tl.idx(kb, tm.s1, tm.s2);
             if (tl.kd[id2] != kd) continue;
@@ -93,6 +114,7 @@ void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp) {
       }
   hp.flops = hp.g1.flops + hp.g3.flops + hp.mix.flops;
 }
+}  // namespace
 
 void check_mma_status(dmrg_ctx* c) {
   int flag = 0;
@@ -172,18 +194,18 @@ void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, dou
     fail(DMRG_ERR_ARG, "precision: FP64, 3xTF32 and BF16x9 are the built forms");
   if (prof) prof->begin(c->stream, hp.g1.flops);
   if (split)
-    run_gemm_split(c, hp.g1t, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n,
-                   split);
+    run_gemm_split(c, hp.g1t, hp.dbase, st->Lenv[hp.le].p, st->Lenv[hp.le].n, x, n, c->X.p,
+                   c->X.n, split);
   else
-    run_gemm(c, hp.g1, hp.dbase, st->Lenv[iL].p, st->Lenv[iL].n, x, n, c->X.p, c->X.n);
+    run_gemm(c, hp.g1, hp.dbase, st->Lenv[hp.le].p, st->Lenv[hp.le].n, x, n, c->X.p, c->X.n);
   if (prof) prof->end(c->stream);
   run_mix(c, hp.mix, hp.dbase, c->X.p, c->X.n, c->Y.p, c->Y.n);
   if (prof) prof->begin(c->stream, hp.g3.flops);
   if (split)
-    run_gemm_split(c, hp.g3t, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n,
+    run_gemm_split(c, hp.g3t, hp.dbase, c->Y.p, c->Y.n, st->Renv[hp.re].p, st->Renv[hp.re].n,
                    y, n, split);
   else
-    run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[iL + 1].p, st->Renv[iL + 1].n, y, n);
+    run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[hp.re].p, st->Renv[hp.re].n, y, n);
   if (prof) prof->end(c->stream);
 }
 

@@ -205,6 +205,18 @@ TwoSiteOp make_two_site_op(const MPOSite& a, const MPOSite& b) {
   return op;
 }
 
+TwoSiteOp make_one_site_op(const MPOSite& a) {
+  TwoSiteOp op;
+  op.d1 = a.d;
+  op.d2 = 1;
+  op.wl = a.wl;
+  op.wr = a.wr;
+  op.out.assign(size_t(a.d) * a.wr, {});
+  for (const auto& e : a.nz)
+    if (e.v != 0.0) op.out[size_t(e.t) * a.wr + e.w2].push_back({e.w, e.s, 0, e.v});
+  return op;
+}
+
 // ------------------------------------------------------------------ task lists
 
 void GemmList::add(int64_t c_off, int ldc, int M, int N, double alpha, double beta) {

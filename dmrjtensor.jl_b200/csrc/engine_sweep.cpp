@@ -11,20 +11,10 @@
 #include <cmath>
 #include <map>
 
-#include "engine.hpp"
+#include "engine_step.hpp"
 
 namespace dmrg {
-namespace {
 
-// Truncation, global over all charge groups (fsvd!, algs/DMRG.jl:387): the weights of every group
-// sorted descending together (ties by group, then index); k_c = the smallest k whose discarded
-// weight is at most cutoff x total (total = mag, or the sum of the weights when mag = 0); keep
-// k = min(maxm, max(minm, k_c)) (maxm > 0), at least 1; with degen_rtol > 0 the cut moves back out
-// of a degenerate multiplet. truncerr = the discarded weight.
-struct Sel {
-  std::vector<int> keep;
-  double truncerr = 0.0;
-};
 Sel select_kept(const std::vector<std::vector<double>>& vals, int maxm, int minm, double cutoff,
                 double mag, double degen_rtol) {
   struct E { double v; int g, i; };
@@ -40,8 +30,8 @@ Sel select_kept(const std::vector<std::vector<double>>& vals, int maxm, int minm
   s.keep.assign(vals.size(), 0);
   const int N = int(flat.size());
   if (N == 0) return s;
-  double tot = 0.0;
-  if (mag == 0.0) for (const E& e : flat) tot += e.v; else tot = mag;
+  for (const E& e : flat) s.total += e.v;
+  const double tot = mag == 0.0 ? s.total : mag;
   std::vector<double> tail(N + 1, 0.0);
   for (int k = N - 1; k >= 0; --k) tail[k] = tail[k + 1] + flat[k].v;
   int kc = N;
@@ -63,136 +53,47 @@ Sel select_kept(const std::vector<std::vector<double>>& vals, int maxm, int minm
   return s;
 }
 
-// Phase timing with CUDA events from the context's persistent pool (profile != 0 only). Events
-// are read once, after the sweep's final synchronisation.
-struct Timing {
-  dmrg_ctx* c;
-  bool on;
-  int used = 0;
-  struct Span { int a, b, cat; };
-  std::vector<Span> spans;
-  double acc[4] = {0, 0, 0, 0};   // heff, env, eig, vec
-  GemmProfile gemm;
-  Timing(dmrg_ctx* ctx, bool enabled) : c(ctx), on(enabled) {}
-  int record() {
-    if (used == int(c->tev.size())) {
-      cudaEvent_t e;
-      cuda_check(cudaEventCreate(&e), "event create");
-      c->tev.push_back(e);
-    }
-    cuda_check(cudaEventRecord(c->tev[used], c->stream), "event record");
-    return used++;
+int Timing::record() {
+  if (used == int(c->tev.size())) {
+    cudaEvent_t e;
+    cuda_check(cudaEventCreate(&e), "event create");
+    c->tev.push_back(e);
   }
-  cudaEvent_t event(int i) const { return c->tev[i]; }
-  int begin() { return on ? record() : -1; }
-  void end(int a, int cat) {
-    if (on && a >= 0) spans.push_back({a, record(), cat});
+  cuda_check(cudaEventRecord(c->tev[used], c->stream), "event record");
+  return used++;
+}
+
+void Timing::flush() {
+  gemm.flush();
+  for (const Span& sp : spans) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->tev[sp.a], c->tev[sp.b]);
+    acc[sp.cat] += ms * 1e-3;
   }
-  void flush() {   // call after a stream sync
-    gemm.flush();
-    for (const Span& sp : spans) {
-      float ms = 0;
-      cudaEventElapsedTime(&ms, c->tev[sp.a], c->tev[sp.b]);
-      acc[sp.cat] += ms * 1e-3;
-    }
-    spans.clear();
-    used = 0;
-  }
-};
+  spans.clear();
+  used = 0;
+}
 
-}  // namespace
-
-namespace {
-
-struct StepOut {
-  double energy = 0, truncerr = 0, wait = 0;
-  int m = 0, nmv = 0;
-  std::vector<double> D;       // kept singular values, descending
-  double heff_flops = 0;
-  int eig_max_n = 0;
-};
-
-struct Piece { int sec, s, off; };
-struct Group {
-  QN q;
-  int n = 0, np = 0, keep = 0, kc = -1;
-  std::vector<Piece> rows, cols;
-  int64_t moff = 0, roff = 0, woff = 0;
-};
-
-void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool final_step,
-             Timing& tm, StepOut& so) {
+// Krylov solve: see engine_step.hpp. P.graph: everything of the solve after its first Heff
+// application (which makes every scratch allocation the step needs) is captured into a CUDA graph
+// and launched as one graph; the context keeps the executable graph and updates it in place from
+// the next step's capture when the kernel sequence has the same shape (it does for a fixed Krylov
+// dimension), so a step costs one graph update and one graph launch instead of one launch per
+// kernel.
+KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp, int64_t n,
+                       bool simple2, bool final_step, Timing& tm, StepOut& so) {
   dmrg_ctx* c = st->ctx;
   cudaStream_t s = c->stream;
-  const MPOSite& ml = st->mpo->site[iL];
-  const MPOSite& mr = st->mpo->site[iR];
-  const Bond Bl = st->bond[iL];
-  const Bond Bc = st->bond[iL + 1];
-  const Bond Br = st->bond[iL + 2];
-  const int d1 = ml.d, d2 = mr.d;
-  if (!st->Lvalid[iL] || !st->Rvalid[iR]) fail(DMRG_ERR_STATE, "environments are not built");
-
-  // psi[iL] (j>0) or psi[iR] (j<0) /= norm  (algs/DMRG.jl:365-369); the squared norm stays on
-  // the device
-  int tv = tm.begin();
-  const int ic = j > 0 ? iL : iR;
-  launch_mdot(s, st->A[ic].p, 0, 1, st->A[ic].p, st->lay[ic].size, c->d_partial,
-              c->d_scal + lz::NRM);
-  launch_scale_rsqrt(s, st->A[ic].p, st->lay[ic].size, c->d_scal + lz::NRM);
-  cuda_check(cudaGetLastError(), "centre normalisation");
-
-  HeffPlan hp;
-  plan_heff(st, iL, hp);
-  const TwoLayout& tl = hp.tl;
-  const SiteLayout& la = st->lay[iL];
-  const SiteLayout& lb = st->lay[iR];
-  GemmList gaa;   // AA = contract(psiL, 3, psiR, 1)
-  for (int ka = 0; ka < tl.nl; ++ka)
-    for (int s1 = 0; s1 < d1; ++s1)
-      for (int s2 = 0; s2 < d2; ++s2) {
-        const int id = tl.idx(ka, s1, s2);
-        const int kd = tl.kd[id];
-        if (kd < 0) continue;
-        gaa.add(tl.off[id], Bl.dim[ka], Bl.dim[ka], Br.dim[kd], 1.0, 0.0);
-        const int kc = la.kb[ka * d1 + s1];
-        if (kc >= 0 && lb.kb[kc * d2 + s2] == kd)
-          gaa.seg(la.off[ka * d1 + s1], Bl.dim[ka], lb.off[kc * d2 + s2], Bc.dim[kc], Bc.dim[kc]);
-      }
-  const bool split = split_form(P.precision) != 0;
-  if (split) prepare_split(hp);
-  tune_gemm(c, hp.g1);
-  tune_gemm(c, hp.g3);
-  tune_gemm(c, gaa);
-  Upload u;
-  u.put(hp.g1);
-  u.put(hp.mix);
-  u.put(hp.g3);
-  u.put(gaa);
-  if (hp.split) {
-    u.put(hp.g1t);
-    u.put(hp.g3t);
-  }
-  hp.dbase = u.send(c, 0);
-  const int64_t n = tl.size;
+  KrylovRun kr;
+  kr.split = split_form(P.precision) != 0;
   const int kdim = std::max(2, std::min(P.krylov, 16));
-  ensure(c, c->K, std::max<int64_t>(int64_t(kdim) * n, 1));
-  ensure(c, c->H, std::max<int64_t>(n, 1));
   double* K = c->K.p;
   double* H = c->H.p;
-  run_gemm(c, gaa, hp.dbase, st->A[iL].p, st->A[iL].n, st->A[iR].p, st->A[iR].n, K, n);
-  cuda_check(cudaGetLastError(), "two-site tensor");
-  tm.end(tv, 3);
-
-  // P.graph: everything of the Krylov step after its first Heff application (which makes every
-  // scratch allocation the step needs) is captured into a CUDA graph and launched as one graph;
-  // the context keeps the executable graph and updates it in place from the next step's capture
-  // when the kernel sequence has the same shape (it does for a fixed Krylov dimension), so a step
-  // costs one graph update and one graph launch instead of one launch per kernel.
   const bool use_graph = P.graph && !P.profile && !(c->batch && c->batch_on);
   bool capturing = false;
   auto heff = [&](const double* x, double* y) {
     const int th = tm.begin();
-    apply_heff(st, iL, hp, x, y, P.precision, P.profile ? &tm.gemm : nullptr);
+    apply_heff(st, hp.le, hp, x, y, P.precision, P.profile ? &tm.gemm : nullptr);
     cuda_check(cudaGetLastError(), "Heff");
     tm.end(th, 0);
     so.nmv += 1;
@@ -204,11 +105,11 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     }
   };
 
-  // Krylov solve with every scalar in device memory (slots lz::*): no host round trip; a
-  // breakdown (beta <= betatest) zeroes the remaining Krylov vectors instead of ending the loop,
-  // and the Ritz step uses only the active ones. The energy is read back with the eigenvalues.
+  // a breakdown (beta <= betatest) zeroes the remaining Krylov vectors instead of ending the
+  // loop, and the Ritz step uses only the active ones
   double* scal = c->d_scal;
-  if (P.krylov <= 2) {
+  int tv = -1;
+  if (simple2) {
     // simplelanczos (algs/DMRG.jl:57-90): H is applied to AA before its normalisation
     heff(K, H);
     tv = tm.begin();
@@ -277,13 +178,12 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     cuda_check(cudaGraphLaunch(c->gexec, s), "graph launch");
     c->graph_launches += 1;
   }
-  const double* psi = H;
   // split form, last bond step of the sweep: the reported energy is the FP64 Rayleigh quotient
   // <psi|H|psi>/<psi|psi> of the Ritz vector (one FP64 matvec; the Krylov vectors are free now)
-  const bool fp64_energy = split && P.fp64_final && final_step;
-  if (fp64_energy) {
+  kr.fp64_energy = kr.split && P.fp64_final && final_step;
+  if (kr.fp64_energy) {
     const int th = tm.begin();
-    apply_heff(st, iL, hp, H, K, DMRG_PREC_FP64, nullptr);
+    apply_heff(st, hp.le, hp, H, K, DMRG_PREC_FP64, nullptr);
     tm.end(th, 0);
     so.nmv += 1;
     so.heff_flops += hp.flops;
@@ -293,9 +193,192 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   }
   cuda_check(cudaMemcpyAsync(c->h_scal + lz::EN, scal + lz::EN, sizeof(double),
                              cudaMemcpyDeviceToHost, s), "energy D2H");
-  if (split)   // timeout flag of the split GEMMs, read back with the energy (bytes of slot 20)
+  if (kr.split)   // timeout flag of the split GEMMs, read back with the energy (bytes of slot 20)
     cuda_check(cudaMemcpyAsync(c->h_scal + 20, c->d_status + STATUS_MMA, sizeof(int),
                                cudaMemcpyDeviceToHost, s), "MMA status D2H");
+  return kr;
+}
+
+double krylov_energy(dmrg_ctx* c, const KrylovRun& kr) {
+  double e = c->h_scal[lz::EN];
+  if (kr.fp64_energy && c->h_scal[lz::KK] > 0) e = c->h_scal[lz::KH] / c->h_scal[lz::KK];
+  if (kr.split) {
+    int flag = 0;
+    std::memcpy(&flag, c->h_scal + 20, sizeof(int));
+    if (flag != 0) {
+      cudaMemsetAsync(c->d_status + STATUS_MMA, 0, sizeof(int), c->stream);
+      fail(DMRG_ERR_TIMEOUT, "split-precision GEMM: a tensor-core MMA completion wait gave up");
+    }
+  }
+  return e;
+}
+
+void plan_rho(dmrg_ctx* c, std::vector<Group>& G, bool rows, RhoSolve& rs, int* eig_max_n) {
+  // side = dimension of the density matrix that is diagonalised (rows of M, or its columns)
+  rs.rows = rows;
+  rs.mtot = rs.rtot = rs.wtot = 0;
+  for (Group& g : G) {
+    const int side = rows ? g.n : g.np;
+    g.moff = rs.mtot; rs.mtot += int64_t(g.n) * g.np;
+    g.roff = rs.rtot; rs.rtot += int64_t(side) * side;
+    g.woff = rs.wtot; rs.wtot += side;
+  }
+  rs.W0 = rs.rtot;
+  rs.WS0 = rs.rtot + rs.wtot;
+  rs.U0 = rs.rtot + 4 * rs.wtot;
+  rs.J0 = 2 * rs.rtot + 4 * rs.wtot;
+  rs.etasks.clear();
+  rs.ttasks.clear();
+  rs.tgroup.clear();
+  rs.uoff.assign(G.size(), 0);
+  for (int gi = 0; gi < int(G.size()); ++gi) {
+    const Group& g = G[gi];
+    const int side = rows ? g.n : g.np;
+    if (side == 0) continue;
+    if (eig_max_n) *eig_max_n = std::max(*eig_max_n, side);
+    if (side <= SYEVT_MID_NMAX) {
+      TridTask t{};
+      t.a_off = g.roff;
+      t.w_off = rs.W0 + g.woff;
+      t.ws_off = rs.WS0 + 3 * g.woff;
+      t.u_off = rs.U0 + g.roff;
+      t.n = side;
+      rs.ttasks.push_back(t);
+      rs.tgroup.push_back(gi);
+      rs.uoff[gi] = t.u_off;
+    } else {
+      EigTask et{};
+      et.a_off = g.roff;
+      et.v_off = g.roff;
+      et.w_off = rs.W0 + g.woff;
+      et.n = side;
+      rs.etasks.push_back(et);
+      rs.uoff[gi] = g.roff;      // block Jacobi returns the eigenvectors in place
+    }
+  }
+  const int64_t ews = eig_workspace(rs.etasks);
+  ensure(c, c->M, std::max<int64_t>(rs.mtot, 1));
+  ensure(c, c->R, std::max<int64_t>(rs.J0 + ews, 1));
+  GemmList& grho = rs.grho;
+  grho.clear();
+  grho.tA = !rows;
+  grho.tB = rows;
+  for (const Group& g : G) {
+    const int side = rows ? g.n : g.np;
+    if (side == 0) continue;
+    grho.add(g.roff, side, side, side, 1.0, 0.0);
+    const int K2 = rows ? g.np : g.n;
+    if (K2 > 0) grho.seg(g.moff, g.n, g.moff, g.n, K2);
+  }
+  tune_gemm(c, grho);
+}
+
+void launch_rho(dmrg_ctx* c, RhoSolve& rs, char* db) {
+  cudaStream_t s = c->stream;
+  run_gemm(c, rs.grho, db, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
+  run_trid_eigvals(c, c->R.p, c->R.n, rs.ttasks, 8);
+  cuda_check(cudaGetLastError(), "density matrix and eigenvalue launch");
+  run_eigs(c, c->R.p, c->R.n, rs.etasks, rs.J0, nullptr);
+  // pinned destination: the copy stays asynchronous and the host waits only in the step's sync
+  if (size_t(std::max<int64_t>(rs.wtot, 1)) > c->h_lam_cap) {
+    if (c->h_lam) cudaFreeHost(c->h_lam);
+    c->h_lam = nullptr;
+    c->h_lam_cap = 0;
+    const size_t cap = std::max<size_t>(size_t(rs.wtot), 4096);
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&c->h_lam), cap * sizeof(double)),
+               "pinned eigenvalue buffer");
+    c->h_lam_cap = cap;
+  }
+  cuda_check(cudaMemcpyAsync(c->h_lam, c->R.p + rs.W0, sizeof(double) * rs.wtot,
+                             cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
+}
+
+std::vector<std::vector<double>> rho_values(dmrg_ctx* c, const std::vector<Group>& G,
+                                            const RhoSolve& rs) {
+  std::vector<std::vector<double>> vals(G.size());
+  for (int g = 0; g < int(G.size()); ++g) {
+    const int side = rs.rows ? G[g].n : G[g].np;
+    vals[g].assign(c->h_lam + G[g].woff, c->h_lam + G[g].woff + side);
+  }
+  return vals;
+}
+
+void launch_rho_vectors(dmrg_ctx* c, const std::vector<Group>& G, const RhoSolve& rs) {
+  std::vector<TridTask> vt;
+  for (size_t a = 0; a < rs.ttasks.size(); ++a) {
+    TridTask t = rs.ttasks[a];
+    t.keep = G[rs.tgroup[a]].keep;
+    if (t.keep > 0) vt.push_back(t);
+  }
+  cuda_check(cudaGetLastError(), "eigenvalue download");
+  run_trid_vectors(c, c->R.p, c->R.n, vt, 6);
+}
+
+namespace {
+
+void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool final_step,
+             Timing& tm, StepOut& so) {
+  dmrg_ctx* c = st->ctx;
+  cudaStream_t s = c->stream;
+  const MPOSite& ml = st->mpo->site[iL];
+  const MPOSite& mr = st->mpo->site[iR];
+  const Bond Bl = st->bond[iL];
+  const Bond Bc = st->bond[iL + 1];
+  const Bond Br = st->bond[iL + 2];
+  const int d1 = ml.d, d2 = mr.d;
+  if (!st->Lvalid[iL] || !st->Rvalid[iR]) fail(DMRG_ERR_STATE, "environments are not built");
+
+  // psi[iL] (j>0) or psi[iR] (j<0) /= norm  (algs/DMRG.jl:365-369); the squared norm stays on
+  // the device
+  int tv = tm.begin();
+  const int ic = j > 0 ? iL : iR;
+  launch_mdot(s, st->A[ic].p, 0, 1, st->A[ic].p, st->lay[ic].size, c->d_partial,
+              c->d_scal + lz::NRM);
+  launch_scale_rsqrt(s, st->A[ic].p, st->lay[ic].size, c->d_scal + lz::NRM);
+  cuda_check(cudaGetLastError(), "centre normalisation");
+
+  HeffPlan hp;
+  plan_heff(st, iL, hp);
+  const TwoLayout& tl = hp.tl;
+  const SiteLayout& la = st->lay[iL];
+  const SiteLayout& lb = st->lay[iR];
+  GemmList gaa;   // AA = contract(psiL, 3, psiR, 1)
+  for (int ka = 0; ka < tl.nl; ++ka)
+    for (int s1 = 0; s1 < d1; ++s1)
+      for (int s2 = 0; s2 < d2; ++s2) {
+        const int id = tl.idx(ka, s1, s2);
+        const int kd = tl.kd[id];
+        if (kd < 0) continue;
+        gaa.add(tl.off[id], Bl.dim[ka], Bl.dim[ka], Br.dim[kd], 1.0, 0.0);
+        const int kc = la.kb[ka * d1 + s1];
+        if (kc >= 0 && lb.kb[kc * d2 + s2] == kd)
+          gaa.seg(la.off[ka * d1 + s1], Bl.dim[ka], lb.off[kc * d2 + s2], Bc.dim[kc], Bc.dim[kc]);
+      }
+  const bool split = split_form(P.precision) != 0;
+  if (split) prepare_split(hp);
+  tune_gemm(c, hp.g1);
+  tune_gemm(c, hp.g3);
+  tune_gemm(c, gaa);
+  Upload u;
+  u.put(hp.g1);
+  u.put(hp.mix);
+  u.put(hp.g3);
+  u.put(gaa);
+  if (hp.split) {
+    u.put(hp.g1t);
+    u.put(hp.g3t);
+  }
+  hp.dbase = u.send(c, 0);
+  const int64_t n = tl.size;
+  const int kdim = std::max(2, std::min(P.krylov, 16));
+  ensure(c, c->K, std::max<int64_t>(int64_t(kdim) * n, 1));
+  ensure(c, c->H, std::max<int64_t>(n, 1));
+  run_gemm(c, gaa, hp.dbase, st->A[iL].p, st->A[iL].n, st->A[iR].p, st->A[iR].n, c->K.p, n);
+  cuda_check(cudaGetLastError(), "two-site tensor");
+  tm.end(tv, 3);
+
+  const KrylovRun kr = krylov_solve(st, P, hp, n, P.krylov <= 2, final_step, tm, so);
+  const double* psi = c->H.p;
 
   // ---------------- reduced density matrix per centre-charge group (algs/DMRG.jl:425-429)
   const int te = tm.begin();
@@ -322,48 +405,8 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
     for (const Piece& p : G[g].rows) { gofrow[p.sec * d1 + p.s] = g; rowoff[p.sec * d1 + p.s] = p.off; }
     for (const Piece& p : G[g].cols) coloff[p.sec * d2 + p.s] = p.off;
   }
-  // side = dimension of the density matrix that is diagonalised (rows of M for j>0, columns
-  // for j<0). R buffer: [rho | eigenvalues | d,e,tau | eigenvectors | block-Jacobi workspace].
-  int64_t mtot = 0, rtot = 0, wtot = 0;
-  for (Group& g : G) {
-    const int side = j > 0 ? g.n : g.np;
-    g.moff = mtot; mtot += int64_t(g.n) * g.np;
-    g.roff = rtot; rtot += int64_t(side) * side;
-    g.woff = wtot; wtot += side;
-  }
-  const int64_t W0 = rtot, WS0 = rtot + wtot, U0 = rtot + 4 * wtot, J0 = 2 * rtot + 4 * wtot;
-  std::vector<EigTask> etasks;
-  std::vector<TridTask> ttasks;
-  std::vector<int> tgroup;
-  std::vector<int64_t> uoff(G.size(), 0);
-  for (int gi = 0; gi < int(G.size()); ++gi) {
-    const Group& g = G[gi];
-    const int side = j > 0 ? g.n : g.np;
-    if (side == 0) continue;
-    so.eig_max_n = std::max(so.eig_max_n, side);
-    if (side <= SYEVT_MID_NMAX) {
-      TridTask t{};
-      t.a_off = g.roff;
-      t.w_off = W0 + g.woff;
-      t.ws_off = WS0 + 3 * g.woff;
-      t.u_off = U0 + g.roff;
-      t.n = side;
-      ttasks.push_back(t);
-      tgroup.push_back(gi);
-      uoff[gi] = t.u_off;
-    } else {
-      EigTask et{};
-      et.a_off = g.roff;
-      et.v_off = g.roff;
-      et.w_off = W0 + g.woff;
-      et.n = side;
-      etasks.push_back(et);
-      uoff[gi] = g.roff;      // block Jacobi returns the eigenvectors in place
-    }
-  }
-  const int64_t ews = eig_workspace(etasks);
-  ensure(c, c->M, std::max<int64_t>(mtot, 1));
-  ensure(c, c->R, std::max<int64_t>(J0 + ews, 1));
+  RhoSolve rs;
+  plan_rho(c, G, j > 0, rs, &so.eig_max_n);
   CopyList gather;
   for (int ka = 0; ka < tl.nl; ++ka)
     for (int s1 = 0; s1 < d1; ++s1)
@@ -376,59 +419,19 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
         gather.add(tl.off[id], Bl.dim[ka], g.moff + rowoff[ka * d1 + s1] + int64_t(co) * g.n, g.n,
                    Bl.dim[ka], Br.dim[kd], 0, 1.0);
       }
-  GemmList grho;
-  grho.tA = j < 0;
-  grho.tB = j > 0;
-  for (const Group& g : G) {
-    const int side = j > 0 ? g.n : g.np;
-    if (side == 0) continue;
-    grho.add(g.roff, side, side, side, 1.0, 0.0);
-    const int K2 = j > 0 ? g.np : g.n;
-    if (K2 > 0) grho.seg(g.moff, g.n, g.moff, g.n, K2);
-  }
-  tune_gemm(c, grho);
   Upload u2;
   u2.put(gather);
-  u2.put(grho);
+  u2.put(rs.grho);
   char* db2 = u2.send(c, 1);
   run_copy(c, gather, db2, psi, n, c->M.p, c->M.n);
-  run_gemm(c, grho, db2, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
-  run_trid_eigvals(c, c->R.p, c->R.n, ttasks, 8);
-  cuda_check(cudaGetLastError(), "density matrix and eigenvalue launch");
-  run_eigs(c, c->R.p, c->R.n, etasks, J0, nullptr);
-  // pinned destination: the copy stays asynchronous and the host waits only in the sync below
-  if (size_t(std::max<int64_t>(wtot, 1)) > c->h_lam_cap) {
-    if (c->h_lam) cudaFreeHost(c->h_lam);
-    c->h_lam = nullptr;
-    c->h_lam_cap = 0;
-    const size_t cap = std::max<size_t>(size_t(wtot), 4096);
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&c->h_lam), cap * sizeof(double)),
-               "pinned eigenvalue buffer");
-    c->h_lam_cap = cap;
-  }
-  const double* lam = c->h_lam;
-  cuda_check(cudaMemcpyAsync(c->h_lam, c->R.p + W0, sizeof(double) * wtot,
-                             cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
+  launch_rho(c, rs, db2);
   const auto w0 = std::chrono::steady_clock::now();
   cuda_check(cudaStreamSynchronize(s), "eigen sync");
   so.wait = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   tuner_collect(c);
-  so.energy = c->h_scal[lz::EN];
-  if (fp64_energy && c->h_scal[lz::KK] > 0) so.energy = c->h_scal[lz::KH] / c->h_scal[lz::KK];
-  if (split) {
-    int flag = 0;
-    std::memcpy(&flag, c->h_scal + 20, sizeof(int));
-    if (flag != 0) {
-      cudaMemsetAsync(c->d_status + STATUS_MMA, 0, sizeof(int), s);
-      fail(DMRG_ERR_TIMEOUT, "split-precision GEMM: a tensor-core MMA completion wait gave up");
-    }
-  }
+  so.energy = krylov_energy(c, kr);
 
-  std::vector<std::vector<double>> vals(G.size());
-  for (int g = 0; g < int(G.size()); ++g) {
-    const int side = j > 0 ? G[g].n : G[g].np;
-    vals[g].assign(lam + G[g].woff, lam + G[g].woff + side);
-  }
+  const std::vector<std::vector<double>> vals = rho_values(c, G, rs);
   const Sel sel = select_kept(vals, P.maxm, P.minm, P.cutoff, 1.0, P.degen_rtol);
   Bond C;
   std::vector<double> kept;
@@ -445,15 +448,8 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   for (size_t a = 0; a < kept.size(); ++a) so.D[a] = std::sqrt(std::max(kept[a], 0.0));
   so.truncerr = sel.truncerr;
   so.m = int(kept.size());
-  // eigenvectors of the kept states of the tridiagonal-path blocks
-  std::vector<TridTask> vt;
-  for (size_t a = 0; a < ttasks.size(); ++a) {
-    TridTask t = ttasks[a];
-    t.keep = G[tgroup[a]].keep;
-    if (t.keep > 0) vt.push_back(t);
-  }
-  cuda_check(cudaGetLastError(), "eigenvalue download");
-  run_trid_vectors(c, c->R.p, c->R.n, vt, 6);
+  launch_rho_vectors(c, G, rs);
+  const std::vector<int64_t>& uoff = rs.uoff;
 
   // ---------------- split back into the two site tensors (algs/DMRG.jl:389-395, 483-490)
   cuda_check(cudaGetLastError(), "eigenvectors");

@@ -400,6 +400,15 @@ class DeviceState:
         check(lib().dmrg_sweep(self.h, self.dmpo.h, C.byref(params), C.byref(st)), self.ctx.h)
         return st.as_dict()
 
+    def sweep3s(self, params: Params, noise: "_lib.Noise"):
+        """One single-site sweep with subspace expansion; ``noise.noise`` (alpha) is updated."""
+        st = SweepStats()
+        check(lib().dmrg_sweep3s(self.h, self.dmpo.h, C.byref(params), C.byref(noise),
+                                 C.byref(st)), self.ctx.h)
+        d = st.as_dict()
+        d["noise"] = noise.noise
+        return d
+
     def __del__(self):
         try:
             if self.h and self.ctx.h:
@@ -429,16 +438,20 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
 
 def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, silent=True,
          method="twosite", krylov=2, precision="fp64", SvNbond=0, degen_rtol=0.0, goal=0.0,
-         cvgE=True, ctx=None, download=True):
-    """Two-site DMRG on the GPU: ``dmrg(psi, mpo; m, minm, sweeps, cutoff)`` of
-    ``algs/DMRG.jl:549-588``. ``maxm`` is accepted as an alias of ``m``; ``m`` may also be a
-    per-sweep list (a bond-dimension ramp). Returns the energy of the last bond step and updates
-    ``psi`` (tensors, ``oc``) in place; per-sweep records go to ``psi.sweep_stats``.
+         cvgE=True, noise=1.0, noise_goal=0.3, noise_incr=0.01, ctx=None, download=True):
+    """DMRG on the GPU: ``dmrg(psi, mpo; m, minm, sweeps, cutoff, method)`` of
+    ``algs/DMRG.jl:549-588``. ``method="twosite"`` (default) runs ``dmrg_twosite``;
+    ``method="3S"`` runs ``dmrg3S`` (``algs/DMRG.jl:655-671``: single-site steps with subspace
+    expansion weighted by ``noise``, adapted by ``alpha_update`` with ``noise_goal`` and
+    ``noise_incr``; Krylov dimension ``max(2, krylov)``).
+    ``maxm`` is accepted as an alias of ``m``; ``m`` may also be a per-sweep list (a bond-dimension
+    ramp). Returns the energy of the last bond step and updates ``psi`` (tensors, ``oc``) in
+    place; per-sweep records go to ``psi.sweep_stats``.
     ``goal > 0`` stops after the first sweep whose energy (``cvgE``) or centre entropy changed by
     less than ``goal`` (``dmrgcvg``, ``algs/DMRG.jl:610-652``; the first sweep is compared with
     the starting energy <psi|H|psi>).
     ``download=False`` leaves the result on the device (``psi`` keeps a handle to it)."""
-    if method != "twosite":
+    if method not in ("twosite", "3S"):
         raise ValueError(f"DMRG method ({method}) not defined")
     mm = m if m is not None else (maxm if maxm is not None else 0)
     sched = list(mm) if np.ndim(mm) else [int(mm)] * int(sweeps)
@@ -447,9 +460,15 @@ def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, si
     dev.env_build()
     energy = 0.0
     stats = []
+    nz = None
+    if method == "3S":
+        nz = _lib.Noise()
+        lib().dmrg_noise_default(C.byref(nz))
+        nz.noise, nz.noise_goal, nz.noise_incr = float(noise), float(noise_goal), float(noise_incr)
     for n, mcur in enumerate(sched):
-        st = dev.sweep(make_params(mcur, minm, cutoff, krylov, precision, SvNbond, degen_rtol,
-                                   goal=goal, cvgE=cvgE))
+        p = make_params(mcur, minm, cutoff, krylov, precision, SvNbond, degen_rtol, goal=goal,
+                        cvgE=cvgE)
+        st = dev.sweep(p) if nz is None else dev.sweep3s(p, nz)
         energy = st["energy"]
         stats.append(st)
         if not silent:

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG_ABI_VERSION 2
+#define DMRG_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define DMRG_API __attribute__((visibility("default")))
@@ -251,6 +251,32 @@ DMRG_API int dmrg_correlationmatrix(dmrg_state* st, int d, const double* Cc, con
  * One optmps sweep (algs/optimizeMPS.jl:790-835): 2(L-1) twostep calls, each followed by an
  * environment update; the centre reverses at the edges. Requires dmrg_env_build first. */
 DMRG_API int dmrg_sweep(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg_sweep_stats* out);
+
+/* Noise schedule of the single-site sweep with subspace expansion (method "3S"): the
+ * noise / noise_goal / noise_incr fields of algvars (algs/optimizeMPS.jl:528-532). */
+typedef struct dmrg_noise {
+  double noise;       /* alpha, the weight of the expansion term (default 1.0): in = its value at the
+                         start of the sweep, out = after the sweep's last alpha_update           */
+  double noise_goal;  /* default 0.3: the site condition of alpha_update (algs/DMRG.jl:289-302) */
+  double noise_incr;  /* default 0.01: alpha's relative step; the centre is expanded while
+                         alpha > noise_incr (alpha_condition, algs/DMRG.jl:335)                */
+  double reserved;
+} dmrg_noise;
+
+/* Fills *nz with the reference defaults (noise 1.0, noise_goal 0.3, noise_incr 0.01). */
+DMRG_API void dmrg_noise_default(dmrg_noise* nz);
+
+/* One optmps sweep with step3S (algs/DMRG.jl:324-360, dmrg3S :655-671): 2(L-1) single-site steps
+ * (Krylov solve of the single-site Heff with max(2, krylov) vectors, expansion by Lexpand /
+ * Rexpand while alpha > noise_incr, truncated move of the centre with weights relative to the
+ * total (moveR! / moveL! with condition, lib/MPS/move.jl:124-199), alpha_update), each followed
+ * by an environment update. p: maxm, minm, cutoff, krylov, precision, svnbond, degen_rtol,
+ * betatest, fp64_final, profile, tune, graph, goal and cvgE as for dmrg_sweep. The lastEnergy of
+ * alpha_update is the previous sweep's energy (the starting energy <psi|H|psi> for the first
+ * sweep after dmrg_env_build); with cvgE = 0 it stays the starting energy (dmrgcvg,
+ * algs/DMRG.jl:626-652). max_truncerr is relative to the total weight of each step. */
+DMRG_API int dmrg_sweep3s(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p,
+                          dmrg_noise* nz, dmrg_sweep_stats* out);
 /* ---------------------------------------------------------------- kernel test hooks
  * No reference counterpart: these expose single device kernels to the parity tests.
  * C[M,N] = op(A) op(B) with the grouped FP64 GEMM (one task, one K segment), host arrays,

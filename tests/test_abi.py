@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol(dmrgb):
 
 def test_abi_version_and_defaults(dmrgb):
     lib = dmrgb.lib()
-    assert lib.dmrg_abi_version() == 2
+    assert lib.dmrg_abi_version() == 3
     p = dmrgb._lib.Params()
     lib.dmrg_params_default(C.byref(p))
     assert (p.minm, p.krylov, p.maxm, p.precision) == (2, 2, 0, 0)
@@ -36,6 +36,11 @@ def test_abi_version_and_defaults(dmrgb):
     assert (p.tune, p.graph) == (1, 1)
     # the ctypes mirrors have the C layout: 80-byte params, stats end with the convergence fields
     assert C.sizeof(dmrgb._lib.Params) == 80
+    # the 3S noise schedule (algs/optimizeMPS.jl:528-532)
+    nz = dmrgb._lib.Noise()
+    lib.dmrg_noise_default(C.byref(nz))
+    assert (nz.noise, nz.noise_goal, nz.noise_incr) == (1.0, 0.3, 0.01)
+    assert C.sizeof(dmrgb._lib.Noise) == 32
 
 
 def test_null_handles_are_rejected(dmrgb):
@@ -44,6 +49,7 @@ def test_null_handles_are_rejected(dmrgb):
     assert lib.dmrg_state_destroy(None) == dmrgb._lib.ERR_ARG
     assert lib.dmrg_mpo_destroy(None) == dmrgb._lib.ERR_ARG
     assert lib.dmrg_sweep(None, None, None, None) == dmrgb._lib.ERR_ARG
+    assert lib.dmrg_sweep3s(None, None, None, None, None) == dmrgb._lib.ERR_ARG
 
 
 def test_context_without_gpu_reports_nocuda(dmrgb):

@@ -1,0 +1,124 @@
+"""Device 3S sweeps (``dmrg_sweep3s``: single-site steps with subspace expansion, the reference's
+``dmrg3S`` / ``method="3S"``, algs/DMRG.jl:324-360,655-671) against the oracle's restatement.
+
+Both start from the same product state and run the same number of sweeps; the comparison is on
+invariants (energy, alpha, largest bond dimension, truncation error), never on the gauge-dependent
+tensors. Tolerances: FP64 throughout, energies to 1e-9 relative per sweep. alpha is a product of
+(1 +- noise_incr) factors, each decided by thresholds such as truncerr <= max(cutoff, 1e-12) that
+converged steps sit right on (truncation errors near 1e-12 known to ~1e-16 absolute), so a
+decision may come out the other way on rounding: alpha agrees to within a few such steps (5%).
+"""
+import numpy as np
+import pytest
+
+from oracle import dmrg3s as o3, ed, models as om
+
+pytestmark = pytest.mark.gpu
+
+SPIN = [(1,), (-1,)]
+HQ = [(0, 0), (1, 1), (1, -1), (2, 0)]
+
+
+def _compare(stats, recs, rtol=1e-9):
+    assert len(stats) == len(recs)
+    for a, b in zip(stats, recs):
+        assert abs(a["energy"] - b["energy"]) <= rtol * abs(b["energy"])
+        assert a["noise"] == pytest.approx(b["noise"], rel=0.05)
+        assert a["biggest_m"] == b["biggestm"]
+        assert abs(a["max_truncerr"] - b["maxtrunc"]) <= 1e-8
+
+
+def test_3s_heisenberg_u1_matches_oracle_per_sweep(dmrgb, ctx):
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    E = dmrgb.dmrg(psi, mpo, m=45, sweeps=12, cutoff=1e-12, method="3S", ctx=ctx)
+    start = om.neel_mps(L)
+    ompo = om.make_mpo([om.heisenberg_bulk()] * L, 2)
+    E0, recs, _ = o3.dmrg3s(start, ompo, [SPIN] * L, om.mps_bond_labels(start, [SPIN] * L),
+                            m=45, sweeps=12, cutoff=1e-12)
+    _compare(psi.sweep_stats, recs)
+    assert abs(E - E0) <= 1e-9 * abs(E0)
+    assert psi.oc == 0
+
+
+def test_3s_dense_matches_oracle_and_reaches_ed(dmrgb, ctx):
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    psi = dmrgb.neelMPS(L)
+    E = dmrgb.dmrg(psi, mpo, m=45, sweeps=30, cutoff=1e-12, method="3S", ctx=ctx)
+    start = om.neel_mps(L)
+    ompo = om.make_mpo([om.heisenberg_bulk()] * L, 2)
+    zero = [[(0,)] * len(b) for b in om.mps_bond_labels(start, [SPIN] * L)]
+    E0, recs, _ = o3.dmrg3s(start, ompo, [[(0,), (0,)]] * L, zero, m=45, sweeps=30, cutoff=1e-12)
+    _compare(psi.sweep_stats[:6], recs[:6])
+    assert abs(E - E0) <= 1e-9 * abs(E0)
+    assert abs(E - ed.sparse_ground_energy(ompo)) < 1e-8
+
+
+def test_3s_hubbard_u1xu1_matches_oracle(dmrgb, ctx):
+    L = 8
+    mpo = dmrgb.makeMPO(dmrgb.hubbardMPO, 4, L).with_qn(dmrgb.HUBBARD_QN)
+    start = om.hubbard_half_filling_mps(L)
+    psi = dmrgb.MPS([np.array(a) for a in start], oc=0)
+    E = dmrgb.dmrg(psi, mpo, m=32, sweeps=8, cutoff=1e-9, method="3S", ctx=ctx)
+    ompo = om.make_mpo([om.hubbard_bulk()] * L, 4)
+    E0, recs, _ = o3.dmrg3s(start, ompo, [HQ] * L, om.mps_bond_labels(start, [HQ] * L), m=32,
+                            sweeps=8, cutoff=1e-9)
+    _compare(psi.sweep_stats, recs, rtol=1e-8)
+    assert abs(E - E0) <= 1e-8 * abs(E0)
+
+
+@pytest.mark.parametrize("krylov", [2, 4])
+def test_3s_krylov_and_goal(dmrgb, ctx, krylov):
+    """Krylov dimension r (params.r) and the dmrgcvg stop (goal) through the 3S sweep."""
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    E = dmrgb.dmrg(psi, mpo, m=45, sweeps=60, cutoff=1e-12, method="3S", krylov=krylov,
+                   goal=1e-10, ctx=ctx)
+    start = om.neel_mps(L)
+    ompo = om.make_mpo([om.heisenberg_bulk()] * L, 2)
+    E0, recs, _ = o3.dmrg3s(start, ompo, [SPIN] * L, om.mps_bond_labels(start, [SPIN] * L),
+                            m=45, sweeps=60, cutoff=1e-12, krylov=krylov, goal=1e-10)
+    assert len(psi.sweep_stats) == len(recs) < 60
+    assert psi.sweep_stats[-1]["converged"] == 1
+    assert abs(E - E0) <= 1e-9 * abs(E0)
+
+
+@pytest.mark.parametrize("precision", ["3xtf32", "bf16x9"])
+def test_3s_split_forms_agree_with_fp64(dmrgb, ctx, precision):
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    a = dmrgb.neelMPS(L)
+    b = dmrgb.neelMPS(L)
+    Ea = dmrgb.dmrg(a, mpo, m=45, sweeps=20, cutoff=1e-12, method="3S", ctx=ctx)
+    Eb = dmrgb.dmrg(b, mpo, m=45, sweeps=20, cutoff=1e-12, method="3S", precision=precision,
+                    ctx=ctx)
+    assert abs(Ea - Eb) < 1e-8
+
+
+def test_3s_then_twosite_on_the_same_state(dmrgb, ctx):
+    """A state optimised by 3S sweeps continues under two-site sweeps (bonds, layouts and
+    environments left consistent by the single-site moves)."""
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    dmrgb.dmrg(psi, mpo, m=45, sweeps=4, cutoff=1e-12, method="3S", ctx=ctx)
+    E = dmrgb.dmrg(psi, mpo, m=45, sweeps=4, cutoff=1e-12, ctx=ctx)
+    assert abs(E - (-4.258035207282883)) < 1e-8
+
+
+def test_3s_dense_and_qn_agree_at_l100(dmrgb, ctx):
+    """test/dmrg_test.jl:82-85 for method "3S": the L=100 Heisenberg chain from the Neel state,
+    dense and U(1) runs at m=45, cutoff 1e-12 agree to 1e-4 (the reference's bar)."""
+    L = 100
+    out = []
+    for qn in (False, True):
+        mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+        if qn:
+            mpo = mpo.with_qn(dmrgb.SPIN_QN)
+        psi = dmrgb.neelMPS(L)
+        out.append(dmrgb.dmrg(psi, mpo, m=45, sweeps=30, cutoff=1e-12, method="3S", ctx=ctx))
+    assert abs(out[0] - out[1]) < 1e-4
+    assert abs(out[1] - (-44.127739)) < 1e-3     # the L=100 chain's two-site energy at m=45..128

@@ -44,4 +44,4 @@ def test_params_mapping(dmrgb):
 def test_dmrg_rejects_other_methods(dmrgb):
     import pytest
     with pytest.raises(ValueError, match="not defined"):
-        dmrgb.dmrg(dmrgb.neelMPS(4), dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, 4), method="3S")
+        dmrgb.dmrg(dmrgb.neelMPS(4), dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, 4), method="2S")

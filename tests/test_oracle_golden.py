@@ -116,3 +116,52 @@ def test_oracle_goal_semantics():
     assert len(info["sweeps"]) == 1
     e0 = info["e0"]
     assert e0 == pytest.approx(od.expect([a.copy() for a in start], mpo), rel=1e-12)
+
+
+# ------------------------------------------------------------------ the 3S method (dmrg3S)
+
+def test_3s_oracle_reaches_ed_with_and_without_charges():
+    """test/dmrg_test.jl:82-85 (method "3S"): the dense and the charge-labelled runs agree (the
+    reference allows 1e-4); both reach ED here."""
+    from oracle import dmrg3s as o3
+    L = 10
+    mpo = heis(L)
+    start = om.neel_mps(L)
+    q = om.mps_bond_labels(start, [SPIN] * L)
+    E, recs, _ = o3.dmrg3s(start, mpo, [SPIN] * L, q, m=45, sweeps=40, cutoff=1e-12)
+    zero = [[(0,)] * len(b) for b in q]
+    Ed, _, _ = o3.dmrg3s(start, mpo, [[(0,), (0,)]] * L, zero, m=45, sweeps=40, cutoff=1e-12)
+    e0 = ed.sparse_ground_energy(mpo)
+    assert abs(E - e0) < 1e-9
+    assert abs(Ed - e0) < 1e-9
+    assert all(r["biggestm"] <= 45 for r in recs)
+    assert recs[-1]["noise"] < recs[0]["noise"]      # alpha decays once the energy settles
+
+
+def test_3s_oracle_hubbard_known_answer():
+    from oracle import dmrg3s as o3
+    p = PINS["hubbard_L10_qn_dmrg"]
+    L = 10
+    hq = [(0, 0), (1, 1), (1, -1), (2, 0)]
+    start = om.hubbard_half_filling_mps(L)
+    E, _, _ = o3.dmrg3s(start, om.make_mpo([om.hubbard_bulk()] * L, 4), [hq] * L,
+                        om.mps_bond_labels(start, [hq] * L), m=45, sweeps=20, cutoff=1e-9)
+    assert abs(E - p["value"]) < p["tol"]
+
+
+def test_alpha_update_rules():
+    """alpha_update (algs/DMRG.jl:289-302): shrink by (1 - dalpha) when the energy did not rise
+    and one of the three conditions holds, else grow; clamped to [1e-42, 1]; IEEE division."""
+    from oracle.dmrg3s import alpha_update
+    # truncation below the cutoff: shrink
+    assert alpha_update(0.5, 1e-14, 1e-12, -1.0, -1.1, 0.3, 0.01) == pytest.approx(0.495)
+    # energy rose: grow, whatever the truncation
+    assert alpha_update(0.5, 0.0, 1e-12, -1.1, -1.0, 0.3, 0.01) == pytest.approx(0.505)
+    # large truncation, energy moving: site condition |trunc E / (E_last/E - 1)| vs noise_goal
+    assert alpha_update(0.5, 1e-3, 1e-12, -1.0, -1.01, 0.3, 0.01) == pytest.approx(0.505)
+    assert alpha_update(0.5, 1e-2, 1e-12, -1.0, -1.01, 0.3, 0.01) == pytest.approx(0.495)
+    # clamps
+    assert alpha_update(1.0, 1.0, 0.0, -1.1, -1.0, 0.3, 0.01) == 1.0
+    assert alpha_update(1e-42, 0.0, 1e-12, -1.0, -1.0, 0.3, 0.5) == 1e-42
+    # equal energies: the site condition is 0/0 (NaN, false) but err_est holds: shrink
+    assert alpha_update(0.5, 0.0, 0.0, -2.0, -2.0, 0.3, 0.1) == pytest.approx(0.45)
