@@ -1,5 +1,6 @@
-"""dmrjtensor_b200 -- a B200-native two-site DMRG engine, drop-in for DMRJtensor.jl's
-``dmrg(psi, mpo; m, sweeps, cutoff)`` path and its ``makeEnv``/``Lupdate``/``Rupdate`` API.
+"""dmrjtensor_b200 -- a B200-native DMRG engine, drop-in for DMRJtensor.jl's
+``dmrg(psi, mpo; m, sweeps, cutoff, method)`` path (two-site and 3S), its ``makeEnv``/``Lupdate``/
+``Rupdate`` API, and ``tdvp``/``tdvp_twosite`` with real prefactors.
 
 The compute runs in ``libdmrgb200.so`` (hand-written sm_100a kernels behind a C ABI,
 ``include/dmrg_b200.h``); this package is the host-side mirror of the reference interface.
@@ -10,7 +11,8 @@ from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heise
                      heisenbergMPO, hubbardMPO, makeMPO, spinOps, tfiMPO)
 from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
                     correlationmatrix, default_context, dmrg, expect, largeMPS, loadMPS,
-                    make_params, makeEnv, mpo_product, neelMPS, product_MPS, randMPS)
+                    make_params, makeEnv, mpo_product, neelMPS, product_MPS, randMPS, tdvp,
+                    tdvp_twosite)
 from .serving import Server, ServerError
 
 
@@ -26,6 +28,6 @@ __all__ = [
     "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
     "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",
     "default_context", "dmrg", "make_params", "makeEnv", "neelMPS", "product_MPS", "randMPS",
-    "expect", "mpo_product", "correlationmatrix", "largeMPS", "loadMPS",
+    "expect", "mpo_product", "correlationmatrix", "largeMPS", "loadMPS", "tdvp", "tdvp_twosite",
     "Server", "ServerError",
 ]

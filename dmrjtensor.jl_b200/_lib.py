@@ -126,6 +126,7 @@ SIGNATURES = {
     "dmrg_params_default": (None, [C.POINTER(Params)]),
     "dmrg_noise_default": (None, [C.POINTER(Noise)]),
     "dmrg_sweep3s": (C.c_int, [_P, _P, C.POINTER(Params), C.POINTER(Noise), C.POINTER(SweepStats)]),
+    "dmrg_tdvp": (C.c_int, [_P, _P, C.POINTER(Params), C.c_double, C.c_int, C.POINTER(SweepStats)]),
     "dmrg_test_gemm": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int,
                                  _DP, C.c_int, _DP, C.c_int]),
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),

@@ -19,7 +19,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxe
          "-Xcompiler", "-fvisibility=hidden"]
 
 SOURCES = ["gemm_f64.cu", "gemm_tf32.cu", "vec_kernels.cu", "jacobi.cu", "jacobi_block.cu", "syevt.cu", "syevt_mid.cu", "noalloc.cu", "engine_layout.cpp", "engine_eig.cpp",
-           "engine_contract.cpp", "engine_sweep.cpp", "engine_3s.cpp", "engine_meas.cpp", "abi.cpp", "server.cpp", "batch.cpp"]
+           "engine_contract.cpp", "engine_sweep.cpp", "engine_3s.cpp", "engine_tdvp.cpp", "engine_meas.cpp", "abi.cpp", "server.cpp", "batch.cpp"]
 
 
 def _needs_build(objs_src):

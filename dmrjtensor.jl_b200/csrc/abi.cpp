@@ -964,6 +964,18 @@ int dmrg_sweep3s(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, dmrg
   });
 }
 
+int dmrg_tdvp(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p, double prefactor,
+              int twosite, dmrg_sweep_stats* out) {
+  if (!st) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    if (mpo != st->mpo) fail(DMRG_ERR_ARG, "state was uploaded with a different MPO");
+    if (!p || !out) fail(DMRG_ERR_ARG, "null params/stats");
+    set_device(c);
+    do_tdvp(st, *p, prefactor, twosite != 0, *out);
+  });
+}
+
 int dmrg_test_syevt(dmrg_ctx* c, int nmat, const int* n, const int* k, double* A, double* w,
                     double* U) {
   if (!c) return DMRG_ERR_ARG;

@@ -325,6 +325,12 @@ struct HeffPlan {
   char* dbase = nullptr;
 };
 void plan_heff(const dmrg_state* st, int iL, HeffPlan& hp);
+// The zero-site Heff of a bond matrix C[a, d] (OC_update, algs/time.jl:205-209):
+// sum L[a,w,b] C[b,c] R[c,w,d] with Lenv[le] on bond Bl and Renv[re] on bond Br (the MPO bond
+// between sites re and le); the same three launches with two trivial sites. C's layout: one
+// block per sector of Bl, against the sector of Br with the same charge.
+void plan_heff_bond(const dmrg_state* st, int le, int re, const Bond& Bl, const Bond& Br,
+                    HeffPlan& hp);
 // The single-site Heff at site i (singlesite_update, algs/optimizeMPS.jl:503-511): the same three
 // launches with a second site of dimension one (charge zero), reading Lenv[i] and Renv[i]; its
 // vector layout is the site layout of A[i].
@@ -412,5 +418,8 @@ void do_sweep(dmrg_state* st, const dmrg_params& p, dmrg_sweep_stats& out);
 // alpha_update (the previous sweep's energy, or the starting energy).
 void do_sweep3s(dmrg_state* st, const dmrg_params& p, const dmrg_noise& nz, double* noise,
                 double last_energy, dmrg_sweep_stats& out);
+// ---- TDVP with a real prefactor (engine_tdvp.cpp): one call of tdvp_twosite (twosite) or tdvp
+void do_tdvp(dmrg_state* st, const dmrg_params& p, double prefactor, bool twosite,
+             dmrg_sweep_stats& out);
 
 }  // namespace dmrg

@@ -66,8 +66,11 @@ Bond select_groups(std::vector<Group>& G, const std::vector<std::vector<double>>
   return C;
 }
 
-void step3s(dmrg_state* st, const dmrg_params& P, double alpha, double noise_incr, int j, int i,
-            bool final_step, Timing& tm, StepOut& so) {
+}  // namespace
+
+void single_site_step(dmrg_state* st, const dmrg_params& P, const SiteMode& md, int j, int i,
+                      bool final_step, Timing& tm, StepOut& so) {
+  const double alpha = md.alpha, noise_incr = md.noise_incr;
   dmrg_ctx* c = st->ctx;
   cudaStream_t s = c->stream;
   const int L = st->L;
@@ -103,9 +106,10 @@ void step3s(dmrg_state* st, const dmrg_params& P, double alpha, double noise_inc
   cuda_check(cudaMemcpyAsync(c->K.p, st->A[i].p, size_t(n) * sizeof(double),
                              cudaMemcpyDeviceToDevice, s), "3S start vector");
   tm.end(tv, 3);
-  const KrylovRun kr = krylov_solve(st, P, hp, n, false, final_step, tm, so);
+  const KrylovRun kr = md.tdvp ? krylov_solve(st, P, hp, n, false, false, tm, so, md.tau, true)
+                               : krylov_solve(st, P, hp, n, false, final_step, tm, so);
   const double* psi = c->H.p;
-  const bool expand = alpha > noise_incr;   // alpha_condition (algs/DMRG.jl:335)
+  const bool expand = !md.tdvp && alpha > noise_incr;   // alpha_condition (algs/DMRG.jl:335)
 
   const int te = tm.begin();
   std::map<QN, Group> gm;
@@ -368,26 +372,61 @@ void step3s(dmrg_state* st, const dmrg_params& P, double alpha, double noise_inc
   u3.put(gv);
   u3.put(gn);
   char* db3 = u3.send(c, 3);
-  ensure(c, c->T1, std::max<int64_t>(vtot, 1));
+  // the bond matrix (U^T M or M V, restricted to the original states): T1 in the 3S step; in the
+  // TDVP step the start vector of its Krylov exponential, c->K (the environment update that comes
+  // first uses T1 as scratch)
+  DBuf& bmb = md.tdvp ? c->K : c->T1;
+  ensure(c, bmb, std::max<int64_t>(md.tdvp ? int64_t(kdim) * vtot : vtot, 1));
   dalloc(c, nC, std::max<int64_t>(nlc.size, 1));
   dalloc(c, nN, std::max<int64_t>(nln.size, 1));
   cuda_check(cudaMemsetAsync(nN.p, 0, size_t(nN.n) * sizeof(double), s), "3S neighbour");
   run_copy(c, cp, db3, c->R.p, c->R.n, nC.p, nC.n);
-  if (j > 0) {
-    run_gemm(c, gv, db3, c->R.p, c->R.n, c->M.p, c->M.n, c->T1.p, c->T1.n);
-    run_gemm(c, gn, db3, c->T1.p, c->T1.n, st->A[in].p, st->A[in].n, nN.p, nN.n);
-  } else {
-    run_gemm(c, gv, db3, c->M.p, c->M.n, c->R.p, c->R.n, c->T1.p, c->T1.n);
-    run_gemm(c, gn, db3, st->A[in].p, st->A[in].n, c->T1.p, c->T1.n, nN.p, nN.n);
-  }
-  cuda_check(cudaGetLastError(), "3S move");
+  if (j > 0)
+    run_gemm(c, gv, db3, c->R.p, c->R.n, c->M.p, c->M.n, bmb.p, bmb.n);
+  else
+    run_gemm(c, gv, db3, c->M.p, c->M.n, c->R.p, c->R.n, bmb.p, bmb.n);
+  const Bond Bold = j > 0 ? Br : Bl;
   dfree(c, st->A[i]);
-  dfree(c, st->A[in]);
   st->A[i] = nC;
-  st->A[in] = nN;
   st->lay[i] = nlc;
-  st->lay[in] = nln;
   st->bond[j > 0 ? i + 1 : i] = C;
+  const double* bm = bmb.p;
+  int64_t bmn = bmb.n;
+  if (md.tdvp) {
+    // tdvp (algs/time.jl:244-274): the environment across the new bond, then the bond matrix
+    // evolved by exp(tau H0) with the zero-site Heff (OC_update, :205-209) between Lenv and Renv
+    double ef = 0.0;
+    if (j > 0) lupdate(st, i, &ef, P.precision); else rupdate(st, i, &ef, P.precision);
+    so.env_flops += ef;
+    HeffPlan hz;
+    const int le = j > 0 ? i + 1 : i, re = j > 0 ? i : i - 1;
+    plan_heff_bond(st, le, re, j > 0 ? C : Bold, j > 0 ? Bold : C, hz);
+    if (hz.tl.size != vtot) fail(DMRG_ERR_ARG, "internal plan check failed: TDVP bond matrix");
+    if (split_form(P.precision)) prepare_split(hz);
+    tune_gemm(c, hz.g1);
+    tune_gemm(c, hz.g3);
+    Upload uz;
+    uz.put(hz.g1);
+    uz.put(hz.mix);
+    uz.put(hz.g3);
+    if (hz.split) {
+      uz.put(hz.g1t);
+      uz.put(hz.g3t);
+    }
+    hz.dbase = uz.send(c, 0);
+    ensure(c, c->H, std::max<int64_t>(vtot, 1));
+    krylov_solve(st, P, hz, vtot, false, false, tm, so, md.tau, true);
+    bm = c->H.p;
+    bmn = c->H.n;
+  }
+  if (j > 0)
+    run_gemm(c, gn, db3, bm, bmn, st->A[in].p, st->A[in].n, nN.p, nN.n);
+  else
+    run_gemm(c, gn, db3, st->A[in].p, st->A[in].n, bm, bmn, nN.p, nN.n);
+  cuda_check(cudaGetLastError(), "single-site move");
+  dfree(c, st->A[in]);
+  st->A[in] = nN;
+  st->lay[in] = nln;
   // environments that read a changed tensor and are not rebuilt by this step's update
   if (j > 0) {
     st->Rvalid[i] = 0;
@@ -398,8 +437,6 @@ void step3s(dmrg_state* st, const dmrg_params& P, double alpha, double noise_inc
   }
   tm.end(te, 2);
 }
-
-}  // namespace
 
 void do_sweep3s(dmrg_state* st, const dmrg_params& P, const dmrg_noise& nz, double* noise,
                 double last_energy, dmrg_sweep_stats& out) {
@@ -423,7 +460,10 @@ void do_sweep3s(dmrg_state* st, const dmrg_params& P, const dmrg_noise& nz, doub
   for (int ns = 0; ns < 2 * (L - 1); ++ns) {
     const int i = st->oc;
     StepOut so;
-    step3s(st, P, alpha, nz.noise_incr, j, i, ns == 2 * (L - 1) - 1, tm, so);
+    SiteMode md;
+    md.alpha = alpha;
+    md.noise_incr = nz.noise_incr;
+    single_site_step(st, P, md, j, i, ns == 2 * (L - 1) - 1, tm, so);
     alpha = alpha_update(alpha, so.truncerr, P.cutoff, last_energy, so.energy, nz.noise_goal,
                          nz.noise_incr);
     const int tenv = tm.begin();

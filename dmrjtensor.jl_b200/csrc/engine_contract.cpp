@@ -38,6 +38,21 @@ void plan_heff1(const dmrg_state* st, int i, HeffPlan& hp) {
     fail(DMRG_ERR_ARG, "internal plan check failed: single-site Heff layout");
 }
 
+void plan_heff_bond(const dmrg_state* st, int le, int re, const Bond& Bl, const Bond& Br,
+                    HeffPlan& hp) {
+  static const std::vector<QN> trivial(1, QN());
+  if (le != re + 1 || re < 0 || le >= st->L) fail(DMRG_ERR_ARG, "zero-site Heff: bad bond");
+  const MPOSite& ms = st->mpo->site[le];
+  TwoSiteOp op;   // identity on the MPO bond
+  op.d1 = op.d2 = 1;
+  op.wl = op.wr = ms.wl;
+  op.out.assign(size_t(ms.wl), {});
+  for (int w = 0; w < ms.wl; ++w) op.out[w].push_back({w, 0, 0, 1.0});
+  hp.le = le;
+  hp.re = re;
+  plan_heff_core(Bl, Br, trivial, trivial, ms.rl, op, st->Llay[le], st->Rlay[re], hp);
+}
+
 namespace {
 void plan_heff_core(const Bond& Bl, const Bond& Br, const std::vector<QN>& p1,
                     const std::vector<QN>& p2, const std::vector<QN>& rl, const TwoSiteOp& op,

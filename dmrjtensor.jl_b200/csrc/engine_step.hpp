@@ -45,7 +45,7 @@ struct StepOut {
   double energy = 0, truncerr = 0, wait = 0;
   int m = 0, nmv = 0;
   std::vector<double> D;       // kept singular values, descending
-  double heff_flops = 0;
+  double heff_flops = 0, env_flops = 0;
   int eig_max_n = 0;
 };
 
@@ -59,9 +59,38 @@ struct KrylovRun {
   bool split = false;
   bool fp64_energy = false;
 };
+// expo: the combination is exp(tau T) e_1 instead of the lowest Ritz vector (krylovTimeEvol).
 KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp, int64_t n,
-                       bool simple2, bool final_step, Timing& tm, StepOut& so);
+                       bool simple2, bool final_step, Timing& tm, StepOut& so, double tau = 0.0,
+                       bool expo = false);
 double krylov_energy(dmrg_ctx* c, const KrylovRun& kr);
+
+// What a bond step optimises: the ground state (DMRG), or one TDVP time step of length tau
+// (Krylov exponential instead of the Ritz vector, truncation weights relative to the total).
+struct StepMode {
+  bool tdvp = false;
+  double tau = 0.0;
+};
+
+// The two-site bond step (twostep, algs/DMRG.jl:362-405; in TDVP mode the first half of a
+// tdvp_twosite step, algs/time.jl:317-353): Krylov on the two-site Heff, density-matrix
+// truncation, split into psi[iL], psi[iR] (j > 0: psi[iL] = U, psi[iR] = U^T psi; j < 0:
+// psi[iL] = psi V, psi[iR] = V^T).
+void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool final_step,
+             Timing& tm, StepOut& so, const StepMode& mode);
+
+// The single-site step (engine_3s.cpp) at site i, direction j: step3S (algs/DMRG.jl:324-360,
+// expansion while alpha > noise_incr) or, in TDVP mode, one step of tdvp (algs/time.jl:240-274):
+// Krylov exponential at the site, truncated decomposition, the environment update across the new
+// bond (done inside the step in this mode), the bond matrix evolved with the zero-site Heff, and
+// its product with the neighbour. so.env_flops counts the update done inside.
+struct SiteMode {
+  bool tdvp = false;
+  double tau = 0.0;
+  double alpha = 0.0, noise_incr = 0.0;
+};
+void single_site_step(dmrg_state* st, const dmrg_params& P, const SiteMode& md, int j, int i,
+                      bool final_step, Timing& tm, StepOut& so);
 
 // Charge groups of a matricised centre tensor: rows and columns are pieces (sector, state) at
 // offsets inside the group matrix M_g [n x np] (column-major, leading dimension n).

@@ -81,7 +81,8 @@ void Timing::flush() {
 // dimension), so a step costs one graph update and one graph launch instead of one launch per
 // kernel.
 KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp, int64_t n,
-                       bool simple2, bool final_step, Timing& tm, StepOut& so) {
+                       bool simple2, bool final_step, Timing& tm, StepOut& so, double tau,
+                       bool expo) {
   dmrg_ctx* c = st->ctx;
   cudaStream_t s = c->stream;
   KrylovRun kr;
@@ -122,7 +123,7 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
     heff(K1, H);
     tv = tm.begin();
     launch_mdot(s, K1, 0, 1, H, n, c->d_partial, scal + lz::ALPHA + 1);
-    launch_ritz(s, scal, 2);
+    launch_ritz(s, scal, 2, 0.0, false);
     launch_lincomb(s, K, n, 2, scal + lz::COEF, H, n);
     tm.end(tv, 3);
   } else {
@@ -148,7 +149,7 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
       tm.end(tv, 3);
     }
     tv = tm.begin();
-    launch_ritz(s, scal, kdim);
+    launch_ritz(s, scal, kdim, tau, expo);
     launch_lincomb(s, K, n, kdim, scal + lz::COEF, H, n);
     tm.end(tv, 3);
   }
@@ -180,7 +181,7 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
   }
   // split form, last bond step of the sweep: the reported energy is the FP64 Rayleigh quotient
   // <psi|H|psi>/<psi|psi> of the Ritz vector (one FP64 matvec; the Krylov vectors are free now)
-  kr.fp64_energy = kr.split && P.fp64_final && final_step;
+  kr.fp64_energy = kr.split && P.fp64_final && final_step && !expo;
   if (kr.fp64_energy) {
     const int th = tm.begin();
     apply_heff(st, hp.le, hp, H, K, DMRG_PREC_FP64, nullptr);
@@ -314,10 +315,8 @@ void launch_rho_vectors(dmrg_ctx* c, const std::vector<Group>& G, const RhoSolve
   run_trid_vectors(c, c->R.p, c->R.n, vt, 6);
 }
 
-namespace {
-
 void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool final_step,
-             Timing& tm, StepOut& so) {
+             Timing& tm, StepOut& so, const StepMode& mode) {
   dmrg_ctx* c = st->ctx;
   cudaStream_t s = c->stream;
   const MPOSite& ml = st->mpo->site[iL];
@@ -377,7 +376,9 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   cuda_check(cudaGetLastError(), "two-site tensor");
   tm.end(tv, 3);
 
-  const KrylovRun kr = krylov_solve(st, P, hp, n, P.krylov <= 2, final_step, tm, so);
+  const KrylovRun kr = mode.tdvp
+      ? krylov_solve(st, P, hp, n, false, false, tm, so, mode.tau, true)
+      : krylov_solve(st, P, hp, n, P.krylov <= 2, final_step, tm, so);
   const double* psi = c->H.p;
 
   // ---------------- reduced density matrix per centre-charge group (algs/DMRG.jl:425-429)
@@ -432,7 +433,9 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   so.energy = krylov_energy(c, kr);
 
   const std::vector<std::vector<double>> vals = rho_values(c, G, rs);
-  const Sel sel = select_kept(vals, P.maxm, P.minm, P.cutoff, 1.0, P.degen_rtol);
+  // the two-site DMRG step truncates with mag = 1 (fsvd!, algs/DMRG.jl:387); the TDVP step with
+  // the svd default mag = 0, weights relative to the total (its vector is not normalised)
+  const Sel sel = select_kept(vals, P.maxm, P.minm, P.cutoff, mode.tdvp ? 0.0 : 1.0, P.degen_rtol);
   Bond C;
   std::vector<double> kept;
   for (int g = 0; g < int(G.size()); ++g) {
@@ -446,7 +449,7 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   std::sort(kept.begin(), kept.end(), std::greater<double>());
   so.D.resize(kept.size());
   for (size_t a = 0; a < kept.size(); ++a) so.D[a] = std::sqrt(std::max(kept[a], 0.0));
-  so.truncerr = sel.truncerr;
+  so.truncerr = mode.tdvp ? (sel.total > 0 ? sel.truncerr / sel.total : 0.0) : sel.truncerr;
   so.m = int(kept.size());
   launch_rho_vectors(c, G, rs);
   const std::vector<int64_t>& uoff = rs.uoff;
@@ -521,8 +524,6 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   tm.end(te, 2);
 }
 
-}  // namespace
-
 void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   dmrg_ctx* c = st->ctx;
   const int L = st->L;
@@ -542,7 +543,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     const int i = st->oc;
     const int iL = j > 0 ? i : i - 1, iR = j > 0 ? i + 1 : i;
     StepOut so;
-    twostep(st, P, j, iL, iR, ns == 2 * (L - 1) - 1, tm, so);
+    twostep(st, P, j, iL, iR, ns == 2 * (L - 1) - 1, tm, so, StepMode{});
     const int tenv = tm.begin();
     double ef = 0.0;
     // split form: the environment updates run on the tensor cores too, except those of the

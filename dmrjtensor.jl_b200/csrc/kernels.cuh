@@ -164,8 +164,9 @@ void launch_lanczos2_orth(cudaStream_t s, double* K, double* H, int64_t n, doubl
 // K_{j+1} = H / beta_j, or 0 after a breakdown (beta_j <= betatest)
 void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, double* scal,
                         int j, double betatest);
-// lowest Ritz pair of the Krylov tridiagonal: s[EN], s[COEF + j]
-void launch_ritz(cudaStream_t s, double* scal, int kdim);
+// lowest Ritz pair of the Krylov tridiagonal: s[EN], s[COEF + j]; with expo the coefficients of
+// exp(tau T) e_1 instead (s[EN] still the lowest eigenvalue)
+void launch_ritz(cudaStream_t s, double* scal, int kdim, double tau, bool expo);
 // out[0] = sum over the pair tasks (total elements `total`; deterministic order)
 void launch_pair_dot(cudaStream_t s, const double* X, const double* Y, const PairTask* tasks,
                      int ntasks, int64_t total, double* partial, double* out);

@@ -304,7 +304,11 @@ __global__ void k_next_vector(const double* __restrict__ H, double* __restrict__
 // order; lanes own the rows/columns of one rotation) until the off-diagonal is at the rounding
 // level of the diagonal, lowest
 // eigenvalue -> s[EN], its eigenvector -> s[COEF + j] (0 for j >= m).
-__global__ void k_ritz(double* s, int kdim) {
+// expo = 0: the lowest Ritz pair (s[EN], s[COEF + j]). expo = 1: s[COEF + j] = (exp(tau T) e_1)_j
+// (krylovTimeEvol, algs/time.jl:182-203: the Krylov vectors are orthonormal, so these are the
+// coefficients of exp(tau H) applied to the normalised start vector), from the eigenpairs of T;
+// when they sum to exactly zero, the first column of I + T instead. s[EN] = lowest eigenvalue.
+__global__ void k_ritz(double* s, int kdim, double tau, int expo) {
   __shared__ double A[MAXK * MAXK], V[MAXK * MAXK];
   const int lane = threadIdx.x;
   int m = 1;
@@ -355,7 +359,23 @@ __global__ void k_ritz(double* s, int kdim) {
   for (int k = 1; k < m; ++k)
     if (A[k + k * m] < A[o + o * m]) o = k;   // lowest; ties keep the lower index
   if (lane == 0) s[lz::EN] = A[o + o * m];
-  for (int k = lane; k < kdim; k += 32) s[lz::COEF + k] = (k < m) ? V[k + o * m] : 0.0;
+  if (!expo) {
+    for (int k = lane; k < kdim; k += 32) s[lz::COEF + k] = (k < m) ? V[k + o * m] : 0.0;
+    return;
+  }
+  // c_k = sum_j V[k,j] exp(tau lambda_j) V[0,j]; every lane forms the sum of all c_k itself (the
+  // same fixed order in each lane) for the zero test
+  double tot = 0.0, mine = 0.0;
+  for (int k = 0; k < m; ++k) {
+    double ck = 0.0;
+    for (int jj = 0; jj < m; ++jj) ck += V[k + jj * m] * exp(tau * A[jj + jj * m]) * V[jj * m];
+    tot += ck;
+    if (k == lane) mine = ck;
+  }
+  if (tot == 0.0) {   // (I + T) e_1
+    mine = lane == 0 ? 1.0 + s[lz::ALPHA] : (lane == 1 && m > 1 ? s[lz::BETA] : 0.0);
+  }
+  for (int k = lane; k < kdim; k += 32) s[lz::COEF + k] = (k < m) ? mine : 0.0;
 }
 
 // y = sum_j c[j] * X_j (y not read), j < k, c in device memory
@@ -479,8 +499,8 @@ void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, 
   count_launch();
 }
 
-void launch_ritz(cudaStream_t s, double* scal, int kdim) {
-  k_ritz<<<1, 32, 0, s>>>(scal, kdim);
+void launch_ritz(cudaStream_t s, double* scal, int kdim, double tau, bool expo) {
+  k_ritz<<<1, 32, 0, s>>>(scal, kdim, tau, expo ? 1 : 0);
   count_launch();
 }
 

@@ -490,6 +490,60 @@ def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, si
     return energy
 
 
+# ------------------------------------------------------------------ time evolution
+
+def _bond_dims(psi: MPS):
+    if psi.tensors is not None:
+        return [a.shape[2] for a in psi.tensors]
+    return [sum(d for _, d in sec) for sec in psi.sectors[1:]]
+
+
+def _tdvp(psi, mpo, m, minm, cutoff, origj, r, prefactor, twosite, precision, ctx, download):
+    pre = complex(prefactor)
+    if pre.imag != 0.0:
+        raise ValueError("complex prefactor: real-time evolution needs complex tensors, which "
+                         "this engine does not hold (a real prefactor evolves in imaginary time)")
+    mm = max(_bond_dims(psi)) if m is None else int(m)
+    dmpo = mpo.device(ctx)
+    dev = psi._dev if (psi._dev is not None and psi._dev.dmpo is dmpo) else DeviceState(psi, dmpo)
+    L = len(psi)
+    if not origj and 0 < dev.oc < L - 1:
+        raise ValueError("origj=false from an interior centre (leftward first) is not available")
+    dev.env_build()    # makeEnv(psi, psi, mpo) at the start of every call (algs/time.jl:214,291)
+    p = make_params(mm, minm, cutoff, r, precision)
+    st = SweepStats()
+    check(lib().dmrg_tdvp(dev.h, dev.dmpo.h, C.byref(p), float(pre.real), 1 if twosite else 0,
+                          C.byref(st)), dev.ctx.h)
+    rec = st.as_dict()
+    psi.sweep_stats = [rec]
+    if download:
+        dev.download_into(psi)
+    else:
+        psi._dev = dev
+        psi.oc = dev.oc
+    return rec["energy"]
+
+
+def tdvp_twosite(psi: MPS, mpo: MPO, m=None, minm=2, cutoff=0.0, origj=True, r=2, prefactor=1.0,
+                 precision="fp64", ctx=None, download=True):
+    """``tdvp_twosite(psi, mpo; m, minm, cutoff, origj, r, prefactor)`` (``algs/time.jl:288-363``)
+    on the GPU: one half sweep of two-site TDVP steps, each applying exp(tau H) (tau =
+    prefactor / (L-1) / 2) by a Krylov exponential with ``r`` vectors to the two-site tensor and
+    then to the site left as centre, with a truncated move between. ``m`` defaults to the largest
+    bond dimension of ``psi``. Real prefactors only (imaginary-time evolution). Returns En of the
+    last Krylov call; ``psi`` is updated in place."""
+    return _tdvp(psi, mpo, m, minm, cutoff, origj, r, prefactor, True, precision, ctx, download)
+
+
+def tdvp(psi: MPS, mpo: MPO, m=None, minm=2, cutoff=0.0, origj=True, r=2, prefactor=1.0,
+         precision="fp64", ctx=None, download=True):
+    """``tdvp(psi, mpo; m, minm, cutoff, origj, r, prefactor)`` (``algs/time.jl:211-286``) on the
+    GPU: single-site TDVP steps (the site by exp(tau H1), tau = prefactor / L / 2, then the bond
+    matrix by exp(tau H0) through the zero-site Heff). One call is one half sweep of L-1 steps
+    (the reference's L-th step would read past the chain's end). Real prefactors only."""
+    return _tdvp(psi, mpo, m, minm, cutoff, origj, r, prefactor, False, precision, ctx, download)
+
+
 # ------------------------------------------------------------------ measurements
 
 def _measure_state(psi: MPS, ctx=None):

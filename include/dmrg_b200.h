@@ -277,6 +277,23 @@ DMRG_API void dmrg_noise_default(dmrg_noise* nz);
  * algs/DMRG.jl:626-652). max_truncerr is relative to the total weight of each step. */
 DMRG_API int dmrg_sweep3s(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p,
                           dmrg_noise* nz, dmrg_sweep_stats* out);
+
+/* One call of tdvp_twosite (twosite = 1, algs/time.jl:288-363) or tdvp (twosite = 0, :211-286)
+ * with a real prefactor: L-1 steps from the centre (rightward from the left edge or an interior
+ * centre, leftward from the right edge), turning at the edge. Each step applies exp(tau H) by
+ * krylovTimeEvol (:182-203: Lanczos with max(2, krylov) vectors, the combination exp(tau T) e_1;
+ * tau = prefactor / (L-1) / 2 two-site, prefactor / L / 2 single-site) to the two-site tensor and
+ * then to the site left as centre (two-site), or to the site and then to the bond matrix through
+ * the zero-site Heff (single-site), with a truncated move (maxm, minm, cutoff, weights relative to
+ * the total) and the environment update between; the new centre is normalised.
+ * p: maxm (the `m` keyword), minm, cutoff, krylov (`r`), precision, degen_rtol, betatest, tune,
+ * graph, profile. out->energy = En of the last Krylov call (the lowest eigenvalue of its
+ * tridiagonal), out->max_truncerr / biggest_m / timings as for a sweep.
+ * The single-site reference runs L steps and its last one reads past the chain's end (its turn
+ * test compares the centre with L+1); this call stops at the edge instead. A complex prefactor
+ * (real-time evolution) needs complex tensors and is not available. Requires dmrg_env_build. */
+DMRG_API int dmrg_tdvp(dmrg_state* st, const dmrg_mpo* mpo, const dmrg_params* p,
+                       double prefactor, int twosite, dmrg_sweep_stats* out);
 /* ---------------------------------------------------------------- kernel test hooks
  * No reference counterpart: these expose single device kernels to the parity tests.
  * C[M,N] = op(A) op(B) with the grouped FP64 GEMM (one task, one K segment), host arrays,

@@ -50,6 +50,7 @@ def test_null_handles_are_rejected(dmrgb):
     assert lib.dmrg_mpo_destroy(None) == dmrgb._lib.ERR_ARG
     assert lib.dmrg_sweep(None, None, None, None) == dmrgb._lib.ERR_ARG
     assert lib.dmrg_sweep3s(None, None, None, None, None) == dmrgb._lib.ERR_ARG
+    assert lib.dmrg_tdvp(None, None, None, 0.0, 1, None) == dmrgb._lib.ERR_ARG
 
 
 def test_context_without_gpu_reports_nocuda(dmrgb):

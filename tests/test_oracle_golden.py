@@ -165,3 +165,40 @@ def test_alpha_update_rules():
     assert alpha_update(1e-42, 0.0, 1e-12, -1.0, -1.0, 0.3, 0.5) == 1e-42
     # equal energies: the site condition is 0/0 (NaN, false) but err_est holds: shrink
     assert alpha_update(0.5, 0.0, 0.0, -2.0, -2.0, 0.3, 0.1) == pytest.approx(0.45)
+
+
+# ------------------------------------------------------------------ TDVP (real prefactor)
+
+def test_krylov_exp_matches_the_matrix_exponential():
+    """krylovTimeEvol (algs/time.jl:182-203) with a full Krylov space is exp(tau H) x / |x|."""
+    import scipy.linalg
+    from oracle.tdvp import krylov_exp
+    rng = np.random.default_rng(4)
+    H = rng.standard_normal((6, 6))
+    H = H + H.T
+    x = rng.standard_normal(6)
+    for tau in (-0.3, 0.0, 0.2):
+        y, En = krylov_exp(lambda v: H @ v, x, 6, tau)
+        ref = scipy.linalg.expm(tau * H) @ (x / np.linalg.norm(x))
+        assert np.max(np.abs(y - ref)) < 1e-10
+        assert abs(En - np.linalg.eigvalsh(H)[0]) < 1e-10
+
+
+def test_tdvp_oracle_imaginary_time_reaches_ed():
+    """tdvp_twosite with a negative real prefactor projects onto the ground state; the single-site
+    form keeps the bond dimensions of its start."""
+    from oracle import tdvp as ot
+    L = 10
+    mpo = heis(L)
+    start = om.neel_mps(L)
+    recs, S = ot.tdvp(start, mpo, [SPIN] * L, om.mps_bond_labels(start, [SPIN] * L), calls=30,
+                      prefactor=-2.0, m=32, cutoff=1e-12, r=2, twosite=True)
+    e0 = ed.sparse_ground_energy(mpo)
+    assert abs(recs[-1][0] - e0) < 1e-9
+    assert abs(od.expect(S.psi, mpo) - e0) < 1e-9
+    psi0 = om.right_canonicalize(om.random_mps(L, 2, 8, np.random.default_rng(3)))
+    labels = [[(0,)] * A.shape[0] for A in psi0] + [[(0,)]]
+    recs1, S1 = ot.tdvp(psi0, mpo, [[(0,), (0,)]] * L, labels, calls=20, prefactor=-2.0, m=32,
+                        cutoff=1e-12, twosite=False)
+    assert all(r[2] <= 8 for r in recs1)
+    assert e0 - 1e-12 < od.expect(S1.psi, mpo) < e0 + 1e-3
