@@ -557,6 +557,67 @@ def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
     return out
 
 
+def method_legs(pkg, ctx, dev, args):
+    """The 3S sweep (dmrg3S) and TDVP (tdvp_twosite, real prefactor) rows: the device against the
+    oracle on the same start (L=100 Heisenberg U(1) from the Neel state, capped bond dimension so
+    that the dense-with-charges oracle finishes in seconds), then the device alone on the headline
+    state (the ramped maxm-1024 two-site state). Times are device-timed per sweep / per call
+    (the oracle's with perf_counter on the host cores)."""
+    from oracle import dmrg3s as o3, models as om, tdvp as ot
+    L, sp = L_CHAIN, [(1,), (-1,)]
+    mpo = pkg.makeMPO(pkg.heisenbergMPO, 2, L).with_qn(pkg.SPIN_QN)
+    ompo = om.make_mpo([om.heisenberg_bulk()] * L, 2)
+    start = om.neel_mps(L)
+    labels = om.mps_bond_labels(start, [sp] * L)
+    out = {}
+    # 3S at maxm 128, 6 sweeps
+    psi = pkg.neelMPS(L)
+    pkg.dmrg(psi, mpo, m=128, sweeps=6, cutoff=CUTOFF, method="3S", ctx=ctx)
+    t = time.perf_counter()
+    e3, recs, _ = o3.dmrg3s(start, ompo, [sp] * L, labels, m=128, sweeps=6, cutoff=CUTOFF)
+    t3 = time.perf_counter() - t
+    d3 = psi.sweep_stats
+    out["dmrg3s_m128_6sweeps"] = {
+        "device_seconds_per_sweep": statistics.mean(x["seconds"] for x in d3),
+        "oracle_seconds_per_sweep": t3 / 6, "oracle_cores": cpu_threads(),
+        "energy_device": d3[-1]["energy"], "energy_oracle": e3,
+        "abs_dE": abs(d3[-1]["energy"] - e3),
+        "noise_device": d3[-1]["noise"], "noise_oracle": recs[-1]["noise"],
+        "biggest_m": d3[-1]["biggest_m"]}
+    # tdvp_twosite at maxm 64, 2 calls, prefactor -1 (imaginary time)
+    psi = pkg.neelMPS(L)
+    dt = []
+    for _ in range(2):
+        en = pkg.tdvp_twosite(psi, mpo, m=64, cutoff=CUTOFF, prefactor=-1.0, ctx=ctx)
+        dt.append(psi.sweep_stats[-1]["seconds"])
+    t = time.perf_counter()
+    orecs, _ = ot.tdvp(start, ompo, [sp] * L, labels, calls=2, prefactor=-1.0, m=64,
+                       cutoff=CUTOFF, twosite=True)
+    tt = time.perf_counter() - t
+    out["tdvp_twosite_m64_2calls"] = {
+        "device_seconds_per_call": statistics.mean(dt), "oracle_seconds_per_call": tt / 2,
+        "En_device": en, "En_oracle": orecs[-1][0], "abs_dEn": abs(en - orecs[-1][0])}
+    # the headline state: 3S sweeps and TDVP calls at maxm 1024
+    p = params(pkg, RAMP[-1], args)
+    nz = pkg._lib.Noise()
+    pkg.lib().dmrg_noise_default(pkg._lib.C.byref(nz))
+    dev.sweep3s(p, nz)
+    st3 = [dev.sweep3s(p, nz) for _ in range(max(args.steps, 1))]
+    out["dmrg3s_headline_state_maxm1024"] = {
+        "seconds_per_sweep": statistics.mean(x["seconds"] for x in st3),
+        "energy": st3[-1]["energy"], "biggest_m": st3[-1]["biggest_m"],
+        "heff_flops_per_sweep": st3[-1]["heff_flops"], "noise": st3[-1]["noise"]}
+    stt = []
+    for _ in range(2):
+        dev.env_build()
+        stt.append(dev.tdvp(p, -0.1, True))
+    out["tdvp_twosite_headline_state_maxm1024"] = {
+        "seconds_per_call": statistics.mean(x["seconds"] for x in stt),
+        "En": stt[-1]["energy"], "biggest_m": stt[-1]["biggest_m"],
+        "max_truncerr": stt[-1]["max_truncerr"], "prefactor": -0.1}
+    return out
+
+
 def cpu_threads():
     try:
         import threadpoolctl
@@ -765,6 +826,7 @@ def run_ours(args, world, rank, local, dist):
                    "capacity_3xtf32": run_serving(pkg, local, args.serve_saturate, saturate=True,
                                                   precision="3xtf32")}
     heff_large = heff_forms(pkg, ctx) if args.chosen else None
+    methods = method_legs(pkg, ctx, dev, args) if args.methods else None
     if rank != 0:
         return
     peak = fp64_gemm_peak(local)
@@ -819,6 +881,7 @@ def run_ours(args, world, rank, local, dist):
         "autotune": tuner,
         "graph": graphs,
         "configs": configs,
+        "methods": methods,
     }
     print(json.dumps(out))
 
@@ -846,6 +909,8 @@ def main():
                     help="skip the split-precision (3xTF32) sweeps")
     ap.add_argument("--heff-only", action="store_true",
                     help="only time the plain and split Heff at the m=1024 dense-equivalent size")
+    ap.add_argument("--no-methods", dest="methods", action="store_false",
+                    help="skip the 3S and TDVP legs")
     ap.add_argument("--no-measure", dest="measure", action="store_false",
                     help="skip the expect / correlationmatrix measurement")
     ap.add_argument("--serve-requests", type=int, default=200,

@@ -400,6 +400,14 @@ class DeviceState:
         check(lib().dmrg_sweep(self.h, self.dmpo.h, C.byref(params), C.byref(st)), self.ctx.h)
         return st.as_dict()
 
+    def tdvp(self, params: Params, prefactor: float, twosite: bool = True):
+        """One call of tdvp_twosite (or tdvp) on the resident state; the environments must be
+        built for its current tensors."""
+        st = SweepStats()
+        check(lib().dmrg_tdvp(self.h, self.dmpo.h, C.byref(params), float(prefactor),
+                              1 if twosite else 0, C.byref(st)), self.ctx.h)
+        return st.as_dict()
+
     def sweep3s(self, params: Params, noise: "_lib.Noise"):
         """One single-site sweep with subspace expansion; ``noise.noise`` (alpha) is updated."""
         st = SweepStats()
@@ -510,11 +518,7 @@ def _tdvp(psi, mpo, m, minm, cutoff, origj, r, prefactor, twosite, precision, ct
     if not origj and 0 < dev.oc < L - 1:
         raise ValueError("origj=false from an interior centre (leftward first) is not available")
     dev.env_build()    # makeEnv(psi, psi, mpo) at the start of every call (algs/time.jl:214,291)
-    p = make_params(mm, minm, cutoff, r, precision)
-    st = SweepStats()
-    check(lib().dmrg_tdvp(dev.h, dev.dmpo.h, C.byref(p), float(pre.real), 1 if twosite else 0,
-                          C.byref(st)), dev.ctx.h)
-    rec = st.as_dict()
+    rec = dev.tdvp(make_params(mm, minm, cutoff, r, precision), pre.real, twosite)
     psi.sweep_stats = [rec]
     if download:
         dev.download_into(psi)
