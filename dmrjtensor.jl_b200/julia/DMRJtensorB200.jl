@@ -1,11 +1,15 @@
 # DMRJtensorB200.jl -- Julia host binding of libdmrgb200.so (C ABI in include/dmrg_b200.h).
 #
-# A drop-in for DMRJtensor's two-site ground-state path. Loading this module after DMRJtensor adds
+# A drop-in for DMRJtensor's ground-state and TDVP paths. Loading this module after DMRJtensor adds
 #   * a method of DMRJtensor.dmrg for the concrete MPS/MPO types (algs/DMRG.jl:549-588): the same
-#     call, dmrg(psi, mpo; m (or maxm), minm, sweeps, cutoff, silent, goal, cvgE, SvNbond, method),
-#     runs every sweep of method "twosite" on the GPU, writes the optimised tensors back into psi
-#     and sets psi.oc as optmps leaves it; other methods go to the reference's own implementation
-#     (`invoke` on the abstract signature), so no call site changes;
+#     call, dmrg(psi, mpo; m (or maxm), minm, sweeps, cutoff, silent, goal, cvgE, SvNbond, method,
+#     noise, noise_goal, noise_incr), runs every sweep of method "twosite" or "3S" on the GPU,
+#     writes the optimised tensors back into psi and sets psi.oc as optmps leaves it; other methods
+#     go to the reference's own implementation (`invoke` on the abstract signature), so no call
+#     site changes;
+#   * methods of DMRJtensor.tdvp_twosite and DMRJtensor.tdvp (algs/time.jl:211-363) that run on
+#     the GPU for a real prefactor (imaginary-time evolution) and real tensors; a complex
+#     prefactor or complex tensors go to the reference's implementation;
 #   * the Env API on device-resident environments (lib/Env/makeEnv.jl:196-246,
 #     lib/MPO_MPS/Lupdate.jl:17-37, Rupdate.jl:17-37): makeEnv_b200(psi, mpo) returns (Lenv, Renv)
 #     whose Lenv[i] / Renv[i] download the dense-equivalent tensor, and Lupdate!(i, Lenv, psi, mpo)
@@ -23,7 +27,7 @@ module DMRJtensorB200
 
 import DMRJtensor
 
-export dmrg_b200, makeEnv_b200, B200Env, B200Side, expect_b200, correlationmatrix_b200,
+export dmrg_b200, tdvp_b200, makeEnv_b200, B200Env, B200Side, expect_b200, correlationmatrix_b200,
        save_b200, load_b200
 
 const libdmrg = get(ENV, "DMRG_B200_LIB", joinpath(@__DIR__, "..", "libdmrgb200.so"))
@@ -75,6 +79,15 @@ mutable struct SweepStats
 end
 SweepStats() = SweepStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0.0, 8), 0, 0, 0, 0, 0, 0,
                           0, 0, 0)
+
+# mirrors struct dmrg_noise (the 3S schedule: noise = alpha, noise_goal, noise_incr)
+mutable struct Noise
+  noise::Cdouble
+  noise_goal::Cdouble
+  noise_incr::Cdouble
+  reserved::Cdouble
+end
+Noise() = Noise(1.0, 0.3, 0.01, 0.0)
 
 lasterror(ctx) = unsafe_string(ccall((:dmrg_last_error, libdmrg), Cstring, (Ptr{Cvoid},), ctx))
 
@@ -269,17 +282,25 @@ upload_mps(ctx, hmpo, psi, ch) =
 
 # ------------------------------------------------------------------------ dmrg
 
-function run_sweeps!(ctx, st, hmpo, p::Params, sweeps, silent)
+function run_sweeps!(ctx, st, hmpo, p::Params, sweeps, silent, nz::Union{Nothing,Noise}=nothing)
   energy = 0.0
   for s = 1:sweeps
     stats = SweepStats()
-    check(ccall((:dmrg_sweep, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Params}, Ref{SweepStats}),
-                st, hmpo, p, stats), ctx.h, "dmrg_sweep")
+    if nz === nothing
+      check(ccall((:dmrg_sweep, libdmrg), Cint,
+                  (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Params}, Ref{SweepStats}), st, hmpo, p, stats),
+            ctx.h, "dmrg_sweep")
+    else
+      check(ccall((:dmrg_sweep3s, libdmrg), Cint,
+                  (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Params}, Ref{Noise}, Ref{SweepStats}),
+                  st, hmpo, p, nz, stats), ctx.h, "dmrg_sweep3s")
+    end
     energy = stats.energy
     if !silent    # dmrgcvg's report (algs/DMRG.jl:614-620)
       println("Sweep $s (back and forth): $(round(stats.seconds, digits=5)) sec")
       println("Largest truncation = $(stats.max_truncerr), m = $(stats.biggest_m)")
       println("Energy at sweep $s is $(round(stats.energy, digits=12))")
+      nz === nothing || println("(alpha = $(round(nz.noise, digits=5)))")
       println()
     end
     if stats.converged != 0
@@ -292,12 +313,14 @@ end
 
 """
     dmrg(psi, mpo; m, maxm, minm=2, sweeps, cutoff, silent, goal, cvgE, SvNbond, method="twosite",
-         krylov=2, precision=0, charges=nothing, device=0, kwargs...)
+         noise, noise_goal, noise_incr, krylov=2, precision=0, charges=nothing, device=0, kwargs...)
 
-The reference's `dmrg` (algs/DMRG.jl:549-588) for `method = "twosite"` on the GPU; defaults come
-from `algvars(psi)` as in the reference. `m` and `maxm` are the same keyword. `krylov > 2` runs
-Lanczos with full re-orthogonalisation instead of the reference's 2-vector step; `precision = 1`
-selects the split-precision (3xTF32) contractions. Other methods run the reference's own code.
+The reference's `dmrg` (algs/DMRG.jl:549-588) for `method = "twosite"` and `method = "3S"` on the
+GPU; defaults come from `algvars(psi)` as in the reference. `m` and `maxm` are the same keyword.
+`krylov > 2` runs Lanczos with full re-orthogonalisation instead of the reference's 2-vector step
+(the 3S step always uses a Krylov space of max(2, krylov) vectors, the reference's `r`);
+`precision = 1` (3xTF32) or `2` (BF16x9) selects the split-precision contractions. Other methods
+run the reference's own code.
 """
 function DMRJtensor.dmrg(psi::DMRJtensor.matrixproductstate, mpo::DMRJtensor.matrixproductoperator;
                          params=DMRJtensor.algvars(psi), method::String="twosite",
@@ -305,29 +328,36 @@ function DMRJtensor.dmrg(psi::DMRJtensor.matrixproductstate, mpo::DMRJtensor.mat
                          sweeps::Integer=params.sweeps, cutoff::Float64=params.cutoff,
                          silent::Bool=params.silent, goal::Float64=params.goal,
                          cvgE::Bool=params.cvgE, SvNbond::Integer=params.SvNbond,
+                         noise::Number=first(params.noise), noise_goal::Float64=params.noise_goal,
+                         noise_incr::Float64=params.noise_incr,
                          krylov::Integer=2, precision::Integer=0, charges=nothing,
                          device::Integer=0, kwargs...)
-  if method != "twosite"
+  if method != "twosite" && method != "3S"
     return invoke(DMRJtensor.dmrg, Tuple{DMRJtensor.MPS,DMRJtensor.MPO}, psi, mpo;
                   params=params, method=method, m=maxm, minm=minm, sweeps=sweeps, cutoff=cutoff,
-                  silent=silent, goal=goal, cvgE=cvgE, SvNbond=SvNbond, kwargs...)
+                  silent=silent, goal=goal, cvgE=cvgE, SvNbond=SvNbond, noise=noise,
+                  noise_goal=noise_goal, noise_incr=noise_incr, kwargs...)
   end
   dmrg_b200(psi, mpo; maxm=maxm, minm=minm, sweeps=sweeps, cutoff=cutoff, silent=silent,
             goal=goal, cvgE=cvgE, SvNbond=SvNbond, krylov=krylov, precision=precision,
-            charges=charges, device=device)
+            charges=charges, device=device, method=method, noise=Float64(noise),
+            noise_goal=noise_goal, noise_incr=noise_incr)
 end
 
 """
     dmrg_b200(psi, mpo; maxm, minm=2, sweeps=1, cutoff=0.0, silent=false, goal=0.0, cvgE=true,
-              SvNbond=0, krylov=2, precision=0, charges=nothing, device=0)
+              SvNbond=0, krylov=2, precision=0, charges=nothing, device=0, method="twosite",
+              noise=1.0, noise_goal=0.3, noise_incr=0.01)
 
-The GPU two-site DMRG behind the `dmrg` method. Returns the energy of the last bond step and
-updates `psi` (tensors and `oc`) in place.
+The GPU DMRG behind the `dmrg` method (two-site, or 3S single-site sweeps with subspace
+expansion). Returns the energy of the last bond step and updates `psi` (tensors and `oc`) in
+place.
 """
 function dmrg_b200(psi, mpo; maxm::Integer=0, minm::Integer=2, sweeps::Integer=1,
                    cutoff::Float64=0.0, silent::Bool=false, goal::Float64=0.0, cvgE::Bool=true,
                    SvNbond::Integer=0, krylov::Integer=2, precision::Integer=0, charges=nothing,
-                   device::Integer=0)
+                   device::Integer=0, method::String="twosite", noise::Float64=1.0,
+                   noise_goal::Float64=0.3, noise_incr::Float64=0.01)
   ctx = context(device)
   ch = site_charges(psi, charges)
   hmpo = upload_mpo(ctx, mpo, ch)
@@ -340,9 +370,82 @@ function dmrg_b200(psi, mpo; maxm::Integer=0, minm::Integer=2, sweeps::Integer=1
     p.maxm, p.minm, p.cutoff, p.krylov, p.precision, p.svnbond = maxm, minm, cutoff, krylov,
                                                                  precision, SvNbond
     p.goal, p.cvgE = goal, cvgE ? 1 : 0
-    energy = run_sweeps!(ctx, st, hmpo, p, sweeps, silent)
+    nz = method == "3S" ? Noise(noise, noise_goal, noise_incr, 0.0) : nothing
+    energy = run_sweeps!(ctx, st, hmpo, p, sweeps, silent, nz)
     write_back!(ctx, st, psi, ch)
     return energy
+  finally
+    ccall((:dmrg_state_destroy, libdmrg), Cint, (Ptr{Cvoid},), st)
+    ccall((:dmrg_mpo_destroy, libdmrg), Cint, (Ptr{Cvoid},), hmpo)
+  end
+end
+
+# ------------------------------------------------------------------------ TDVP
+
+"""
+    tdvp_twosite(psi, mpo; m, minm=2, cutoff=0., origj=true, r=2, prefactor=1., precision=0,
+                 charges=nothing, device=0)
+    tdvp(psi, mpo; ...)
+
+The reference's TDVP calls (algs/time.jl:211-363) on the GPU when `prefactor` is real and the
+tensors are real: one half sweep of steps, each propagator exp(tau H) applied by a Krylov
+exponential with `r` vectors. Returns En of the last Krylov call and updates `psi` in place. A
+complex prefactor (real-time evolution) or complex tensors run the reference's own code. The
+single-site form stops at the chain's edge after L-1 steps.
+"""
+function DMRJtensor.tdvp_twosite(psi::DMRJtensor.matrixproductstate,
+                                 mpo::DMRJtensor.matrixproductoperator;
+                                 m::Integer=maximum([size(psi[w], 3) for w = 1:length(psi)]),
+                                 minm::Integer=2, cutoff::Real=0., origj::Bool=true,
+                                 r::Integer=2, prefactor::Number=1., precision::Integer=0,
+                                 charges=nothing, device::Integer=0)
+  if !gpu_tdvp_ok(psi, prefactor, origj)
+    return invoke(DMRJtensor.tdvp_twosite, Tuple{DMRJtensor.MPS,DMRJtensor.MPO}, psi, mpo;
+                  m=m, minm=minm, cutoff=cutoff, origj=origj, r=r, prefactor=prefactor)
+  end
+  tdvp_b200(psi, mpo, true; m=m, minm=minm, cutoff=Float64(cutoff), r=r,
+            prefactor=Float64(real(prefactor)), precision=precision, charges=charges,
+            device=device)
+end
+
+function DMRJtensor.tdvp(psi::DMRJtensor.matrixproductstate, mpo::DMRJtensor.matrixproductoperator;
+                         m::Integer=maximum([size(psi[w], 3) for w = 1:length(psi)]),
+                         minm::Integer=2, cutoff::Real=0., origj::Bool=true, r::Integer=2,
+                         prefactor::Number=1., precision::Integer=0, charges=nothing,
+                         device::Integer=0)
+  if !gpu_tdvp_ok(psi, prefactor, origj)
+    return invoke(DMRJtensor.tdvp, Tuple{DMRJtensor.MPS,DMRJtensor.MPO}, psi, mpo;
+                  m=m, minm=minm, cutoff=cutoff, origj=origj, r=r, prefactor=prefactor)
+  end
+  tdvp_b200(psi, mpo, false; m=m, minm=minm, cutoff=Float64(cutoff), r=r,
+            prefactor=Float64(real(prefactor)), precision=precision, charges=charges,
+            device=device)
+end
+
+gpu_tdvp_ok(psi, prefactor, origj) =
+  imag(prefactor) == 0 && !(eltype(psi.A[1]) <: Complex) &&
+  (origj || psi.oc == 1 || psi.oc == length(psi))
+
+function tdvp_b200(psi, mpo, twosite::Bool; m::Integer, minm::Integer=2, cutoff::Float64=0.0,
+                   r::Integer=2, prefactor::Float64=1.0, precision::Integer=0, charges=nothing,
+                   device::Integer=0)
+  ctx = context(device)
+  ch = site_charges(psi, charges)
+  hmpo = upload_mpo(ctx, mpo, ch)
+  st = upload_mps(ctx, hmpo, psi, ch)
+  try
+    # makeEnv(psi, psi, mpo) at the start of every call (algs/time.jl:214,291)
+    check(ccall((:dmrg_env_build, libdmrg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), st, hmpo), ctx.h,
+          "dmrg_env_build")
+    p = Params()
+    ccall((:dmrg_params_default, libdmrg), Cvoid, (Ref{Params},), p)
+    p.maxm, p.minm, p.cutoff, p.krylov, p.precision = m, minm, cutoff, r, precision
+    stats = SweepStats()
+    check(ccall((:dmrg_tdvp, libdmrg), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Params}, Cdouble, Cint, Ref{SweepStats}),
+                st, hmpo, p, prefactor, twosite ? 1 : 0, stats), ctx.h, "dmrg_tdvp")
+    write_back!(ctx, st, psi, ch)
+    return stats.energy
   finally
     ccall((:dmrg_state_destroy, libdmrg), Cint, (Ptr{Cvoid},), st)
     ccall((:dmrg_mpo_destroy, libdmrg), Cint, (Ptr{Cvoid},), hmpo)

@@ -63,3 +63,26 @@ def test_context_without_gpu_reports_nocuda(dmrgb):
     assert b"no CUDA device" in dmrgb.lib().dmrg_last_error(None)
     with pytest.raises(dmrgb.DmrgError):
         dmrgb.Context(0)
+
+
+def test_julia_binding_calls_only_declared_entry_points():
+    """No Julia runtime exists here, so the shim's ccalls are checked as text: every symbol it
+    calls is declared in the header, and its struct mirrors have the C field counts."""
+    jl = (HEADER.parents[1] / "dmrjtensor.jl_b200" / "julia" / "DMRJtensorB200.jl").read_text()
+    called = set(re.findall(r"ccall\(\(:(dmrg_\w+), libdmrg\)", jl))
+    assert {"dmrg_sweep", "dmrg_sweep3s", "dmrg_tdvp", "dmrg_mps_upload_blocks"} <= called
+    assert called <= set(declared())
+    txt = HEADER.read_text()
+
+    def c_fields(name):
+        body = re.search(r"typedef struct " + name + r" \{(.*?)\} " + name + ";", txt, re.S).group(1)
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        return len(re.findall(r"\b(?:int|double|size_t)\s+\w+", body))
+
+    def jl_fields(name):
+        body = re.search(r"mutable struct " + name + r"\n(.*?)\nend", jl, re.S).group(1)
+        return len([ln for ln in body.splitlines() if "::" in ln])
+
+    assert jl_fields("Params") == c_fields("dmrg_params")
+    assert jl_fields("Noise") == c_fields("dmrg_noise")
+    assert jl_fields("SweepStats") == c_fields("dmrg_sweep_stats")
