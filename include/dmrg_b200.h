@@ -220,9 +220,7 @@ DMRG_API int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const 
  * [ml, d1, d2, mr] column-major vectors; every intermediate lives in one fixed device array inside
  * the library (9 MiB per GPU that loads the library, kept until exit), limited to 2^20 doubles of
  * vector/intermediate data and 1 MiB of task descriptors: larger two-site spaces are rejected with
- * DMRG_ERR_BUDGET. Nothing is allocated, no cudaMalloc/cudaFree is called. The first call on a
- * device looks up the array's device address, so make that first call before any stream capture.
- * The call runs on the context's own stream, which is not ordered after the caller's streams:
+ * DMRG_ERR_BUDGET. Nothing is allocated, no cudaMalloc/cudaFree is called. The call runs on the context's own stream, which is not ordered after the caller's streams:
  * finish writing psi_in first (for example synchronise the stream that produced it). psi_in and
  * psi_out may be the same buffer (the input is read completely before the output is written).
  * Calls share the array: calls that overlap on the GPU race. Returns after the result is written. */
