@@ -4,19 +4,23 @@
 // do not fit in shared memory.
 //
 // Launch 1 (k_trid_mid_vals): the Householder steps run on the matrix in place in global memory
-// (L2-resident: a 512 x 512 block is 2 MB) until the trailing block is small enough for shared
-// memory (m <= ms); it is then copied there and the remaining steps run on the copy, which is
-// written back at the end (its strictly lower part holds the last reflectors). Per step: the
-// product p = tau B v by columns (B is symmetric: p_j = tau B(:,j).v, one warp per column, a
-// warp sum per column), one block barrier, then the rank-2 update B -= v w^T + w v^T by the other
-// warps while warp 0 updates the next pivot column first and builds the next reflector from it.
+// (L2-resident: a 512 x 512 block is 2 MB) until the trailing block's lower triangle fits in
+// shared memory in packed form (m <= mp, about 230 beside the vectors); it is then copied there
+// and the remaining steps run on the copy, which is written back at the end (its strictly lower
+// part holds the last reflectors). Global steps: the product p = tau B v by columns (B is
+// symmetric: p_j = tau B(:,j).v, one warp per column, four columns in flight), one block barrier,
+// then the rank-2 update B -= v w^T + w v^T by the other warps while warp 0 updates the next pivot
+// column first and builds the next reflector from it. Packed steps: the same with p by row pairs
+// (the stored part of row a along the diagonal direction and of column a below it).
 // Eigenvalues by trisection as in syevt.cu, in rounds of 256 eigenvalues.
 // Launch 2 (k_trid_mid_vectors): inverse iteration (one thread per kept vector, LU factors in a
 // global workspace interleaved by thread so that every factor access of a warp is one line),
 // Cholesky QR (a second pass unless the Gram matrix is within 1e-3/k of the identity; classical
-// Gram-Schmidt with restarts if a pivot shows nearly dependent vectors), back-transformation
-// U = H_0 ... H_{n-3} Z in blocks of 8 reflectors (compact WY) reading the reflectors from the
-// matrix in global memory.
+// Gram-Schmidt with restarts if a pivot shows nearly dependent vectors); the vectors Z of the
+// tridiagonal matrix stay in the workspace.
+// Launch 3 (k_trid_mid_backtransform): U = H_0 ... H_{n-3} Z in blocks of 8 reflectors (compact
+// WY), one CTA per slice of 32 kept vectors with its slice of Z in shared memory, the reflectors
+// read from the matrix in global memory (every slice is independent of the others).
 #include "kernels.cuh"
 #include "syevt_common.cuh"
 
@@ -26,6 +30,8 @@ namespace {
 constexpr int MT = 512;             // threads per CTA
 constexpr int NW = MT / 32;         // warps
 constexpr int MID_BT_NB = 8;        // reflectors per back-transformation block
+// columns per warp and pass in the product p = tau B v and in the rank-2 update (fewer for the
+// 16-row variant, whose register budget under 512 threads is the same)
 constexpr size_t MID_SMEM_LIMIT = 227 * 1024 - 2048;
 
 // Householder reflector of x = col[0..m) (one warp): H x = beta e_1 with v[0] = 1,
@@ -53,46 +59,43 @@ __device__ void house_warp(double* __restrict__ col, int m, double* __restrict__
   tau_o = t;
 }
 
+// Packed lower-triangular storage of the trailing block once it fits in shared memory: column j
+// (0-based, of the block of size m0 copied at the switch) holds rows j..m0-1 from offset pk(j).
+__device__ __forceinline__ int pk(int j, int m0) { return j * m0 - (j * (j - 1)) / 2; }
+
 // RM = register rows per lane: n <= 32 RM.
 template <int RM>
 __global__ void __launch_bounds__(MT, 1)
-k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, int ms) {
+k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, int mp) {
+  constexpr int CW = RM >= 16 ? 2 : 4;
+  constexpr int CU = RM >= 16 ? 1 : 2;
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n;
   if (n < 3 || n > 32 * RM) return;
   extern __shared__ double sm[];
-  double* S = sm;                          // ms x ms: the trailing block once it fits
-  double* vb = S + size_t(ms) * ms;        // 2 x n: reflector of this step / of the next
+  double* vb = sm;                         // 2 x n: reflector of this step / of the next
   double* p = vb + 2 * n;                  // n
   double* d = p + n;                       // n
   double* e = d + n;                       // n
   double* e2 = e + n;                      // n
   double* tau = e2 + n;                    // n
+  double* S = tau + n;                     // packed trailing block, mp (mp + 1) / 2
   __shared__ double kw[NW];
   __shared__ double s_lo, s_hi;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double* Ag = base + tk.a_off;
   double* B = Ag + n + 1;                  // trailing block of step 0, A[1:, 1:]
-  int ld = n;
-  int k_sw = -1;                           // step at which the trailing block moved to S
+  const int ld = n;
   if (warp == 0) {
     double be, ta;
     house_warp(Ag + 1, n - 1, vb, be, ta, lane);
     if (lane == 0) { d[0] = Ag[0]; e[0] = be; tau[0] = ta; }
   }
   __syncthreads();
-  for (int k = 0; k + 2 < n; ++k) {
+  // steps on the matrix in global memory while the trailing block is larger than mp
+  int k = 0;
+  for (; k + 2 < n && n - k - 1 > mp; ++k) {
     const int m = n - k - 1;
-    if (k_sw < 0 && m <= ms) {
-      for (int x = tid; x < m * m; x += MT) {
-        const int i = x % m, j = x / m;
-        S[i + j * ms] = B[i + int64_t(j) * ld];
-      }
-      B = S;
-      ld = ms;
-      k_sw = k;
-      __syncthreads();
-    }
     const double* v = vb + (k & 1) * n;
     double* vn = vb + ((k + 1) & 1) * n;
     const double t = tau[k];
@@ -103,21 +106,38 @@ k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, i
         const int i = lane + 32 * r;
         vr[r] = (i < m) ? v[i] : 0.0;
       }
+      // CW columns per warp at a time: their loads are independent, so a lane keeps CW * RM
+      // loads in flight instead of RM (the steps on the L2-resident matrix are latency-bound)
       double kpart = 0.0;
-      for (int j = warp; j < m; j += NW) {
-        const double* col = B + int64_t(j) * ld;
-        double s0 = 0.0, s1 = 0.0;
+      for (int j0 = warp; j0 < m; j0 += CW * NW) {
+        double sc[CW];
 #pragma unroll
-        for (int r = 0; r < RM; r += 2) {
-          const int i0 = lane + 32 * r, i1 = i0 + 32;
-          if (i0 < m) s0 += col[i0] * vr[r];
-          if (r + 1 < RM && i1 < m) s1 += col[i1] * vr[r + 1];
+        for (int c = 0; c < CW; ++c) {
+          const int j = j0 + c * NW;
+          double s0 = 0.0, s1 = 0.0;
+          if (j < m) {
+            const double* col = B + int64_t(j) * ld;
+#pragma unroll
+            for (int r = 0; r < RM; r += 2) {
+              const int i0 = lane + 32 * r, i1 = i0 + 32;
+              if (i0 < m) s0 += col[i0] * vr[r];
+              if (r + 1 < RM && i1 < m) s1 += col[i1] * vr[r + 1];
+            }
+          }
+          sc[c] = s0 + s1;
         }
-        const double sj = wsum(s0 + s1);
+#pragma unroll
+        for (int c = 0; c < CW; ++c) sc[c] = wsum(sc[c]);
         if (lane == 0) {
-          const double pj = t * sj;
-          p[j] = pj;
-          kpart += pj * v[j];
+#pragma unroll
+          for (int c = 0; c < CW; ++c) {
+            const int j = j0 + c * NW;
+            if (j < m) {
+              const double pj = t * sc[c];
+              p[j] = pj;
+              kpart += pj * v[j];
+            }
+          }
         }
       }
       if (lane == 0) kw[warp] = kpart;
@@ -179,16 +199,36 @@ k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, i
         }
       }
     } else {
-      // columns 1..m-1, rows 1..m-1 (row 0 of B is never read again)
-      for (int j = warp; j < m; j += NW - 1) {
-        const double vj = v[j], wj = p[j] - hk * vj;
-        double* col = B + int64_t(j) * ld;
+      // columns 1..m-1, rows 1..m-1 (row 0 of B is never read again); CU columns at a time
+      double vi[RM], wi[RM];
 #pragma unroll
-        for (int r = 0; r < RM; ++r) {
-          const int i = 1 + lane + 32 * r;
-          if (i < m) {
-            const double vi = v[i], wi = p[i] - hk * vi;
-            col[i] = col[i] - (vi * wj + wi * vj);
+      for (int r = 0; r < RM; ++r) {
+        const int i = 1 + lane + 32 * r;
+        vi[r] = (i < m) ? v[i] : 0.0;
+        wi[r] = (i < m) ? p[i] - hk * vi[r] : 0.0;
+      }
+      for (int j0 = warp; j0 < m; j0 += CU * (NW - 1)) {
+        double cv[CU][RM];
+#pragma unroll
+        for (int c = 0; c < CU; ++c) {
+          const int j = j0 + c * (NW - 1);
+#pragma unroll
+          for (int r = 0; r < RM; ++r) {
+            const int i = 1 + lane + 32 * r;
+            cv[c][r] = (j < m && i < m) ? B[int64_t(j) * ld + i] : 0.0;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < CU; ++c) {
+          const int j = j0 + c * (NW - 1);
+          if (j < m) {
+            const double vj = v[j], wj = p[j] - hk * vj;
+            double* col = B + int64_t(j) * ld;
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+              const int i = 1 + lane + 32 * r;
+              if (i < m) col[i] = cv[c][r] - (vi[r] * wj + wi[r] * vj);
+            }
           }
         }
       }
@@ -196,21 +236,140 @@ k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, i
     __syncthreads();
     B += ld + 1;
   }
-  // B now addresses A[n-1, n-1] (the storage of the last steps)
-  if (tid == 0) {
-    d[n - 2] = B[-(ld + 1)];
-    e[n - 2] = B[-ld];
+
+  // the trailing block of step k_sw into shared memory (lower triangle, packed), then the
+  // remaining steps there: p = tau B v by row pairs (thread 2a sums row a's stored part b <= a
+  // along the diagonal direction, thread 2a+1 the column a part b > a), the rank-2 update by
+  // columns, warp 0 updating the pivot column first and building the next reflector from it
+  const int k_sw = k, m0 = n - k - 1;
+  for (int x = tid; x < m0 * m0; x += MT) {
+    const int i = x % m0, j = x / m0;
+    if (i >= j) S[pk(j, m0) + i - j] = B[i + int64_t(j) * ld];
+  }
+  __syncthreads();
+  for (; k + 2 < n; ++k) {
+    const int s0 = k - k_sw, m = n - k - 1;
+    const double* v = vb + (k & 1) * n;
+    double* vn = vb + ((k + 1) & 1) * n;
+    const double t = tau[k];
+    const int pks0 = pk(s0, m0);
+    {
+      const int a = tid >> 1, h = tid & 1;
+      double sa = 0.0, sb = 0.0;
+      if (a < m) {
+        if (h == 0) {                      // b = 0..a: element (a, b) in column s0 + b
+          int idx = pks0 + a;
+          int b = 0;
+          for (; b + 1 <= a; b += 2) {
+            sa += S[idx] * v[b];
+            idx += m - b - 1;
+            sb += S[idx] * v[b + 1];
+            idx += m - b - 2;
+          }
+          if (b <= a) sa += S[idx] * v[b];
+        } else {                           // b = a+1..m-1: element (b, a) in column s0 + a
+          const double* col = S + pk(s0 + a, m0) - a;
+          int b = a + 1;
+          for (; b + 2 <= m; b += 2) {
+            sa += col[b] * v[b];
+            sb += col[b + 1] * v[b + 1];
+          }
+          if (b < m) sa += col[b] * v[b];
+        }
+      }
+      double sum = sa + sb;
+      sum += __shfl_xor_sync(FULL, sum, 1);
+      double kpart = 0.0;
+      if (a < m && h == 0) {
+        const double pa = t * sum;
+        p[a] = pa;
+        kpart = pa * v[a];
+      }
+      kpart = wsum(kpart);
+      if (lane == 0) kw[warp] = kpart;
+    }
+    __syncthreads();
+    double K = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) K += kw[w];
+    const double hk = 0.5 * t * K;
+    if (warp == 0) {
+      double* B0 = S + pks0;               // pivot column: rows 0..m-1
+      const double v0 = v[0];
+      const double w0 = p[0] - hk * v0;
+      double c[RM];
+#pragma unroll
+      for (int r = 0; r < RM; ++r) {
+        const int i = lane + 32 * r;
+        double vi = 0.0, pi = 0.0, bi = 0.0;
+        if (i < m) { vi = v[i]; pi = p[i]; bi = B0[i]; }
+        const double wi = pi - hk * vi;
+        c[r] = bi - (vi * w0 + wi * v0);
+      }
+      if (k + 3 < n) {
+        double part = 0.0;
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = lane + 32 * r;
+          if (i >= 2 && i < m) part += c[r] * c[r];
+        }
+        const double xn2 = wsum(part);
+        const double alpha = __shfl_sync(FULL, c[0], 1);
+        double tn, sc, beta;
+        if (xn2 == 0.0) {
+          tn = 0.0; sc = 0.0; beta = alpha;
+        } else {
+          beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+          tn = (beta - alpha) / beta;
+          sc = 1.0 / (alpha - beta);
+        }
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = lane + 32 * r;
+          if (i >= 1 && i < m) {
+            const double vi = (i == 1) ? 1.0 : c[r] * sc;
+            vn[i - 1] = vi;
+            if (i >= 2) B0[i] = vi;        // reflector tail, below the subdiagonal
+          }
+        }
+        if (lane == 0) {
+          d[k + 1] = c[0];
+          e[k + 1] = beta;
+          tau[k + 1] = tn;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+          const int i = lane + 32 * r;
+          if (i < m) B0[i] = c[r];
+        }
+      }
+    } else {
+      for (int j = warp; j < m; j += NW - 1) {   // columns 1..m-1, rows j..m-1
+        const double vj = v[j], wj = p[j] - hk * vj;
+        double* col = S + pk(s0 + j, m0) - j;
+        for (int i = j + lane; i < m; i += 32) {
+          const double vi = v[i], wi = p[i] - hk * vi;
+          col[i] = col[i] - (vi * wj + wi * vj);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {   // the last 2 x 2 block: A[n-2.., n-2..] at packed column s0f - 1 and s0f
+    const int s0f = (n - 2) - k_sw;
+    d[n - 2] = S[pk(s0f - 1, m0)];
+    e[n - 2] = S[pk(s0f - 1, m0) + 1];
     tau[n - 2] = 0.0;
-    d[n - 1] = B[0];
+    d[n - 1] = S[pk(s0f, m0)];
     e[n - 1] = 0.0;
     tau[n - 1] = 0.0;
   }
-  if (k_sw >= 0) {   // the shared copy back into the caller's matrix (its reflector tails)
-    const int m0 = n - k_sw - 1;
+  {   // the packed block back into the caller's matrix (its reflector tails)
     double* G = Ag + int64_t(k_sw + 1) * n + (k_sw + 1);
     for (int x = tid; x < m0 * m0; x += MT) {
       const int i = x % m0, j = x / m0;
-      G[i + int64_t(j) * n] = S[i + j * ms];
+      if (i >= j) G[i + int64_t(j) * n] = S[pk(j, m0) + i - j];
     }
   }
   __syncthreads();
@@ -280,9 +439,7 @@ __host__ __device__ inline int64_t mid_vec_workspace(int n, int k) {
 }
 
 __host__ __device__ inline size_t mid_vec_smem(int n, int k) {
-  const int nblk = n >= 3 ? (n - 2 + MID_BT_NB - 1) / MID_BT_NB : 0;
-  return sizeof(double) * (2 * size_t(n) + size_t(MID_BT_NB) * k + size_t(nblk) * 64 +
-                           size_t(NW) * 64 + 2 * size_t(k)) + 64;
+  return sizeof(double) * (2 * size_t(n) + 2 * size_t(k)) + 64;
 }
 
 __global__ void __launch_bounds__(MT, 1)
@@ -292,14 +449,10 @@ k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks
   const int n = tk.n, kk = tk.keep;
   if (n < 3 || kk <= 0) return;
   const int ldz = kk | 1;
-  const int nblk = (n - 2 + MID_BT_NB - 1) / MID_BT_NB;
   extern __shared__ double sm[];
   double* d = sm;                          // n
   double* e = d + n;                       // n
-  double* Y = e + n;                       // MID_BT_NB x kk
-  double* Tb = Y + MID_BT_NB * kk;         // nblk x 64: T factor of each reflector block
-  double* Sw = Tb + nblk * 64;             // NW x 64: reflector Gram entries
-  double* rinv = Sw + NW * 64;             // kk
+  double* rinv = e + n;                    // kk
   double* sq = rinv + kk;                  // kk
   __shared__ double red[32];
   __shared__ double s_tn;
@@ -312,8 +465,6 @@ k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks
   double* G = Z + int64_t(n) * ldz;                        // kk x kk row-major, upper triangle
   const double* ws = base + tk.ws_off;
   const double* W = base + tk.w_off;
-  const double* V = base + tk.a_off;       // reflector k: V[k n + r], r > k + 1 (unit at k + 1)
-  const double* tau = ws + 2 * n;
   for (int i = tid; i < n; i += MT) { d[i] = ws[i]; e[i] = ws[n + i]; }
   if (warp == 0) {
     double tn = 0.0;
@@ -435,7 +586,39 @@ k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks
       __syncthreads();
     }
   }
-  // ---- back-transformation U = H_0 H_1 ... H_{n-3} Z in blocks of MID_BT_NB reflectors
+}
+
+// Back-transformation U = H_0 H_1 ... H_{n-3} Z for one slice of BT_W kept vectors per CTA
+// (blockIdx.y = slice): the slice of Z is staged in shared memory, the reflectors are read from
+// the matrix in global memory (L2-resident, shared by the slices), applied in blocks of
+// MID_BT_NB with their compact-WY T factors (built by each CTA: cheap next to the product).
+constexpr int BT_W = 32;
+__global__ void __launch_bounds__(MT, 1)
+k_trid_mid_backtransform(double* __restrict__ base, const TridTask* __restrict__ tasks,
+                         const double* __restrict__ xws) {
+  const TridTask tk = tasks[blockIdx.x];
+  const int n = tk.n, kk = tk.keep;
+  const int q0 = blockIdx.y * BT_W;
+  if (n < 3 || q0 >= kk) return;
+  const int w = min(BT_W, kk - q0);
+  const int ldz = kk | 1;
+  const int nblk = (n - 2 + MID_BT_NB - 1) / MID_BT_NB;
+  extern __shared__ double sm[];
+  double* Zs = sm;                               // n x BT_W, row-major (Zs[r * BT_W + q])
+  double* Wv = Zs + size_t(n) * BT_W;            // MID_BT_NB x BT_W
+  double* Yv = Wv + MID_BT_NB * BT_W;            // MID_BT_NB x BT_W
+  double* Tb = Yv + MID_BT_NB * BT_W;            // nblk x 64
+  double* Sw = Tb + size_t(nblk) * 64;           // NW x 64
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double* X = xws + tk.x_off;
+  const double* Z = X + 4 * int64_t(n) * kk + (int64_t(n) * kk + 1) / 2;
+  const double* V = base + tk.a_off;             // reflector k: V[k n + r], r > k + 1
+  const double* tau = base + tk.ws_off + 2 * n;
+  for (int x = tid; x < n * BT_W; x += MT) {
+    const int r = x / BT_W, q = x - r * BT_W;
+    Zs[x] = q < w ? Z[int64_t(r) * ldz + q0 + q] : 0.0;
+  }
+  // T factor of every reflector block (one warp per block)
   for (int bb = warp; bb < nblk; bb += NW) {
     const int k0 = bb * MID_BT_NB, nb = min(MID_BT_NB, n - 2 - k0);
     double* Sg = Sw + warp * 64;
@@ -467,11 +650,11 @@ k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks
         if (i == a) {
           v = tau[k0 + a];
         } else if (i > a && i < nb) {
-          double s = 0.0;
+          double sacc = 0.0;
 #pragma unroll
           for (int c = 0; c < MID_BT_NB; ++c)
-            if (c >= a && c < i) s += Tr[c] * Sg[c * 8 + i];
-          v = -tau[k0 + i] * s;
+            if (c >= a && c < i) sacc += Tr[c] * Sg[c * 8 + i];
+          v = -tau[k0 + i] * sacc;
         }
         Tr[i] = v;
       }
@@ -484,79 +667,67 @@ k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks
   for (int bb = nblk - 1; bb >= 0; --bb) {
     const int k0 = bb * MID_BT_NB, nb = min(MID_BT_NB, n - 2 - k0);
     const double* T = Tb + bb * 64;
-    {   // Y = T (V^T Z): 8-lane groups, lane a = reflector, group = vector q
-      const int g8 = tid >> 3, a = tid & 7, ng8 = MT >> 3;
-      for (int qb = 0; qb < kk; qb += ng8) {
-        const int q = qb + g8;
-        double y = 0.0;
-        if (q < kk && a < nb) {
-          const int k = k0 + a;
-          const double* vk = V + int64_t(k) * n;
-          double s0 = Z[int64_t(k + 1) * ldz + q], s1 = 0.0, s2 = 0.0, s3 = 0.0;
-          int r = k + 2;
-          for (; r + 4 <= n; r += 4) {
-            double vv[4], zz[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) { vv[u] = vk[r + u]; zz[u] = Z[int64_t(r + u) * ldz + q]; }
-            s0 += vv[0] * zz[0]; s1 += vv[1] * zz[1]; s2 += vv[2] * zz[2]; s3 += vv[3] * zz[3];
-          }
-          for (; r < n; ++r) s0 += vk[r] * Z[int64_t(r) * ldz + q];
-          y = (s0 + s1) + (s2 + s3);
-        }
-        double y2 = 0.0;
-#pragma unroll
-        for (int c = 0; c < MID_BT_NB; ++c) {
-          const double yc = __shfl_sync(FULL, y, c, 8);
-          if (c >= a && c < nb) y2 += T[a * 8 + c] * yc;
-        }
-        if (q < kk && a < nb) Y[a * kk + q] = y2;
+    {   // W = V^T Zs: pair (a, q) with the rows split between the two halves of the block
+      const int half = tid / (MT / 2), pq = tid - half * (MT / 2);
+      const int a = pq / BT_W, q = pq - a * BT_W;
+      double sacc = 0.0;
+      if (a < nb) {
+        const int k = k0 + a;
+        const double* vk = V + int64_t(k) * n;
+        if (half == 0) sacc = Zs[(k + 1) * BT_W + q];
+        for (int r = k + 2 + half; r < n; r += 2) sacc += vk[r] * Zs[r * BT_W + q];
       }
+      if (half == 1 && a < MID_BT_NB) Wv[a * BT_W + q] = sacc;
+      __syncthreads();
+      if (half == 0 && a < MID_BT_NB) Wv[a * BT_W + q] += sacc;
     }
     __syncthreads();
-    // Z -= V Y on rows r0..n-1: a thread owns row r (its reflector entries in registers) and
-    // the vectors q = g, g + Gc, ... of its group g
-    const int r0 = k0 + 1, nr = n - r0;
-    const int Gc = max(1, MT / nr);
-    for (int rt = tid; rt < Gc * nr; rt += MT) {
-      const int g = rt / nr, r = r0 + (rt - g * nr);
-      double va[MID_BT_NB];
+    if (tid < MID_BT_NB * BT_W) {         // Y = T W
+      const int a = tid / BT_W, q = tid - a * BT_W;
+      double y = 0.0;
+      if (a < nb)
+        for (int c = a; c < nb; ++c) y += T[a * 8 + c] * Wv[c * BT_W + q];
+      Yv[a * BT_W + q] = y;
+    }
+    __syncthreads();
+    // Zs -= V Y on rows k0+1..n-1
+    for (int x = (k0 + 1) * BT_W + tid; x < n * BT_W; x += MT) {
+      const int r = x / BT_W, q = x - r * BT_W;
+      double sacc = 0.0;
 #pragma unroll
       for (int a = 0; a < MID_BT_NB; ++a) {
         const int k = k0 + a;
-        va[a] = (a >= nb) ? 0.0 : (r == k + 1) ? 1.0 : (r > k + 1 ? V[int64_t(k) * n + r] : 0.0);
+        if (a < nb && r >= k + 1) {
+          const double va = (r == k + 1) ? 1.0 : V[int64_t(k) * n + r];
+          sacc += va * Yv[a * BT_W + q];
+        }
       }
-      double* zr = Z + int64_t(r) * ldz;
-      for (int q = g; q < kk; q += Gc) {
-        double s0 = 0.0;
-#pragma unroll
-        for (int a = 0; a < MID_BT_NB; ++a)
-          if (a < nb) s0 += va[a] * Y[a * kk + q];
-        zr[q] -= s0;
-      }
+      Zs[x] -= sacc;
     }
     __syncthreads();
   }
   double* U = base + tk.u_off;
-  for (int64_t x = tid; x < int64_t(n) * kk; x += MT) {
-    const int q = int(x / n), r = int(x - int64_t(q) * n);
-    U[x] = Z[int64_t(r) * ldz + q];
+  for (int x = tid; x < n * w; x += MT) {
+    const int q = x / n, r = x - q * n;
+    U[int64_t(q0 + q) * n + r] = Zs[r * BT_W + q];
   }
 }
 
-int mid_ms(int max_n) {
-  // largest trailing block that fits in shared memory beside the 7 n vectors
+int mid_mp(int max_n) {
+  // largest trailing block whose packed lower triangle fits in shared memory beside the 7 n
+  // vectors (at least 2: the last steps always run there)
   const size_t avail = MID_SMEM_LIMIT - sizeof(double) * 7 * size_t(max_n) - 64;
-  int ms = 8;
-  while (size_t(ms + 8) * (ms + 8) * sizeof(double) <= avail) ms += 8;
-  return ms;
+  int mp = 2;
+  while (size_t(mp + 1) * (mp + 2) / 2 * sizeof(double) <= avail) ++mp;
+  return mp;
 }
 
 template <int RM>
 void launch_vals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks, int max_n) {
-  const int ms = mid_ms(max_n);
-  const size_t sm = sizeof(double) * (size_t(ms) * ms + 7 * size_t(max_n)) + 64;
+  const int mp = mid_mp(max_n);
+  const size_t sm = sizeof(double) * (size_t(mp) * (mp + 1) / 2 + 7 * size_t(max_n)) + 64;
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vals<RM>), sm);
-  k_trid_mid_vals<RM><<<ntasks, MT, sm, s>>>(base, tasks, ms);
+  k_trid_mid_vals<RM><<<ntasks, MT, sm, s>>>(base, tasks, mp);
   count_launch();
 }
 
@@ -577,6 +748,13 @@ void launch_trid_mid_vectors(cudaStream_t s, double* base, const TridTask* tasks
   const size_t sm = mid_vec_smem(max_n, max_k);
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vectors), sm);
   k_trid_mid_vectors<<<ntasks, MT, sm, s>>>(base, tasks, xws);
+  count_launch();
+  const int nblk = max_n >= 3 ? (max_n - 2 + MID_BT_NB - 1) / MID_BT_NB : 0;
+  const size_t sb = sizeof(double) * (size_t(max_n) * BT_W + 2 * MID_BT_NB * BT_W +
+                                      size_t(nblk) * 64 + NW * 64);
+  raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_backtransform), sb);
+  const dim3 grid(ntasks, (max_k + BT_W - 1) / BT_W);
+  k_trid_mid_backtransform<<<grid, MT, sb, s>>>(base, tasks, xws);
   count_launch();
 }
 

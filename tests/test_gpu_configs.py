@@ -92,14 +92,17 @@ def test_capped_config_matches_oracle(dmrgb, ctx, name):
 
 
 def test_density_matrix_blocks_above_the_tridiagonal_limit(dmrgb, ctx):
-    """Dense chain whose centre density matrix (m=64, d=2: side 128) is larger than the
-    tridiagonal kernel's limit (112), so the block-Jacobi path runs inside the sweep."""
+    """Dense chain whose centre density matrix (m=64, d=2: side 128) is larger than the small
+    tridiagonal kernel's limit (112), so the mid-size kernels run inside the sweep. The cutoff
+    (1e-10) keeps the cut away from eigenvalues at the rounding level (~1e-16): at such a cut a
+    noise-level state may or may not be kept, and a kept one enlarges the variational space of
+    the following steps."""
     L = 12
     mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
     psi = dmrgb.randMPS(2, L, 64, seed=7)
     ref = [a.copy() for a in psi.tensors]
-    E = dmrgb.dmrg(psi, mpo, m=100, sweeps=3, cutoff=1e-14, krylov=2, ctx=ctx)
+    E = dmrgb.dmrg(psi, mpo, m=100, sweeps=3, cutoff=1e-10, krylov=2, ctx=ctx)
     E0, info = od.dmrg(ref, om.make_mpo([om.heisenberg_bulk()] * L, 2), m=100, sweeps=3,
-                       cutoff=1e-14, krylov=2, trunc="rho")
+                       cutoff=1e-10, krylov=2, trunc="rho")
     assert max(s["eig_max_n"] for s in psi.sweep_stats) > 112
     _compare(psi, E, E0, info)
