@@ -45,8 +45,14 @@ void run_trid_eigvals(dmrg_ctx* c, double* base, int64_t nbase, const std::vecto
 void run_trid_vectors(dmrg_ctx* c, double* base, int64_t nbase, std::vector<TridTask> t,
                       int slot) {
   check_trid(t, nbase, true);
-  std::vector<TridTask> small, mid;
-  int ns = 0, ks = 0, nm = 0, km = 0;
+  // mid-size blocks in two launches: those whose Gram matrix fits in shared memory beside the
+  // block's vectors, and the rest (which then keep the whole L1 for their global-memory Gram)
+  std::vector<TridTask> small, mid[2];
+  int ns = 0, ks = 0, nm[2] = {0, 0}, km[2] = {0, 0};
+  int nmax = 0;
+  for (const TridTask& x : t)
+    if (x.keep > 0 && x.n > SYEVT_NMAX) nmax = std::max(nmax, x.n);
+  const int kg = nmax > 0 ? syevt_mid_gram_limit(nmax) : 0;
   int64_t xw = 0;
   for (TridTask x : t) {
     if (x.keep <= 0) continue;
@@ -57,22 +63,25 @@ void run_trid_vectors(dmrg_ctx* c, double* base, int64_t nbase, std::vector<Trid
     } else {
       x.x_off = xw;
       xw += syevt_mid_workspace(x.n, x.keep);
-      mid.push_back(x);
-      nm = std::max(nm, x.n);
-      km = std::max(km, x.keep);
+      const int g = x.keep <= kg ? 0 : 1;
+      mid[g].push_back(x);
+      nm[g] = std::max(nm[g], x.n);
+      km[g] = std::max(km[g], x.keep);
     }
   }
-  if (small.empty() && mid.empty()) return;
-  if (!mid.empty()) ensure(c, c->W, xw);
+  if (small.empty() && mid[0].empty() && mid[1].empty()) return;
+  if (xw > 0) ensure(c, c->W, xw);
   Upload u;
-  const size_t o1 = u.put(small), o2 = u.put(mid);
+  const size_t o1 = u.put(small), o2 = u.put(mid[0]), o3 = u.put(mid[1]);
   char* db = u.send(c, slot);
   if (!small.empty())
     launch_trid_vectors(c->stream, base, reinterpret_cast<const TridTask*>(db + o1),
                         int(small.size()), ns, ks);
-  if (!mid.empty())
-    launch_trid_mid_vectors(c->stream, base, reinterpret_cast<const TridTask*>(db + o2),
-                            int(mid.size()), nm, km, c->W.p);
+  for (int g = 0; g < 2; ++g)
+    if (!mid[g].empty())
+      launch_trid_mid_vectors(c->stream, base,
+                              reinterpret_cast<const TridTask*>(db + (g == 0 ? o2 : o3)),
+                              int(mid[g].size()), nm[g], km[g], c->W.p);
   cuda_check(cudaGetLastError(), "tridiagonal eigenvectors");
 }
 

@@ -76,7 +76,7 @@ struct TridTask {
   int64_t ws_off;  // 3n workspace: d, e, tau
   int64_t u_off;   // n x keep eigenvectors (launch 2)
   int n, keep;
-  int64_t x_off;   // mid-size launch 2: workspace offset (syevt_mid_workspace(n, keep) doubles)
+  int64_t x_off;   // mid-size launches 2-3: workspace offset (syevt_mid_workspace(n, keep) doubles)
 };
 size_t syevt_smem_vals(int n);
 size_t syevt_smem_vecs(int n, int k);
@@ -84,6 +84,9 @@ void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, in
 void launch_trid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
                          int max_n, int max_k);
 int64_t syevt_mid_workspace(int n, int k);
+// Largest kept count whose Gram matrix the mid-size vector kernel holds in shared memory for
+// blocks up to max_n (tasks above it take the global-memory path; launch them separately).
+int syevt_mid_gram_limit(int max_n);
 void launch_trid_mid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
                              int max_n);
 // xws: workspace base of the tasks' x_off

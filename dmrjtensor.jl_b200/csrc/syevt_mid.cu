@@ -438,13 +438,24 @@ __host__ __device__ inline int64_t mid_vec_workspace(int n, int k) {
   return 4 * int64_t(n) * k + (int64_t(n) * k + 1) / 2 + int64_t(n) * ldz + int64_t(k) * k + 8;
 }
 
-__host__ __device__ inline size_t mid_vec_smem(int n, int k) {
-  return sizeof(double) * (2 * size_t(n) + 2 * size_t(k)) + 64;
+// Packed upper triangle by rows of a k x k matrix: row p starts at gpk(p, k).
+__host__ __device__ __forceinline__ int gpk(int p, int k) { return p * k - (p * (p - 1)) / 2; }
+
+// Shared memory of k_trid_mid_vectors: d, e (n each), rinv, sq (k each) and, for k <= kg, the
+// packed Gram matrix. kg = the largest k for which all of it fits.
+__host__ __device__ inline size_t mid_vec_smem_k(int n, int k, bool gram) {
+  return sizeof(double) * (2 * size_t(n) + 2 * size_t(k) +
+                           (gram ? size_t(k) * (k + 1) / 2 : 0)) + 64;
+}
+int mid_vec_kg(int max_n) {
+  int kg = 0;
+  while (mid_vec_smem_k(max_n, kg + 1, true) <= MID_SMEM_LIMIT) ++kg;
+  return kg;
 }
 
 __global__ void __launch_bounds__(MT, 1)
 k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks,
-                   double* __restrict__ xws) {
+                   double* __restrict__ xws, int kg) {
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n, kk = tk.keep;
   if (n < 3 || kk <= 0) return;
@@ -491,8 +502,108 @@ k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks
     }
   }
   __syncthreads();
-  // ---- Cholesky QR
+  // ---- Cholesky QR: G = Z^T Z = R^T R with R = D^(1/2) U (U unit upper), Z <- Z U^-1 D^(-1/2);
+  // a second pass unless G was within 1e-3/k of the identity. When the packed upper triangle of
+  // G fits in shared memory (kk <= kg) it lives there: the Gram matrix by 4 x 4 register tiles,
+  // the elimination by one warp per row, the solve by one thread per row in blocks of 32
+  // columns held in registers. Otherwise G stays in the global workspace.
+  const bool gsm = kk <= kg;
+  double* Gs = sq + kk;                    // packed: G(p, q), q >= p, at gpk(p) + q - p
   for (int pass = 0; pass < 2; ++pass) {
+    if (gsm) {
+      const int nb4 = (kk + 3) >> 2, ntile = nb4 * (nb4 + 1) / 2;
+      for (int x = tid; x < ntile; x += MT) {
+        int I = 0;
+        while ((I + 1) * nb4 - ((I + 1) * I) / 2 <= x) ++I;
+        const int J = I + (x - (I * nb4 - (I * (I - 1)) / 2));
+        double acc[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] = 0.0;
+        for (int r = 0; r < n; ++r) {
+          const double* zr = Z + int64_t(r) * ldz;
+          double a[4], b[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int ca = 4 * I + u, cb = 4 * J + u;
+            a[u] = ca < kk ? zr[ca] : 0.0;
+            b[u] = cb < kk ? zr[cb] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int w2 = 0; w2 < 4; ++w2) acc[u * 4 + w2] += a[u] * b[w2];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int w2 = 0; w2 < 4; ++w2) {
+            const int pp = 4 * I + u, q = 4 * J + w2;
+            if (pp <= q && q < kk) {
+              const double gv = acc[u * 4 + w2];
+              Gs[gpk(pp, kk) + q - pp] = gv;
+              if (pass == 0 && fabs(gv - (pp == q ? 1.0 : 0.0)) > 1e-3 / kk) s_need2 = 1;
+            }
+          }
+      }
+      __syncthreads();
+      for (int j = 0; j < kk; ++j) {
+        const double* rowj = Gs + gpk(j, kk) - j;      // rowj[q] = G(j, q), q >= j
+        const double gjj = rowj[j];
+        if (!(gjj > 1e-8) && tid == 0) s_flag = 1;
+        const double inv = 1.0 / fmax(gjj, 1e-300);
+        for (int pr = j + 1 + warp; pr < kk; pr += NW) {
+          const double f = rowj[pr] * inv;
+          double* rowp = Gs + gpk(pr, kk) - pr;
+          for (int q = pr + lane; q < kk; q += 32) rowp[q] -= f * rowj[q];
+        }
+        __syncthreads();
+      }
+      for (int q = tid; q < kk; q += MT) {
+        const double g = fmax(Gs[gpk(q, kk)], 1e-300);
+        rinv[q] = 1.0 / g;
+        sq[q] = sqrt(g);
+      }
+      __syncthreads();
+      if (s_flag) break;
+      for (int r = tid; r < n; r += MT) {
+        double* zr = Z + int64_t(r) * ldz;
+        for (int q0 = 0; q0 < kk; q0 += 32) {
+          const int qb = min(32, kk - q0);
+          double acc[32];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) acc[c] = c < qb ? zr[q0 + c] : 0.0;
+#pragma unroll 4
+          for (int pp = 0; pp < q0; ++pp) {
+            const double y = zr[pp];
+            const double* gr = Gs + gpk(pp, kk) - pp;  // gr[q] = G(pp, q)
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+              if (c < qb) acc[c] -= y * gr[q0 + c];
+          }
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            if (c < qb) {
+              const double* gc = Gs + gpk(q0, kk) - q0;  // row q0, then down the block
+              double sacc = acc[c];
+              int off = 0;
+#pragma unroll
+              for (int c2 = 0; c2 < 32; ++c2) {
+                if (c2 < c) sacc -= acc[c2] * gc[off + q0 + c];
+                off += kk - (q0 + c2) - 1;             // gpk(p + 1) - (p + 1) - (gpk(p) - p)
+              }
+              acc[c] = sacc * rinv[q0 + c];
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 32; ++c)
+            if (c < qb) zr[q0 + c] = acc[c];
+        }
+        for (int q = 0; q < kk; ++q) zr[q] *= sq[q];
+      }
+      __syncthreads();
+      if (!s_need2) break;
+      continue;
+    }
     for (int x = tid; x < kk * kk; x += MT) {
       const int pp = x / kk, q = x - pp * kk;
       if (pp > q) continue;
@@ -734,6 +845,7 @@ void launch_vals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks
 }  // namespace
 
 int64_t syevt_mid_workspace(int n, int k) { return mid_vec_workspace(n, k); }
+int syevt_mid_gram_limit(int max_n) { return mid_vec_kg(max_n); }
 
 void launch_trid_mid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
                              int max_n) {
@@ -745,9 +857,11 @@ void launch_trid_mid_eigvals(cudaStream_t s, double* base, const TridTask* tasks
 void launch_trid_mid_vectors(cudaStream_t s, double* base, const TridTask* tasks, int ntasks,
                              int max_n, int max_k, double* xws) {
   if (ntasks <= 0) return;
-  const size_t sm = mid_vec_smem(max_n, max_k);
+  // the Gram matrix in shared memory only when every task's fits (callers split the tasks)
+  const int kg = max_k <= mid_vec_kg(max_n) ? max_k : 0;
+  const size_t sm = mid_vec_smem_k(max_n, max_k, kg > 0);
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vectors), sm);
-  k_trid_mid_vectors<<<ntasks, MT, sm, s>>>(base, tasks, xws);
+  k_trid_mid_vectors<<<ntasks, MT, sm, s>>>(base, tasks, xws, kg);
   count_launch();
   const int nblk = max_n >= 3 ? (max_n - 2 + MID_BT_NB - 1) / MID_BT_NB : 0;
   const size_t sb = sizeof(double) * (size_t(max_n) * BT_W + 2 * MID_BT_NB * BT_W +
