@@ -464,7 +464,11 @@ def config_leg(pkg, ctx, which, fp64_peak, tf32_peak, bf16_peak, tmpdir):
         for rep in range(2):
             dev = pkg.DeviceState.load(ckpt, dmpo)
             dev.env_build()
+            if rep == 1:    # a profiler can select exactly this sweep's launches
+                nvtx("push", f"{which}_same_state_{form}")
             s = dev.sweep(pkg.make_params(maxm=sched[-1], minm=2, cutoff=cutoff, precision=form))
+            if rep == 1:
+                nvtx("pop")
             rec = {"sweep_seconds": s["seconds"], "energy": s["energy"],
                    "host_seconds": s["host_seconds"], "wait_seconds": s["wait_seconds"]}
             del dev
@@ -616,6 +620,30 @@ def method_legs(pkg, ctx, dev, args):
         "En": stt[-1]["energy"], "biggest_m": stt[-1]["biggest_m"],
         "max_truncerr": stt[-1]["max_truncerr"], "prefactor": -0.1}
     return out
+
+
+def eig_only(pkg, ctx, n, k, reps=3):
+    """One density-matrix eigensolve of an n x n block keeping k vectors through the library's
+    kernel hook (dmrg_test_syevt): a synthetic DMRG-like density matrix M M^T with column scales
+    exp(-c / 12), seed 7. The case the eigensolver captures use; prints device-visible seconds
+    per call and the residual of the returned pairs."""
+    import ctypes as C
+    rng = np.random.default_rng(7)
+    M = rng.standard_normal((n, 2 * n)) * np.exp(-np.arange(2 * n) / 12.0)
+    rho = M @ M.T
+    dp = C.POINTER(C.c_double)
+    times = []
+    for _ in range(reps):
+        A = np.asfortranarray(rho.copy())
+        w = np.zeros(n)
+        U = np.zeros((n, k), order="F")
+        t0 = time.perf_counter()
+        pkg._lib.check(pkg.lib().dmrg_test_syevt(ctx.h, 1, (C.c_int * 1)(n), (C.c_int * 1)(k),
+                                                 A.ctypes.data_as(dp), w.ctypes.data_as(dp),
+                                                 U.ctypes.data_as(dp)), ctx.h)
+        times.append(time.perf_counter() - t0)
+    res = float(np.max(np.abs(rho @ U - U * w[:k])) / w[0])
+    return {"n": n, "keep": k, "seconds_per_call_host": min(times), "residual": res}
 
 
 def cpu_threads():
@@ -909,6 +937,9 @@ def main():
                     help="skip the split-precision (3xTF32) sweeps")
     ap.add_argument("--heff-only", action="store_true",
                     help="only time the plain and split Heff at the m=1024 dense-equivalent size")
+    ap.add_argument("--eig-only", default=None, metavar="N,K",
+                    help="only one N x N density-matrix eigensolve keeping K vectors (the "
+                         "eigensolver captures' case)")
     ap.add_argument("--no-methods", dest="methods", action="store_false",
                     help="skip the 3S and TDVP legs")
     ap.add_argument("--no-measure", dest="measure", action="store_false",
@@ -937,6 +968,10 @@ def main():
                 out[f"capacity_{prec}"] = run_serving(pkg, local, args.serve_saturate,
                                                       saturate=True, precision=prec)
             print(json.dumps({"serving": out}))
+        elif args.eig_only:
+            n, k = (int(x) for x in args.eig_only.split(","))
+            pkg = load_pkg()
+            print(json.dumps({"eig_only": eig_only(pkg, pkg.Context(local), n, k)}))
         elif args.heff_only:
             # the plain and split Heff forms alone (the kernel-profiling case)
             pkg = load_pkg()
