@@ -24,7 +24,7 @@ class Params(C.Structure):
                 ("krylov", C.c_int), ("precision", C.c_int), ("svnbond", C.c_int),
                 ("degen_rtol", C.c_double), ("betatest", C.c_double), ("fp64_final", C.c_int),
                 ("profile", C.c_int), ("cvgE", C.c_int), ("tune", C.c_int),
-                ("goal", C.c_double), ("graph", C.c_int), ("reserved1", C.c_int)]
+                ("goal", C.c_double), ("graph", C.c_int), ("halfsweep", C.c_int)]
 
 
 class SweepStats(C.Structure):

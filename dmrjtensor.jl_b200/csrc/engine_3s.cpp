@@ -457,18 +457,19 @@ void do_sweep3s(dmrg_state* st, const dmrg_params& P, const dmrg_noise& nz, doub
   int j = st->dir;
   const int j0 = j;
   double alpha = *noise;
-  for (int ns = 0; ns < 2 * (L - 1); ++ns) {
+  const int nsteps = P.halfsweep ? L - 1 : 2 * (L - 1);   // halfsweep (algs/DMRG.jl:253)
+  for (int ns = 0; ns < nsteps; ++ns) {
     const int i = st->oc;
     StepOut so;
     SiteMode md;
     md.alpha = alpha;
     md.noise_incr = nz.noise_incr;
-    single_site_step(st, P, md, j, i, ns == 2 * (L - 1) - 1, tm, so);
+    single_site_step(st, P, md, j, i, ns == nsteps - 1, tm, so);
     alpha = alpha_update(alpha, so.truncerr, P.cutoff, last_energy, so.energy, nz.noise_goal,
                          nz.noise_incr);
     const int tenv = tm.begin();
     double ef = 0.0;
-    const int eprec = (split_form(P.precision) && !(P.fp64_final && j != j0))
+    const int eprec = (split_form(P.precision) && !(P.fp64_final && (P.halfsweep || j != j0)))
                           ? P.precision : DMRG_PREC_FP64;
     if (j > 0) lupdate(st, i, &ef, eprec); else rupdate(st, i, &ef, eprec);
     cuda_check(cudaGetLastError(), "environment update");

@@ -539,18 +539,19 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   const int t0 = tm.record();
   int j = st->dir;
   const int j0 = j;
-  for (int ns = 0; ns < 2 * (L - 1); ++ns) {
+  const int nsteps = P.halfsweep ? L - 1 : 2 * (L - 1);   // halfsweep (algs/DMRG.jl:253)
+  for (int ns = 0; ns < nsteps; ++ns) {
     const int i = st->oc;
     const int iL = j > 0 ? i : i - 1, iR = j > 0 ? i + 1 : i;
     StepOut so;
-    twostep(st, P, j, iL, iR, ns == 2 * (L - 1) - 1, tm, so, StepMode{});
+    twostep(st, P, j, iL, iR, ns == nsteps - 1, tm, so, StepMode{});
     const int tenv = tm.begin();
     double ef = 0.0;
     // split form: the environment updates run on the tensor cores too, except those of the
     // second half-sweep when the sweep's energy is the FP64 Rayleigh quotient (fp64_final): that
     // half-sweep builds, from the final site tensors, every environment the last bond step reads,
     // so the quotient is exact FP64 arithmetic on the final Ritz vector
-    const int eprec = (split_form(P.precision) && !(P.fp64_final && j != j0))
+    const int eprec = (split_form(P.precision) && !(P.fp64_final && (P.halfsweep || j != j0)))
                           ? P.precision : DMRG_PREC_FP64;
     if (j > 0) lupdate(st, i, &ef, eprec); else rupdate(st, i, &ef, eprec);
     cuda_check(cudaGetLastError(), "environment update");

@@ -48,7 +48,7 @@ mutable struct Params
   tune::Cint
   goal::Cdouble
   graph::Cint
-  reserved1::Cint
+  halfsweep::Cint
 end
 Params() = Params(0, 0, 0.0, 0, 0, 0, 0.0, 0.0, 0, 0, 0, 0, 0.0, 0, 0)
 
@@ -330,18 +330,19 @@ function DMRJtensor.dmrg(psi::DMRJtensor.matrixproductstate, mpo::DMRJtensor.mat
                          cvgE::Bool=params.cvgE, SvNbond::Integer=params.SvNbond,
                          noise::Number=first(params.noise), noise_goal::Float64=params.noise_goal,
                          noise_incr::Float64=params.noise_incr,
+                         halfsweep::Bool=params.halfsweep,
                          krylov::Integer=2, precision::Integer=0, charges=nothing,
                          device::Integer=0, kwargs...)
   if method != "twosite" && method != "3S"
     return invoke(DMRJtensor.dmrg, Tuple{DMRJtensor.MPS,DMRJtensor.MPO}, psi, mpo;
                   params=params, method=method, m=maxm, minm=minm, sweeps=sweeps, cutoff=cutoff,
                   silent=silent, goal=goal, cvgE=cvgE, SvNbond=SvNbond, noise=noise,
-                  noise_goal=noise_goal, noise_incr=noise_incr, kwargs...)
+                  noise_goal=noise_goal, noise_incr=noise_incr, halfsweep=halfsweep, kwargs...)
   end
   dmrg_b200(psi, mpo; maxm=maxm, minm=minm, sweeps=sweeps, cutoff=cutoff, silent=silent,
             goal=goal, cvgE=cvgE, SvNbond=SvNbond, krylov=krylov, precision=precision,
             charges=charges, device=device, method=method, noise=Float64(noise),
-            noise_goal=noise_goal, noise_incr=noise_incr)
+            noise_goal=noise_goal, noise_incr=noise_incr, halfsweep=halfsweep)
 end
 
 """
@@ -357,7 +358,7 @@ function dmrg_b200(psi, mpo; maxm::Integer=0, minm::Integer=2, sweeps::Integer=1
                    cutoff::Float64=0.0, silent::Bool=false, goal::Float64=0.0, cvgE::Bool=true,
                    SvNbond::Integer=0, krylov::Integer=2, precision::Integer=0, charges=nothing,
                    device::Integer=0, method::String="twosite", noise::Float64=1.0,
-                   noise_goal::Float64=0.3, noise_incr::Float64=0.01)
+                   noise_goal::Float64=0.3, noise_incr::Float64=0.01, halfsweep::Bool=false)
   ctx = context(device)
   ch = site_charges(psi, charges)
   hmpo = upload_mpo(ctx, mpo, ch)
@@ -370,6 +371,7 @@ function dmrg_b200(psi, mpo; maxm::Integer=0, minm::Integer=2, sweeps::Integer=1
     p.maxm, p.minm, p.cutoff, p.krylov, p.precision, p.svnbond = maxm, minm, cutoff, krylov,
                                                                  precision, SvNbond
     p.goal, p.cvgE = goal, cvgE ? 1 : 0
+    p.halfsweep = halfsweep ? 1 : 0
     nz = method == "3S" ? Noise(noise, noise_goal, noise_incr, 0.0) : nothing
     energy = run_sweeps!(ctx, st, hmpo, p, sweeps, silent, nz)
     write_back!(ctx, st, psi, ch)

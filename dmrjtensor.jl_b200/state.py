@@ -427,7 +427,7 @@ class DeviceState:
 
 def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
                 degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0, goal=0.0, cvgE=True,
-                tune=True, graph=True):
+                tune=True, graph=True, halfsweep=False):
     p = Params()
     lib().dmrg_params_default(C.byref(p))
     p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)
@@ -439,6 +439,7 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
     p.goal, p.cvgE = float(goal), 1 if cvgE else 0
     p.tune = 1 if tune else 0
     p.graph = 1 if graph else 0
+    p.halfsweep = 1 if halfsweep else 0
     return p
 
 
@@ -446,7 +447,8 @@ def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=
 
 def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, silent=True,
          method="twosite", krylov=2, precision="fp64", SvNbond=0, degen_rtol=0.0, goal=0.0,
-         cvgE=True, noise=1.0, noise_goal=0.3, noise_incr=0.01, ctx=None, download=True):
+         cvgE=True, noise=1.0, noise_goal=0.3, noise_incr=0.01, halfsweep=False, ctx=None,
+         download=True):
     """DMRG on the GPU: ``dmrg(psi, mpo; m, minm, sweeps, cutoff, method)`` of
     ``algs/DMRG.jl:549-588``. ``method="twosite"`` (default) runs ``dmrg_twosite``;
     ``method="3S"`` runs ``dmrg3S`` (``algs/DMRG.jl:655-671``: single-site steps with subspace
@@ -458,6 +460,8 @@ def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, si
     ``goal > 0`` stops after the first sweep whose energy (``cvgE``) or centre entropy changed by
     less than ``goal`` (``dmrgcvg``, ``algs/DMRG.jl:610-652``; the first sweep is compared with
     the starting energy <psi|H|psi>).
+    ``halfsweep=True`` makes every sweep one direction only (L-1 bond steps), as the reference's
+    ``halfsweep`` does (``algs/DMRG.jl:253``).
     ``download=False`` leaves the result on the device (``psi`` keeps a handle to it)."""
     if method not in ("twosite", "3S"):
         raise ValueError(f"DMRG method ({method}) not defined")
@@ -475,7 +479,7 @@ def dmrg(psi: MPS, mpo: MPO, m=None, maxm=None, minm=2, sweeps=1, cutoff=0.0, si
         nz.noise, nz.noise_goal, nz.noise_incr = float(noise), float(noise_goal), float(noise_incr)
     for n, mcur in enumerate(sched):
         p = make_params(mcur, minm, cutoff, krylov, precision, SvNbond, degen_rtol, goal=goal,
-                        cvgE=cvgE)
+                        cvgE=cvgE, halfsweep=halfsweep)
         st = dev.sweep(p) if nz is None else dev.sweep3s(p, nz)
         energy = st["energy"]
         stats.append(st)

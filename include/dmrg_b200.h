@@ -96,7 +96,10 @@ typedef struct dmrg_params {
   int graph;         /* 1 (default): the Lanczos step after its first Heff runs as one CUDA graph
                         (captured per step, the context's executable updated in place); 0: plain
                         launches. Same numbers either way */
-  int reserved1;
+  int halfsweep;     /* 1: a sweep is L-1 bond steps in the current direction (halfsweep of
+                        algs/DMRG.jl:253), the direction carrying over to the next call; 0
+                        (default): 2(L-1) steps, back and forth. With a split precision and
+                        fp64_final every environment update of a half sweep is FP64 */
 } dmrg_params;
 
 /* Per-sweep record (what dmrgcvg prints, algs/DMRG.jl:610-652, plus timings). */

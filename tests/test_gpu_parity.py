@@ -210,3 +210,18 @@ def test_block_upload_round_trip_at_a_4096_bond(dmrgb, ctx):
     L2 = od.Lupdate(od.Lupdate(np.ones((1, 1, 1)), dense[0], dense[0], W[0]), dense[1], dense[1], W[1])
     dev.lupdate(1)
     assert _rel(dev.env(2, True), L2) < RTOL_CONTRACT
+
+
+def test_two_half_sweeps_are_one_sweep(dmrgb, ctx):
+    """halfsweep (algs/DMRG.jl:253): a sweep of L-1 steps in the current direction; two of them
+    run exactly the steps of one full sweep, so every number is the same."""
+    L = 10
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    a, b = dmrgb.neelMPS(L), dmrgb.neelMPS(L)
+    Ea = dmrgb.dmrg(a, mpo, m=45, sweeps=3, cutoff=1e-12, ctx=ctx)
+    Eb = dmrgb.dmrg(b, mpo, m=45, sweeps=6, cutoff=1e-12, halfsweep=True, ctx=ctx)
+    assert Ea == Eb
+    assert a.oc == b.oc == 0
+    c = dmrgb.neelMPS(L)
+    dmrgb.dmrg(c, mpo, m=45, sweeps=1, cutoff=1e-12, halfsweep=True, ctx=ctx)
+    assert c.oc == L - 1
