@@ -9,9 +9,9 @@
 //     updates the next pivot column first and builds the next reflector (look-ahead). The
 //     reflector vectors are written into the strictly lower part of the caller's matrix, d/e/tau
 //     into a small per-block workspace;
-//   * all eigenvalues of T by trisection (two threads per eigenvalue, two Sturm counts per
-//     step) to an absolute width of 8.9e-16 ||T||, with a division-free Sturm count (see
-//     sturm_below).
+//   * all eigenvalues of T by multisection (2, 4 or 8 threads per eigenvalue as n allows, one
+//     Sturm count each per step) to an absolute width of 8.9e-16 ||T||, with a division-free
+//     Sturm count (see sturm_below).
 // The host then truncates globally and asks for the top-k vectors of each block.
 // Launch 2 (k_trid_vectors):
 //   * eigenvectors of T by inverse iteration on (T - lambda I) with partial-pivoting LU, one
@@ -257,30 +257,39 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
     }
   }
   __syncthreads();
-  // trisection: threads 2i and 2i+1 count at the two interior points of eigenvalue i's interval
+  // multisection: a group of P lanes per eigenvalue (P = 2, 4 or 8 as n allows with 256 threads)
+  // counts at the P interior points x_g = a + (g + 1) w / (P + 1) of its interval; the counts
+  // are nondecreasing in x, so the group's ballot bits read 0..01..1 and the first set bit g
+  // brackets the eigenvalue in [x_(g-1), x_g] (no bit: [x_(P-1), b]). The interval shrinks by
+  // P + 1 per step: ~32 steps for P = 2, ~22 for P = 4, ~16 for P = 8.
   const double tn = fmax(fabs(s_lo), fabs(s_hi));
   const double tol = 8.9e-16 * tn;
-  const int ei = tid >> 1, h = tid & 1;
+  const int P = n <= TE_THREADS / 8 ? 8 : (n <= TE_THREADS / 4 ? 4 : 2);
+  const int ei = tid / P, h = tid % P;
   const int target = n - 1 - ei;           // i-th largest = (n-1-i)-th smallest
+  const double frac = 1.0 / double(P + 1);
   bool done = ei >= n;
   double a = s_lo, b = s_hi;
-  for (int it = 0; it < 200; ++it) {       // width / 3 per step: ~32 steps
+  for (int it = 0; it < 200; ++it) {
     if (__all_sync(FULL, done)) break;
-    double x0 = 0.0, x1 = 0.0;
     bool below = false;
+    const double w = b - a;
     if (!done) {
-      const double w = b - a;
-      x0 = a + w * (1.0 / 3.0);
-      x1 = a + w * (2.0 / 3.0);
-      if (w <= tol || !(a < x0 && x0 < x1 && x1 < b)) done = true;   // converged / no progress
-      else below = sturm_below(d, e2, n, h ? x1 : x0) > target;
+      const double xl = a + w * frac, xh = a + w * (double(P) * frac);
+      if (w <= tol || !(a < xl && xl < xh && xh < b)) done = true;   // converged / no progress
+      else below = sturm_below(d, e2, n, a + w * (double(h + 1) * frac)) > target;
     }
-    const bool other = __shfl_xor_sync(FULL, below, 1);
+    const unsigned bal = __ballot_sync(FULL, below);
     if (!done) {
-      const bool r0 = h ? other : below, r1 = h ? below : other;
-      if (r0) b = x0;
-      else if (r1) { a = x0; b = x1; }
-      else a = x1;
+      const unsigned bits = (bal >> (lane - h)) & ((1u << P) - 1u);
+      if (bits == 0) {
+        a = a + w * (double(P) * frac);
+      } else {
+        const int g = __ffs(bits) - 1;
+        const double xg = a + w * (double(g + 1) * frac);
+        if (g > 0) a = a + w * (double(g) * frac);
+        b = xg;
+      }
     }
   }
   if (h == 0 && ei < n) base[tk.w_off + ei] = 0.5 * (a + b);
