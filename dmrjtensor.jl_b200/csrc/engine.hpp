@@ -116,11 +116,22 @@ struct GemmList {
   size_t t_off = 0, s_off = 0;  // byte offsets inside the uploaded slot
   int bm = GEMM_BM;              // tile rows the tile counts refer to
   int bn = GEMM_BN;              // tile columns the tile counts refer to
-  void clear() { tasks.clear(); segs.clear(); tiles = 0; flops = 0; }
+  // image plan of the image-fed split form (lists retiled to TF32_TILE_N_PRESPLIT or
+  // TF32_TILE_N_WIDE): the distinct A and B operand windows as panels, and the image chunks of
+  // every segment
+  std::vector<ImgPanel> pa, pb;
+  std::vector<SegImg> si;
+  int64_t img_a = 0, img_b = 0;  // image chunks of A and of B
+  size_t pa_off = 0, pb_off = 0, si_off = 0;
+  void clear() {
+    tasks.clear(); segs.clear(); pa.clear(); pb.clear(); si.clear();
+    tiles = 0; flops = 0; img_a = img_b = 0;
+  }
   void add(int64_t c_off, int ldc, int M, int N, double alpha, double beta);
   void seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K);
 };
-// The same products tiled for the split-precision kernel (TF32_TILE_M x bn tiles).
+// The same products tiled for the split-precision kernel (TF32_TILE_M x bn tiles); with
+// bn = TF32_TILE_N_PRESPLIT or TF32_TILE_N_WIDE also the image plan.
 GemmList retile(const GemmList& g, int bm, int bn);
 
 struct MixList {
@@ -263,7 +274,15 @@ struct Upload {
     if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
     return off;
   }
-  void put(GemmList& g) { g.t_off = put(g.tasks); g.s_off = put(g.segs); }
+  void put(GemmList& g) {
+    g.t_off = put(g.tasks);
+    g.s_off = put(g.segs);
+    if (!g.si.empty()) {
+      g.pa_off = put(g.pa);
+      g.pb_off = put(g.pb);
+      g.si_off = put(g.si);
+    }
+  }
   void put(MixList& m) { m.t_off = put(m.tasks); m.m_off = put(m.terms); }
   void put(CopyList& c) { c.t_off = put(c.tasks); }
   char* send(dmrg_ctx* c, int slot);   // returns the device base of the copied bytes
@@ -283,9 +302,13 @@ void tune_gemm(dmrg_ctx* c, GemmList& g);
 // Folds the timings of completed trial launches into the tuner (no synchronisation).
 void tuner_collect(dmrg_ctx* c);
 // The same list on a split-precision tcgen05 kernel (form SPLIT_TF32X3 or SPLIT_BF16X9); the list
-// must be retiled. Lists of at least SPLIT_PRESPLIT_FLOPS convert their operands once into split
-// records first.
+// must be retiled. Lists of at least SPLIT_PRESPLIT_FLOPS take the image-fed form: their operand
+// windows are converted once into chunk images first.
 constexpr double SPLIT_PRESPLIT_FLOPS = 1e9;
+// Tile width of a list's split form: TF32_TILE_N_DIRECT below SPLIT_PRESPLIT_FLOPS, else the
+// image-fed width (TF32_TILE_N_PRESPLIT or TF32_TILE_N_WIDE) whose schedule the cost model
+// finishes first.
+int split_tile_n(const GemmList& g);
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
                     const double* B, int64_t nB, double* C, int64_t nC, int form);
 // The split form of a precision (0 for DMRG_PREC_FP64).

@@ -142,12 +142,8 @@ void check_mma_status(dmrg_ctx* c) {
 }
 
 void prepare_split(HeffPlan& hp) {
-  // large lists take the pre-split form with 128-column tiles, small ones the direct form
-  auto bn = [](const GemmList& g) {
-    return g.flops >= SPLIT_PRESPLIT_FLOPS ? TF32_TILE_N_PRESPLIT : TF32_TILE_N_DIRECT;
-  };
-  hp.g1t = retile(hp.g1, TF32_TILE_M, bn(hp.g1));
-  hp.g3t = retile(hp.g3, TF32_TILE_M, bn(hp.g3));
+  hp.g1t = retile(hp.g1, TF32_TILE_M, split_tile_n(hp.g1));
+  hp.g3t = retile(hp.g3, TF32_TILE_M, split_tile_n(hp.g3));
   hp.split = true;
 }
 
@@ -398,12 +394,6 @@ void plan_right_step(const Bond& Bl, const Bond& Br, const MPOSite& ms, const Si
         g3.seg(lay.goff[kb], Bl.dim[kb], t2off[ka * wl + w], lay.gcols[kb], lay.gcols[kb]);
     }
 }
-
-namespace {
-int split_tile_n(const GemmList& g) {
-  return g.flops >= SPLIT_PRESPLIT_FLOPS ? TF32_TILE_N_PRESPLIT : TF32_TILE_N_DIRECT;
-}
-}  // namespace
 
 void put_step(Upload& u, StepPlan& sp, int split) {
   u.put(sp.g1);

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <tuple>
 
 #include "engine.hpp"
 
@@ -236,6 +237,54 @@ void GemmList::add(int64_t c_off, int ldc, int M, int N, double alpha, double be
   tasks.push_back(t);
 }
 
+// The image plan of a list retiled to TF32_TILE_M x g.bn (image-fed form): one panel per
+// distinct operand window (offset, leading dimension, rows, K), its chunk images after those of
+// the panels before it; A row tiles of SPLIT_IMG_ROWS rows, B row tiles of g.bn rows.
+static void plan_images(GemmList& g) {
+  using Key = std::tuple<int64_t, int, int, int>;
+  std::map<Key, int> ia, ib;
+  g.pa.clear();
+  g.pb.clear();
+  g.si.assign(g.segs.size(), SegImg{});
+  g.img_a = g.img_b = 0;
+  auto panel = [](std::map<Key, int>& idx, std::vector<ImgPanel>& ps, int64_t& total,
+                  int64_t off, int ld, int rows, int K, int kcontig, int tile_rows) {
+    const Key k{off, ld, rows, K};
+    auto it = idx.find(k);
+    if (it == idx.end()) {
+      ImgPanel p{};
+      p.off = off;
+      p.ld = ld;
+      p.rows = rows;
+      p.K = K;
+      p.kcontig = kcontig;
+      p.kchunks = (K + SPLIT_IMG_K - 1) / SPLIT_IMG_K;
+      p.img0 = total;
+      total += int64_t((rows + tile_rows - 1) / tile_rows) * p.kchunks;
+      it = idx.emplace(k, int(ps.size())).first;
+      ps.push_back(p);
+    }
+    return ps[it->second];
+  };
+  for (const GemmTask& t : g.tasks) {
+    if (t.M <= 0 || t.N <= 0) continue;
+    for (int q = 0; q < t.nseg; ++q) {
+      const GemmSeg& s = g.segs[t.seg0 + q];
+      if (s.K <= 0) continue;
+      SegImg& m = g.si[t.seg0 + q];
+      // op(A) is M x K: K contiguous when A is stored transposed; op(B) is K x N, read as the
+      // N x K window of B^T: K contiguous when B is stored untransposed
+      const ImgPanel a =
+          panel(ia, g.pa, g.img_a, s.a_off, s.lda, t.M, s.K, g.tA ? 1 : 0, SPLIT_IMG_ROWS);
+      const ImgPanel b = panel(ib, g.pb, g.img_b, s.b_off, s.ldb, t.N, s.K, g.tB ? 0 : 1, g.bn);
+      m.a_img = a.img0;
+      m.a_kchunks = a.kchunks;
+      m.b_img = b.img0;
+      m.b_kchunks = b.kchunks;
+    }
+  }
+}
+
 GemmList retile(const GemmList& g, int bm, int bn) {
   GemmList r;
   r.tA = g.tA;
@@ -251,7 +300,48 @@ GemmList retile(const GemmList& g, int bm, int bn) {
     t.tile0 = r.tiles;
     r.tiles += t.tiles_m * ((t.N + bn - 1) / bn);
   }
+  if (bm == TF32_TILE_M && (bn == TF32_TILE_N_PRESPLIT || bn == TF32_TILE_N_WIDE)) plan_images(r);
   return r;
+}
+
+// A 256-column tile runs its MMAs at about this many times the rate of a 128-column one: per
+// TF32 product it reads 12 KB of operands from shared memory in 128 cycles against 8 KB in 64.
+constexpr double WIDE_TILE_RATE = 1.3;
+
+int split_tile_n(const GemmList& g) {
+  if (g.flops < SPLIT_PRESPLIT_FLOPS) return TF32_TILE_N_DIRECT;
+  // the image-fed kernel runs one CTA per SM and hands out tiles round-robin: the makespan of
+  // each width is the largest CTA load (tile work = columns x K chunks) over its rate
+  const int P = std::max(device_sm_count(), 1);
+  double best = 0;
+  int pick = TF32_TILE_N_PRESPLIT;
+  for (int bn : {TF32_TILE_N_PRESPLIT, TF32_TILE_N_WIDE}) {
+    int64_t ntiles = 0;
+    for (const GemmTask& t : g.tasks)
+      if (t.M > 0 && t.N > 0)
+        ntiles += int64_t((t.M + TF32_TILE_M - 1) / TF32_TILE_M) * ((t.N + bn - 1) / bn);
+    const int grid = int(std::min<int64_t>(ntiles, P));
+    if (grid == 0) return TF32_TILE_N_PRESPLIT;
+    std::vector<double> load(grid, 0.0);
+    int64_t tile = 0;
+    for (const GemmTask& t : g.tasks) {
+      if (t.M <= 0 || t.N <= 0) continue;
+      double kch = 0;
+      for (int q = 0; q < t.nseg; ++q) {
+        const int K = g.segs[t.seg0 + q].K;
+        if (K > 0) kch += (K + SPLIT_IMG_K - 1) / SPLIT_IMG_K;
+      }
+      const int64_t n = int64_t((t.M + TF32_TILE_M - 1) / TF32_TILE_M) * ((t.N + bn - 1) / bn);
+      for (int64_t i = 0; i < n; ++i, ++tile) load[tile % grid] += bn * kch;
+    }
+    const double span = *std::max_element(load.begin(), load.end()) /
+                        (bn == TF32_TILE_N_WIDE ? WIDE_TILE_RATE : 1.0);
+    if (bn == TF32_TILE_N_PRESPLIT || span < best) {
+      best = span;
+      pick = bn;
+    }
+  }
+  return pick;
 }
 
 void GemmList::seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K) {
@@ -470,9 +560,9 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
                     const double* B, int64_t nB, double* C, int64_t nC, int form) {
   if (form != SPLIT_TF32X3 && form != SPLIT_BF16X9) bad_plan("split gemm form");
   if (g.tiles == 0) return;
-  if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_PRESPLIT))
+  if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_PRESPLIT &&
+                              g.bn != TF32_TILE_N_WIDE))
     bad_plan("split gemm tiling");
-  int64_t extA = 0, extB = 0;   // elements of A and B the tasks touch: [0, ext)
   for (const GemmTask& t : g.tasks) {
     if (t.M <= 0 || t.N <= 0) continue;
     if (t.ldc < t.M || !in_range(t.c_off, (t.M - 1) + int64_t(t.N - 1) * t.ldc, nC)) bad_plan("gemm C");
@@ -482,22 +572,57 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
       const int64_t eb = g.tB ? (t.N - 1) + int64_t(s.K - 1) * s.ldb : (s.K - 1) + int64_t(t.N - 1) * s.ldb;
       if (s.lda < (g.tA ? s.K : t.M) || !in_range(s.a_off, ea, nA)) bad_plan("gemm A");
       if (s.ldb < (g.tB ? t.N : s.K) || !in_range(s.b_off, eb, nB)) bad_plan("gemm B");
-      extA = std::max(extA, s.a_off + ea + 1);
-      extB = std::max(extB, s.b_off + eb + 1);
     }
   }
   const GemmTask* tasks = reinterpret_cast<const GemmTask*>(dbase + g.t_off);
   const GemmSeg* segs = reinterpret_cast<const GemmSeg*>(dbase + g.s_off);
-  if (g.bn == TF32_TILE_N_PRESPLIT) {   // retiled for the pre-split form (large lists)
-    // convert each operand element once instead of once per tile that reads it
-    ensure(c, c->SA, std::max<int64_t>(extA, 1));
-    ensure(c, c->SB, std::max<int64_t>(extB, 1));
-    uint2* pa = reinterpret_cast<uint2*>(c->SA.p);
-    uint2* pb = reinterpret_cast<uint2*>(c->SB.p);
-    launch_presplit(form, c->stream, A, pa, extA);
-    launch_presplit(form, c->stream, B, pb, extB);
-    launch_gemm_split_presplit(form, c->stream, g.tA, g.tB, pa, pb, C, tasks, int(g.tasks.size()),
-                               segs, g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
+  if (g.bn != TF32_TILE_N_DIRECT) {   // image-fed form (large lists)
+    // every chunk a segment's tiles copy lies inside the images, and every panel the pack pass
+    // reads lies inside its operand
+    if (g.si.size() != g.segs.size()) bad_plan("split gemm images");
+    for (const GemmTask& t : g.tasks) {
+      if (t.M <= 0 || t.N <= 0) continue;
+      const int64_t tiles_n = (t.N + g.bn - 1) / g.bn;
+      for (int q = 0; q < t.nseg; ++q) {
+        const GemmSeg& s = g.segs[t.seg0 + q];
+        if (s.K <= 0) continue;
+        const SegImg& m = g.si[t.seg0 + q];
+        const int kch = (s.K + SPLIT_IMG_K - 1) / SPLIT_IMG_K;
+        if (m.a_kchunks != kch || m.b_kchunks != kch || m.a_img < 0 || m.b_img < 0 ||
+            m.a_img + int64_t(t.tiles_m) * kch > g.img_a || m.b_img + tiles_n * kch > g.img_b)
+          bad_plan("split gemm images");
+      }
+    }
+    auto check_panels = [](const std::vector<ImgPanel>& ps, int64_t total, int64_t n,
+                           int tile_rows) {
+      int64_t next = 0;
+      for (const ImgPanel& p : ps) {
+        if (p.rows <= 0 || p.K <= 0 || p.img0 != next ||
+            p.kchunks != (p.K + SPLIT_IMG_K - 1) / SPLIT_IMG_K)
+          bad_plan("split gemm panels");
+        const int64_t last = p.kcontig ? (p.K - 1) + int64_t(p.rows - 1) * p.ld
+                                       : (p.rows - 1) + int64_t(p.K - 1) * p.ld;
+        if (p.ld < (p.kcontig ? p.K : p.rows) || !in_range(p.off, last, n))
+          bad_plan("split gemm panels");
+        next += int64_t((p.rows + tile_rows - 1) / tile_rows) * p.kchunks;
+      }
+      if (next != total) bad_plan("split gemm panels");
+    };
+    check_panels(g.pa, g.img_a, nA, SPLIT_IMG_ROWS);
+    check_panels(g.pb, g.img_b, nB, g.bn);
+    const int64_t cba = split_image_chunk_bytes(form, SPLIT_IMG_ROWS);
+    const int64_t cbb = split_image_chunk_bytes(form, g.bn);
+    ensure(c, c->SA, std::max<int64_t>((g.img_a * cba + 7) / 8, 1));
+    ensure(c, c->SB, std::max<int64_t>((g.img_b * cbb + 7) / 8, 1));
+    unsigned char* ia = reinterpret_cast<unsigned char*>(c->SA.p);
+    unsigned char* ib = reinterpret_cast<unsigned char*>(c->SB.p);
+    launch_pack_images(form, c->stream, A, ia, reinterpret_cast<const ImgPanel*>(dbase + g.pa_off),
+                       int(g.pa.size()), g.img_a, SPLIT_IMG_ROWS);
+    launch_pack_images(form, c->stream, B, ib, reinterpret_cast<const ImgPanel*>(dbase + g.pb_off),
+                       int(g.pb.size()), g.img_b, g.bn);
+    launch_gemm_split_images(form, g.bn, c->stream, ia, ib, C, tasks, int(g.tasks.size()), segs,
+                             reinterpret_cast<const SegImg*>(dbase + g.si_off), g.tiles, c->nsm,
+                             c->d_status + STATUS_MMA);
     return;
   }
   launch_gemm_split(form, c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs,

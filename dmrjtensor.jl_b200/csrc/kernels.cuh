@@ -108,18 +108,36 @@ void launch_gemm_f64(cudaStream_t s, int tile, bool transA, bool transB, const d
 // products; err[0] is set when an MMA completion wait gave up.
 constexpr int SPLIT_TF32X3 = 1, SPLIT_BF16X9 = 2;
 constexpr int TF32_TILE_M = 128;
-constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_PRESPLIT = 128;
+constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_PRESPLIT = 128, TF32_TILE_N_WIDE = 256;
 void launch_gemm_split(int form, cudaStream_t s, bool transA, bool transB, const double* A,
                        const double* B, double* C, const GemmTask* tasks, int ntasks,
                        const GemmSeg* segs, int total_tiles, int grid_cap, int* err);
-// The same GEMM on pre-split operands: A and B hold 8-byte records of the split parts at the
-// element offsets the tasks address (launch_presplit writes them from FP64; bit-identical
-// results).
-void launch_presplit(int form, cudaStream_t s, const double* x, uint2* recs, int64_t n);
-void launch_gemm_split_presplit(int form, cudaStream_t s, bool transA, bool transB,
-                                const uint2* A, const uint2* B, double* C, const GemmTask* tasks,
-                                int ntasks, const GemmSeg* segs, int total_tiles, int grid_cap,
-                                int* err);
+// Image-fed form for large lists (tiles TF32_TILE_M x bn, bn = TF32_TILE_N_PRESPLIT or
+// TF32_TILE_N_WIDE). Every distinct operand window of the list (an ImgPanel: element (r, k) at
+// off + r + k*ld, or off + k + r*ld when kcontig) is converted once into chunk images: row tiles
+// (SPLIT_IMG_ROWS rows for A, bn rows for B) x K chunks of SPLIT_IMG_K, each chunk the split
+// planes of the tile in the MMA's shared-memory layout, zero outside the window. Chunk (rt, kc)
+// of a panel is image chunk img0 + rt * kchunks + kc. The GEMM then moves whole chunks with bulk
+// copies; a segment finds its chunks through its SegImg.
+constexpr int SPLIT_IMG_ROWS = 128, SPLIT_IMG_K = 32;
+struct ImgPanel {
+  int64_t off, img0;
+  int ld, rows, K, kcontig;
+  int kchunks, pad;
+};
+struct SegImg {
+  int64_t a_img, b_img;      // first image chunk of the segment's A and B panels
+  int a_kchunks, b_kchunks;  // chunks per row tile of those panels
+};
+// bytes of one chunk image with `rows` rows (SPLIT_IMG_ROWS or TF32_TILE_N_WIDE)
+int64_t split_image_chunk_bytes(int form, int rows);
+// writes the chunk images (`rows` rows each) of panels[0, npanels) (total_chunks in all) from x
+void launch_pack_images(int form, cudaStream_t s, const double* x, unsigned char* img,
+                        const ImgPanel* panels, int npanels, int64_t total_chunks, int rows);
+void launch_gemm_split_images(int form, int bn, cudaStream_t s, const unsigned char* imgA,
+                              const unsigned char* imgB, double* C, const GemmTask* tasks,
+                              int ntasks, const GemmSeg* segs, const SegImg* simg,
+                              int total_tiles, int grid_cap, int* err);
 // slot of the context's status words that the split-precision GEMM sets on a timeout
 constexpr int STATUS_MMA = 8;
 

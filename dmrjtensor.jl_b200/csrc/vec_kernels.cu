@@ -9,6 +9,8 @@ namespace dmrg {
 namespace {
 
 constexpr int MIX_COLS = 32;      // columns per mixing / copy tile
+constexpr int MIX_TALL = 64;      // mixing blocks of at least this many rows: a warp per column
+constexpr int MIX_ROWS_PER_LANE = 4;
 constexpr int RED_BLOCKS = 296;   // 2 x 148 SMs
 constexpr int RED_THREADS = 256;
 constexpr int MAXK = 16;
@@ -63,6 +65,38 @@ __global__ void k_mix(const double* __restrict__ in, double* __restrict__ out,
     const MixTask tk = tasks[lo];
     const int c0 = (tile - tk.tile0) * MIX_COLS;
     const int ncol = min(MIX_COLS, tk.cols - c0);
+    if (tk.rows >= MIX_TALL) {
+      // tall blocks: a warp per column, MIX_ROWS_PER_LANE rows per lane (rows lane + 32 j of a
+      // 128-row slab), so that every thread has that many independent loads of a term in flight
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+      for (int cc = warp; cc < ncol; cc += nwarp) {
+        const int64_t c = c0 + cc;
+        for (int r0 = 0; r0 < tk.rows; r0 += 32 * MIX_ROWS_PER_LANE) {
+          double acc[MIX_ROWS_PER_LANE];
+#pragma unroll
+          for (int j = 0; j < MIX_ROWS_PER_LANE; ++j) acc[j] = 0.0;
+#pragma unroll 2
+          for (int q = 0; q < tk.nterm; ++q) {
+            const MixTerm tm = terms[tk.term0 + q];
+            const double* src = in + tm.in_off + c * tm.ld;
+            double v[MIX_ROWS_PER_LANE];
+#pragma unroll
+            for (int j = 0; j < MIX_ROWS_PER_LANE; ++j) {
+              const int r = r0 + lane + 32 * j;
+              v[j] = r < tk.rows ? src[r] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < MIX_ROWS_PER_LANE; ++j) acc[j] += tm.coef * v[j];
+          }
+#pragma unroll
+          for (int j = 0; j < MIX_ROWS_PER_LANE; ++j) {
+            const int r = r0 + lane + 32 * j;
+            if (r < tk.rows) out[tk.out_off + r + c * tk.ld] = acc[j];
+          }
+        }
+      }
+      continue;
+    }
     const int nel = ncol * tk.rows;
     for (int e = threadIdx.x; e < nel; e += blockDim.x) {
       const int r = e % tk.rows, c = c0 + e / tk.rows;
