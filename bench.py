@@ -537,10 +537,13 @@ def tf32_gemm_peak(device):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
+def heff_forms(pkg, ctx, m=1024, L=22, reps=5, tf32_peak=None, bf16_peak=None):
     """Heff at the dense-equivalent size of the headline workload at maxm 1024 (dense random MPS,
     bond dimension 1024 either side of the centre bond): device time per application in the plain
-    FP64 form and the 3xTF32 tensor-core form, algorithmic TFLOP/s of each."""
+    FP64 form and the 3xTF32 / BF16x9 tensor-core forms, algorithmic TFLOP/s of each, and each
+    split form's fraction of its algorithmic ceiling (TF32 peak / 3, BF16 peak / 9). The timed
+    applications follow a warm-up one with the same plan, as the Lanczos iterations of a bond step
+    follow its first: the environments' chunk images are packed by the warm-up and reused."""
     import ctypes as C
     lib = pkg.lib()
     mpo = pkg.makeMPO(pkg.heisenbergMPO, 2, L)
@@ -558,6 +561,10 @@ def heff_forms(pkg, ctx, m=1024, L=22, reps=5):
         out[name] = {"seconds": sec.value, "tflops": fl.value / sec.value / 1e12}
     out["speedup_3xtf32"] = out["fp64"]["seconds"] / out["3xtf32"]["seconds"]
     out["speedup_bf16x9"] = out["fp64"]["seconds"] / out["bf16x9"]["seconds"]
+    for name, peak, k in (("3xtf32", tf32_peak, 3), ("bf16x9", bf16_peak, 9)):
+        if peak:
+            out[name]["ceiling_tflops"] = peak / k
+            out[name]["frac_of_ceiling"] = out[name]["tflops"] / (peak / k)
     return out
 
 
@@ -853,13 +860,14 @@ def run_ours(args, world, rank, local, dist):
                                                              saturate=True, batched=False),
                    "capacity_3xtf32": run_serving(pkg, local, args.serve_saturate, saturate=True,
                                                   precision="3xtf32")}
-    heff_large = heff_forms(pkg, ctx) if args.chosen else None
     methods = method_legs(pkg, ctx, dev, args) if args.methods else None
     if rank != 0:
         return
     peak = fp64_gemm_peak(local)
     tf32_peak = tf32_gemm_peak(local)
     bf16_peak = measured_bf16_peak()
+    heff_large = (heff_forms(pkg, ctx, tf32_peak=tf32_peak, bf16_peak=bf16_peak)
+                  if args.chosen else None)
     configs = {}
     if args.configs:
         with tempfile.TemporaryDirectory() as td:
@@ -975,7 +983,9 @@ def main():
         elif args.heff_only:
             # the plain and split Heff forms alone (the kernel-profiling case)
             pkg = load_pkg()
-            print(json.dumps({"heff_forms_m1024": heff_forms(pkg, pkg.Context(local))}))
+            print(json.dumps({"heff_forms_m1024": heff_forms(
+                pkg, pkg.Context(local), tf32_peak=tf32_gemm_peak(local),
+                bf16_peak=measured_bf16_peak())}))
         else:
             run_ours(args, world, rank, local, dist)
     finally:

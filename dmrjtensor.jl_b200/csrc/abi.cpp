@@ -864,8 +864,13 @@ int dmrg_test_heff_time(dmrg_state* st, const dmrg_mpo* mpo, int iL, int precisi
     const int64_t n = std::max<int64_t>(hp.tl.size, 1);
     ensure(c, c->K, n);
     ensure(c, c->H, n);
-    cuda_check(cudaMemsetAsync(c->K.p, 0, size_t(n) * sizeof(double), c->stream), "vector");
-    apply_heff(st, iL, hp, c->K.p, c->H.p, precision);   // warm-up
+    // a fixed non-zero vector (zero operands would run the tensor pipe at lower power)
+    std::vector<double> v(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) v[size_t(i)] = std::sin(0.37 * double(i) + 0.1);
+    cuda_check(cudaMemcpyAsync(c->K.p, v.data(), size_t(n) * sizeof(double),
+                               cudaMemcpyHostToDevice, c->stream), "vector");
+    cuda_check(cudaStreamSynchronize(c->stream), "vector");
+    apply_heff(st, iL, hp, c->K.p, c->H.p, precision);   // warm-up (packs the environments)
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "event");
     cuda_check(cudaEventCreate(&e1), "event");

@@ -210,7 +210,9 @@ struct dmrg_ctx {
   double* d_floors = nullptr;    // block-Jacobi per-group thresholds
   // growable scratch buffers
   dmrg::DBuf X, Y, K, H, M, R, W, T1, T2;
-  dmrg::DBuf SA, SB;             // pre-split (hi, lo) operand pairs of the split GEMM (8 B each)
+  dmrg::DBuf SA, SB;             // chunk images of the split GEMM's operands (scratch)
+  dmrg::DBuf SL, SR;             // chunk images of the Heff's environments (one plan at a time)
+  uint64_t sl_key = 0, sr_key = 0;   // which plan and form SL / SR hold (0: none)
   std::map<void*, size_t> sizes;
 };
 
@@ -309,8 +311,22 @@ constexpr double SPLIT_PRESPLIT_FLOPS = 1e9;
 // image-fed width (TF32_TILE_N_PRESPLIT or TF32_TILE_N_WIDE) whose schedule the cost model
 // finishes first.
 int split_tile_n(const GemmList& g);
+// Options of the image-fed form: an operand's images in a persistent buffer, packed only when
+// *key differs from want (an environment, fixed over the applications of one Heff plan); and A
+// given as the MPO mixing's input (the plan's fused covers) instead of the mixed blocks.
+struct HeffPlan;
+struct ImgCache {
+  DBuf* buf = nullptr;
+  uint64_t* key = nullptr;
+  uint64_t want = 0;
+};
+struct SplitOpts {
+  ImgCache a, b;
+  const HeffPlan* fuse = nullptr;
+};
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
-                    const double* B, int64_t nB, double* C, int64_t nC, int form);
+                    const double* B, int64_t nB, double* C, int64_t nC, int form,
+                    const SplitOpts* opts = nullptr);
 // The split form of a precision (0 for DMRG_PREC_FP64).
 inline int split_form(int precision) {
   return precision == DMRG_PREC_3XTF32 ? SPLIT_TF32X3
@@ -338,11 +354,18 @@ struct GemmProfile {
 // ---- contractions (engine_contract.cpp)
 struct HeffPlan {
   int le = 0, re = 0;            // the environments it reads: Lenv[le], Renv[re]
+  uint64_t gen = 0;              // unique per plan (keys the environment images of the split form)
   TwoLayout tl;
   GemmList g1, g3;
   GemmList g1t, g3t;             // retiled copies for the split-precision kernel (when used)
   bool split = false;
   MixList mix;
+  // split form with g3t image-fed: the mixing fused into the pack of g3t's A panels (per panel
+  // its covers' range; the covers' terms are mix.terms)
+  bool fused = false;
+  std::vector<int2> fuse_range;
+  std::vector<MixCover> fuse_cover;
+  size_t fr_off = 0, fc_off = 0;
   int64_t x_size = 0, y_size = 0;
   double flops = 0;
   char* dbase = nullptr;
@@ -358,9 +381,13 @@ void plan_heff_bond(const dmrg_state* st, int le, int re, const Bond& Bl, const 
 // launches with a second site of dimension one (charge zero), reading Lenv[i] and Renv[i]; its
 // vector layout is the site layout of A[i].
 void plan_heff1(const dmrg_state* st, int i, HeffPlan& hp);
-// Uploads the Heff task lists; with precision DMRG_PREC_3XTF32 also the retiled copies.
+// Uploads the Heff task lists (tuning the FP64 lists first); with a split precision also the
+// retiled copies.
 void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision = DMRG_PREC_FP64);
-// Adds the retiled split-precision lists to a plan (before its upload).
+// Adds the Heff lists to an upload (the split lists and the fused mixing's covers when prepared).
+void put_heff(Upload& u, HeffPlan& hp);
+// Adds the retiled split-precision lists to a plan (before its upload), and the fused mixing's
+// covers when the second GEMM is image-fed.
 void prepare_split(HeffPlan& hp);
 // y = Heff x for vectors in the tl layout (device pointers); reads Lenv[hp.le] and Renv[hp.re].
 // Fails (DMRG_ERR_TIMEOUT) if a split-precision GEMM reported an MMA wait that gave up since the

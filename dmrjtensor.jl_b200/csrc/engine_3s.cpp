@@ -86,19 +86,7 @@ void single_site_step(dmrg_state* st, const dmrg_params& P, const SiteMode& md, 
   int tv = tm.begin();
   HeffPlan hp;
   plan_heff1(st, i, hp);
-  const bool split = split_form(P.precision) != 0;
-  if (split) prepare_split(hp);
-  tune_gemm(c, hp.g1);
-  tune_gemm(c, hp.g3);
-  Upload u;
-  u.put(hp.g1);
-  u.put(hp.mix);
-  u.put(hp.g3);
-  if (hp.split) {
-    u.put(hp.g1t);
-    u.put(hp.g3t);
-  }
-  hp.dbase = u.send(c, 0);
+  upload_heff(c, hp, 0, P.precision);
   const int64_t n = lay.size;
   const int kdim = std::max(2, std::min(P.krylov, 16));
   ensure(c, c->K, std::max<int64_t>(int64_t(kdim) * n, 1));
@@ -402,18 +390,7 @@ void single_site_step(dmrg_state* st, const dmrg_params& P, const SiteMode& md, 
     const int le = j > 0 ? i + 1 : i, re = j > 0 ? i : i - 1;
     plan_heff_bond(st, le, re, j > 0 ? C : Bold, j > 0 ? Bold : C, hz);
     if (hz.tl.size != vtot) fail(DMRG_ERR_ARG, "internal plan check failed: TDVP bond matrix");
-    if (split_form(P.precision)) prepare_split(hz);
-    tune_gemm(c, hz.g1);
-    tune_gemm(c, hz.g3);
-    Upload uz;
-    uz.put(hz.g1);
-    uz.put(hz.mix);
-    uz.put(hz.g3);
-    if (hz.split) {
-      uz.put(hz.g1t);
-      uz.put(hz.g3t);
-    }
-    hz.dbase = uz.send(c, 0);
+    upload_heff(c, hz, 0, P.precision);
     ensure(c, c->H, std::max<int64_t>(vtot, 1));
     krylov_solve(st, P, hz, vtot, false, false, tm, so, md.tau, true);
     bm = c->H.p;

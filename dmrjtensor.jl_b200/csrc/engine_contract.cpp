@@ -6,6 +6,7 @@
 //   3. psi'_(ka,t1,t2) = Y * R_ka'   one GEMM per output block, K = the stacked (d, w'') rows
 // Lupdate / Rupdate (lib/MPO_MPS/Lupdate.jl:17-26, Rupdate.jl:17-26) in the same three shapes.
 #include <algorithm>
+#include <atomic>
 #include <map>
 
 #include "engine.hpp"
@@ -128,6 +129,9 @@ void plan_heff_core(const Bond& Bl, const Bond& Br, const std::vector<QN>& p1,
           hp.g3.seg(yoff[id], Bl.dim[ka], RL.goff[kap], RL.rows[kap], RL.rows[kap]);
       }
   hp.flops = hp.g1.flops + hp.g3.flops + hp.mix.flops;
+  static std::atomic<uint64_t> next_gen{1};
+  hp.gen = next_gen.fetch_add(1);
+  hp.split = hp.fused = false;
 }
 }  // namespace
 
@@ -141,10 +145,44 @@ void check_mma_status(dmrg_ctx* c) {
   }
 }
 
+// The mixing fused into the image pack of g3t's A panels (windows of the mixed blocks Y): each
+// panel gets the mixing tasks that write its columns, in column order. False when g3t is not
+// image-fed or some panel is not tiled exactly by them; the plan then keeps the mixing launch.
+static bool plan_fusion(HeffPlan& hp) {
+  const GemmList& g = hp.g3t;
+  hp.fuse_range.assign(g.pa.size(), make_int2(0, 0));
+  hp.fuse_cover.clear();
+  if (g.bn == TF32_TILE_N_DIRECT || g.pa.empty()) return false;
+  std::vector<std::pair<int64_t, int>> outs;   // (out_off, mixing task), written tasks only
+  for (int i = 0; i < int(hp.mix.tasks.size()); ++i)
+    if (hp.mix.tasks[i].rows > 0 && hp.mix.tasks[i].cols > 0)
+      outs.emplace_back(hp.mix.tasks[i].out_off, i);
+  std::sort(outs.begin(), outs.end());
+  for (size_t pi = 0; pi < g.pa.size(); ++pi) {
+    const ImgPanel& p = g.pa[pi];
+    if (p.kcontig) return false;
+    const int64_t end = p.off + int64_t(p.ld) * p.K;
+    auto it = std::lower_bound(outs.begin(), outs.end(), std::make_pair(p.off, -1));
+    hp.fuse_range[pi].x = int(hp.fuse_cover.size());
+    int next = 0;
+    for (; it != outs.end() && it->first < end; ++it) {
+      const MixTask& t = hp.mix.tasks[it->second];
+      if (t.ld != p.ld || t.rows != p.rows || (t.out_off - p.off) % p.ld != 0) return false;
+      if ((t.out_off - p.off) / p.ld != next) return false;
+      hp.fuse_cover.push_back(MixCover{next, t.cols, t.term0, t.nterm});
+      next += t.cols;
+    }
+    if (next != p.K) return false;
+    hp.fuse_range[pi].y = int(hp.fuse_cover.size()) - hp.fuse_range[pi].x;
+  }
+  return true;
+}
+
 void prepare_split(HeffPlan& hp) {
   hp.g1t = retile(hp.g1, TF32_TILE_M, split_tile_n(hp.g1));
   hp.g3t = retile(hp.g3, TF32_TILE_M, split_tile_n(hp.g3));
   hp.split = true;
+  hp.fused = plan_fusion(hp);
 }
 
 void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision) {
@@ -152,14 +190,22 @@ void upload_heff(dmrg_ctx* c, HeffPlan& hp, int slot, int precision) {
   tune_gemm(c, hp.g1);
   tune_gemm(c, hp.g3);
   Upload u;
+  put_heff(u, hp);
+  hp.dbase = u.send(c, slot);
+}
+
+void put_heff(Upload& u, HeffPlan& hp) {
   u.put(hp.g1);
   u.put(hp.mix);
   u.put(hp.g3);
   if (hp.split) {
     u.put(hp.g1t);
     u.put(hp.g3t);
+    if (hp.fused) {
+      hp.fr_off = u.put(hp.fuse_range);
+      hp.fc_off = u.put(hp.fuse_cover);
+    }
   }
-  hp.dbase = u.send(c, slot);
 }
 
 void GemmProfile::begin(cudaStream_t s, double fl) {
@@ -203,19 +249,30 @@ void apply_heff(dmrg_state* st, int iL, const HeffPlan& hp, const double* x, dou
   if (split && !hp.split) fail(DMRG_ERR_STATE, "split-precision Heff lists were not uploaded");
   if (precision != DMRG_PREC_FP64 && !split)
     fail(DMRG_ERR_ARG, "precision: FP64, 3xTF32 and BF16x9 are the built forms");
+  // split forms: the environments' images are packed once per plan (the first application)
+  // and kept while this plan's applications follow one another; with the fused form the mixing
+  // happens inside the pack of the second GEMM's operand
+  const uint64_t want = hp.gen * 4 + uint64_t(split);
   if (prof) prof->begin(c->stream, hp.g1.flops);
-  if (split)
+  if (split) {
+    SplitOpts o1;
+    o1.a = ImgCache{&c->SL, &c->sl_key, want};
     run_gemm_split(c, hp.g1t, hp.dbase, st->Lenv[hp.le].p, st->Lenv[hp.le].n, x, n, c->X.p,
-                   c->X.n, split);
-  else
+                   c->X.n, split, &o1);
+  } else {
     run_gemm(c, hp.g1, hp.dbase, st->Lenv[hp.le].p, st->Lenv[hp.le].n, x, n, c->X.p, c->X.n);
+  }
   if (prof) prof->end(c->stream);
-  run_mix(c, hp.mix, hp.dbase, c->X.p, c->X.n, c->Y.p, c->Y.n);
+  const bool fused = split && hp.fused;
+  if (!fused) run_mix(c, hp.mix, hp.dbase, c->X.p, c->X.n, c->Y.p, c->Y.n);
   if (prof) prof->begin(c->stream, hp.g3.flops);
-  if (split)
-    run_gemm_split(c, hp.g3t, hp.dbase, c->Y.p, c->Y.n, st->Renv[hp.re].p, st->Renv[hp.re].n,
-                   y, n, split);
-  else
+  if (split) {
+    SplitOpts o3;
+    o3.b = ImgCache{&c->SR, &c->sr_key, want};
+    o3.fuse = fused ? &hp : nullptr;
+    run_gemm_split(c, hp.g3t, hp.dbase, fused ? c->X.p : c->Y.p, fused ? c->X.n : c->Y.n,
+                   st->Renv[hp.re].p, st->Renv[hp.re].n, y, n, split, &o3);
+  } else
     run_gemm(c, hp.g3, hp.dbase, c->Y.p, c->Y.n, st->Renv[hp.re].p, st->Renv[hp.re].n, y, n);
   if (prof) prof->end(c->stream);
 }

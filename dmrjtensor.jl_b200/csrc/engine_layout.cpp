@@ -557,7 +557,8 @@ void tuner_collect(dmrg_ctx* c) {
 }
 
 void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A, int64_t nA,
-                    const double* B, int64_t nB, double* C, int64_t nC, int form) {
+                    const double* B, int64_t nB, double* C, int64_t nC, int form,
+                    const SplitOpts* opts) {
   if (form != SPLIT_TF32X3 && form != SPLIT_BF16X9) bad_plan("split gemm form");
   if (g.tiles == 0) return;
   if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_PRESPLIT &&
@@ -594,7 +595,7 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
       }
     }
     auto check_panels = [](const std::vector<ImgPanel>& ps, int64_t total, int64_t n,
-                           int tile_rows) {
+                           int tile_rows, bool extent) {
       int64_t next = 0;
       for (const ImgPanel& p : ps) {
         if (p.rows <= 0 || p.K <= 0 || p.img0 != next ||
@@ -602,29 +603,83 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
           bad_plan("split gemm panels");
         const int64_t last = p.kcontig ? (p.K - 1) + int64_t(p.rows - 1) * p.ld
                                        : (p.rows - 1) + int64_t(p.K - 1) * p.ld;
-        if (p.ld < (p.kcontig ? p.K : p.rows) || !in_range(p.off, last, n))
+        if (extent && (p.ld < (p.kcontig ? p.K : p.rows) || !in_range(p.off, last, n)))
           bad_plan("split gemm panels");
         next += int64_t((p.rows + tile_rows - 1) / tile_rows) * p.kchunks;
       }
       if (next != total) bad_plan("split gemm panels");
     };
-    check_panels(g.pa, g.img_a, nA, SPLIT_IMG_ROWS);
-    check_panels(g.pb, g.img_b, nB, g.bn);
+    const HeffPlan* fuse = opts ? opts->fuse : nullptr;
+    if (fuse) {
+      // A is the mixing input: the covers of every A panel tile its columns, and every term a
+      // cover sums reads inside the input
+      const MixList& mx = fuse->mix;
+      if (!fuse->fused || fuse->fuse_range.size() != g.pa.size()) bad_plan("split gemm mixing");
+      for (size_t i = 0; i < g.pa.size(); ++i) {
+        const ImgPanel& p = g.pa[i];
+        const int2 r = fuse->fuse_range[i];
+        if (p.kcontig || r.y < 1 || r.x < 0 || size_t(r.x) + r.y > fuse->fuse_cover.size())
+          bad_plan("split gemm mixing");
+        int next = 0;
+        for (int j = r.x; j < r.x + r.y; ++j) {
+          const MixCover& cv = fuse->fuse_cover[j];
+          if (cv.col0 != next || cv.ncols <= 0 || cv.term0 < 0 || cv.nterm < 0 ||
+              size_t(cv.term0) + cv.nterm > mx.terms.size())
+            bad_plan("split gemm mixing");
+          next += cv.ncols;
+          for (int q = cv.term0; q < cv.term0 + cv.nterm; ++q) {
+            const MixTerm& tm = mx.terms[q];
+            if (tm.ld < p.rows ||
+                !in_range(tm.in_off, (p.rows - 1) + int64_t(cv.ncols - 1) * tm.ld, nA))
+              bad_plan("split gemm mixing");
+          }
+        }
+        if (next != p.K) bad_plan("split gemm mixing");
+      }
+    }
+    check_panels(g.pa, g.img_a, nA, SPLIT_IMG_ROWS, fuse == nullptr);
+    check_panels(g.pb, g.img_b, nB, g.bn, true);
     const int64_t cba = split_image_chunk_bytes(form, SPLIT_IMG_ROWS);
     const int64_t cbb = split_image_chunk_bytes(form, g.bn);
-    ensure(c, c->SA, std::max<int64_t>((g.img_a * cba + 7) / 8, 1));
-    ensure(c, c->SB, std::max<int64_t>((g.img_b * cbb + 7) / 8, 1));
-    unsigned char* ia = reinterpret_cast<unsigned char*>(c->SA.p);
-    unsigned char* ib = reinterpret_cast<unsigned char*>(c->SB.p);
-    launch_pack_images(form, c->stream, A, ia, reinterpret_cast<const ImgPanel*>(dbase + g.pa_off),
-                       int(g.pa.size()), g.img_a, SPLIT_IMG_ROWS);
-    launch_pack_images(form, c->stream, B, ib, reinterpret_cast<const ImgPanel*>(dbase + g.pb_off),
-                       int(g.pb.size()), g.img_b, g.bn);
+    // an operand's images: the scratch buffer, or a cache that is packed when its key differs
+    // (a cache that has to grow loses its contents)
+    auto images = [&](const ImgCache* cache, DBuf& scratch, int64_t bytes, bool& pack) {
+      const int64_t n = std::max<int64_t>((bytes + 7) / 8, 1);
+      pack = true;
+      if (!cache || !cache->buf) {
+        ensure(c, scratch, n);
+        return reinterpret_cast<unsigned char*>(scratch.p);
+      }
+      if (cache->buf->n < n) {
+        *cache->key = 0;
+        ensure(c, *cache->buf, n);
+      }
+      pack = *cache->key != cache->want;
+      *cache->key = cache->want;
+      return reinterpret_cast<unsigned char*>(cache->buf->p);
+    };
+    bool pack_a = true, pack_b = true;
+    unsigned char* ia = images(opts ? &opts->a : nullptr, c->SA, g.img_a * cba, pack_a);
+    unsigned char* ib = images(opts ? &opts->b : nullptr, c->SB, g.img_b * cbb, pack_b);
+    const ImgPanel* pa = reinterpret_cast<const ImgPanel*>(dbase + g.pa_off);
+    if (pack_a && fuse)
+      launch_pack_mix_images(form, c->stream, A, ia, pa,
+                             reinterpret_cast<const int2*>(fuse->dbase + fuse->fr_off),
+                             reinterpret_cast<const MixCover*>(fuse->dbase + fuse->fc_off),
+                             reinterpret_cast<const MixTerm*>(fuse->dbase + fuse->mix.m_off),
+                             int(g.pa.size()), g.img_a, SPLIT_IMG_ROWS);
+    else if (pack_a)
+      launch_pack_images(form, c->stream, A, ia, pa, int(g.pa.size()), g.img_a, SPLIT_IMG_ROWS);
+    if (pack_b)
+      launch_pack_images(form, c->stream, B, ib,
+                         reinterpret_cast<const ImgPanel*>(dbase + g.pb_off), int(g.pb.size()),
+                         g.img_b, g.bn);
     launch_gemm_split_images(form, g.bn, c->stream, ia, ib, C, tasks, int(g.tasks.size()), segs,
                              reinterpret_cast<const SegImg*>(dbase + g.si_off), g.tiles, c->nsm,
                              c->d_status + STATUS_MMA);
     return;
   }
+  if (opts && opts->fuse) bad_plan("split gemm mixing");   // fused mixing needs the image form
   launch_gemm_split(form, c->stream, g.tA, g.tB, A, B, C, tasks, int(g.tasks.size()), segs,
                     g.tiles, c->nsm * 3, c->d_status + STATUS_MMA);
 }

@@ -359,14 +359,8 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   tune_gemm(c, hp.g3);
   tune_gemm(c, gaa);
   Upload u;
-  u.put(hp.g1);
-  u.put(hp.mix);
-  u.put(hp.g3);
+  put_heff(u, hp);
   u.put(gaa);
-  if (hp.split) {
-    u.put(hp.g1t);
-    u.put(hp.g3t);
-  }
   hp.dbase = u.send(c, 0);
   const int64_t n = tl.size;
   const int kdim = std::max(2, std::min(P.krylov, 16));

@@ -32,18 +32,7 @@ void evolve_site(dmrg_state* st, const dmrg_params& P, int i, double tau, Timing
   if (!st->Lvalid[i] || !st->Rvalid[i]) fail(DMRG_ERR_STATE, "environments are not built");
   HeffPlan hp;
   plan_heff1(st, i, hp);
-  if (split_form(P.precision)) prepare_split(hp);
-  tune_gemm(c, hp.g1);
-  tune_gemm(c, hp.g3);
-  Upload u;
-  u.put(hp.g1);
-  u.put(hp.mix);
-  u.put(hp.g3);
-  if (hp.split) {
-    u.put(hp.g1t);
-    u.put(hp.g3t);
-  }
-  hp.dbase = u.send(c, 0);
+  upload_heff(c, hp, 0, P.precision);
   const int64_t n = st->lay[i].size;
   const int kdim = std::max(2, std::min(P.krylov, 16));
   ensure(c, c->K, std::max<int64_t>(int64_t(kdim) * n, 1));

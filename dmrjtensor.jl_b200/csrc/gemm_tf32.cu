@@ -493,6 +493,77 @@ k_pack_images(const double* __restrict__ x, unsigned char* __restrict__ img,
   }
 }
 
+// The pack of an operand that is the MPO mixing of x (see MixCover): the same units as
+// k_pack_images, each element summed over its cover's terms in term order (the sums of the
+// mixing kernel, bit for bit). A unit's QE columns usually share one cover: then the term loop
+// is outside and each term's QE loads go out together.
+template <class F>
+__global__ void __launch_bounds__(PACK_THREADS)
+k_pack_mix_images(const double* __restrict__ x, unsigned char* __restrict__ img,
+                  const ImgPanel* __restrict__ panels, const int2* __restrict__ ranges,
+                  const MixCover* __restrict__ covers, const MixTerm* __restrict__ terms,
+                  int npanels, int64_t total_chunks, int R) {
+  constexpr int QE = F::QE;
+  const int plane = R * IK * F::EB, units = R * (IK / QE);
+  for (int64_t ch = blockIdx.x; ch < total_chunks; ch += gridDim.x) {
+    int lo = 0, hi = npanels - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (panels[mid].img0 <= ch) lo = mid; else hi = mid - 1;
+    }
+    const ImgPanel p = panels[lo];
+    const int2 rg = ranges[lo];
+    const int local = int(ch - p.img0);
+    const int rt = local / p.kchunks, kc = local - (local / p.kchunks) * p.kchunks;
+    unsigned char* dst = img + ch * int64_t(F::PLANES) * plane;
+    for (int u = threadIdx.x; u < units; u += PACK_THREADS) {
+      const int kstep = u / (2 * R), w = u - kstep * (2 * R);
+      const int row = (w >> 4) * 8 + (w & 7), kq = 2 * kstep + ((w >> 3) & 1);
+      const int gr = rt * R + row;
+      const int k0 = kc * IK + kq * QE;
+      double v[QE];
+#pragma unroll
+      for (int j = 0; j < QE; ++j) v[j] = 0.0;
+      if (gr < p.rows && k0 < p.K) {
+        int ci = rg.x;
+        while (ci < rg.x + rg.y - 1 && k0 >= covers[ci].col0 + covers[ci].ncols) ++ci;
+        const MixCover cv = covers[ci];
+        if (k0 + QE <= min(p.K, cv.col0 + cv.ncols)) {
+          for (int q = 0; q < cv.nterm; ++q) {
+            const MixTerm tm = terms[cv.term0 + q];
+            const double* src = x + tm.in_off + gr + int64_t(k0 - cv.col0) * tm.ld;
+            double t[QE];
+#pragma unroll
+            for (int j = 0; j < QE; ++j) t[j] = src[int64_t(j) * tm.ld];
+#pragma unroll
+            for (int j = 0; j < QE; ++j) v[j] += tm.coef * t[j];
+          }
+        } else {
+          // the unit straddles two covers or the panel's last column
+#pragma unroll
+          for (int j = 0; j < QE; ++j) {
+            const int gk = k0 + j;
+            if (gk >= p.K) continue;
+            int cj = rg.x;
+            while (cj < rg.x + rg.y - 1 && gk >= covers[cj].col0 + covers[cj].ncols) ++cj;
+            const MixCover cw = covers[cj];
+            double acc = 0.0;
+            for (int q = 0; q < cw.nterm; ++q) {
+              const MixTerm tm = terms[cw.term0 + q];
+              acc += tm.coef * x[tm.in_off + gr + int64_t(gk - cw.col0) * tm.ld];
+            }
+            v[j] = acc;
+          }
+        }
+      }
+      uint2 rec[QE];
+#pragma unroll
+      for (int j = 0; j < QE; ++j) rec[j] = split_rec(F{}, v[j]);
+      store_unit(F{}, dst, plane, u * 16, rec);
+    }
+  }
+}
+
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -718,6 +789,16 @@ void launch_pack(cudaStream_t s, const double* x, unsigned char* img, const ImgP
   count_launch();
 }
 
+template <class F>
+void launch_pack_mix(cudaStream_t s, const double* x, unsigned char* img, const ImgPanel* panels,
+                     const int2* ranges, const MixCover* covers, const MixTerm* terms,
+                     int npanels, int64_t total_chunks, int rows) {
+  const int grid = int(total_chunks < 4096 ? total_chunks : 4096);
+  k_pack_mix_images<F><<<grid, PACK_THREADS, 0, s>>>(x, img, panels, ranges, covers, terms,
+                                                     npanels, total_chunks, rows);
+  count_launch();
+}
+
 template <class F, int BN>
 void launch_img(cudaStream_t s, const unsigned char* imgA, const unsigned char* imgB, double* C,
                 const GemmTask* tasks, int ntasks, const GemmSeg* segs, const SegImg* simg,
@@ -764,6 +845,17 @@ void launch_pack_images(int form, cudaStream_t s, const double* x, unsigned char
   if (rows != SPLIT_IMG_ROWS && rows != TF32_TILE_N_WIDE) return;
   if (form == SPLIT_BF16X9) launch_pack<FormBF16>(s, x, img, panels, npanels, total_chunks, rows);
   else launch_pack<FormTF32>(s, x, img, panels, npanels, total_chunks, rows);
+}
+
+void launch_pack_mix_images(int form, cudaStream_t s, const double* x, unsigned char* img,
+                            const ImgPanel* panels, const int2* ranges, const MixCover* covers,
+                            const MixTerm* terms, int npanels, int64_t total_chunks, int rows) {
+  if (total_chunks <= 0 || npanels <= 0) return;
+  if (rows != SPLIT_IMG_ROWS && rows != TF32_TILE_N_WIDE) return;
+  if (form == SPLIT_BF16X9)
+    launch_pack_mix<FormBF16>(s, x, img, panels, ranges, covers, terms, npanels, total_chunks, rows);
+  else
+    launch_pack_mix<FormTF32>(s, x, img, panels, ranges, covers, terms, npanels, total_chunks, rows);
 }
 
 void launch_gemm_split_images(int form, int bn, cudaStream_t s, const unsigned char* imgA,

@@ -103,9 +103,9 @@ void launch_gemm_f64(cudaStream_t s, int tile, bool transA, bool transB, const d
                      const double* B, double* C, const GemmTask* tasks, int ntasks,
                      const GemmSeg* segs, int total_tiles, int grid_cap);
 
-// Split-precision grouped GEMM on tcgen05 (FP32 accumulation in TMEM, FP64 in/out), tiles of
-// TF32_TILE_M x (64 or 128): form SPLIT_TF32X3 = three TF32 products, SPLIT_BF16X9 = nine BF16
-// products; err[0] is set when an MMA completion wait gave up.
+// Split-precision grouped GEMM on tcgen05 (FP32 accumulation in TMEM, FP64 in/out), direct form
+// with tiles of TF32_TILE_M x TF32_TILE_N_DIRECT: form SPLIT_TF32X3 = three TF32 products,
+// SPLIT_BF16X9 = nine BF16 products; err[0] is set when an MMA completion wait gave up.
 constexpr int SPLIT_TF32X3 = 1, SPLIT_BF16X9 = 2;
 constexpr int TF32_TILE_M = 128;
 constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_PRESPLIT = 128, TF32_TILE_N_WIDE = 256;
@@ -134,6 +134,16 @@ int64_t split_image_chunk_bytes(int form, int rows);
 // writes the chunk images (`rows` rows each) of panels[0, npanels) (total_chunks in all) from x
 void launch_pack_images(int form, cudaStream_t s, const double* x, unsigned char* img,
                         const ImgPanel* panels, int npanels, int64_t total_chunks, int rows);
+// The MPO mixing fused into the image pack of an operand (the mixed blocks are never written):
+// columns [col0, col0 + ncols) of a panel are sum_t coef_t * x[in_off_t + r + (k - col0) * ld_t]
+// over the mixing terms [term0, term0 + nterm) (MixTerm); a panel's covers (ranges[panel] =
+// first cover, count) are sorted by col0 and tile its K columns.
+struct MixCover {
+  int col0, ncols, term0, nterm;
+};
+void launch_pack_mix_images(int form, cudaStream_t s, const double* x, unsigned char* img,
+                            const ImgPanel* panels, const int2* ranges, const MixCover* covers,
+                            const MixTerm* terms, int npanels, int64_t total_chunks, int rows);
 void launch_gemm_split_images(int form, int bn, cudaStream_t s, const unsigned char* imgA,
                               const unsigned char* imgB, double* C, const GemmTask* tasks,
                               int ntasks, const GemmSeg* segs, const SegImg* simg,

@@ -6,7 +6,10 @@ invariants (energy, alpha, largest bond dimension, truncation error), never on t
 tensors. Tolerances: FP64 throughout, energies to 1e-9 relative per sweep. alpha is a product of
 (1 +- noise_incr) factors, each decided by thresholds such as truncerr <= max(cutoff, 1e-12) that
 converged steps sit right on (truncation errors near 1e-12 known to ~1e-16 absolute), so a
-decision may come out the other way on rounding: alpha agrees to within a few such steps (5%).
+decision may come out the other way on rounding: a different but equally accurate eigensolver
+(bisection against multisection of the same Sturm counts) moves the trajectory of the L=10 run by
+about four such decisions. alpha agrees to within five flipped decisions: a factor
+(1.01 / 0.99)^5, relative 12%.
 """
 import numpy as np
 import pytest
@@ -23,7 +26,7 @@ def _compare(stats, recs, rtol=1e-9):
     assert len(stats) == len(recs)
     for a, b in zip(stats, recs):
         assert abs(a["energy"] - b["energy"]) <= rtol * abs(b["energy"])
-        assert a["noise"] == pytest.approx(b["noise"], rel=0.05)
+        assert a["noise"] == pytest.approx(b["noise"], rel=0.12)
         assert a["biggest_m"] == b["biggestm"]
         assert abs(a["max_truncerr"] - b["maxtrunc"]) <= 1e-8
 
