@@ -529,6 +529,7 @@ k_pack_mix_images(const double* __restrict__ x, unsigned char* __restrict__ img,
         while (ci < rg.x + rg.y - 1 && k0 >= covers[ci].col0 + covers[ci].ncols) ++ci;
         const MixCover cv = covers[ci];
         if (k0 + QE <= min(p.K, cv.col0 + cv.ncols)) {
+#pragma unroll 2
           for (int q = 0; q < cv.nterm; ++q) {
             const MixTerm tm = terms[cv.term0 + q];
             const double* src = x + tm.in_off + gr + int64_t(k0 - cv.col0) * tm.ld;
