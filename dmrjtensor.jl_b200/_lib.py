@@ -132,6 +132,7 @@ SIGNATURES = {
     "dmrg_test_eigh": (C.c_int, [_P, C.c_int, _IP, _DP, _DP]),
     "dmrg_test_syevt": (C.c_int, [_P, C.c_int, _IP, _IP, _DP, _DP, _DP]),
     "dmrg_test_heff_time": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _DP, _DP]),
+    "dmrg_test_heff_apply_repeat": (C.c_int, [_P, _P, C.c_int, _DP, _DP, C.c_int, C.c_int]),
     "dmrg_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_P)]),
     "dmrg_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_longlong)]),
     "dmrg_server_poll": (C.c_int, [_P, C.c_longlong, C.c_int, C.POINTER(Result)]),

@@ -797,13 +797,16 @@ int dmrg_twosite_dims(const dmrg_state* st, const dmrg_mpo* mpo, int iL, int* di
   return DMRG_OK;
 }
 
-int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
-                    double* psi_out, int precision) {
+// psi_out = Heff psi_in (dense-equivalent host arrays), the last of `reps` applications of one
+// plan to the same vector
+static int heff_apply_reps(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
+                           double* psi_out, int precision, int reps) {
   if (!st) return DMRG_ERR_ARG;
   dmrg_ctx* c = st->ctx;
   return guarded(c, [&] {
     if (mpo != st->mpo) fail(DMRG_ERR_ARG, "state was uploaded with a different MPO");
-    if (iL < 0 || iL + 1 >= st->L || !psi_in || !psi_out) fail(DMRG_ERR_ARG, "bad arguments");
+    if (iL < 0 || iL + 1 >= st->L || !psi_in || !psi_out || reps < 1)
+      fail(DMRG_ERR_ARG, "bad arguments");
     if (!st->Lvalid[iL] || !st->Rvalid[iL + 1]) fail(DMRG_ERR_STATE, "environments not built");
     set_device(c);
     HeffPlan hp;
@@ -831,7 +834,7 @@ int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* p
     ensure(c, c->H, int64_t(h.size()));
     cuda_check(cudaMemcpyAsync(c->K.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice,
                                c->stream), "psi upload");
-    apply_heff(st, iL, hp, c->K.p, c->H.p, precision);
+    for (int r = 0; r < reps; ++r) apply_heff(st, iL, hp, c->K.p, c->H.p, precision);
     cuda_check(cudaMemcpyAsync(h.data(), c->H.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
                                c->stream), "psi download");
     cuda_check(cudaStreamSynchronize(c->stream), "heff sync");
@@ -847,6 +850,17 @@ int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* p
               psi_out[at(ol[ka] + ca, s1, s2, orr[kd] + cb)] = h[tl.off[id] + ca + int64_t(cb) * Bl.dim[ka]];
         }
   });
+}
+
+
+int dmrg_heff_apply(dmrg_state* st, const dmrg_mpo* mpo, int iL, const double* psi_in,
+                    double* psi_out, int precision) {
+  return heff_apply_reps(st, mpo, iL, psi_in, psi_out, precision, 1);
+}
+
+int dmrg_test_heff_apply_repeat(dmrg_state* st, const dmrg_mpo* mpo, int iL,
+                                const double* psi_in, double* psi_out, int precision, int reps) {
+  return heff_apply_reps(st, mpo, iL, psi_in, psi_out, precision, reps);
 }
 
 int dmrg_test_heff_time(dmrg_state* st, const dmrg_mpo* mpo, int iL, int precision, int reps,

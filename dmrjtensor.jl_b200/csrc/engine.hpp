@@ -116,7 +116,7 @@ struct GemmList {
   size_t t_off = 0, s_off = 0;  // byte offsets inside the uploaded slot
   int bm = GEMM_BM;              // tile rows the tile counts refer to
   int bn = GEMM_BN;              // tile columns the tile counts refer to
-  // image plan of the image-fed split form (lists retiled to TF32_TILE_N_PRESPLIT or
+  // image plan of the image-fed split form (lists retiled to TF32_TILE_N_IMAGE or
   // TF32_TILE_N_WIDE): the distinct A and B operand windows as panels, and the image chunks of
   // every segment
   std::vector<ImgPanel> pa, pb;
@@ -131,7 +131,7 @@ struct GemmList {
   void seg(int64_t a_off, int lda, int64_t b_off, int ldb, int K);
 };
 // The same products tiled for the split-precision kernel (TF32_TILE_M x bn tiles); with
-// bn = TF32_TILE_N_PRESPLIT or TF32_TILE_N_WIDE also the image plan.
+// bn = TF32_TILE_N_IMAGE or TF32_TILE_N_WIDE also the image plan.
 GemmList retile(const GemmList& g, int bm, int bn);
 
 struct MixList {
@@ -304,11 +304,11 @@ void tune_gemm(dmrg_ctx* c, GemmList& g);
 // Folds the timings of completed trial launches into the tuner (no synchronisation).
 void tuner_collect(dmrg_ctx* c);
 // The same list on a split-precision tcgen05 kernel (form SPLIT_TF32X3 or SPLIT_BF16X9); the list
-// must be retiled. Lists of at least SPLIT_PRESPLIT_FLOPS take the image-fed form: their operand
+// must be retiled. Lists of at least SPLIT_IMAGE_FLOPS take the image-fed form: their operand
 // windows are converted once into chunk images first.
-constexpr double SPLIT_PRESPLIT_FLOPS = 1e9;
-// Tile width of a list's split form: TF32_TILE_N_DIRECT below SPLIT_PRESPLIT_FLOPS, else the
-// image-fed width (TF32_TILE_N_PRESPLIT or TF32_TILE_N_WIDE) whose schedule the cost model
+constexpr double SPLIT_IMAGE_FLOPS = 1e9;
+// Tile width of a list's split form: TF32_TILE_N_DIRECT below SPLIT_IMAGE_FLOPS, else the
+// image-fed width (TF32_TILE_N_IMAGE or TF32_TILE_N_WIDE) whose schedule the cost model
 // finishes first.
 int split_tile_n(const GemmList& g);
 // Options of the image-fed form: an operand's images in a persistent buffer, packed only when

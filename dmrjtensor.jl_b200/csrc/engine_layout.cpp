@@ -300,7 +300,7 @@ GemmList retile(const GemmList& g, int bm, int bn) {
     t.tile0 = r.tiles;
     r.tiles += t.tiles_m * ((t.N + bn - 1) / bn);
   }
-  if (bm == TF32_TILE_M && (bn == TF32_TILE_N_PRESPLIT || bn == TF32_TILE_N_WIDE)) plan_images(r);
+  if (bm == TF32_TILE_M && (bn == TF32_TILE_N_IMAGE || bn == TF32_TILE_N_WIDE)) plan_images(r);
   return r;
 }
 
@@ -309,19 +309,19 @@ GemmList retile(const GemmList& g, int bm, int bn) {
 constexpr double WIDE_TILE_RATE = 1.3;
 
 int split_tile_n(const GemmList& g) {
-  if (g.flops < SPLIT_PRESPLIT_FLOPS) return TF32_TILE_N_DIRECT;
+  if (g.flops < SPLIT_IMAGE_FLOPS) return TF32_TILE_N_DIRECT;
   // the image-fed kernel runs one CTA per SM and hands out tiles round-robin: the makespan of
   // each width is the largest CTA load (tile work = columns x K chunks) over its rate
   const int P = std::max(device_sm_count(), 1);
   double best = 0;
-  int pick = TF32_TILE_N_PRESPLIT;
-  for (int bn : {TF32_TILE_N_PRESPLIT, TF32_TILE_N_WIDE}) {
+  int pick = TF32_TILE_N_IMAGE;
+  for (int bn : {TF32_TILE_N_IMAGE, TF32_TILE_N_WIDE}) {
     int64_t ntiles = 0;
     for (const GemmTask& t : g.tasks)
       if (t.M > 0 && t.N > 0)
         ntiles += int64_t((t.M + TF32_TILE_M - 1) / TF32_TILE_M) * ((t.N + bn - 1) / bn);
     const int grid = int(std::min<int64_t>(ntiles, P));
-    if (grid == 0) return TF32_TILE_N_PRESPLIT;
+    if (grid == 0) return TF32_TILE_N_IMAGE;
     std::vector<double> load(grid, 0.0);
     int64_t tile = 0;
     for (const GemmTask& t : g.tasks) {
@@ -336,7 +336,7 @@ int split_tile_n(const GemmList& g) {
     }
     const double span = *std::max_element(load.begin(), load.end()) /
                         (bn == TF32_TILE_N_WIDE ? WIDE_TILE_RATE : 1.0);
-    if (bn == TF32_TILE_N_PRESPLIT || span < best) {
+    if (bn == TF32_TILE_N_IMAGE || span < best) {
       best = span;
       pick = bn;
     }
@@ -561,7 +561,7 @@ void run_gemm_split(dmrg_ctx* c, const GemmList& g, char* dbase, const double* A
                     const SplitOpts* opts) {
   if (form != SPLIT_TF32X3 && form != SPLIT_BF16X9) bad_plan("split gemm form");
   if (g.tiles == 0) return;
-  if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_PRESPLIT &&
+  if (g.bm != TF32_TILE_M || (g.bn != TF32_TILE_N_DIRECT && g.bn != TF32_TILE_N_IMAGE &&
                               g.bn != TF32_TILE_N_WIDE))
     bad_plan("split gemm tiling");
   for (const GemmTask& t : g.tasks) {

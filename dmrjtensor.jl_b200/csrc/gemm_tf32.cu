@@ -45,8 +45,8 @@ namespace {
 constexpr int TBM = 128, TBK = 32;
 constexpr int TT = 128;                          // 4 warps (direct form)
 constexpr long long WAIT_LIMIT = 1ll << 22;      // try_wait rounds before giving up (direct form)
-static_assert(TF32_TILE_N_DIRECT == 64 && TF32_TILE_N_PRESPLIT == 128, "tile widths");
-static_assert(SPLIT_IMG_ROWS == TBM && TF32_TILE_N_PRESPLIT == 128 && TF32_TILE_N_WIDE == 256,
+static_assert(TF32_TILE_N_DIRECT == 64 && TF32_TILE_N_IMAGE == 128, "tile widths");
+static_assert(SPLIT_IMG_ROWS == TBM && TF32_TILE_N_IMAGE == 128 && TF32_TILE_N_WIDE == 256,
               "image tile shapes");
 
 // The two split forms. A 16-byte unit of a staged plane holds QE consecutive K elements of one
@@ -820,7 +820,7 @@ void launch_img_bn(int bn, cudaStream_t s, const unsigned char* imgA, const unsi
     launch_img<F, TF32_TILE_N_WIDE>(s, imgA, imgB, C, tasks, ntasks, segs, simg, total_tiles,
                                     grid_cap, err);
   else
-    launch_img<F, TF32_TILE_N_PRESPLIT>(s, imgA, imgB, C, tasks, ntasks, segs, simg, total_tiles,
+    launch_img<F, TF32_TILE_N_IMAGE>(s, imgA, imgB, C, tasks, ntasks, segs, simg, total_tiles,
                                         grid_cap, err);
 }
 

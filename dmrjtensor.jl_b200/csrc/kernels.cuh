@@ -108,11 +108,11 @@ void launch_gemm_f64(cudaStream_t s, int tile, bool transA, bool transB, const d
 // SPLIT_BF16X9 = nine BF16 products; err[0] is set when an MMA completion wait gave up.
 constexpr int SPLIT_TF32X3 = 1, SPLIT_BF16X9 = 2;
 constexpr int TF32_TILE_M = 128;
-constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_PRESPLIT = 128, TF32_TILE_N_WIDE = 256;
+constexpr int TF32_TILE_N_DIRECT = 64, TF32_TILE_N_IMAGE = 128, TF32_TILE_N_WIDE = 256;
 void launch_gemm_split(int form, cudaStream_t s, bool transA, bool transB, const double* A,
                        const double* B, double* C, const GemmTask* tasks, int ntasks,
                        const GemmSeg* segs, int total_tiles, int grid_cap, int* err);
-// Image-fed form for large lists (tiles TF32_TILE_M x bn, bn = TF32_TILE_N_PRESPLIT or
+// Image-fed form for large lists (tiles TF32_TILE_M x bn, bn = TF32_TILE_N_IMAGE or
 // TF32_TILE_N_WIDE). Every distinct operand window of the list (an ImgPanel: element (r, k) at
 // off + r + k*ld, or off + k + r*ld when kcontig) is converted once into chunk images: row tiles
 // (SPLIT_IMG_ROWS rows for A, bn rows for B) x K chunks of SPLIT_IMG_K, each chunk the split

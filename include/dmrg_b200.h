@@ -318,6 +318,14 @@ DMRG_API int dmrg_test_syevt(dmrg_ctx* ctx, int nmat, const int* n, const int* k
 DMRG_API int dmrg_test_heff_time(dmrg_state* st, const dmrg_mpo* mpo, int iL, int precision,
                                  int reps, double* seconds, double* flops);
 
+/* Test hook (no counterpart in the reference): dmrg_heff_apply's result after `reps` >= 1
+ * applications of one Heff plan to psi_in. From the second application on, the split forms reuse
+ * the environment images the first one packed, as the Lanczos iterations of a bond step do; the
+ * result equals one application's bit for bit. */
+DMRG_API int dmrg_test_heff_apply_repeat(dmrg_state* st, const dmrg_mpo* mpo, int iL,
+                                         const double* psi_in, double* psi_out, int precision,
+                                         int reps);
+
 /* Fills *p with the reference defaults (minm 2, krylov 2, betatest 1e-10, ...). */
 DMRG_API void dmrg_params_default(dmrg_params* p);
 

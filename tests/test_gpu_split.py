@@ -2,8 +2,10 @@
 products) against the plain FP64 form.
 
 One Heff application agrees with FP64 to FP32 accuracy (the split products accumulate in FP32,
-relative 1e-5 here), in the direct form (small lists) and the pre-split form; whole DMRG runs from the same start agree in energy within 1e-8, the
-reported energy of a sweep being the FP64 Rayleigh quotient of the final Ritz vector.
+relative 1e-5 here), in the direct form (small lists) and the image-fed form (large lists, with the
+MPO mixing fused into the pack of the second GEMM's operand); whole DMRG runs from the same start
+agree in energy within 1e-8, the reported energy of a sweep being the FP64 Rayleigh quotient of
+the final Ritz vector.
 """
 import ctypes as C
 
@@ -51,9 +53,10 @@ def test_split_heff_matches_fp64(dmrgb, ctx, qn, form):
 
 
 @pytest.mark.parametrize("form", FORMS)
-def test_split_heff_presplit_form_matches_fp64(dmrgb, ctx, form):
+def test_split_heff_image_form_matches_fp64(dmrgb, ctx, form):
     """Bond dimension 384 either side: every Heff GEMM list is above 1 GFLOP and takes the
-    pre-split form (operands converted once into (hi, lo) pairs). The second GEMM accumulates
+    image-fed form (operand windows converted once into chunk images of their split parts; the
+    mixing summed inside the pack of the second GEMM's operand). The second GEMM accumulates
     K = d w m = 3840 products in FP32 (ten times the first test's), so the bound is relative 5e-5
     here (measured 1.3e-5)."""
     L, iL = 20, 9
@@ -68,6 +71,30 @@ def test_split_heff_presplit_form_matches_fp64(dmrgb, ctx, form):
     y64 = _heff(dmrgb, dev, iL, x, 0)
     y32 = _heff(dmrgb, dev, iL, x, form)
     assert np.max(np.abs(y32 - y64)) <= 5e-5 * np.max(np.abs(y64))
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_split_heff_cached_environment_images(dmrgb, ctx, form):
+    """The applications of one plan after its first reuse the environment images the first packed
+    (as a bond step's Lanczos iterations do): the fourth application of a plan gives the first's
+    result bit for bit, at the image-fed size of the test above."""
+    L, iL = 20, 9
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L)
+    psi = dmrgb.randMPS(2, L, 384, seed=8, oc=iL)
+    Lenv, _ = dmrgb.makeEnv(psi, mpo, ctx=ctx)
+    dev = Lenv.dev
+    d = (C.c_int * 4)()
+    assert dmrgb.lib().dmrg_twosite_dims(dev.h, dev.dmpo.h, iL, d) == 0
+    x = np.asfortranarray(np.random.default_rng(10).standard_normal(tuple(d)))
+    dp = C.POINTER(C.c_double)
+    y1 = np.zeros_like(x, order="F")
+    y4 = np.zeros_like(x, order="F")
+    for y, reps in ((y1, 1), (y4, 4)):
+        code = dmrgb.lib().dmrg_test_heff_apply_repeat(dev.h, dev.dmpo.h, iL, x.ctypes.data_as(dp),
+                                                       y.ctypes.data_as(dp), form, reps)
+        assert code == 0, dmrgb.lib().dmrg_last_error(dev.ctx.h)
+    assert np.array_equal(y1, y4)
+    assert np.array_equal(y1, _heff(dmrgb, dev, iL, x, form))
 
 
 @pytest.mark.parametrize("form", ["3xtf32", "bf16x9"])
