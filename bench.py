@@ -344,10 +344,11 @@ def run_serving(pkg, device, nreq, rate=20.0, slots=16, seed=5, saturate=False, 
 
 
 def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
-    """``expect(psi, H)`` and ``correlationmatrix`` on the device: on the resident maxm-1024 state
-    of the sweep workload, and on the same chain after a short maxm-64 run where the CPU oracle
-    (dense, centre-moving) finishes in seconds and is timed beside the device on identical
-    tensors."""
+    """``expect(psi, H)``, ``correlationmatrix`` and the two-point ``correlation`` on the device:
+    on the resident maxm-1024 state of the sweep workload, and on the same chain after a short
+    maxm-64 run where the CPU oracle (dense; centre-moving for the matrix, the reference's loop
+    for ``correlation`` over the first 20 sites) finishes in seconds and is timed beside the
+    device on identical tensors."""
     Sp, Sm, Sz = pkg.spinOps()[:3]
     psi = pkg.MPS()
     psi._dev = dev
@@ -363,14 +364,22 @@ def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
     t_zz = time.perf_counter() - t
     n2 = pkg.kernel_launches()
     t = time.perf_counter()
-    pkg.correlationmatrix(psi, Sp, Sm, ctx=ctx)
+    rho_pm = pkg.correlationmatrix(psi, Sp, Sm, ctx=ctx)
     t_pm = time.perf_counter() - t
+    n3 = pkg.kernel_launches()
+    t = time.perf_counter()
+    om_pm = pkg.correlation(psi, Sp, Sm, ctx=ctx)
+    t_corr = time.perf_counter() - t
+    n4 = pkg.kernel_launches()
     out = {"state": f"heisenberg L={L_CHAIN} U(1), maxm {RAMP[-1]} (resident)",
            "expect_seconds": t_exp, "expect_launches": n1 - n0,
            "expect_rel_diff_vs_sweep_energy": abs(E - energy) / abs(energy),
            "correlationmatrix_zz_seconds": t_zz, "correlationmatrix_pm_seconds": t_pm,
            "correlationmatrix_launches": n2 - n1,
-           "zz_max_abs_row_sum": float(np.max(np.abs(rho.sum(axis=1))))}
+           "zz_max_abs_row_sum": float(np.max(np.abs(rho.sum(axis=1)))),
+           "correlation_pm_seconds": t_corr, "correlation_pm_launches": n4 - n3,
+           "correlation_pm_max_abs_diff_vs_correlationmatrix":
+               float(np.max(np.abs(om_pm - rho_pm)))}
     small = pkg.neelMPS(L_CHAIN)
     pkg.dmrg(small, mpo, m=m_small, sweeps=2, cutoff=CUTOFF, ctx=ctx)
     pkg.correlationmatrix(small, Sz, Sz, ctx=ctx)    # untimed warm-up
@@ -380,8 +389,13 @@ def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
     t = time.perf_counter()
     rho_s = pkg.correlationmatrix(small, Sz, Sz, ctx=ctx)
     t_zz_s = time.perf_counter() - t
+    first = range(1, 21)
+    t = time.perf_counter()
+    om_s = pkg.correlation(small, Sp, Sm, sites=(first, first), ctx=ctx)
+    t_corr_s = time.perf_counter() - t
     cmp = {"state": f"heisenberg L={L_CHAIN} U(1) after 2 sweeps at maxm {m_small}",
-           "device_expect_seconds": t_exp_s, "device_correlationmatrix_zz_seconds": t_zz_s}
+           "device_expect_seconds": t_exp_s, "device_correlationmatrix_zz_seconds": t_zz_s,
+           "device_correlation_pm_20x20_seconds": t_corr_s}
     if cpu:
         from oracle import measure as omeas, models as omod
         dense = [np.array(small[i]) for i in range(L_CHAIN)]
@@ -392,9 +406,14 @@ def run_measurements(pkg, ctx, dev, mpo, energy, cpu=True, m_small=64):
         t = time.perf_counter()
         rho_o = omeas.correlationmatrix(dense, small.oc, Sz, Sz)
         t_zz_o = time.perf_counter() - t
+        t = time.perf_counter()
+        om_o = omeas.correlation(dense, (Sp, Sm), sites=[list(range(20))] * 2)
+        t_corr_o = time.perf_counter() - t
         cmp.update({"oracle_expect_seconds": t_exp_o, "oracle_correlationmatrix_zz_seconds": t_zz_o,
+                    "oracle_correlation_pm_20x20_seconds": t_corr_o,
                     "oracle_cores": cpu_threads(), "abs_dE": abs(E_s - E_o),
-                    "max_abs_drho": float(np.max(np.abs(rho_s - rho_o)))})
+                    "max_abs_drho": float(np.max(np.abs(rho_s - rho_o))),
+                    "max_abs_domega": float(np.max(np.abs(om_s - om_o)))})
     out["vs_oracle"] = cmp
     return out
 

@@ -10,7 +10,7 @@ from ._lib import DmrgError, PREC, lib
 from .models import (HUBBARD_QN, SPIN_QN, XXZ, cylinder_bonds, fermionOps, heisenbergCylinderMPO,
                      heisenbergMPO, hubbardMPO, makeMPO, spinOps, tfiMPO)
 from .state import (MPO, MPS, Context, DeviceMPO, DeviceState, Env, Lupdate, Rupdate, applyOps,
-                    correlationmatrix, default_context, dmrg, expect, largeMPS, loadMPS,
+                    correlation, correlationmatrix, default_context, dmrg, expect, largeMPS, loadMPS,
                     make_params, makeEnv, mpo_product, neelMPS, product_MPS, randMPS, tdvp,
                     tdvp_twosite)
 from .serving import Server, ServerError
@@ -28,6 +28,6 @@ __all__ = [
     "heisenbergCylinderMPO", "heisenbergMPO", "hubbardMPO", "makeMPO", "spinOps", "tfiMPO", "MPO",
     "MPS", "Context", "DeviceMPO", "DeviceState", "Env", "Lupdate", "Rupdate", "applyOps",
     "default_context", "dmrg", "make_params", "makeEnv", "neelMPS", "product_MPS", "randMPS",
-    "expect", "mpo_product", "correlationmatrix", "largeMPS", "loadMPS", "tdvp", "tdvp_twosite",
+    "expect", "mpo_product", "correlation", "correlationmatrix", "largeMPS", "loadMPS", "tdvp", "tdvp_twosite",
     "Server", "ServerError",
 ]

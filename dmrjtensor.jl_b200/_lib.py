@@ -119,6 +119,7 @@ SIGNATURES = {
     "dmrg_env_step": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP,
                                 _DP, _DP, _DP, _DP]),
     "dmrg_correlationmatrix": (C.c_int, [_P, C.c_int, _DP, _DP, _DP, _DP]),
+    "dmrg_correlation": (C.c_int, [_P, C.c_int, C.c_int, _IP, _DP, _IP, _IP, _DP, _DP]),
     "dmrg_heff_apply": (C.c_int, [_P, _P, C.c_int, _DP, _DP, C.c_int]),
     "dmrg_heff_apply_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
     "dmrg_twosite_dims": (C.c_int, [_P, _P, C.c_int, _IP]),

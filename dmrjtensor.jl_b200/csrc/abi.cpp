@@ -754,6 +754,17 @@ int dmrg_correlationmatrix(dmrg_state* st, int d, const double* Cc, const double
   });
 }
 
+int dmrg_correlation(dmrg_state* st, int d, int nops, const int* oplen, const double* ops,
+                     const int* nsites, const int* sites, const double* trails, double* omega) {
+  if (!st || d <= 0 || nops <= 0 || !oplen || !ops || !nsites || !sites || !omega)
+    return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    set_device(c);
+    measure_correlation_n(st, d, nops, oplen, ops, nsites, sites, trails, omega, nullptr);
+  });
+}
+
 int dmrg_env_get(dmrg_state* st, int site, int left, double* out, int* dims) {
   if (!st) return DMRG_ERR_ARG;
   dmrg_ctx* c = st->ctx;

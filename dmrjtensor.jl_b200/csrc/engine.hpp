@@ -446,6 +446,13 @@ void rupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP6
 double measure_expect(dmrg_state* st, const dmrg_mpo* H, double* flops);
 // rho (L x L, column-major): two-point correlations of Cc and Ca with an optional trail F
 // (d x d column-major operators [bra, ket]; F may be null), normalised by <psi|psi>.
+// correlation(psi, ops...; sites, trail) with dualpsi = psi: operator g has lens[g] d x d factors
+// (packed in `ops`), start positions sites[..] (nsites[g] entries, 0-based; the last lens[g] - 1
+// are not used as starts, as in the reference) and an optional trail (trails: n matrices or
+// null); omega has prod_g (nsites[g] - lens[g] + 1) entries, the first operator's index fastest.
+void measure_correlation_n(dmrg_state* st, int d, int n, const int* lens, const double* ops,
+                           const int* nsites, const int* sites, const double* trails,
+                           double* omega, double* flops);
 void measure_correlation(dmrg_state* st, int d, const double* Cc, const double* Ca,
                          const double* F, double* rho, double* flops);
 

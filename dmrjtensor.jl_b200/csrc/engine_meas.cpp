@@ -20,10 +20,24 @@
 // charge conservation an operator must change the charge by one fixed amount, which becomes the
 // label of the w = 1 environment bond (r(w') = r(w) + p(ket) - p(bra)).
 //
+// correlation (lib/MPO_MPS/correlation.jl:98-237, dualpsi = psi): for operators 1..n, operator g
+// a product of len_g single-site factors on consecutive sites starting at p_g, and optional
+// trails F_g,
+//   omega[p_1, ..., p_n] = <psi| prod_s O(s) |psi>,   O(s) = A_1(s) A_2(s) ... A_n(s),
+// A_g(s) = F_g for s < p_g, factor s - p_g of operator g on its sites, the identity elsewhere (the
+// order in which the reference applies them to its copy of the ket). Not normalised. The device
+// runs one column (positions of operators 2..n) at a time: right environments R[s] through
+// A_2..A_n from the right end, the left chain X[s] through A_1's trail and A_2..A_n, and at each
+// position of operator 1 the chain through its factors contracted with R. Steps that share site,
+// operator and charge label share one plan.
+//
 // Every step of a measurement is planned on the host and uploaded in one descriptor copy; the
 // launches then run back to back on the context stream and the results are read back once.
 #include <algorithm>
 #include <cmath>
+#include <deque>
+#include <map>
+#include <tuple>
 
 #include "engine.hpp"
 
@@ -413,6 +427,229 @@ void measure_correlation(dmrg_state* st, int d, const double* Cc_, const double*
         rho[j + size_t(i) * L] = v;
       }
     }
+    if (flops) *flops = fl;
+  } catch (...) {
+    release();
+    throw;
+  }
+  release();
+}
+
+void measure_correlation_n(dmrg_state* st, int d, int n, const int* lens, const double* ops,
+                           const int* nsites, const int* sites, const double* trails,
+                           double* omega, double* flops) {
+  dmrg_ctx* c = st->ctx;
+  const int L = st->L;
+  if (n < 1 || n > 8) fail(DMRG_ERR_ARG, "correlation: between 1 and 8 operators");
+  for (int i = 0; i < L; ++i)
+    if (st->mpo->site[i].d != d)
+      fail(DMRG_ERR_SHAPE, "correlation: operator dimension differs from a site's");
+  check_edges(st);
+  const size_t dd = size_t(d) * d;
+  std::vector<double> Id(dd, 0.0);
+  for (int a = 0; a < d; ++a) Id[size_t(a) * (d + 1)] = 1.0;
+  // operators, trails (an identity trail is none) and the start positions of each operator
+  std::vector<std::vector<std::vector<double>>> O(n);
+  std::vector<std::vector<double>> F(n);
+  std::vector<std::vector<int>> pos(n);
+  size_t oat = 0, sat = 0;
+  int64_t total = 1;
+  for (int g = 0; g < n; ++g) {
+    if (lens[g] < 1 || lens[g] > L) fail(DMRG_ERR_ARG, "correlation: bad operator length");
+    for (int k = 0; k < lens[g]; ++k, oat += dd) O[g].emplace_back(ops + oat, ops + oat + dd);
+    if (trails) {
+      std::vector<double> t(trails + size_t(g) * dd, trails + size_t(g + 1) * dd);
+      if (t != Id) F[g] = t;
+    }
+    const int base = nsites[g] - (lens[g] - 1);
+    if (nsites[g] < 1 || base < 1) fail(DMRG_ERR_ARG, "correlation: no position for an operator");
+    for (int y = 0; y < base; ++y) {
+      const int p = sites[sat + y];
+      if (p < 0 || p + lens[g] > L) fail(DMRG_ERR_ARG, "correlation: an operator runs off the chain");
+      pos[g].push_back(p);
+    }
+    sat += size_t(nsites[g]);
+    total *= base;
+    if (total > (int64_t(1) << 24)) fail(DMRG_ERR_BUDGET, "correlation: too many entries");
+  }
+  const int base1 = int(pos[0].size()), len1 = lens[0];
+  const int64_t ncol = total / base1;
+  if (ncol * int64_t(L) > (int64_t(1) << 22))
+    fail(DMRG_ERR_BUDGET, "correlation: too many positions of operators 2..n for this chain");
+  const QN zero;
+
+  // ---- plans, shared by site, direction, incoming charge label and operator
+  std::deque<StepPlan> plans;            // stable references
+  std::vector<QN> plan_out;              // charge label of each plan's output environment
+  std::map<std::tuple<int, int, int, int, std::vector<double>>, int> memo;
+  auto step = [&](bool left, int s, QN label, const std::vector<double>& M,
+                  const EnvLayout& in) -> int {
+    auto key = std::make_tuple(left ? 0 : 1, s, label.v[0], label.v[1], M);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+    const MPOSite ms = op_site(M, d, st->mpo->site[s].p, label, left);
+    plans.emplace_back();
+    if (left) plan_left_step(st->bond[s], st->bond[s + 1], ms, st->lay[s], in, plans.back());
+    else plan_right_step(st->bond[s], st->bond[s + 1], ms, st->lay[s], in, plans.back());
+    plan_out.push_back(left ? ms.rr[0] : ms.rl[0]);
+    memo.emplace(key, int(plans.size()) - 1);
+    return int(plans.size()) - 1;
+  };
+  std::deque<PairPlan> pairs;
+  std::map<std::tuple<int, int, int, int, int>, int> pmemo;
+  auto pair = [&](int b, QN lx, const EnvLayout& X, QN ly, const EnvLayout& Y) -> int {
+    auto key = std::make_tuple(b, lx.v[0], lx.v[1], ly.v[0], ly.v[1]);
+    auto it = pmemo.find(key);
+    if (it != pmemo.end()) return it->second;
+    pairs.push_back(plan_pair(st->bond[b], X, Y));
+    pmemo.emplace(key, int(pairs.size()) - 1);
+    return int(pairs.size()) - 1;
+  };
+  const EnvLayout ELb = make_left_env_layout(st->bond[0], {zero});
+  const EnvLayout ERb = make_right_env_layout(st->bond[L], {zero});
+  if (ELb.other[0] != 0 || ERb.other[0] != 0)
+    fail(DMRG_ERR_QN, "edge sectors of the MPS do not connect");
+  std::vector<std::vector<int>> ystart(L);   // operator-1 entries y starting at each site
+  int last1 = 0;
+  for (int y = 0; y < base1; ++y) {
+    ystart[pos[0][y]].push_back(y);
+    last1 = std::max(last1, pos[0][y]);
+  }
+  struct Column {
+    std::vector<int> R, X, Y, P;   // right chain by site, left chain by site, operator-1 factors
+  };                                // (y * len1 + k), pair contraction per y
+  std::vector<Column> cols(static_cast<size_t>(ncol));
+  std::vector<std::vector<double>> S(L);
+  std::vector<int> at(n, 0);
+  for (int64_t col = 0; col < ncol; ++col) {
+    int64_t r = col;
+    for (int g = 1; g < n; ++g) {   // positions of operators 2..n, the first of them fastest
+      at[g] = int(r % int64_t(pos[g].size()));
+      r /= int64_t(pos[g].size());
+    }
+    for (int s = 0; s < L; ++s) {   // A_2(s) ... A_n(s)
+      std::vector<double> M = Id;
+      for (int g = 1; g < n; ++g) {
+        const int p = pos[g][at[g]];
+        if (s < p) { if (!F[g].empty()) M = matmul(M, F[g], d); }
+        else if (s < p + lens[g]) M = matmul(M, O[g][s - p], d);
+      }
+      S[s] = M;
+    }
+    Column& q = cols[size_t(col)];
+    std::vector<QN> rl(L + 1);
+    std::vector<const EnvLayout*> rlay(L + 1);
+    rl[L] = zero;
+    rlay[L] = &ERb;
+    q.R.assign(L, -1);
+    for (int s = L - 1; s >= 0; --s) {
+      const int k = step(false, s, rl[s + 1], S[s], *rlay[s + 1]);
+      q.R[s] = k;
+      rl[s] = plan_out[k];
+      rlay[s] = &plans[k].out;
+    }
+    QN xl = zero;
+    const EnvLayout* xlay = &ELb;
+    q.X.assign(L, -1);
+    q.Y.assign(size_t(base1) * len1, -1);
+    q.P.assign(base1, -1);
+    for (int s = 0; s <= last1; ++s) {
+      for (int y : ystart[s]) {
+        QN yl = xl;
+        const EnvLayout* ylay = xlay;
+        for (int k = 0; k < len1; ++k) {
+          const int j = step(true, s + k, yl, matmul(O[0][k], S[s + k], d), *ylay);
+          q.Y[size_t(y) * len1 + k] = j;
+          yl = plan_out[j];
+          ylay = &plans[j].out;
+        }
+        q.P[y] = pair(s + len1, yl, *ylay, rl[s + len1], *rlay[s + len1]);
+      }
+      if (s < last1) {
+        const int j = step(true, s, xl, F[0].empty() ? S[s] : matmul(F[0], S[s], d), *xlay);
+        q.X[s] = j;
+        xl = plan_out[j];
+        xlay = &plans[j].out;
+      }
+    }
+  }
+
+  // ---- one upload, buffers sized by the largest environment at each bond
+  int64_t t1 = 1, t2 = 1, lmax = 1;
+  std::vector<int64_t> rmax(L + 1, 1);
+  Upload u;
+  for (auto& sp : plans) {
+    plan_scratch(sp, t1, t2);
+    put_step(u, sp);
+  }
+  for (const Column& q : cols)
+    for (int s = 0; s < L; ++s) rmax[s] = std::max(rmax[s], plans[q.R[s]].out.size);
+  for (const StepPlan& sp : plans) lmax = std::max(lmax, sp.out.size);
+  for (auto& pp : pairs) pp.off = u.put(pp.t);
+  std::vector<DBuf> R(L + 1);
+  DBuf XB, X[2], Y[2], out;
+  auto release = [&] {
+    for (auto& b : R) dfree(c, b);
+    dfree(c, XB);
+    for (int a = 0; a < 2; ++a) {
+      dfree(c, X[a]);
+      dfree(c, Y[a]);
+    }
+    dfree(c, out);
+  };
+  try {
+    char* db = u.send(c, MEAS_SLOT);
+    ensure(c, c->T1, t1);
+    ensure(c, c->T2, t2);
+    for (int b = 0; b <= L; ++b) dalloc(c, R[b], rmax[b]);
+    dalloc(c, XB, 1);
+    for (int a = 0; a < 2; ++a) {
+      dalloc(c, X[a], lmax);
+      dalloc(c, Y[a], lmax);
+    }
+    dalloc(c, out, total);
+    cuda_check(cudaMemsetAsync(out.p, 0, sizeof(double) * size_t(total), c->stream),
+               "correlation clear");
+    set_one(c, R[L]);
+    set_one(c, XB);
+    double fl = 0.0;
+    for (int64_t col = 0; col < ncol; ++col) {
+      const Column& q = cols[size_t(col)];
+      for (int s = L - 1; s >= 0; --s) {
+        const StepPlan& sp = plans[q.R[s]];
+        run_step(c, sp, db, R[s + 1].p, R[s + 1].n, st->A[s], R[s].p, R[s].n);
+        fl += sp.flops();
+      }
+      const DBuf* xin = &XB;
+      for (int s = 0; s <= last1; ++s) {
+        for (int y : ystart[s]) {
+          const DBuf* yin = xin;
+          for (int k = 0; k < len1; ++k) {
+            const StepPlan& sp = plans[q.Y[size_t(y) * len1 + k]];
+            DBuf& yo = Y[k & 1];
+            run_step(c, sp, db, yin->p, yin->n, st->A[s + k], yo.p, yo.n);
+            fl += sp.flops();
+            yin = &yo;
+          }
+          const PairPlan& pp = pairs[q.P[y]];
+          if (!pp.t.empty()) {
+            run_pair(c, pp, db, *yin, R[s + len1], out.p + y + int64_t(base1) * col);
+            fl += 2.0 * pp.total;
+          }
+        }
+        if (s < last1) {
+          const StepPlan& sp = plans[q.X[s]];
+          DBuf& xo = X[s & 1];
+          run_step(c, sp, db, xin->p, xin->n, st->A[s], xo.p, xo.n);
+          fl += sp.flops();
+          xin = &xo;
+        }
+      }
+    }
+    cuda_check(cudaGetLastError(), "correlation launches");
+    cuda_check(cudaMemcpyAsync(omega, out.p, sizeof(double) * size_t(total),
+                               cudaMemcpyDeviceToHost, c->stream), "correlation download");
+    cuda_check(cudaStreamSynchronize(c->stream), "correlation sync");
     if (flops) *flops = fl;
   } catch (...) {
     release();

@@ -28,6 +28,7 @@ module DMRJtensorB200
 import DMRJtensor
 
 export dmrg_b200, tdvp_b200, makeEnv_b200, B200Env, B200Side, expect_b200, correlationmatrix_b200,
+       correlation_b200,
        save_b200, load_b200
 
 const libdmrg = get(ENV, "DMRG_B200_LIB", joinpath(@__DIR__, "..", "libdmrgb200.so"))
@@ -609,6 +610,30 @@ function correlationmatrix_b200(s::B200Side, Cc::Matrix{Float64}, Ca::Matrix{Flo
               (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
               s.env.st, d, Cc, Ca, F, rho), s.env.ctx.h, "dmrg_correlationmatrix")
   rho
+end
+
+# correlation(psi, ops...; sites, trail) (lib/MPO_MPS/correlation.jl:73-237) with dualpsi = psi:
+# each operator a d x d Float64 matrix O[bra, ket] or a vector of them on consecutive sites,
+# `sites` 1-based start ranges (default 1:L), `trail` one matrix, a tuple of them, or ().
+function correlation_b200(s::B200Side, ops...; sites=ntuple(i -> 1:s.env.L, length(ops)),
+                          trail=())
+  n = length(ops)
+  fs = [o isa AbstractVector ? collect(o) : [o] for o in ops]
+  lens = Cint[length(f) for f in fs]
+  d = size(fs[1][1], 1)
+  opbuf = reduce(vcat, [vec(Matrix{Float64}(m)) for f in fs for m in f])
+  starts = [Cint[x - 1 for x in sq] for sq in sites]
+  base = [length(starts[g]) - (lens[g] - 1) for g = 1:n]
+  tl = trail isa Tuple ? collect(trail) : (trail isa AbstractMatrix ? [trail] : collect(trail))
+  tb = isempty(tl) ? C_NULL : reduce(vcat, [vec(Matrix{Float64}(tl[(g - 1) % length(tl) + 1]))
+                                            for g = 1:n])
+  omega = zeros(Float64, base...)
+  check(ccall((:dmrg_correlation, libdmrg), Cint,
+              (Ptr{Cvoid}, Cint, Cint, Ptr{Cint}, Ptr{Cdouble}, Ptr{Cint}, Ptr{Cint}, Ptr{Cdouble},
+               Ptr{Cdouble}),
+              s.env.st, d, n, lens, opbuf, Cint[length(x) for x in starts], reduce(vcat, starts), tb,
+              omega), s.env.ctx.h, "dmrg_correlation")
+  omega
 end
 
 # Checkpoint of the device state (the persistence of largeMPS / loadMPS,

@@ -248,6 +248,23 @@ DMRG_API int dmrg_expect(dmrg_state* st, const dmrg_mpo* H, double* value);
 DMRG_API int dmrg_correlationmatrix(dmrg_state* st, int d, const double* Cc, const double* Ca,
                                     const double* trail, double* rho);
 
+/* correlation(psi, ops...; sites, trail) (lib/MPO_MPS/correlation.jl:98-237) with dualpsi = psi:
+ * omega[p_1, ..., p_n] = <psi| prod_s O(s) |psi>, not normalised, with O(s) = A_1(s) ... A_n(s)
+ * and A_g(s) = trail_g left of operator g, factor s - p_g of operator g on its oplen[g]
+ * consecutive sites, the identity elsewhere (the order in which the reference applies them).
+ * ops: the factors of every operator, d x d column-major O[bra, ket], operator 1 first; sites:
+ * nsites[g] 0-based start candidates of operator g, concatenated, of which the first
+ * nsites[g] - oplen[g] + 1 are used (as in the reference); trails: nops matrices or NULL (an
+ * identity trail is none). omega: prod_g (nsites[g] - oplen[g] + 1) values, operator 1's index
+ * fastest. The reference indexes its result by the site numbers themselves, so the two agree
+ * when every sites list is 0, 1, ...; for three or more operators the reference reuses right
+ * environments of an earlier position combination (its Renv array is updated in place from the
+ * rightmost operator of the current combination, which can lie left of the previous one's), and
+ * its values there differ from the definition above, which this computes. */
+DMRG_API int dmrg_correlation(dmrg_state* st, int d, int nops, const int* oplen,
+                              const double* ops, const int* nsites, const int* sites,
+                              const double* trails, double* omega);
+
 /* ---------------------------------------------------------------- the sweep
  * One optmps sweep (algs/optimizeMPS.jl:790-835): 2(L-1) twostep calls, each followed by an
  * environment update; the centre reverses at the edges. Requires dmrg_env_build first. */

@@ -132,3 +132,139 @@ def ed_correlation(v, L, Cc, Ca, trail=None):
             ops[j] = Ca
             rho[i, j] = rho[j, i] = float(v @ (_kron_all(ops) @ v)) / nrm
     return rho
+
+
+# ------------------------------------------------------------------ n-point correlation
+
+def _apply(O, A):
+    """``contract([2,1,3], O, 2, A, 2)``: the operator O[bra, ket] on the ket of a site tensor."""
+    return np.einsum("ts,asb->atb", O, A)
+
+
+def _lstep(Lm, A, B):
+    """Left environment step <A|.|B> from bond b to b+1: Lm[a_bra, a_ket] -> [b_bra, b_ket]."""
+    return np.einsum("xy,xsb,ysc->bc", Lm, A, B)
+
+
+def _rstep(Rm, A, B):
+    """Right environment step from bond b+1 to b: Rm[b_bra, b_ket] -> [a_bra, a_ket]."""
+    return np.einsum("xy,asx,csy->ac", Rm, A, B)
+
+
+def _oplists(ops):
+    return [list(o) if isinstance(o, (list, tuple)) else [np.asarray(o)] for o in ops]
+
+
+def _trails(trail, n, d):
+    if trail is None or (isinstance(trail, (list, tuple)) and len(trail) == 0):
+        return [None] * n
+    if isinstance(trail, (list, tuple)):
+        sub = [np.asarray(trail[w % len(trail)]) for w in range(n)]
+    else:
+        sub = [np.asarray(trail)] * n
+    return [None if np.allclose(F, np.eye(d)) else F for F in sub]
+
+
+def correlation(psi, ops, sites=None, trail=None):
+    """Literal restatement of ``correlation(dualpsi = psi, psi, ops...; sites, trail)``
+    (``lib/MPO_MPS/correlation.jl:98-237``) on a dense MPS: omega[p_1, ..., p_n] with operator k
+    at ``sites[k][p_k]`` (0-based here; an operator given as a list acts on that many consecutive
+    sites). For each combination of the positions of operators 2..n the ket copy gets operators
+    n..2 (each after its trail on every site left of it, ``subtrail``), the right environments are
+    rebuilt from the rightmost of them down (in place, ``Renv[a-1] = Rupdate(Renv[a], ...)``), and
+    operator 1 runs over its positions with the left environment carried along, its trail left on
+    each site it has passed. The multi-index of operators 2..n advances with its first index
+    fastest (the increment of TensorPACK's ``position_incrementer!``, which is not vendored; its
+    behaviour here is inferred from this call site). Not normalised. ``sites`` must be contiguous
+    ranges starting at site 0 for the result to be indexed like the reference's (which stores at
+    the site numbers themselves)."""
+    L = len(psi)
+    d = np.asarray(psi[0]).shape[1]
+    O = _oplists(ops)
+    n = len(O)
+    lens = [len(o) for o in O]
+    if sites is None:
+        sites = [list(range(L)) for _ in range(n)]
+    F = _trails(trail, n, d)
+    base = [len(sites[k]) - (lens[k] - 1) for k in range(n)]
+    # makeEnv(dualpsi, psi): Lenv[i] left of site i, Renv[i] right of site i
+    Lenv = [None] * L
+    Renv = [None] * L
+    Lenv[0] = np.ones((1, 1))
+    for i in range(L - 1):
+        Lenv[i + 1] = _lstep(Lenv[i], psi[i], psi[i])
+    Renv[L - 1] = np.ones((1, 1))
+    for i in range(L - 1, 0, -1):
+        Renv[i - 1] = _rstep(Renv[i], psi[i], psi[i])
+    omega = np.zeros(base)
+    bpos = [0] * n
+    while all(bpos[w] < base[w] for w in range(n)):
+        save = [np.asarray(A) for A in psi]
+        pos = [sites[w][bpos[w]] for w in range(n)]
+        maxops = 0
+        for g in range(n - 1, 0, -1):
+            maxops = max(pos[g] + lens[g] - 1, maxops)
+            for p in range(lens[g]):
+                save[pos[g] + p] = _apply(O[g][p], save[pos[g] + p])
+            if F[g] is not None:
+                for w in range(pos[g]):
+                    save[w] = _apply(F[g], save[w])
+        for a in range(maxops, 0, -1):
+            Renv[a - 1] = _rstep(Renv[a], psi[a], save[a])
+        for y in range(base[0]):
+            w = sites[0][y]
+            X = Lenv[w]
+            for p in range(lens[0]):
+                X = _lstep(X, psi[w + p], _apply(O[0][p], save[w + p]))
+            res = float(np.sum(X * Renv[w + lens[0] - 1]))
+            omega[(y,) + tuple(bpos[1:])] = res
+            if F[0] is not None:
+                save[w] = _apply(F[0], save[w])
+            if y + 1 < len(sites[0]):
+                for r in range(w, sites[0][y + 1] + 1):
+                    if r < L - 1:
+                        Lenv[r + 1] = _lstep(Lenv[r], psi[r], save[r])
+        # position_incrementer!: the first index is exhausted, carry into the next ones
+        bpos[0] = base[0]
+        k = 0
+        while k < n - 1 and bpos[k] >= base[k]:
+            bpos[k] = 0
+            bpos[k + 1] += 1
+            k += 1
+        if n == 1:
+            break
+    return omega
+
+
+def ed_correlation_n(v, L, d, ops, sites=None, trail=None):
+    """omega[p_1, ..., p_n] = <v| prod_s O(s) |v> from the full state vector (small L only), with
+    O(s) = A_1(s) A_2(s) ... A_n(s), A_g(s) = trail_g if s lies left of operator g's first site,
+    operator g's factor on its sites, the identity elsewhere (the order in which the reference
+    applies them to the ket). Not normalised."""
+    O = _oplists(ops)
+    n = len(O)
+    lens = [len(o) for o in O]
+    if sites is None:
+        sites = [list(range(L)) for _ in range(n)]
+    F = _trails(trail, n, d)
+    base = [len(sites[k]) - (lens[k] - 1) for k in range(n)]
+    Id = np.eye(d)
+    V = np.asarray(v, dtype=float).reshape((d,) * L)
+    omega = np.zeros(base)
+    for idx in np.ndindex(*base):
+        pos = [sites[g][idx[g]] for g in range(n)]
+        W = V
+        for s in range(L):
+            M = Id
+            for g in range(n):
+                if s < pos[g]:
+                    A = F[g] if F[g] is not None else Id
+                elif s < pos[g] + lens[g]:
+                    A = O[g][s - pos[g]]
+                else:
+                    A = Id
+                M = M @ A
+            if not np.array_equal(M, Id):
+                W = np.moveaxis(np.tensordot(M, W, axes=(1, s)), 0, s)
+        omega[idx] = float(np.sum(V * W))
+    return omega

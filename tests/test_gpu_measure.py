@@ -149,3 +149,72 @@ def test_expect_of_an_operator_product(dmrgb, ctx):
     E = dmrgb.dmrg(gs, qmpo, m=64, sweeps=4, cutoff=1e-12, ctx=ctx)
     var = dmrgb.expect(gs, qmpo, qmpo, ctx=ctx) - dmrgb.expect(gs, qmpo, ctx=ctx) ** 2
     assert -1e-9 <= var <= 1e-6, (E, var)
+
+
+# ------------------------------------------------------------------ correlation (n-point)
+
+def _corr_cases():
+    Sp, Sm, Sz, _, Sx, _, _ = mo.spin_ops()
+    F = np.diag([1.0, -1.0])
+    return [((Sz,), None), ((Sp, Sm), None), ((Sz, Sx), F), (([Sp, Sz], Sm), None),
+            ((Sz, [Sm, Sp]), F), ((Sz, Sz, Sz), None), ((Sp, Sz, Sm), F)]
+
+
+@pytest.mark.parametrize("case", range(7))
+def test_correlation_n_dense_random(dmrgb, ctx, case):
+    """``correlation`` (``lib/MPO_MPS/correlation.jl:73-237``) on a dense random unnormalised
+    state against the full-vector definition: one, two and three operators, trails, multi-site
+    operators in first and second place (relative 1e-12 of the largest entry)."""
+    L, d = 8, 2
+    psi = dmrgb.randMPS(2, L, 6, seed=12, oc=2)
+    ops, tr = _corr_cases()[case]
+    omega = dmrgb.correlation(psi, *ops, trail=() if tr is None else tr, ctx=ctx)
+    ref = om.ed_correlation_n(om.mps_vector(_dense(psi)), L, d, ops, trail=tr)
+    assert omega.shape == ref.shape
+    assert np.max(np.abs(omega - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert psi.oc == 2
+
+
+def test_correlation_n_u1_equals_reference_loop_and_correlation_matrix(dmrgb, ctx):
+    """On the U(1) state a DMRG run leaves, two operators: the device equals the oracle's
+    restatement of the reference's loop, and (normalised state) the correlation matrix, as the
+    reference's own test checks (``test/MPmeas_test.jl:335-341``); S+ S+ changes the charge by 2
+    and gives exact zeros."""
+    L = 12
+    mpo = dmrgb.makeMPO(dmrgb.heisenbergMPO, 2, L).with_qn(dmrgb.SPIN_QN)
+    psi = dmrgb.neelMPS(L)
+    dmrgb.dmrg(psi, mpo, m=48, sweeps=4, cutoff=1e-12, ctx=ctx)
+    Sp, Sm, Sz, _, _, _, _ = mo.spin_ops()
+    dense = _dense(psi)
+    for ops in [(Sp, Sm), (Sz, Sz), (Sm, Sp)]:
+        omega = dmrgb.correlation(psi, *ops, ctx=ctx)
+        assert np.max(np.abs(omega - om.correlation(dense, ops))) <= 1e-10
+    nrm = float(np.sum(om.mps_vector(dense) ** 2))
+    M = dmrgb.correlation(psi, Sp, Sm, ctx=ctx) / nrm
+    assert np.max(np.abs(M - dmrgb.correlationmatrix(psi, Sp, Sm, ctx=ctx))) <= 1e-10
+    assert np.array_equal(dmrgb.correlation(psi, Sp, Sp, ctx=ctx), np.zeros((L, L)))
+
+
+def test_correlation_n_hubbard_trail_and_site_lists(dmrgb, ctx):
+    """Hubbard U(1)xU(1) after DMRG (d = 4): the fermion pair with its Jordan-Wigner trail
+    against the full-vector definition, with the default sites and with explicit 1-based site
+    lists (entries indexed by their place in each list)."""
+    L, d = 6, 4
+    start = mo.hubbard_half_filling_mps(L)
+    mpo = dmrgb.makeMPO(dmrgb.hubbardMPO, d, L).with_qn(dmrgb.HUBBARD_QN)
+    psi = dmrgb.MPS([np.array(a) for a in start], oc=0)
+    dmrgb.dmrg(psi, mpo, m=64, sweeps=4, cutoff=1e-10, ctx=ctx)
+    Cup, Cdn, F, Nup, _, _, _, _ = mo.fermion_ops()
+    v = om.mps_vector(_dense(psi))
+    ops = (Cup.T, Cup)
+    omega = dmrgb.correlation(psi, *ops, trail=F, ctx=ctx)
+    ref = om.ed_correlation_n(v, L, d, ops, trail=F)
+    assert np.max(np.abs(omega - ref)) <= 1e-10
+    sites = ([2, 4, 5], [1, 3, 6])
+    omega = dmrgb.correlation(psi, Cdn.T, Cdn, Nup, sites=(sites[0], sites[1], [2, 6]),
+                              trail=(F, F, np.eye(d)), ctx=ctx)
+    ref = om.ed_correlation_n(v, L, d, (Cdn.T, Cdn, Nup),
+                              sites=[[s - 1 for s in sites[0]], [s - 1 for s in sites[1]], [1, 5]],
+                              trail=(F, F, np.eye(d)))
+    assert omega.shape == (3, 3, 2)
+    assert np.max(np.abs(omega - ref)) <= 1e-10
