@@ -120,6 +120,8 @@ SIGNATURES = {
                                 _DP, _DP, _DP, _DP]),
     "dmrg_correlationmatrix": (C.c_int, [_P, C.c_int, _DP, _DP, _DP, _DP]),
     "dmrg_correlation": (C.c_int, [_P, C.c_int, C.c_int, _IP, _DP, _IP, _IP, _DP, _DP]),
+    "dmrg_mps_download_all_blocks": (C.c_int, [_P, _DP, C.POINTER(C.c_int64)]),
+    "dmrg_bonds_info": (C.c_int, [_P, _IP, _IP, _IP]),
     "dmrg_heff_apply": (C.c_int, [_P, _P, C.c_int, _DP, _DP, C.c_int]),
     "dmrg_heff_apply_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
     "dmrg_twosite_dims": (C.c_int, [_P, _P, C.c_int, _IP]),

@@ -65,6 +65,20 @@ void upload_site(dmrg_ctx* c, DBuf& buf, const std::vector<double>& h) {
   cuda_check(cudaStreamSynchronize(c->stream), "MPS upload sync");
 }
 
+// The context's pinned staging buffer, at least n doubles (its previous user has synchronised).
+double* stage(dmrg_ctx* c, size_t n) {
+  if (n > c->h_stage_cap) {
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_cap = 0;
+    const size_t cap = std::max({n, 2 * c->h_stage_cap, size_t(1) << 20});   // rare regrowth
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&c->h_stage), cap * sizeof(double)),
+               "pinned staging");
+    c->h_stage_cap = cap;
+  }
+  return c->h_stage;
+}
+
 dmrg_state* new_state(dmrg_ctx* c, const dmrg_mpo* mpo, int oc) {
   const int L = mpo->L;
   if (oc < 0 || oc >= L) fail(DMRG_ERR_ARG, "orthogonality centre out of range");
@@ -184,6 +198,7 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaFree(c->d_status);
   cudaFreeHost(c->h_scal);
   if (c->h_lam) cudaFreeHost(c->h_lam);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
   cudaFree(c->d_flags);
   cudaFreeHost(c->h_flags);
   cudaFree(c->d_floors);
@@ -417,11 +432,24 @@ int dmrg_mps_upload_blocks(dmrg_ctx* c, const dmrg_mpo* mpo, const int* nsec,
             fail(DMRG_ERR_ARG, "sector charges must be strictly increasing");
         }
       }
+      // every site through the pinned staging buffer, one synchronisation at the end
+      size_t total = 0;
       for (int i = 0; i < L; ++i) {
         st->lay[i] = make_site_layout(st->bond[i], mpo->site[i].p, st->bond[i + 1]);
-        std::vector<double> h(data[i], data[i] + st->lay[i].size);
-        upload_site(c, st->A[i], h);
+        total += size_t(st->lay[i].size);
       }
+      double* h = stage(c, std::max<size_t>(total, 1));
+      size_t at = 0;
+      for (int i = 0; i < L; ++i) {
+        const size_t n = size_t(st->lay[i].size);
+        if (n) std::memcpy(h + at, data[i], n * sizeof(double));
+        dalloc(c, st->A[i], std::max<int64_t>(int64_t(n), 1));
+        if (n)
+          cuda_check(cudaMemcpyAsync(st->A[i].p, h + at, n * sizeof(double),
+                                     cudaMemcpyHostToDevice, c->stream), "MPS upload");
+        at += n;
+      }
+      cuda_check(cudaStreamSynchronize(c->stream), "MPS upload sync");
     } catch (...) {
       for (auto& b : st->A) dfree(c, b);
       delete st;
@@ -651,6 +679,44 @@ int dmrg_mps_download_blocks(dmrg_state* st, int site, double* out) {
                                cudaMemcpyDeviceToHost, c->stream), "MPS download");
     cuda_check(cudaStreamSynchronize(c->stream), "MPS download sync");
   });
+}
+
+int dmrg_mps_download_all_blocks(dmrg_state* st, double* out, int64_t* sizes) {
+  if (!st) return DMRG_ERR_ARG;
+  dmrg_ctx* c = st->ctx;
+  return guarded(c, [&] {
+    size_t total = 0;
+    for (int i = 0; i < st->L; ++i) {
+      if (sizes) sizes[i] = st->lay[i].size;
+      total += size_t(st->lay[i].size);
+    }
+    if (!out) return;
+    set_device(c);
+    size_t at = 0;
+    for (int i = 0; i < st->L; ++i) {
+      const size_t n = size_t(st->lay[i].size);
+      if (n)
+        cuda_check(cudaMemcpyAsync(out + at, st->A[i].p, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream), "MPS download");
+      at += n;
+    }
+    cuda_check(cudaStreamSynchronize(c->stream), "MPS download sync");
+  });
+}
+
+int dmrg_bonds_info(const dmrg_state* st, int* nsec, int* qn, int* dims) {
+  if (!st || !nsec) return DMRG_ERR_ARG;
+  size_t k = 0;
+  for (int b = 0; b <= st->L; ++b) {
+    const Bond& B = st->bond[b];
+    nsec[b] = B.nsec();
+    for (int j = 0; j < B.nsec(); ++j, ++k) {
+      if (dims) dims[k] = B.dim[j];
+      if (qn)
+        for (int a = 0; a < st->nsym; ++a) qn[k * st->nsym + a] = B.q[j].v[a];
+    }
+  }
+  return DMRG_OK;
 }
 
 int dmrg_mps_download(dmrg_state* st, int site, double* out, int* mlo, int* mro) {

@@ -201,6 +201,8 @@ struct dmrg_ctx {
   int* d_status = nullptr;
   double* h_scal = nullptr;      // pinned mirror of d_scal
   double* h_lam = nullptr;       // pinned eigenvalue download buffer (grow-only)
+  double* h_stage = nullptr;     // pinned staging of MPS uploads (grow-only, idle
+  size_t h_stage_cap = 0;        // between calls: every user synchronises before returning)
   size_t h_lam_cap = 0;
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> tev;  // phase-timing events, reused across sweeps

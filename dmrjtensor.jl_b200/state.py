@@ -314,6 +314,37 @@ class DeviceState:
         check(lib().dmrg_bond_info(self.h, b, C.byref(n), q, dd), self.ctx.h)
         return [(tuple(q[k * ns:(k + 1) * ns]), dd[k]) for k in range(n.value)]
 
+    def bonds(self):
+        """Every bond's sectors [(charges, dim), ...], bond 0 first (one call)."""
+        L, ns = self.L, self.dmpo.nsym
+        nsec = np.zeros(L + 1, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        check(lib().dmrg_bonds_info(self.h, nsec.ctypes.data_as(ip), None, None), self.ctx.h)
+        tot = int(nsec.sum())
+        q = np.zeros(max(tot * ns, 1), dtype=np.int32)
+        dd = np.zeros(max(tot, 1), dtype=np.int32)
+        check(lib().dmrg_bonds_info(self.h, nsec.ctypes.data_as(ip), q.ctypes.data_as(ip),
+                                    dd.ctypes.data_as(ip)), self.ctx.h)
+        ql, dl = q.tolist(), dd.tolist()
+        out, k = [], 0
+        for b in range(L + 1):
+            out.append([(tuple(ql[(k + j) * ns:(k + j + 1) * ns]), dl[k + j])
+                        for j in range(int(nsec[b]))])
+            k += int(nsec[b])
+        return out
+
+    def all_site_blocks(self):
+        """Every site's blocks (one call, one device synchronisation)."""
+        sizes = np.zeros(self.L, dtype=np.int64)
+        sp = C.POINTER(C.c_int64)
+        check(lib().dmrg_mps_download_all_blocks(self.h, None, sizes.ctypes.data_as(sp)),
+              self.ctx.h)
+        flat = np.empty(max(int(sizes.sum()), 1))
+        check(lib().dmrg_mps_download_all_blocks(self.h, flat.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 sizes.ctypes.data_as(sp)), self.ctx.h)
+        cuts = np.cumsum(sizes)[:-1]
+        return [a.copy() for a in np.split(flat[:int(sizes.sum())], cuts)]
+
     def site_blocks(self, i):
         n = C.c_int64()
         check(lib().dmrg_site_size(self.h, i, C.byref(n)), self.ctx.h)
@@ -334,8 +365,8 @@ class DeviceState:
         """Write the device MPS back into ``psi`` (block form when charges are present)."""
         use_blocks = (self.dmpo.nsym > 0) if blocks is None else blocks
         if use_blocks:
-            psi.sectors = [self.bond(b) for b in range(self.L + 1)]
-            psi.blocks = [self.site_blocks(i) for i in range(self.L)]
+            psi.sectors = self.bonds()
+            psi.blocks = self.all_site_blocks()
             psi.phys = [list(map(tuple, self.dmpo.mpo.qlabels[i])) if self.dmpo.nsym
                         else [()] * self.dmpo.d[i] for i in range(self.L)]
             psi.tensors = None

@@ -185,6 +185,14 @@ DMRG_API int dmrg_bond_info(const dmrg_state* st, int bond, int* nsec, int* qn, 
 /* Number of doubles of site i in block form. */
 DMRG_API int dmrg_site_size(const dmrg_state* st, int site, int64_t* n_blocks_doubles);
 DMRG_API int dmrg_mps_download_blocks(dmrg_state* st, int site, double* out);
+/* Every site's blocks at once, back to back (site 0 first), with one synchronisation; sizes
+ * (L entries, optional) gets each site's count in doubles, and a NULL
+ * `out` only fills sizes. No counterpart in the reference: the download side of the state copy
+ * that dmrg() makes (the per-site dmrg_mps_download_blocks, batched). */
+DMRG_API int dmrg_mps_download_all_blocks(dmrg_state* st, double* out, int64_t* sizes);
+/* Every bond's sectors at once: nsec[b] for b = 0..L, and (optional) the sectors' charges
+ * (nsym ints each) and dims, bond 0 first. The batched form of dmrg_bond_info. */
+DMRG_API int dmrg_bonds_info(const dmrg_state* st, int* nsec, int* qn, int* dims);
 /* Dense-equivalent download of site i: out [ml, d, mr] column-major in the grouped bond order;
  * ml/mr receive the bond sizes (out may be NULL to query them). */
 DMRG_API int dmrg_mps_download(dmrg_state* st, int site, double* out, int* ml, int* mr);

@@ -181,8 +181,9 @@ def test_functional_env_updates_match_oracle(dmrgb, ctx):
 def test_block_upload_round_trip_at_a_4096_bond(dmrgb, ctx):
     """The block-form upload (dmrg_mps_upload_blocks, what the Julia binding sends for a Qtens
     MPS) at a bond of dimension 4096 in three U(1) sectors, the size of the 4x16 cylinder's largest
-    bond: the blocks come back bit for bit, and the environments built from them agree with the
-    dense-equivalent contraction of the same state."""
+    bond: the blocks come back bit for bit, through the per-site and the batched downloads, and
+    the environments built from them agree with the dense-equivalent contraction of the same
+    state."""
     rng = np.random.default_rng(4)
     sectors = [[((0,), 1)], [((-1,), 1), ((1,), 1)], [((-2,), 1000), ((0,), 2096), ((2,), 1000)],
                [((-1,), 1), ((1,), 1)], [((0,), 1)]]
@@ -204,6 +205,10 @@ def test_block_upload_round_trip_at_a_4096_bond(dmrgb, ctx):
     assert dev.bond(2) == sectors[2]
     for i in range(4):
         assert np.array_equal(dev.site_blocks(i), blocks[i])
+    # the batched downloads (every bond / every site in one call) give the same
+    assert dev.bonds() == [dev.bond(b) for b in range(5)] == sectors
+    for a, b in zip(dev.all_site_blocks(), blocks):
+        assert np.array_equal(a, b)
     dev.env_build()
     dense = [dev.site_dense(i) for i in range(4)]
     W = [np.asarray(w) for w in mpo.W]
