@@ -455,8 +455,9 @@ double measure_expect(dmrg_state* st, const dmrg_mpo* H, double* flops);
 void measure_correlation_n(dmrg_state* st, int d, int n, const int* lens, const double* ops,
                            const int* nsites, const int* sites, const double* trails,
                            double* omega, double* flops);
+// (norm, optional: receives <psi|psi>, by which rho was divided)
 void measure_correlation(dmrg_state* st, int d, const double* Cc, const double* Ca,
-                         const double* F, double* rho, double* flops);
+                         const double* F, double* rho, double* flops, double* norm = nullptr);
 
 // ---- eigensolves (engine_eig.cpp)
 // Tridiagonal-path eigenvalues of every task (n <= SYEVT_MID_NMAX; small and mid-size blocks in

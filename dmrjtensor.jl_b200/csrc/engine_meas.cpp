@@ -262,7 +262,7 @@ double measure_expect(dmrg_state* st, const dmrg_mpo* H, double* flops) {
 }
 
 void measure_correlation(dmrg_state* st, int d, const double* Cc_, const double* Ca_,
-                         const double* F_, double* rho, double* flops) {
+                         const double* F_, double* rho, double* flops, double* norm_out) {
   dmrg_ctx* c = st->ctx;
   const int L = st->L;
   for (int i = 0; i < L; ++i)
@@ -419,6 +419,7 @@ void measure_correlation(dmrg_state* st, int d, const double* Cc_, const double*
     const double nrm = h[size_t(L) * L];
     if (!(nrm > 0.0) || !std::isfinite(nrm))
       fail(DMRG_ERR_STATE, "correlationmatrix: <psi|psi> is not positive");
+    if (norm_out) *norm_out = nrm;
     for (int i = 0; i < L; ++i) {
       rho[i + size_t(i) * L] = h[i + size_t(i) * L] / nrm;
       for (int j = i + 1; j < L; ++j) {
@@ -474,6 +475,35 @@ void measure_correlation_n(dmrg_state* st, int d, int n, const int* lens, const 
   }
   const int base1 = int(pos[0].size()), len1 = lens[0];
   const int64_t ncol = total / base1;
+
+  // Two single-site operators over every site with no trail, or with one trail F, F F = I (a
+  // Jordan-Wigner string): every entry is one of the batched correlation matrix's. For p1 <= p2
+  // O(s) is F F = I left of p1, O1 F at p1, F between, O2 at p2: row p1, column p2 of
+  // correlationmatrix(O1, O2; F); for p1 > p2 it is F O2 = (F O2 F) F at p2, F between, O1 at
+  // p1: row p2, column p1 of correlationmatrix(F O2 F, O1; F). Both times <psi|psi>.
+  bool every_site = n == 2 && lens[0] == 1 && lens[1] == 1 && nsites[0] == L && nsites[1] == L;
+  for (int g = 0; every_site && g < 2; ++g)
+    for (int y = 0; y < L; ++y) every_site = every_site && pos[g][y] == y;
+  const bool same_trail = F[0] == F[1];
+  bool involution = F[0].empty();
+  if (!involution && same_trail) {
+    const std::vector<double> FF = matmul(F[0], F[0], d);
+    involution = true;
+    for (size_t e = 0; e < dd; ++e) involution = involution && std::fabs(FF[e] - Id[e]) <= 1e-14;
+  }
+  if (every_site && same_trail && involution) {
+    const double* Fp = F[0].empty() ? nullptr : F[0].data();
+    std::vector<double> up(size_t(L) * L), lo(size_t(L) * L);
+    double nrm = 0.0, f1 = 0.0, f2 = 0.0;
+    measure_correlation(st, d, O[0][0].data(), O[1][0].data(), Fp, up.data(), &f1, &nrm);
+    const std::vector<double> C2 = F[0].empty() ? O[1][0] : matmul(matmul(F[0], O[1][0], d), F[0], d);
+    measure_correlation(st, d, C2.data(), O[0][0].data(), Fp, lo.data(), &f2, nullptr);
+    for (int p2 = 0; p2 < L; ++p2)
+      for (int p1 = 0; p1 < L; ++p1)
+        omega[p1 + size_t(L) * p2] = nrm * (p1 <= p2 ? up[p1 + size_t(L) * p2] : lo[p2 + size_t(L) * p1]);
+    if (flops) *flops = f1 + f2;
+    return;
+  }
   if (ncol * int64_t(L) > (int64_t(1) << 22))
     fail(DMRG_ERR_BUDGET, "correlation: too many positions of operators 2..n for this chain");
   const QN zero;
