@@ -759,8 +759,7 @@ int dmrg_env_build(dmrg_state* st, const dmrg_mpo* mpo) {
     set_device(c);
     free_envs(st);
     env_boundaries(st);
-    for (int i = 0; i < st->oc; ++i) lupdate(st, i, nullptr);
-    for (int i = st->L - 1; i > st->oc; --i) rupdate(st, i, nullptr);
+    build_envs(st);
     cuda_check(cudaStreamSynchronize(c->stream), "env build sync");
     st->env_built = true;
     st->have_last = false;

@@ -440,6 +440,9 @@ void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int w
                     double* env_out);
 
 void env_boundaries(dmrg_state* st);
+// Lenv[1..oc] and Renv[oc..L-2] from the boundaries (env_boundaries first): every step planned,
+// one descriptor upload, then the launches back to back (FP64, as lupdate / rupdate).
+void build_envs(dmrg_state* st);
 void lupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP64);
 void rupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP64);
 
