@@ -65,19 +65,6 @@ void upload_site(dmrg_ctx* c, DBuf& buf, const std::vector<double>& h) {
   cuda_check(cudaStreamSynchronize(c->stream), "MPS upload sync");
 }
 
-// The context's pinned staging buffer, at least n doubles (its previous user has synchronised).
-double* stage(dmrg_ctx* c, size_t n) {
-  if (n > c->h_stage_cap) {
-    if (c->h_stage) cudaFreeHost(c->h_stage);
-    c->h_stage = nullptr;
-    c->h_stage_cap = 0;
-    const size_t cap = std::max({n, 2 * c->h_stage_cap, size_t(1) << 20});   // rare regrowth
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&c->h_stage), cap * sizeof(double)),
-               "pinned staging");
-    c->h_stage_cap = cap;
-  }
-  return c->h_stage;
-}
 
 dmrg_state* new_state(dmrg_ctx* c, const dmrg_mpo* mpo, int oc) {
   const int L = mpo->L;
@@ -198,7 +185,6 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaFree(c->d_status);
   cudaFreeHost(c->h_scal);
   if (c->h_lam) cudaFreeHost(c->h_lam);
-  if (c->h_stage) cudaFreeHost(c->h_stage);
   cudaFree(c->d_flags);
   cudaFreeHost(c->h_flags);
   cudaFree(c->d_floors);
@@ -432,22 +418,15 @@ int dmrg_mps_upload_blocks(dmrg_ctx* c, const dmrg_mpo* mpo, const int* nsec,
             fail(DMRG_ERR_ARG, "sector charges must be strictly increasing");
         }
       }
-      // every site through the pinned staging buffer, one synchronisation at the end
-      size_t total = 0;
+      // every site straight from the caller's arrays (a copy from pageable memory returns once
+      // the driver has staged it), one synchronisation at the end
       for (int i = 0; i < L; ++i) {
         st->lay[i] = make_site_layout(st->bond[i], mpo->site[i].p, st->bond[i + 1]);
-        total += size_t(st->lay[i].size);
-      }
-      double* h = stage(c, std::max<size_t>(total, 1));
-      size_t at = 0;
-      for (int i = 0; i < L; ++i) {
         const size_t n = size_t(st->lay[i].size);
-        if (n) std::memcpy(h + at, data[i], n * sizeof(double));
         dalloc(c, st->A[i], std::max<int64_t>(int64_t(n), 1));
         if (n)
-          cuda_check(cudaMemcpyAsync(st->A[i].p, h + at, n * sizeof(double),
+          cuda_check(cudaMemcpyAsync(st->A[i].p, data[i], n * sizeof(double),
                                      cudaMemcpyHostToDevice, c->stream), "MPS upload");
-        at += n;
       }
       cuda_check(cudaStreamSynchronize(c->stream), "MPS upload sync");
     } catch (...) {
@@ -759,7 +738,8 @@ int dmrg_env_build(dmrg_state* st, const dmrg_mpo* mpo) {
     set_device(c);
     free_envs(st);
     env_boundaries(st);
-    build_envs(st);
+    for (int i = 0; i < st->oc; ++i) lupdate(st, i, nullptr);
+    for (int i = st->L - 1; i > st->oc; --i) rupdate(st, i, nullptr);
     cuda_check(cudaStreamSynchronize(c->stream), "env build sync");
     st->env_built = true;
     st->have_last = false;

@@ -201,8 +201,6 @@ struct dmrg_ctx {
   int* d_status = nullptr;
   double* h_scal = nullptr;      // pinned mirror of d_scal
   double* h_lam = nullptr;       // pinned eigenvalue download buffer (grow-only)
-  double* h_stage = nullptr;     // pinned staging of MPS uploads (grow-only, idle
-  size_t h_stage_cap = 0;        // between calls: every user synchronises before returning)
   size_t h_lam_cap = 0;
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> tev;  // phase-timing events, reused across sweeps
@@ -440,9 +438,6 @@ void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int w
                     double* env_out);
 
 void env_boundaries(dmrg_state* st);
-// Lenv[1..oc] and Renv[oc..L-2] from the boundaries (env_boundaries first): every step planned,
-// one descriptor upload, then the launches back to back (FP64, as lupdate / rupdate).
-void build_envs(dmrg_state* st);
 void lupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP64);
 void rupdate(dmrg_state* st, int i, double* flops, int precision = DMRG_PREC_FP64);
 

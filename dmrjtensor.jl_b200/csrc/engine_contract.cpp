@@ -557,56 +557,6 @@ void env_step_dense(dmrg_ctx* c, bool left, int ml, int d, int mr, int wl, int w
   dfree(c, dA); dfree(c, dB); dfree(c, din); dfree(c, dout);
 }
 
-void build_envs(dmrg_state* st) {
-  dmrg_ctx* c = st->ctx;
-  const int L = st->L, oc = st->oc;
-  if (!st->Lvalid[0] || !st->Rvalid[L - 1]) fail(DMRG_ERR_STATE, "environment boundaries not set");
-  // every step planned (and tuned) first, one descriptor upload, then the launches back to back:
-  // the same plans and launches as lupdate / rupdate step by step
-  std::vector<StepPlan> lp(size_t(std::max(oc, 0)));
-  std::vector<StepPlan> rp(size_t(std::max(L - 1 - oc, 0)));   // rp[k]: site L-1-k
-  Upload u;
-  int64_t t1 = 1, t2 = 1;
-  for (int i = 0; i < oc; ++i) {
-    plan_left_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i],
-                   i ? lp[i - 1].out : st->Llay[0], lp[i]);
-    tune_gemm(c, lp[i].g1);
-    tune_gemm(c, lp[i].g3);
-    put_step(u, lp[i], 0);
-    t1 = std::max(t1, lp[i].t1);
-    t2 = std::max(t2, lp[i].t2);
-  }
-  for (size_t k = 0; k < rp.size(); ++k) {
-    const int i = L - 1 - int(k);
-    plan_right_step(st->bond[i], st->bond[i + 1], st->mpo->site[i], st->lay[i],
-                    k ? rp[k - 1].out : st->Rlay[L - 1], rp[k]);
-    tune_gemm(c, rp[k].g1);
-    tune_gemm(c, rp[k].g3);
-    put_step(u, rp[k], 0);
-    t1 = std::max(t1, rp[k].t1);
-    t2 = std::max(t2, rp[k].t2);
-  }
-  if (lp.empty() && rp.empty()) return;
-  char* db = u.send(c, 2);
-  ensure(c, c->T1, t1);
-  ensure(c, c->T2, t2);
-  for (int i = 0; i < oc; ++i) {
-    st->Llay[i + 1] = lp[i].out;
-    dalloc(c, st->Lenv[i + 1], std::max<int64_t>(lp[i].out.size, 1));
-    run_step(c, lp[i], db, st->Lenv[i].p, st->Lenv[i].n, st->A[i], st->Lenv[i + 1].p,
-             st->Lenv[i + 1].n);
-    st->Lvalid[i + 1] = 1;
-  }
-  for (size_t k = 0; k < rp.size(); ++k) {
-    const int i = L - 1 - int(k);
-    st->Rlay[i - 1] = rp[k].out;
-    dalloc(c, st->Renv[i - 1], std::max<int64_t>(rp[k].out.size, 1));
-    run_step(c, rp[k], db, st->Renv[i].p, st->Renv[i].n, st->A[i], st->Renv[i - 1].p,
-             st->Renv[i - 1].n);
-    st->Rvalid[i - 1] = 1;
-  }
-}
-
 void lupdate(dmrg_state* st, int i, double* flops, int precision) {
   dmrg_ctx* c = st->ctx;
   if (i < 0 || i + 1 >= st->L) fail(DMRG_ERR_ARG, "lupdate: site out of range");
