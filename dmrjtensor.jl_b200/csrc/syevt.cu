@@ -9,7 +9,7 @@
 //     updates the next pivot column first and builds the next reflector (look-ahead). The
 //     reflector vectors are written into the strictly lower part of the caller's matrix, d/e/tau
 //     into a small per-block workspace;
-//   * all eigenvalues of T by multisection (2, 4 or 8 threads per eigenvalue as n allows, one
+//   * all eigenvalues of T by multisection (2, 3, 4 or 8 threads per eigenvalue as n allows, one
 //     Sturm count each per step) to an absolute width of 8.9e-16 ||T||, with a division-free
 //     Sturm count (see sturm_below).
 // The host then truncates globally and asks for the top-k vectors of each block.
@@ -257,15 +257,18 @@ k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
     }
   }
   __syncthreads();
-  // multisection: a group of P lanes per eigenvalue (P = 2, 4 or 8 as n allows with 256 threads)
-  // counts at the P interior points x_g = a + (g + 1) w / (P + 1) of its interval; the counts
-  // are nondecreasing in x, so the group's ballot bits read 0..01..1 and the first set bit g
-  // brackets the eigenvalue in [x_(g-1), x_g] (no bit: [x_(P-1), b]). The interval shrinks by
-  // P + 1 per step: ~32 steps for P = 2, ~22 for P = 4, ~16 for P = 8.
+  // multisection: a group of P lanes per eigenvalue (P = 2, 3, 4 or 8 as n allows with 256
+  // threads; a group never straddles a warp: for P = 3 each warp holds ten groups, lanes 30-31
+  // idle) counts at the P interior points x_g = a + (g + 1) w / (P + 1) of its interval; the
+  // counts are nondecreasing in x, so the group's ballot bits read 0..01..1 and the first set bit
+  // g brackets the eigenvalue in [x_(g-1), x_g] (no bit: [x_(P-1), b]). The interval shrinks by
+  // P + 1 per step: ~32 steps for P = 2, ~27 for P = 3, ~22 for P = 4, ~16 for P = 8.
   const double tn = fmax(fabs(s_lo), fabs(s_hi));
   const double tol = 8.9e-16 * tn;
-  const int P = n <= TE_THREADS / 8 ? 8 : (n <= TE_THREADS / 4 ? 4 : 2);
-  const int ei = tid / P, h = tid % P;
+  const int P = n <= TE_THREADS / 8 ? 8
+                : (n <= TE_THREADS / 4 ? 4 : (n <= (TE_THREADS / 32) * 10 ? 3 : 2));
+  const int ei = P == 3 ? (lane < 30 ? warp * 10 + lane / 3 : n) : tid / P;
+  const int h = P == 3 ? lane % 3 : tid % P;
   const int target = n - 1 - ei;           // i-th largest = (n-1-i)-th smallest
   const double frac = 1.0 / double(P + 1);
   bool done = ei >= n;
