@@ -12,6 +12,7 @@
 #include <utility>
 
 #include "kernels.cuh"
+#include "launch.cuh"
 
 namespace dmrg {
 namespace {
@@ -50,6 +51,7 @@ __global__ void __launch_bounds__(THREADS)
 k_gemm_f64(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
            const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
            int total_tiles) {
+  grid_entry();
   using TL = F64Tile<BM, BN>;
   constexpr int LDS_A = TL::LDS_A, LDS_B = TL::LDS_B, MI = TL::MI, NI = TL::NI;
   constexpr int A_PER = TL::A_PER, B_PER = TL::B_PER;
@@ -168,7 +170,8 @@ void launch_variant(cudaStream_t s, const double* A, const double* B, double* C,
   constexpr size_t SM = F64Tile<BM, BN>::SMEM;
   raise_smem_limit(reinterpret_cast<const void*>(k_gemm_f64<BM, BN, TA, TB>), SM);
   int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_f64<BM, BN, TA, TB><<<grid, THREADS, SM, s>>>(A, B, C, tasks, ntasks, segs, total_tiles);
+  launch_k(k_gemm_f64<BM, BN, TA, TB>, grid, THREADS, SM, s, A, B, C, tasks, ntasks, segs,
+           total_tiles);
   count_launch();
 }
 

@@ -38,6 +38,7 @@
 // Both forms stage the same split planes and issue the same MMAs in the same order, so their
 // results are bit-identical.
 #include "kernels.cuh"
+#include "launch.cuh"
 
 namespace dmrg {
 namespace {
@@ -267,6 +268,7 @@ __global__ void __launch_bounds__(TT, 3)
 k_gemm_split(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
              const GemmTask* __restrict__ tasks, int ntasks, const GemmSeg* __restrict__ segs,
              int total_tiles, int* err) {
+  grid_entry();
   using TL = Tile<F>;
   constexpr int TBN = TL::BN, KQ = TL::KQ, QE = F::QE;
   constexpr int A_BYTES = TL::A_BYTES, B_BYTES = TL::B_BYTES;
@@ -464,6 +466,7 @@ template <class F>
 __global__ void __launch_bounds__(PACK_THREADS)
 k_pack_images(const double* __restrict__ x, unsigned char* __restrict__ img,
               const ImgPanel* __restrict__ panels, int npanels, int64_t total_chunks, int R) {
+  grid_entry();
   const int plane = R * IK * F::EB, units = R * (IK / F::QE);
   for (int64_t ch = blockIdx.x; ch < total_chunks; ch += gridDim.x) {
     int lo = 0, hi = npanels - 1;
@@ -503,6 +506,7 @@ k_pack_mix_images(const double* __restrict__ x, unsigned char* __restrict__ img,
                   const ImgPanel* __restrict__ panels, const int2* __restrict__ ranges,
                   const MixCover* __restrict__ covers, const MixTerm* __restrict__ terms,
                   int npanels, int64_t total_chunks, int R) {
+  grid_entry();
   constexpr int QE = F::QE;
   const int plane = R * IK * F::EB, units = R * (IK / QE);
   for (int64_t ch = blockIdx.x; ch < total_chunks; ch += gridDim.x) {
@@ -598,6 +602,7 @@ k_gemm_img(const unsigned char* __restrict__ imgA, const unsigned char* __restri
            double* __restrict__ C, const GemmTask* __restrict__ tasks, int ntasks,
            const GemmSeg* __restrict__ segs, const SegImg* __restrict__ simg, int total_tiles,
            int* err) {
+  grid_entry();
   using I = Img<F, BN>;
   constexpr int S = I::STAGES;
   extern __shared__ unsigned char smraw[];
@@ -763,8 +768,8 @@ void launch_variant(cudaStream_t s, const double* A, const double* B, double* C,
                     int grid_cap, int* err) {
   raise_smem_limit(reinterpret_cast<const void*>(k_gemm_split<F, TA, TB>), Tile<F>::SMEM);
   const int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_split<F, TA, TB><<<grid, TT, Tile<F>::SMEM, s>>>(A, B, C, tasks, ntasks, segs,
-                                                          total_tiles, err);
+  launch_k(k_gemm_split<F, TA, TB>, grid, TT, Tile<F>::SMEM, s, A, B, C, tasks, ntasks, segs,
+           total_tiles, err);
   count_launch();
 }
 
@@ -786,7 +791,7 @@ template <class F>
 void launch_pack(cudaStream_t s, const double* x, unsigned char* img, const ImgPanel* panels,
                  int npanels, int64_t total_chunks, int rows) {
   const int grid = int(total_chunks < 4096 ? total_chunks : 4096);
-  k_pack_images<F><<<grid, PACK_THREADS, 0, s>>>(x, img, panels, npanels, total_chunks, rows);
+  launch_k(k_pack_images<F>, grid, PACK_THREADS, 0, s, x, img, panels, npanels, total_chunks, rows);
   count_launch();
 }
 
@@ -795,8 +800,8 @@ void launch_pack_mix(cudaStream_t s, const double* x, unsigned char* img, const 
                      const int2* ranges, const MixCover* covers, const MixTerm* terms,
                      int npanels, int64_t total_chunks, int rows) {
   const int grid = int(total_chunks < 4096 ? total_chunks : 4096);
-  k_pack_mix_images<F><<<grid, PACK_THREADS, 0, s>>>(x, img, panels, ranges, covers, terms,
-                                                     npanels, total_chunks, rows);
+  launch_k(k_pack_mix_images<F>, grid, PACK_THREADS, 0, s, x, img, panels, ranges, covers, terms,
+           npanels, total_chunks, rows);
   count_launch();
 }
 
@@ -807,8 +812,8 @@ void launch_img(cudaStream_t s, const unsigned char* imgA, const unsigned char* 
   using I = Img<F, BN>;
   raise_smem_limit(reinterpret_cast<const void*>(k_gemm_img<F, BN>), I::SMEM);
   const int grid = total_tiles < grid_cap ? total_tiles : grid_cap;
-  k_gemm_img<F, BN><<<grid, IMG_THREADS, I::SMEM, s>>>(imgA, imgB, C, tasks, ntasks, segs, simg,
-                                                       total_tiles, err);
+  launch_k(k_gemm_img<F, BN>, grid, IMG_THREADS, I::SMEM, s, imgA, imgB, C, tasks, ntasks, segs,
+           simg, total_tiles, err);
   count_launch();
 }
 

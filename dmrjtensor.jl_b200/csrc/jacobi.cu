@@ -10,6 +10,7 @@
 // after a sweep without rotations. Eigenvalues are returned descending, ties by index, and the
 // matching eigenvectors overwrite the input matrix column by column.
 #include "kernels.cuh"
+#include "launch.cuh"
 
 namespace dmrg {
 namespace {
@@ -20,6 +21,7 @@ constexpr int JAC_MAX_SWEEPS = 40;
 __global__ void __launch_bounds__(JAC_THREADS)
 k_jacobi(double* __restrict__ base, const EigTask* __restrict__ tasks, int in_smem,
          int* status) {
+  grid_entry();
   const EigTask tk = tasks[blockIdx.x];
   const int n = tk.n;
   if (n <= 0) return;
@@ -175,7 +177,7 @@ void launch_jacobi(cudaStream_t s, double* base, const EigTask* tasks, int ntask
   const bool small = max_n <= 100;
   const size_t smem = jacobi_smem(max_n, small);
   raise_smem_limit(reinterpret_cast<const void*>(k_jacobi), smem);
-  k_jacobi<<<ntasks, JAC_THREADS, smem, s>>>(base, tasks, small ? 1 : 0, status);
+  launch_k(k_jacobi, ntasks, JAC_THREADS, smem, s, base, tasks, small ? 1 : 0, status);
   count_launch();
 }
 

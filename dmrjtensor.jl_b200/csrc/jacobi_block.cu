@@ -12,6 +12,7 @@
 // |a_pq| <= 1e-15 sqrt(|a_pp a_qq|), or below the larger of 1e-15 ||A||_F and 1e-14 ||S||_F,
 // the rounding level of the pivot matrix S's own rotations.
 #include "kernels.cuh"
+#include "launch.cuh"
 
 namespace dmrg {
 namespace {
@@ -32,6 +33,7 @@ __device__ __forceinline__ int64_t pidx(int x, int I, int J) {
 }
 
 __global__ void k_bj_init(double* __restrict__ base, const BlockEigGroup* __restrict__ g, int ng) {
+  grid_entry();
   const BlockEigGroup gr = g[blockIdx.y];
   const int64_t NN = int64_t(gr.N) * gr.N;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < NN;
@@ -44,6 +46,7 @@ __global__ void k_bj_init(double* __restrict__ base, const BlockEigGroup* __rest
 
 __global__ void k_bj_norm(double* __restrict__ base, const BlockEigGroup* __restrict__ g,
                           double* __restrict__ floor_out) {
+  grid_entry();
   const BlockEigGroup gr = g[blockIdx.x];
   double f = 0.0;
   const int64_t nn = int64_t(gr.n) * gr.n;
@@ -67,6 +70,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
 k_bj_solve(double* __restrict__ base, const BlockEigGroup* __restrict__ g,
            const int2* __restrict__ pairs, int npairs, int r, const double* __restrict__ floors,
            int* __restrict__ flags) {
+  grid_entry();
   const int2 pk = pairs[blockIdx.x];
   const BlockEigGroup gr = g[pk.x];
   const int nb = gr.N / B;
@@ -166,6 +170,7 @@ k_bj_solve(double* __restrict__ base, const BlockEigGroup* __restrict__ g,
 __global__ void __launch_bounds__(UPD_THREADS)
 k_bj_update(double* __restrict__ base, const BlockEigGroup* __restrict__ g,
             const int4* __restrict__ tiles, int r) {
+  grid_entry();
   const int4 tl = tiles[blockIdx.x];
   const BlockEigGroup gr = g[tl.x];
   const int nb = gr.N / B;
@@ -260,6 +265,7 @@ k_bj_update(double* __restrict__ base, const BlockEigGroup* __restrict__ g,
 // off-diagonal Frobenius norm of each padded matrix: flags[g] = 1 while off(A) > tol ||A||_F
 __global__ void k_bj_offnorm(const double* __restrict__ base, const BlockEigGroup* __restrict__ g,
                              const double* __restrict__ floors, int* __restrict__ flags) {
+  grid_entry();
   const BlockEigGroup gr = g[blockIdx.x];
   double f = 0.0;
   const int64_t NN = int64_t(gr.N) * gr.N;
@@ -284,6 +290,7 @@ __global__ void k_bj_offnorm(const double* __restrict__ base, const BlockEigGrou
 
 // Sorted eigenpairs of the converged padded problem back into the caller's layout.
 __global__ void k_bj_finish(double* __restrict__ base, const BlockEigGroup* __restrict__ g) {
+  grid_entry();
   const BlockEigGroup gr = g[blockIdx.x];
   extern __shared__ double lam[];
   int* rank = reinterpret_cast<int*>(lam + gr.n);
@@ -322,8 +329,8 @@ void launch_block_jacobi(cudaStream_t s, double* base, const BlockEigPlan& pl, i
                          int* flags_host, double* floors_dev, int* sweeps_done) {
   const int ng = pl.ngroups;
   if (ng == 0) { if (sweeps_done) *sweeps_done = 0; return; }
-  k_bj_init<<<dim3(64, ng), 256, 0, s>>>(base, pl.groups, ng);
-  k_bj_norm<<<ng, 512, 0, s>>>(base, pl.groups, floors_dev);
+  launch_k(k_bj_init, dim3(64, ng), 256, 0, s, base, pl.groups, ng);
+  launch_k(k_bj_norm, ng, 512, 0, s, base, pl.groups, floors_dev);
   count_launch(2);
   raise_smem_limit(reinterpret_cast<const void*>(k_bj_update), UPD_SMEM);
   raise_smem_limit(reinterpret_cast<const void*>(k_bj_solve), SOLVE_SMEM);
@@ -332,12 +339,12 @@ void launch_block_jacobi(cudaStream_t s, double* base, const BlockEigPlan& pl, i
   for (; sw < pl.max_sweeps; ++sw) {
     cudaMemsetAsync(flags_dev, 0, sizeof(int) * ng, s);
     for (int r = 0; r < nbmax - 1; ++r) {
-      k_bj_solve<<<pl.npairs, SOLVE_THREADS, SOLVE_SMEM, s>>>(base, pl.groups, pl.pairs, pl.npairs, r,
-                                                     floors_dev, flags_dev);
-      k_bj_update<<<pl.ntiles, UPD_THREADS, UPD_SMEM, s>>>(base, pl.groups, pl.tiles, r);
+      launch_k(k_bj_solve, pl.npairs, SOLVE_THREADS, SOLVE_SMEM, s, base, pl.groups, pl.pairs,
+               pl.npairs, r, floors_dev, flags_dev);
+      launch_k(k_bj_update, pl.ntiles, UPD_THREADS, UPD_SMEM, s, base, pl.groups, pl.tiles, r);
       count_launch(2);
     }
-    k_bj_offnorm<<<ng, 512, 0, s>>>(base, pl.groups, floors_dev, flags_dev);
+    launch_k(k_bj_offnorm, ng, 512, 0, s, base, pl.groups, floors_dev, flags_dev);
     count_launch();
     cudaMemcpyAsync(flags_host, flags_dev, sizeof(int) * ng, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -348,7 +355,7 @@ void launch_block_jacobi(cudaStream_t s, double* base, const BlockEigPlan& pl, i
   if (sweeps_done) *sweeps_done = sw;
   size_t fs = sizeof(double) * pl.maxn + sizeof(int) * pl.maxn;
   raise_smem_limit(reinterpret_cast<const void*>(k_bj_finish), fs);
-  k_bj_finish<<<ng, 512, fs, s>>>(base, pl.groups);
+  launch_k(k_bj_finish, ng, 512, fs, s, base, pl.groups);
   count_launch();
 }
 

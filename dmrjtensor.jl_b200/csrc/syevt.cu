@@ -25,6 +25,7 @@
 //   * back-transformation U = Q Z with the stored reflectors, in blocks of 8 (compact WY form
 //     I - V T V^T, LAPACK dlarft order).
 #include "kernels.cuh"
+#include "launch.cuh"
 #include "syevt_common.cuh"
 
 namespace dmrg {
@@ -71,6 +72,7 @@ __device__ void householder_col(double* __restrict__ A, int n, int k, double* __
 
 __global__ void __launch_bounds__(TE_THREADS)
 k_trid_eigvals(double* __restrict__ base, const TridTask* __restrict__ tasks) {
+  grid_entry();
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n;
   if (n <= 0) return;
@@ -315,6 +317,7 @@ __host__ __device__ size_t vec_layout_bytes(int n, int k, int nslot) {
 
 __global__ void __launch_bounds__(TV_THREADS)
 k_trid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks, int nslot) {
+  grid_entry();
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n, kk = tk.keep;
   if (n <= 0 || kk <= 0) return;
@@ -603,7 +606,7 @@ void launch_trid_eigvals(cudaStream_t s, double* base, const TridTask* tasks, in
   if (ntasks <= 0) return;
   const size_t sm = syevt_smem_vals(max_n);
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_eigvals), sm);
-  k_trid_eigvals<<<ntasks, TE_THREADS, sm, s>>>(base, tasks);
+  launch_k(k_trid_eigvals, ntasks, TE_THREADS, sm, s, base, tasks);
   count_launch();
 }
 
@@ -613,7 +616,7 @@ void launch_trid_vectors(cudaStream_t s, double* base, const TridTask* tasks, in
   const int nslot = vec_slots(max_n, max_k);
   const size_t sm = vec_layout_bytes(max_n, max_k, nslot);
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_vectors), sm);
-  k_trid_vectors<<<ntasks, TV_THREADS, sm, s>>>(base, tasks, nslot);
+  launch_k(k_trid_vectors, ntasks, TV_THREADS, sm, s, base, tasks, nslot);
   count_launch();
 }
 

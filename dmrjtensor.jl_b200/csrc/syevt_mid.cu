@@ -22,6 +22,7 @@
 // WY), one CTA per slice of 32 kept vectors with its slice of Z in shared memory, the reflectors
 // read from the matrix in global memory (every slice is independent of the others).
 #include "kernels.cuh"
+#include "launch.cuh"
 #include "syevt_common.cuh"
 
 namespace dmrg {
@@ -67,6 +68,7 @@ __device__ __forceinline__ int pk(int j, int m0) { return j * m0 - (j * (j - 1))
 template <int RM>
 __global__ void __launch_bounds__(MT, 1)
 k_trid_mid_vals(double* __restrict__ base, const TridTask* __restrict__ tasks, int mp) {
+  grid_entry();
   constexpr int CW = RM >= 16 ? 2 : 4;
   constexpr int CU = RM >= 16 ? 1 : 2;
   const TridTask tk = tasks[blockIdx.x];
@@ -456,6 +458,7 @@ int mid_vec_kg(int max_n) {
 __global__ void __launch_bounds__(MT, 1)
 k_trid_mid_vectors(double* __restrict__ base, const TridTask* __restrict__ tasks,
                    double* __restrict__ xws, int kg) {
+  grid_entry();
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n, kk = tk.keep;
   if (n < 3 || kk <= 0) return;
@@ -707,6 +710,7 @@ constexpr int BT_W = 32;
 __global__ void __launch_bounds__(MT, 1)
 k_trid_mid_backtransform(double* __restrict__ base, const TridTask* __restrict__ tasks,
                          const double* __restrict__ xws) {
+  grid_entry();
   const TridTask tk = tasks[blockIdx.x];
   const int n = tk.n, kk = tk.keep;
   const int q0 = blockIdx.y * BT_W;
@@ -838,7 +842,7 @@ void launch_vals(cudaStream_t s, double* base, const TridTask* tasks, int ntasks
   const int mp = mid_mp(max_n);
   const size_t sm = sizeof(double) * (size_t(mp) * (mp + 1) / 2 + 7 * size_t(max_n)) + 64;
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vals<RM>), sm);
-  k_trid_mid_vals<RM><<<ntasks, MT, sm, s>>>(base, tasks, mp);
+  launch_k(k_trid_mid_vals<RM>, ntasks, MT, sm, s, base, tasks, mp);
   count_launch();
 }
 
@@ -861,14 +865,14 @@ void launch_trid_mid_vectors(cudaStream_t s, double* base, const TridTask* tasks
   const int kg = max_k <= mid_vec_kg(max_n) ? max_k : 0;
   const size_t sm = mid_vec_smem_k(max_n, max_k, kg > 0);
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_vectors), sm);
-  k_trid_mid_vectors<<<ntasks, MT, sm, s>>>(base, tasks, xws, kg);
+  launch_k(k_trid_mid_vectors, ntasks, MT, sm, s, base, tasks, xws, kg);
   count_launch();
   const int nblk = max_n >= 3 ? (max_n - 2 + MID_BT_NB - 1) / MID_BT_NB : 0;
   const size_t sb = sizeof(double) * (size_t(max_n) * BT_W + 2 * MID_BT_NB * BT_W +
                                       size_t(nblk) * 64 + NW * 64);
   raise_smem_limit(reinterpret_cast<const void*>(k_trid_mid_backtransform), sb);
   const dim3 grid(ntasks, (max_k + BT_W - 1) / BT_W);
-  k_trid_mid_backtransform<<<grid, MT, sb, s>>>(base, tasks, xws);
+  launch_k(k_trid_mid_backtransform, grid, MT, sb, s, base, tasks, xws);
   count_launch();
 }
 

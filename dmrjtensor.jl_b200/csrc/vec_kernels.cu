@@ -4,6 +4,7 @@
 #include <algorithm>
 
 #include "kernels.cuh"
+#include "launch.cuh"
 
 namespace dmrg {
 namespace {
@@ -56,6 +57,7 @@ __device__ void finish_rows(const double* partial, int nb, int k, double* out, u
 __global__ void k_mix(const double* __restrict__ in, double* __restrict__ out,
                       const MixTask* __restrict__ tasks, int ntasks,
                       const MixTerm* __restrict__ terms, int total_tiles) {
+  grid_entry();
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
     int lo = 0, hi = ntasks - 1;
     while (lo < hi) {
@@ -112,6 +114,7 @@ __global__ void k_mix(const double* __restrict__ in, double* __restrict__ out,
 
 __global__ void k_copy(const double* __restrict__ src, double* __restrict__ dst,
                        const CopyTask* __restrict__ tasks, int ntasks, int total_tiles) {
+  grid_entry();
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
     int lo = 0, hi = ntasks - 1;
     while (lo < hi) {
@@ -136,6 +139,7 @@ __global__ void k_copy(const double* __restrict__ src, double* __restrict__ dst,
 __global__ void k_mdot_partial(const double* __restrict__ X, int64_t ldx, int k,
                                const double* __restrict__ y, int64_t n, double* partial,
                                double* out, unsigned* counter) {
+  grid_entry();
   double acc[MAXK];
 #pragma unroll
   for (int j = 0; j < MAXK; ++j) acc[j] = 0.0;
@@ -167,6 +171,7 @@ __global__ void k_mdot_partial(const double* __restrict__ X, int64_t ldx, int k,
 __global__ void k_pair_dot(const double* __restrict__ X, const double* __restrict__ Y,
                            const PairTask* __restrict__ tasks, int ntasks, int64_t total,
                            double* partial, double* out, unsigned* counter) {
+  grid_entry();
   double acc = 0.0;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += stride) {
@@ -196,6 +201,7 @@ __global__ void k_pair_dot(const double* __restrict__ X, const double* __restric
 __global__ void k_pair_dot_rows(const double* __restrict__ X, int64_t x_stride,
                                 const double* __restrict__ Y, const PairTask* __restrict__ tasks,
                                 int ntasks, double* out, int64_t out_stride) {
+  grid_entry();
   const double* Xr = X + int64_t(blockIdx.x) * x_stride;
   double acc = 0.0;
   for (int k = 0; k < ntasks; ++k) {
@@ -221,6 +227,7 @@ __global__ void k_pair_dot_rows(const double* __restrict__ X, int64_t x_stride,
 __global__ void k_axpby(int64_t n, double a, const double* ap, double asign,
                         const double* __restrict__ x, double b, const double* bp, double bsign,
                         double* y, int b_recip) {
+  grid_entry();
   double aa = a, bb = b;
   if (ap) aa = asign * (*ap);
   if (bp) bb = bsign * (b_recip ? 1.0 / (*bp) : (*bp));
@@ -233,6 +240,7 @@ __global__ void k_axpby(int64_t n, double a, const double* ap, double asign,
 
 __global__ void k_msub(const double* __restrict__ X, int64_t ldx, int k,
                        const double* __restrict__ c, double* y, int64_t n) {
+  grid_entry();
   double cc[MAXK];
 #pragma unroll
   for (int j = 0; j < MAXK; ++j) cc[j] = j < k ? c[j] : 0.0;
@@ -247,12 +255,14 @@ __global__ void k_msub(const double* __restrict__ X, int64_t ldx, int k,
 }
 
 __global__ void k_scale(double* x, int64_t n, double a) {
+  grid_entry();
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) x[i] *= a;
 }
 
 // x *= 1/sqrt(*nrm2) when *nrm2 > 0 (normalisation by a device-resident squared norm)
 __global__ void k_scale_rsqrt(double* x, int64_t n, const double* nrm2) {
+  grid_entry();
   const double v = *nrm2;
   const double a = (v > 0.0) ? 1.0 / sqrt(v) : 1.0;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
@@ -262,6 +272,7 @@ __global__ void k_scale_rsqrt(double* x, int64_t n, const double* nrm2) {
 // partial rows 0/1: this block's share of <x,x> and <x,y>
 __global__ void k_dot2_partial(const double* __restrict__ x, const double* __restrict__ y,
                                int64_t n, double* partial, double* out, unsigned* counter) {
+  grid_entry();
   double sxx = 0.0, sxy = 0.0;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -288,6 +299,7 @@ __global__ void k_dot2_partial(const double* __restrict__ x, const double* __res
 // of <H,H> in partial row 0.
 __global__ void k_lanczos2_orth(double* K, double* H, int64_t n, double* s, double* partial,
                                 unsigned* counter) {
+  grid_entry();
   const double nn = sqrt(s[lz::KK]);
   const double inv = 1.0 / nn;
   const double a1 = s[lz::KH] / nn;
@@ -320,6 +332,7 @@ __global__ void k_lanczos2_orth(double* K, double* H, int64_t n, double* s, doub
 // and the activity of K_{j+1}.
 __global__ void k_next_vector(const double* __restrict__ H, double* __restrict__ Kn, int64_t n,
                               double* s, int j, double betatest) {
+  grid_entry();
   const bool act = (j == 0) || (s[lz::ACT + j] != 0.0);
   const double b = sqrt(s[lz::B2 + j]);
   const bool ok = act && (b > betatest);
@@ -343,6 +356,7 @@ __global__ void k_next_vector(const double* __restrict__ H, double* __restrict__
 // coefficients of exp(tau H) applied to the normalised start vector), from the eigenpairs of T;
 // when they sum to exactly zero, the first column of I + T instead. s[EN] = lowest eigenvalue.
 __global__ void k_ritz(double* s, int kdim, double tau, int expo) {
+  grid_entry();
   __shared__ double A[MAXK * MAXK], V[MAXK * MAXK];
   const int lane = threadIdx.x;
   int m = 1;
@@ -415,6 +429,7 @@ __global__ void k_ritz(double* s, int kdim, double tau, int expo) {
 // y = sum_j c[j] * X_j (y not read), j < k, c in device memory
 __global__ void k_lincomb(const double* __restrict__ X, int64_t ldx, int k,
                           const double* __restrict__ c, double* __restrict__ y, int64_t n) {
+  grid_entry();
   double cc[MAXK];
 #pragma unroll
   for (int j = 0; j < MAXK; ++j) cc[j] = j < k ? c[j] : 0.0;
@@ -447,7 +462,7 @@ void launch_mix(cudaStream_t s, const double* in, double* out, const MixTask* ta
                 const MixTerm* terms, int total_tiles) {
   if (total_tiles <= 0) return;
   int grid = total_tiles < 4096 ? total_tiles : 4096;
-  k_mix<<<grid, 256, 0, s>>>(in, out, tasks, ntasks, terms, total_tiles);
+  launch_k(k_mix, grid, 256, 0, s, in, out, tasks, ntasks, terms, total_tiles);
   count_launch();
 }
 
@@ -455,14 +470,14 @@ void launch_copy(cudaStream_t s, const double* src, double* dst, const CopyTask*
                  int ntasks, int total_tiles) {
   if (total_tiles <= 0) return;
   int grid = total_tiles < 4096 ? total_tiles : 4096;
-  k_copy<<<grid, 256, 0, s>>>(src, dst, tasks, ntasks, total_tiles);
+  launch_k(k_copy, grid, 256, 0, s, src, dst, tasks, ntasks, total_tiles);
   count_launch();
 }
 
 void launch_mdot(cudaStream_t s, const double* X, int64_t ldx, int k, const double* y, int64_t n,
                  double* partial, double* out) {
-  k_mdot_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(X, ldx, k, y, n, partial, out,
-                                                    reduction_counter(partial));
+  launch_k(k_mdot_partial, RED_BLOCKS, RED_THREADS, 0, s, X, ldx, k, y, n, partial, out,
+           reduction_counter(partial));
   count_launch();
 }
 
@@ -470,40 +485,40 @@ void launch_axpby(cudaStream_t s, int64_t n, double a, const double* ap, double 
                   const double* x, double b, const double* bp, double bsign, double* y,
                   int b_recip) {
   if (n <= 0) return;
-  k_axpby<<<grid_for(n), RED_THREADS, 0, s>>>(n, a, ap, asign, x, b, bp, bsign, y, b_recip);
+  launch_k(k_axpby, grid_for(n), RED_THREADS, 0, s, n, a, ap, asign, x, b, bp, bsign, y, b_recip);
   count_launch();
 }
 
 void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c, double* y,
                  int64_t n) {
   if (n <= 0 || k <= 0) return;
-  k_msub<<<grid_for(n), RED_THREADS, 0, s>>>(X, ldx, k, c, y, n);
+  launch_k(k_msub, grid_for(n), RED_THREADS, 0, s, X, ldx, k, c, y, n);
   count_launch();
 }
 
 void launch_scale(cudaStream_t s, double* x, int64_t n, double a) {
   if (n <= 0) return;
-  k_scale<<<grid_for(n), RED_THREADS, 0, s>>>(x, n, a);
+  launch_k(k_scale, grid_for(n), RED_THREADS, 0, s, x, n, a);
   count_launch();
 }
 
 void launch_scale_rsqrt(cudaStream_t s, double* x, int64_t n, const double* nrm2) {
   if (n <= 0) return;
-  k_scale_rsqrt<<<grid_for(n), RED_THREADS, 0, s>>>(x, n, nrm2);
+  launch_k(k_scale_rsqrt, grid_for(n), RED_THREADS, 0, s, x, n, nrm2);
   count_launch();
 }
 
 void launch_dot2(cudaStream_t s, const double* x, const double* y, int64_t n, double* partial,
                  double* out) {
-  k_dot2_partial<<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, y, n, partial, out,
-                                                    reduction_counter(partial));
+  launch_k(k_dot2_partial, RED_BLOCKS, RED_THREADS, 0, s, x, y, n, partial, out,
+           reduction_counter(partial));
   count_launch();
 }
 
 void launch_lanczos2_orth(cudaStream_t s, double* K, double* H, int64_t n, double* scal,
                           double* partial) {
-  k_lanczos2_orth<<<RED_BLOCKS, RED_THREADS, 0, s>>>(K, H, n, scal, partial,
-                                                     reduction_counter(partial));
+  launch_k(k_lanczos2_orth, RED_BLOCKS, RED_THREADS, 0, s, K, H, n, scal, partial,
+           reduction_counter(partial));
   count_launch();
 }
 
@@ -514,8 +529,8 @@ void launch_pair_dot(cudaStream_t s, const double* X, const double* Y, const Pai
     return;
   }
   const int grid = int(std::min<int64_t>(RED_BLOCKS, (total + RED_THREADS - 1) / RED_THREADS));
-  k_pair_dot<<<grid, RED_THREADS, 0, s>>>(X, Y, tasks, ntasks, total, partial, out,
-                                          reduction_counter(partial));
+  launch_k(k_pair_dot, grid, RED_THREADS, 0, s, X, Y, tasks, ntasks, total, partial, out,
+           reduction_counter(partial));
   count_launch();
 }
 
@@ -523,25 +538,26 @@ void launch_pair_dot_rows(cudaStream_t s, const double* X, int64_t x_stride, con
                           const PairTask* tasks, int ntasks, int nrows, double* out,
                           int64_t out_stride) {
   if (nrows <= 0) return;
-  k_pair_dot_rows<<<nrows, RED_THREADS, 0, s>>>(X, x_stride, Y, tasks, ntasks, out, out_stride);
+  launch_k(k_pair_dot_rows, nrows, RED_THREADS, 0, s, X, x_stride, Y, tasks, ntasks, out,
+           out_stride);
   count_launch();
 }
 
 void launch_next_vector(cudaStream_t s, const double* H, double* Kn, int64_t n, double* scal,
                         int j, double betatest) {
-  k_next_vector<<<grid_for(n), RED_THREADS, 0, s>>>(H, Kn, n, scal, j, betatest);
+  launch_k(k_next_vector, grid_for(n), RED_THREADS, 0, s, H, Kn, n, scal, j, betatest);
   count_launch();
 }
 
 void launch_ritz(cudaStream_t s, double* scal, int kdim, double tau, bool expo) {
-  k_ritz<<<1, 32, 0, s>>>(scal, kdim, tau, expo ? 1 : 0);
+  launch_k(k_ritz, 1, 32, 0, s, scal, kdim, tau, expo ? 1 : 0);
   count_launch();
 }
 
 void launch_lincomb(cudaStream_t s, const double* X, int64_t ldx, int k, const double* c,
                     double* y, int64_t n) {
   if (n <= 0 || k <= 0) return;
-  k_lincomb<<<grid_for(n), RED_THREADS, 0, s>>>(X, ldx, k, c, y, n);
+  launch_k(k_lincomb, grid_for(n), RED_THREADS, 0, s, X, ldx, k, c, y, n);
   count_launch();
 }
 
