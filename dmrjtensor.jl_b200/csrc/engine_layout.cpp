@@ -403,10 +403,15 @@ void CopyList::add(int64_t src_off, int lds, int64_t dst_off, int ldd, int rows,
 
 char* Upload::send(dmrg_ctx* c, int slot) {
   DescSlot& s = c->slot[slot];
-  if (s.ev) cuda_check(cudaEventSynchronize(s.ev), "descriptor slot wait");
   size_t need = bytes.size() < 16 ? 16 : bytes.size();
+  // Lists that fit a kernel's parameter block travel with a launch (no staging, no copy
+  // engine); stream order keeps the slot's previous readers ahead of the write. The launch
+  // writes whole 16-byte words, so the slot must hold the rounded-up size.
+  if ((need + 15) / 16 * 16 <= s.cap && launch_upload(c->stream, bytes.data(), bytes.size(), s.d))
+    return s.d;
+  if (s.ev) cuda_check(cudaEventSynchronize(s.ev), "descriptor slot wait");
   if (need > s.cap) {
-    size_t cap = std::max(need, s.cap * 2);
+    size_t cap = (std::max(need, s.cap * 2) + 15) / 16 * 16;
     if (s.h) cudaFreeHost(s.h);
     if (s.d) cudaFreeAsync(s.d, c->stream);
     cuda_check(cudaMallocHost(reinterpret_cast<void**>(&s.h), cap), "cudaMallocHost(desc)");

@@ -169,6 +169,10 @@ void launch_msub(cudaStream_t s, const double* X, int64_t ldx, int k, const doub
                  double* y, int64_t n);
 void launch_scale(cudaStream_t s, double* x, int64_t n, double a);
 void launch_zero(cudaStream_t s, double* x, int64_t n);
+// Descriptor bytes [src, src + bytes) to the device address dst (16-byte aligned) as one launch
+// whose parameter block carries them; false (nothing launched) above UPLOAD_PARAM_MAX bytes.
+constexpr int UPLOAD_PARAM_MAX = 32704;
+bool launch_upload(cudaStream_t s, const void* src, size_t bytes, void* dst);
 
 // Device-resident Krylov scalars: slots of the context's 256-double scalar array. The Krylov
 // solve of a bond step runs without host round trips; the host reads only the energy (EN).

@@ -2,6 +2,7 @@
 // strided block copies (gathers/scatters), and the Lanczos vector operations with deterministic
 // two-stage warp-shuffle reductions (fixed grid, fixed order: bit-identical from run to run).
 #include <algorithm>
+#include <cstring>
 
 #include "kernels.cuh"
 #include "launch.cuh"
@@ -564,6 +565,42 @@ void launch_lincomb(cudaStream_t s, const double* X, int64_t ldx, int k, const d
 void launch_zero(cudaStream_t s, double* x, int64_t n) {
   if (n <= 0) return;
   cudaMemsetAsync(x, 0, size_t(n) * sizeof(double), s);
+}
+
+// Descriptor upload carried by the launch itself: the bytes travel as the kernel's parameter
+// block (up to 32 KB of parameters on sm_70 and later), and the kernel writes them to the
+// descriptor slot. Unlike a host-to-device copy this needs no copy engine between two kernels
+// and chains with them through programmatic dependent launch.
+template <int N>
+struct ParamBlob {
+  uint4 v[N / 16];
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_upload(const __grid_constant__ ParamBlob<N> blob,
+                                                uint4* __restrict__ dst, int nvec) {
+  grid_entry();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nvec) dst[i] = blob.v[i];
+}
+
+template <int N>
+void upload_blob(cudaStream_t s, const void* src, size_t bytes, void* dst) {
+  ParamBlob<N> b;
+  const int nvec = int((bytes + 15) / 16);
+  b.v[nvec - 1] = make_uint4(0u, 0u, 0u, 0u);
+  std::memcpy(b.v, src, bytes);
+  launch_k(k_upload<N>, (nvec + 255) / 256, 256, 0, s, b, reinterpret_cast<uint4*>(dst), nvec);
+  count_launch();
+}
+
+bool launch_upload(cudaStream_t s, const void* src, size_t bytes, void* dst) {
+  if (bytes == 0 || bytes > size_t(UPLOAD_PARAM_MAX) || (reinterpret_cast<uintptr_t>(dst) & 15))
+    return false;
+  if (bytes <= 2048) upload_blob<2048>(s, src, bytes, dst);
+  else if (bytes <= 8192) upload_blob<8192>(s, src, bytes, dst);
+  else upload_blob<UPLOAD_PARAM_MAX>(s, src, bytes, dst);
+  return true;
 }
 
 }  // namespace dmrg
