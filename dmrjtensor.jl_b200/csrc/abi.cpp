@@ -189,6 +189,12 @@ int dmrg_ctx_destroy(dmrg_ctx* c) {
   cudaFreeHost(c->h_flags);
   cudaFree(c->d_floors);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->env_stream) {
+    cudaStreamSynchronize(c->env_stream);
+    cudaStreamDestroy(c->env_stream);
+    cudaEventDestroy(c->env_fork);
+    cudaEventDestroy(c->env_join);
+  }
   cudaStreamDestroy(c->stream);
   delete c;
   return DMRG_OK;

@@ -214,6 +214,13 @@ struct dmrg_ctx {
   dmrg::DBuf SL, SR;             // chunk images of the Heff's environments (one plan at a time)
   uint64_t sl_key = 0, sr_key = 0;   // which plan and form SL / SR hold (0: none)
   std::map<void*, size_t> sizes;
+  // Two-site sweeps run each environment update on env_stream, forked from `stream` once the
+  // new site tensor is written (env_fork) and joined before the next Krylov solve (env_join),
+  // so that it overlaps the split GEMM, the next centre normalisation and the next AA product.
+  cudaStream_t env_stream = nullptr;
+  cudaEvent_t env_fork = nullptr, env_join = nullptr;
+  bool env_overlap = false;      // inside such a sweep: twostep records env_fork
+  bool env_pending = false;      // env_join recorded and not yet waited on by `stream`
 };
 
 struct dmrg_mpo {

@@ -64,6 +64,9 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
                        bool simple2, bool final_step, Timing& tm, StepOut& so, double tau = 0.0,
                        bool expo = false);
 double krylov_energy(dmrg_ctx* c, const KrylovRun& kr);
+// Makes the context's stream wait for an environment update still running on env_stream
+// (a no-op when none is pending). krylov_solve calls it before its first Heff application.
+void join_env(dmrg_ctx* c);
 
 // What a bond step optimises: the ground state (DMRG), or one TDVP time step of length tau
 // (Krylov exponential instead of the Ritz vector, truncation weights relative to the total).

@@ -85,6 +85,7 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
                        bool expo) {
   dmrg_ctx* c = st->ctx;
   cudaStream_t s = c->stream;
+  join_env(c);
   KrylovRun kr;
   kr.split = split_form(P.precision) != 0;
   const int kdim = std::max(2, std::min(P.krylov, 16));
@@ -198,6 +199,12 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
     cuda_check(cudaMemcpyAsync(c->h_scal + 20, c->d_status + STATUS_MMA, sizeof(int),
                                cudaMemcpyDeviceToHost, s), "MMA status D2H");
   return kr;
+}
+
+void join_env(dmrg_ctx* c) {
+  if (!c->env_pending) return;
+  c->env_pending = false;
+  cuda_check(cudaStreamWaitEvent(c->stream, c->env_join, 0), "environment join");
 }
 
 double krylov_energy(dmrg_ctx* c, const KrylovRun& kr) {
@@ -497,13 +504,17 @@ void twostep(dmrg_state* st, const dmrg_params& P, int j, int iL, int iR, bool f
   u3.put(gs);
   char* db3 = u3.send(c, 3);
   cuda_check(cudaGetLastError(), "split upload");
+  // the copy writes the site tensor that the environment update reads (nA for j > 0, nB for
+  // j < 0): a sweep that overlaps its environment updates forks them off here
   if (j > 0) {
     run_copy(c, cp, db3, c->R.p, c->R.n, nA.p, nA.n);
     cuda_check(cudaGetLastError(), "split copy");
+    if (c->env_overlap) cuda_check(cudaEventRecord(c->env_fork, s), "environment fork");
     run_gemm(c, gs, db3, c->R.p, c->R.n, c->M.p, c->M.n, nB.p, nB.n);
   } else {
     run_copy(c, cp, db3, c->R.p, c->R.n, nB.p, nB.n);
     cuda_check(cudaGetLastError(), "split copy");
+    if (c->env_overlap) cuda_check(cudaEventRecord(c->env_fork, s), "environment fork");
     run_gemm(c, gs, db3, c->M.p, c->M.n, c->R.p, c->R.n, nA.p, nA.n);
   }
   cuda_check(cudaGetLastError(), "split");
@@ -530,6 +541,27 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
   const int svn_site = std::min(std::max(2, svn + 1), L) - 1;   // 0-based i of SvNcheck!
   const auto h0 = std::chrono::steady_clock::now();
   Timing tm(c, P.profile != 0);
+  // Environment updates on their own stream (dmrg_ctx::env_stream), except in profiled sweeps
+  // (their phase timings are taken on one stream) and in served solves (their Heff launches go
+  // to the shared batcher).
+  const bool overlap = !P.profile && !c->batch;
+  if (overlap && !c->env_stream) {
+    cuda_check(cudaStreamCreateWithFlags(&c->env_stream, cudaStreamNonBlocking), "env stream");
+    cuda_check(cudaEventCreateWithFlags(&c->env_fork, cudaEventDisableTiming), "env event");
+    cuda_check(cudaEventCreateWithFlags(&c->env_join, cudaEventDisableTiming), "env event");
+  }
+  // on every exit, errors included: the context's own stream back in place, nothing pending
+  struct EnvGuard {
+    dmrg_ctx* c;
+    cudaStream_t main;
+    ~EnvGuard() {
+      c->stream = main;
+      if (c->env_pending) cudaStreamWaitEvent(main, c->env_join, 0);
+      c->env_pending = false;
+      c->env_overlap = false;
+    }
+  } guard{c, c->stream};
+  c->env_overlap = overlap;
   const int t0 = tm.record();
   int j = st->dir;
   const int j0 = j;
@@ -547,8 +579,17 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     // so the quotient is exact FP64 arithmetic on the final Ritz vector
     const int eprec = (split_form(P.precision) && !(P.fp64_final && (P.halfsweep || j != j0)))
                           ? P.precision : DMRG_PREC_FP64;
+    if (overlap) {
+      cuda_check(cudaStreamWaitEvent(c->env_stream, c->env_fork, 0), "environment fork");
+      c->stream = c->env_stream;
+    }
     if (j > 0) lupdate(st, i, &ef, eprec); else rupdate(st, i, &ef, eprec);
     cuda_check(cudaGetLastError(), "environment update");
+    if (overlap) {
+      c->stream = guard.main;
+      cuda_check(cudaEventRecord(c->env_join, c->env_stream), "environment join");
+      c->env_pending = true;
+    }
     tm.end(tenv, 1);
     out.energy = so.energy;
     out.max_truncerr = std::max(out.max_truncerr, so.truncerr);
@@ -571,6 +612,7 @@ void do_sweep(dmrg_state* st, const dmrg_params& P, dmrg_sweep_stats& out) {
     if ((st->oc == L - 1 && j > 0) || (st->oc == 0 && j < 0)) j = -j;
   }
   st->dir = j;
+  join_env(c);
   const int t1 = tm.record();
   cuda_check(cudaEventSynchronize(tm.event(t1)), "sweep sync");
   if (split_form(P.precision)) check_mma_status(c);   // the last environment update
