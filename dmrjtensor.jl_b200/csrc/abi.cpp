@@ -155,6 +155,7 @@ int dmrg_ctx_create(int device, size_t hbm_budget_bytes, dmrg_ctx** out) {
       cuda_check(cudaMalloc(&c->d_status, 16 * sizeof(int)), "status");
       cuda_check(cudaMemsetAsync(c->d_status, 0, 16 * sizeof(int), c->stream), "status clear");
       cuda_check(cudaMallocHost(&c->h_scal, 256 * sizeof(double)), "pinned scalars");
+      c->dv_scal = device_view(c->h_scal);
       cuda_check(cudaMalloc(&c->d_flags, c->max_groups * sizeof(int)), "flags");
       cuda_check(cudaMallocHost(&c->h_flags, c->max_groups * sizeof(int)), "pinned flags");
       cuda_check(cudaMalloc(&c->d_floors, c->max_groups * sizeof(double)), "floors");

@@ -202,6 +202,8 @@ struct dmrg_ctx {
   double* h_scal = nullptr;      // pinned mirror of d_scal
   double* h_lam = nullptr;       // pinned eigenvalue download buffer (grow-only)
   size_t h_lam_cap = 0;
+  double* dv_scal = nullptr;     // device addresses of h_scal / h_lam (null: not mapped, the
+  double* dv_lam = nullptr;      // downloads then use a copy engine)
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> tev;  // phase-timing events, reused across sweeps
   int max_groups = 4096;
@@ -272,6 +274,12 @@ EnvLayout make_right_env_layout(const Bond& B, const std::vector<QN>& r);
 TwoSiteOp make_two_site_op(const MPOSite& a, const MPOSite& b);
 // One MPO site in the two-site form with a trivial second site (d2 = 1): out[t * wr + w'].
 TwoSiteOp make_one_site_op(const MPOSite& a);
+
+// Device-to-host transfer of `bytes` (a multiple of 4) into pinned host memory at dst: written by
+// a kernel through view, dst's device address, when there is one; else an asynchronous copy.
+void to_host(dmrg_ctx* c, void* dst, void* view, const void* src, size_t bytes, const char* what);
+// The device address of pinned host memory h, or null when the device cannot address it.
+double* device_view(double* h);
 
 // ---- descriptor upload
 struct Upload {

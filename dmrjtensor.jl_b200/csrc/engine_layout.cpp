@@ -401,6 +401,25 @@ void CopyList::add(int64_t src_off, int lds, int64_t dst_off, int ldd, int rows,
   tasks.push_back(t);
 }
 
+void to_host(dmrg_ctx* c, void* dst, void* view, const void* src, size_t bytes,
+             const char* what) {
+  if (view && bytes % 4 == 0) {
+    launch_to_host(c->stream, src, view, bytes);
+    cuda_check(cudaGetLastError(), what);
+  } else {
+    cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream), what);
+  }
+}
+
+double* device_view(double* h) {
+  void* d = nullptr;
+  if (!h || cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return static_cast<double*>(d);
+}
+
 char* Upload::send(dmrg_ctx* c, int slot) {
   DescSlot& s = c->slot[slot];
   size_t need = bytes.size() < 16 ? 16 : bytes.size();

@@ -190,14 +190,14 @@ KrylovRun krylov_solve(dmrg_state* st, const dmrg_params& P, const HeffPlan& hp,
     so.nmv += 1;
     so.heff_flops += hp.flops;
     launch_dot2(s, H, K, n, c->d_partial, scal + lz::KK);
-    cuda_check(cudaMemcpyAsync(c->h_scal + lz::KK, scal + lz::KK, 2 * sizeof(double),
-                               cudaMemcpyDeviceToHost, s), "Rayleigh quotient D2H");
+    to_host(c, c->h_scal + lz::KK, c->dv_scal ? c->dv_scal + lz::KK : nullptr, scal + lz::KK,
+            2 * sizeof(double), "Rayleigh quotient D2H");
   }
-  cuda_check(cudaMemcpyAsync(c->h_scal + lz::EN, scal + lz::EN, sizeof(double),
-                             cudaMemcpyDeviceToHost, s), "energy D2H");
+  to_host(c, c->h_scal + lz::EN, c->dv_scal ? c->dv_scal + lz::EN : nullptr, scal + lz::EN,
+          sizeof(double), "energy D2H");
   if (kr.split)   // timeout flag of the split GEMMs, read back with the energy (bytes of slot 20)
-    cuda_check(cudaMemcpyAsync(c->h_scal + 20, c->d_status + STATUS_MMA, sizeof(int),
-                               cudaMemcpyDeviceToHost, s), "MMA status D2H");
+    to_host(c, c->h_scal + 20, c->dv_scal ? c->dv_scal + 20 : nullptr, c->d_status + STATUS_MMA,
+            sizeof(int), "MMA status D2H");
   return kr;
 }
 
@@ -282,23 +282,24 @@ void plan_rho(dmrg_ctx* c, std::vector<Group>& G, bool rows, RhoSolve& rs, int* 
 }
 
 void launch_rho(dmrg_ctx* c, RhoSolve& rs, char* db) {
-  cudaStream_t s = c->stream;
   run_gemm(c, rs.grho, db, c->M.p, c->M.n, c->M.p, c->M.n, c->R.p, c->R.n);
   run_trid_eigvals(c, c->R.p, c->R.n, rs.ttasks, 8);
   cuda_check(cudaGetLastError(), "density matrix and eigenvalue launch");
   run_eigs(c, c->R.p, c->R.n, rs.etasks, rs.J0, nullptr);
-  // pinned destination: the copy stays asynchronous and the host waits only in the step's sync
+  // pinned destination: the transfer stays asynchronous and the host waits only in the step's
+  // sync
   if (size_t(std::max<int64_t>(rs.wtot, 1)) > c->h_lam_cap) {
     if (c->h_lam) cudaFreeHost(c->h_lam);
     c->h_lam = nullptr;
+    c->dv_lam = nullptr;
     c->h_lam_cap = 0;
     const size_t cap = std::max<size_t>(size_t(rs.wtot), 4096);
     cuda_check(cudaMallocHost(reinterpret_cast<void**>(&c->h_lam), cap * sizeof(double)),
                "pinned eigenvalue buffer");
     c->h_lam_cap = cap;
+    c->dv_lam = device_view(c->h_lam);
   }
-  cuda_check(cudaMemcpyAsync(c->h_lam, c->R.p + rs.W0, sizeof(double) * rs.wtot,
-                             cudaMemcpyDeviceToHost, s), "eigenvalues D2H");
+  to_host(c, c->h_lam, c->dv_lam, c->R.p + rs.W0, sizeof(double) * rs.wtot, "eigenvalues D2H");
 }
 
 std::vector<std::vector<double>> rho_values(dmrg_ctx* c, const std::vector<Group>& G,

@@ -173,6 +173,9 @@ void launch_zero(cudaStream_t s, double* x, int64_t n);
 // whose parameter block carries them; false (nothing launched) above UPLOAD_PARAM_MAX bytes.
 constexpr int UPLOAD_PARAM_MAX = 32704;
 bool launch_upload(cudaStream_t s, const void* src, size_t bytes, void* dst);
+// bytes (a multiple of 4) from device memory to pinned host memory whose device address is
+// dst_view (cudaHostGetDevicePointer), written by one launch.
+void launch_to_host(cudaStream_t s, const void* src, void* dst_view, size_t bytes);
 
 // Device-resident Krylov scalars: slots of the context's 256-double scalar array. The Krylov
 // solve of a bond step runs without host round trips; the host reads only the energy (EN).

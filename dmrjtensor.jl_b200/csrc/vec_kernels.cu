@@ -594,6 +594,27 @@ void upload_blob(cudaStream_t s, const void* src, size_t bytes, void* dst) {
   count_launch();
 }
 
+// The reverse direction for the few words the host reads back each bond step (the energy, the
+// status words, the density-matrix eigenvalues): a kernel stores them straight into pinned host
+// memory through its device address, so the transfer chains with the kernels before it instead
+// of waiting for a copy engine. Stream synchronisation makes the stores visible to the host.
+__global__ void __launch_bounds__(256) k_to_host(const uint32_t* __restrict__ src,
+                                                 uint32_t* __restrict__ dst, int64_t nwords) {
+  grid_entry();
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nwords; i += stride)
+    dst[i] = src[i];
+}
+
+void launch_to_host(cudaStream_t s, const void* src, void* dst_view, size_t bytes) {
+  const int64_t nwords = int64_t(bytes / 4);
+  if (nwords <= 0) return;
+  const int grid = int(std::min<int64_t>((nwords + 255) / 256, 64));
+  launch_k(k_to_host, grid, 256, 0, s, reinterpret_cast<const uint32_t*>(src),
+           reinterpret_cast<uint32_t*>(dst_view), nwords);
+  count_launch();
+}
+
 bool launch_upload(cudaStream_t s, const void* src, size_t bytes, void* dst) {
   if (bytes == 0 || bytes > size_t(UPLOAD_PARAM_MAX) || (reinterpret_cast<uintptr_t>(dst) & 15))
     return false;
