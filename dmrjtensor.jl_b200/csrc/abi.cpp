@@ -119,7 +119,7 @@ void dmrg_params_default(dmrg_params* p) {
   p->cvgE = 1;
   p->goal = 0.0;
   p->tune = 1;
-  p->graph = 1;
+  p->graph = 0;
 }
 
 const char* dmrg_last_error(const dmrg_ctx* ctx) {

@@ -458,7 +458,7 @@ class DeviceState:
 
 def make_params(maxm=0, minm=2, cutoff=0.0, krylov=2, precision="fp64", svnbond=0,
                 degen_rtol=0.0, betatest=1e-10, fp64_final=1, profile=0, goal=0.0, cvgE=True,
-                tune=True, graph=True, halfsweep=False):
+                tune=True, graph=False, halfsweep=False):
     p = Params()
     lib().dmrg_params_default(C.byref(p))
     p.maxm, p.minm, p.cutoff = int(maxm), int(minm), float(cutoff)

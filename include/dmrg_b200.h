@@ -93,9 +93,10 @@ typedef struct dmrg_params {
                         |S - S_last| < goal (cvgE = 0); E_last starts at <psi|H|psi> of the state
                         the environments were built for (startval, algs/optimizeMPS.jl:255-258,
                         365-371), S_last at 0. 0 (the default) never converges: all sweeps run */
-  int graph;         /* 1 (default): the Lanczos step after its first Heff runs as one CUDA graph
-                        (captured per step, the context's executable updated in place); 0: plain
-                        launches. Same numbers either way */
+  int graph;         /* 1: the Lanczos step after its first Heff runs as one CUDA graph (captured
+                        per step, the context's executable updated in place); 0 (default): plain
+                        launches, chained by programmatic dependent launch, which measure as fast
+                        or faster. Same numbers either way */
   int halfsweep;     /* 1: a sweep is L-1 bond steps in the current direction (halfsweep of
                         algs/DMRG.jl:253), the direction carrying over to the next call; 0
                         (default): 2(L-1) steps, back and forth. With a split precision and

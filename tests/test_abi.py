@@ -33,7 +33,7 @@ def test_abi_version_and_defaults(dmrgb):
     assert p.betatest == 1e-10
     # algvars defaults (algs/optimizeMPS.jl:527-528): energy convergence test, goal 0 (never stops)
     assert (p.cvgE, p.goal) == (1, 0.0)
-    assert (p.tune, p.graph) == (1, 1)
+    assert (p.tune, p.graph) == (1, 0)
     # the ctypes mirrors have the C layout: 80-byte params, stats end with the convergence fields
     assert C.sizeof(dmrgb._lib.Params) == 80
     # the 3S noise schedule (algs/optimizeMPS.jl:528-532)
